@@ -1,0 +1,142 @@
+"""dort_b200 -- B200-native (sm_100a) path-tracing hot path of the dort renderer.
+
+Python host mirror of the C ABI in ``include/dort_gpu.h``.  Every call goes
+through the CUDA library ``libdort_gpu.so`` built in-tree; nothing here
+computes a ray query or a render on the CPU.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _abi
+from ._abi import (DortError, MISS, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_LAMBERT,
+                   MAT_MIRROR, MAT_PHONG)
+
+__all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
+           "MAT_LAMBERT", "MAT_MIRROR", "MAT_DIELECTRIC", "MAT_PHONG", "MAT_CONDUCTOR"]
+
+
+def _ptr(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class _DescHolder:
+    """Keeps the numpy arrays a SceneDesc points to alive."""
+
+    def __init__(self):
+        self.keep = []
+        self.desc = _abi.SceneDesc()
+
+    def arr(self, a, dtype):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype)
+        self.keep.append(a)
+        return ctypes.c_void_p(a.ctypes.data)
+
+
+def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None,
+               sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_to_world=None,
+               bvh_width: int = 8) -> _DescHolder:
+    h = _DescHolder()
+    d = h.desc
+    verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
+    tris = np.ascontiguousarray(tris, np.uint32).reshape(-1, 3)
+    d.struct_size = ctypes.sizeof(_abi.SceneDesc)
+    d.verts = h.arr(verts, np.float32)
+    d.vert_count = len(verts)
+    d.tris = h.arr(tris, np.uint32)
+    d.tri_count = len(tris)
+    d.tri_material = h.arr(tri_material, np.uint32)
+    if materials:
+        mats = (_abi.Material * len(materials))()
+        for i, m in enumerate(materials):
+            mats[i].kind = m.get("kind", MAT_LAMBERT)
+            mats[i].color = (ctypes.c_float * 3)(*m.get("color", (0.0, 0.0, 0.0)))
+            mats[i].color2 = (ctypes.c_float * 3)(*m.get("color2", (0.0, 0.0, 0.0)))
+            p = list(m.get("param", ())) + [0.0] * 4
+            mats[i].param = (ctypes.c_float * 4)(*p[:4])
+        h.keep.append(mats)
+        d.materials = ctypes.cast(mats, ctypes.c_void_p)
+        d.material_count = len(materials)
+    d.tri_emission = h.arr(tri_emission, np.float32)
+    if sky_rgb is not None:
+        sky = np.ascontiguousarray(sky_rgb, np.float32)
+        d.sky_rgb = h.arr(sky, np.float32)
+        d.sky_height, d.sky_width = sky.shape[0], sky.shape[1]
+    d.sky_const = (ctypes.c_float * 3)(*sky_const)
+    if sky_to_world is not None:
+        d.sky_to_world = (ctypes.c_float * 9)(*np.asarray(sky_to_world, np.float32).ravel())
+    d.bvh_width = bvh_width
+    return h
+
+
+class Scene:
+    """A scene resident on the current CUDA device (dort_gpu_scene_create)."""
+
+    def __init__(self, verts, tris, **kw):
+        self._holder = scene_desc(verts, tris, **kw)
+        h = ctypes.c_void_p()
+        _abi.check(_abi.lib().dort_gpu_scene_create(ctypes.byref(self._holder.desc),
+                                                    ctypes.byref(h)))
+        self.handle = h
+        self.tri_count = self._holder.desc.tri_count
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _abi.lib().dort_gpu_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def stats(self) -> dict:
+        out = (ctypes.c_double * 8)()
+        _abi.check(_abi.lib().dort_gpu_scene_stats(self.handle, out))
+        return {"nodes": int(out[0]), "depth": int(out[1]), "tris": int(out[2]),
+                "emissive": int(out[3]), "device_bytes": int(out[4]),
+                "build_ms": out[5]}
+
+    def raycast(self, rays, any_hit: bool = False):
+        """Host arrays in and out (dort_gpu_raycast)."""
+        rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+        n = len(rays)
+        prim = np.zeros(n, np.uint32)
+        tb = None if any_hit else np.zeros((n, 3), np.float32)
+        _abi.check(_abi.lib().dort_gpu_raycast(self.handle, _ptr(rays), n, int(any_hit),
+                                               _ptr(prim), _ptr(tb)))
+        return prim if any_hit else (prim, tb)
+
+    def raycast_device(self, d_rays: int, n: int, d_prim: int, d_tb: int | None,
+                       any_hit: bool = False, stream: int = 0):
+        """Device pointers (ints) on a CUDA stream handle (int)."""
+        _abi.check(_abi.lib().dort_gpu_raycast_device(
+            self.handle, ctypes.c_void_p(d_rays), n, int(any_hit), ctypes.c_void_p(d_prim),
+            ctypes.c_void_p(d_tb) if d_tb else None, ctypes.c_void_p(stream)))
+
+    def raycast_timed(self, d_rays: int, n: int, d_prim: int, d_tb: int | None,
+                      any_hit: bool = False, stream: int = 0, repeat: int = 1) -> float:
+        ms = ctypes.c_float(0.0)
+        _abi.check(_abi.lib().dort_gpu_raycast_timed(
+            self.handle, ctypes.c_void_p(d_rays), n, int(any_hit), ctypes.c_void_p(d_prim),
+            ctypes.c_void_p(d_tb) if d_tb else None, ctypes.c_void_p(stream), repeat,
+            ctypes.byref(ms)))
+        return ms.value
+
+
+def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8):
+    """Runs the device traversal code compiled for the host (diagnostic)."""
+    h = scene_desc(verts, tris, bvh_width=bvh_width)
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    n = len(rays)
+    prim = np.zeros(n, np.uint32)
+    tb = None if any_hit else np.zeros((n, 3), np.float32)
+    depth = ctypes.c_uint32(0)
+    _abi.check(_abi.lib().dort_gpu_host_check_raycast(ctypes.byref(h.desc), _ptr(rays), n,
+                                                      int(any_hit), _ptr(prim), _ptr(tb),
+                                                      ctypes.byref(depth)))
+    if any_hit:
+        return prim, depth.value
+    return prim, tb, depth.value

@@ -1,0 +1,96 @@
+"""ctypes view of the C ABI in include/dort_gpu.h.
+
+Loads the in-tree ``libdort_gpu.so``.  There is no fallback: if the library
+is missing or fails to load, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libdort_gpu.so")
+
+c_u32 = ctypes.c_uint32
+c_i32 = ctypes.c_int
+c_size = ctypes.c_size_t
+c_f = ctypes.c_float
+c_p = ctypes.c_void_p
+
+DORT_OK = 0
+STATUS_NAMES = {
+    0: "DORT_OK", -1: "DORT_ERR_INVALID", -2: "DORT_ERR_CUDA", -3: "DORT_ERR_OOM",
+    -4: "DORT_ERR_TIMEOUT", -5: "DORT_ERR_UNSUPPORTED", -6: "DORT_ERR_DEVICE",
+}
+MISS = 0xFFFFFFFF
+
+MAT_LAMBERT, MAT_MIRROR, MAT_DIELECTRIC, MAT_PHONG, MAT_CONDUCTOR = range(5)
+
+
+class Material(ctypes.Structure):
+    _fields_ = [("kind", c_u32), ("color", c_f * 3), ("color2", c_f * 3),
+                ("param", c_f * 4)]
+
+
+class SceneDesc(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", c_u32),
+        ("verts", c_p), ("vert_count", c_u32),
+        ("tris", c_p), ("tri_count", c_u32),
+        ("tri_material", c_p),
+        ("materials", c_p), ("material_count", c_u32),
+        ("tri_emission", c_p),
+        ("sky_rgb", c_p), ("sky_width", c_u32), ("sky_height", c_u32),
+        ("sky_const", c_f * 3),
+        ("sky_to_world", c_f * 9),
+        ("bvh_width", c_u32),
+        ("reserved", c_u32 * 7),
+    ]
+
+
+class DortError(RuntimeError):
+    """A C-ABI call returned a negative status."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(
+                f"{LIB_PATH} is missing: build it with `python -m dort_b200.build` "
+                "(the CUDA library is required; there is no CPU fallback)")
+        L = ctypes.CDLL(LIB_PATH)
+        L.dort_gpu_last_error.restype = ctypes.c_char_p
+        L.dort_gpu_last_error.argtypes = []
+        L.dort_gpu_abi_version.restype = c_i32
+        L.dort_gpu_scene_create.restype = c_i32
+        L.dort_gpu_scene_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.POINTER(c_p)]
+        L.dort_gpu_scene_destroy.restype = c_i32
+        L.dort_gpu_scene_destroy.argtypes = [c_p]
+        L.dort_gpu_scene_stats.restype = c_i32
+        L.dort_gpu_scene_stats.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_raycast.restype = c_i32
+        L.dort_gpu_raycast.argtypes = [c_p, c_p, c_size, c_i32, c_p, c_p]
+        L.dort_gpu_raycast_device.restype = c_i32
+        L.dort_gpu_raycast_device.argtypes = [c_p, c_p, c_size, c_i32, c_p, c_p, c_p]
+        L.dort_gpu_raycast_timed.restype = c_i32
+        L.dort_gpu_raycast_timed.argtypes = [c_p, c_p, c_size, c_i32, c_p, c_p, c_p,
+                                             c_i32, ctypes.POINTER(c_f)]
+        L.dort_gpu_host_check_raycast.restype = c_i32
+        L.dort_gpu_host_check_raycast.argtypes = [ctypes.POINTER(SceneDesc), c_p, c_size,
+                                                  c_i32, c_p, c_p, ctypes.POINTER(c_u32)]
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != DORT_OK:
+        msg = lib().dort_gpu_last_error().decode(errors="replace")
+        raise DortError(status, msg)

@@ -1,0 +1,454 @@
+// Host-side wide BVH construction: binned SAH binary build, greedy collapse
+// to up to 8 children, octant slot assignment and conservative 8-bit
+// quantization.  See bvh_build.h for the node format.
+//
+// The reference's own build (src/dort/bvh.cpp:98-383) differs on purpose:
+// it defaults to middle splits, its SAH uses 12 buckets on one axis with an
+// area formula missing the x*y term (include/dort/box.hpp:29) and integer
+// costs.  Hit results do not depend on the tree shape (closest hit is a
+// property of the triangle set), so the device tree is free to be a better
+// one.
+#include "bvh_build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <limits>
+#include <thread>
+
+namespace dort_gpu {
+namespace {
+
+struct Aabb {
+  float lo[3] = {INFINITY, INFINITY, INFINITY};
+  float hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  void grow(const Aabb& b) {
+    for(int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], b.lo[a]);
+      hi[a] = std::max(hi[a], b.hi[a]);
+    }
+  }
+  void grow(const float* p) {
+    for(int a = 0; a < 3; ++a) {
+      lo[a] = std::min(lo[a], p[a]);
+      hi[a] = std::max(hi[a], p[a]);
+    }
+  }
+  bool empty() const { return !(lo[0] <= hi[0]); }
+  double area() const {
+    if(empty()) { return 0.0; }
+    double x = double(hi[0]) - lo[0], y = double(hi[1]) - lo[1], z = double(hi[2]) - lo[2];
+    return 2.0 * (x * y + y * z + z * x);
+  }
+};
+
+struct BinNode {
+  Aabb box;
+  uint32_t left = 0, right = 0;   // internal: children
+  uint32_t first = 0, count = 0;  // leaf: range in the primitive order
+  uint32_t tri_total = 0;         // triangles below this node
+};
+
+struct Prim {
+  Aabb box;
+  float c[3];
+};
+
+class BinaryBuilder {
+ public:
+  BinaryBuilder(std::vector<Prim>& prims, const BuildOptions& o)
+      : prims_(prims), opts_(o) {
+    order_.resize(prims.size());
+    for(uint32_t i = 0; i < order_.size(); ++i) { order_[i] = i; }
+  }
+
+  std::vector<BinNode> nodes;
+  std::vector<uint32_t> order_;
+
+  void build() {
+    nodes.reserve(prims_.size() * 2 / std::max(1u, opts_.max_leaf_tris) + 16);
+    nodes.emplace_back();
+    build_rec(0, 0, uint32_t(prims_.size()), 0);
+  }
+
+ private:
+  std::vector<Prim>& prims_;
+  const BuildOptions& opts_;
+
+  // Splits are SAH-binned on all three axes; a degenerate or over-deep node
+  // falls back to an object-median split so that the depth stays bounded.
+  void build_rec(uint32_t node_idx, uint32_t begin, uint32_t end, uint32_t depth) {
+    uint32_t n = end - begin;
+    Aabb box, cbox;
+    for(uint32_t i = begin; i < end; ++i) {
+      const Prim& p = prims_[order_[i]];
+      box.grow(p.box);
+      cbox.grow(p.c);
+    }
+    nodes[node_idx].box = box;
+    nodes[node_idx].tri_total = n;
+
+    const double c_trav = 1.0, c_isect = 1.0;
+    if(n <= 1) { make_leaf(node_idx, begin, n); return; }
+
+    int best_axis = -1;
+    uint32_t best_bin = 0;
+    double best_cost = std::numeric_limits<double>::infinity();
+    uint32_t nb = std::max(2u, std::min(opts_.bins, 64u));
+    bool force_median = depth >= 36;
+
+    if(!force_median) {
+      for(int a = 0; a < 3; ++a) {
+        double ext = double(cbox.hi[a]) - cbox.lo[a];
+        if(!(ext > 0.0)) { continue; }
+        Aabb bins[64];
+        uint32_t counts[64] = {0};
+        double k = nb / ext;
+        for(uint32_t i = begin; i < end; ++i) {
+          const Prim& p = prims_[order_[i]];
+          int b = int((double(p.c[a]) - cbox.lo[a]) * k);
+          b = std::min(std::max(b, 0), int(nb) - 1);
+          bins[b].grow(p.box);
+          counts[b] += 1;
+        }
+        double right_area[64];
+        uint32_t right_count[64];
+        Aabb acc;
+        uint32_t cnt = 0;
+        for(int b = int(nb) - 1; b > 0; --b) {
+          acc.grow(bins[b]);
+          cnt += counts[b];
+          right_area[b] = acc.area();
+          right_count[b] = cnt;
+        }
+        Aabb lacc;
+        uint32_t lcnt = 0;
+        for(uint32_t b = 0; b + 1 < nb; ++b) {
+          lacc.grow(bins[b]);
+          lcnt += counts[b];
+          uint32_t rc = right_count[b + 1];
+          if(lcnt == 0 || rc == 0) { continue; }
+          double cost = lacc.area() * lcnt + right_area[b + 1] * rc;
+          if(cost < best_cost) { best_cost = cost; best_axis = a; best_bin = b; }
+        }
+      }
+    }
+
+    double parent_area = std::max(box.area(), 1e-300);
+    double split_cost = c_trav + c_isect * best_cost / parent_area;
+    double leaf_cost = c_isect * n;
+    if(n <= opts_.max_leaf_tris && (best_axis < 0 || leaf_cost <= split_cost)) {
+      make_leaf(node_idx, begin, n);
+      return;
+    }
+
+    uint32_t mid;
+    if(best_axis >= 0) {
+      int a = best_axis;
+      double ext = double(cbox.hi[a]) - cbox.lo[a];
+      double k = nb / ext;
+      auto it = std::partition(order_.begin() + begin, order_.begin() + end,
+          [&](uint32_t idx) {
+            int b = int((double(prims_[idx].c[a]) - cbox.lo[a]) * k);
+            b = std::min(std::max(b, 0), int(nb) - 1);
+            return uint32_t(b) <= best_bin;
+          });
+      mid = uint32_t(it - order_.begin());
+    } else {
+      mid = begin;  // fall through to the median split below
+    }
+    if(mid == begin || mid == end) {
+      int a = 0;
+      for(int k = 1; k < 3; ++k) {
+        if(cbox.hi[k] - cbox.lo[k] > cbox.hi[a] - cbox.lo[a]) { a = k; }
+      }
+      mid = begin + n / 2;
+      std::nth_element(order_.begin() + begin, order_.begin() + mid,
+          order_.begin() + end, [&](uint32_t x, uint32_t y) {
+            return prims_[x].c[a] < prims_[y].c[a];
+          });
+    }
+
+    uint32_t l = uint32_t(nodes.size());
+    nodes.emplace_back();
+    nodes.emplace_back();
+    nodes[node_idx].left = l;
+    nodes[node_idx].right = l + 1;
+    nodes[node_idx].count = 0;
+    build_rec(l, begin, mid, depth + 1);
+    build_rec(l + 1, mid, end, depth + 1);
+  }
+
+  void make_leaf(uint32_t node_idx, uint32_t begin, uint32_t n) {
+    nodes[node_idx].first = begin;
+    nodes[node_idx].count = n;
+    nodes[node_idx].left = nodes[node_idx].right = 0;
+  }
+};
+
+// Picks the quantization grid of one axis: step 2^e, origin p one step below
+// the node's lower bound, 253 steps covering the extent; returns false if the
+// exponent cannot be represented.
+bool quantize_axis(float node_lo, float node_hi, const float* clo, const float* chi,
+                   int n, float& p_out, uint8_t& e_out, uint8_t* qlo, uint8_t* qhi) {
+  double lo = node_lo, hi = node_hi;
+  double ext = hi - lo;
+  double mag = std::max(std::fabs(lo), std::fabs(hi));
+  double min_step = std::max(mag * std::ldexp(1.0, -20), std::ldexp(1.0, -100));
+  double step = std::max(ext / 253.0, min_step);
+  int e = int(std::ceil(std::log2(step)));
+  for(int attempt = 0; attempt < 8; ++attempt, ++e) {
+    if(e + 127 < 1 || e + 127 > 254) { return false; }
+    double s = std::ldexp(1.0, e);
+    double pd = lo - s;
+    float pf = float(pd);
+    if(double(pf) > pd) { pf = std::nextafter(pf, -INFINITY); }
+    bool ok = true;
+    for(int i = 0; i < n && ok; ++i) {
+      double ql = std::floor((double(clo[i]) - pf) / s) - 1.0;
+      double qh = std::ceil((double(chi[i]) - pf) / s) + 1.0;
+      if(ql < 0.0 || qh > 255.0) { ok = false; break; }
+      // the dequantized planes must enclose the child with at least one step
+      if(double(pf) + ql * s > double(clo[i]) - s * 0.999 ||
+         double(pf) + qh * s < double(chi[i]) + s * 0.999) { ok = false; break; }
+      qlo[i] = uint8_t(ql);
+      qhi[i] = uint8_t(qh);
+    }
+    if(ok) {
+      p_out = pf;
+      e_out = uint8_t(e + 127);
+      return true;
+    }
+  }
+  return false;
+}
+
+struct Collapser {
+  const std::vector<BinNode>& bn;
+  const std::vector<uint32_t>& order;
+  const float* verts;
+  const uint32_t* tris;
+  const BuildOptions& opts;
+  WideBvh& out;
+  std::string& err;
+
+  struct Pending {
+    uint32_t bin;       // binary node to expand into a wide node
+    uint32_t wide;      // its index in out.nodes
+    uint32_t depth;
+  };
+
+  void collect_tris(uint32_t b, std::vector<uint32_t>& dst) const {
+    if(bn[b].count > 0 || (bn[b].left == 0 && bn[b].right == 0)) {
+      for(uint32_t i = 0; i < bn[b].count; ++i) { dst.push_back(order[bn[b].first + i]); }
+      return;
+    }
+    collect_tris(bn[b].left, dst);
+    collect_tris(bn[b].right, dst);
+  }
+
+  bool is_leaf(uint32_t b) const { return bn[b].left == 0 && bn[b].right == 0; }
+
+  bool run() {
+    out.nodes.clear();
+    out.tris.clear();
+    if(bn.empty() || bn[0].tri_total == 0) { out.depth = 0; return true; }
+    out.nodes.emplace_back();
+    std::vector<Pending> queue;
+    queue.push_back({0, 0, 1});
+    uint32_t max_depth = 1;
+    size_t head = 0;
+    uint32_t width = std::min(8u, std::max(2u, opts.width));
+    while(head < queue.size()) {
+      Pending cur = queue[head++];
+      max_depth = std::max(max_depth, cur.depth);
+      // Candidate children: open the largest internal candidate until full.
+      std::vector<uint32_t> cands;
+      if(is_leaf(cur.bin)) {
+        cands.push_back(cur.bin);
+      } else {
+        cands.push_back(bn[cur.bin].left);
+        cands.push_back(bn[cur.bin].right);
+      }
+      while(cands.size() < width) {
+        int best = -1;
+        double best_area = -1.0;
+        for(size_t i = 0; i < cands.size(); ++i) {
+          if(is_leaf(cands[i])) { continue; }
+          double a = bn[cands[i]].box.area();
+          if(a > best_area) { best_area = a; best = int(i); }
+        }
+        if(best < 0) { break; }
+        uint32_t b = cands[best];
+        cands[best] = bn[b].left;
+        cands.push_back(bn[b].right);
+      }
+      size_t n = cands.size();
+
+      // Node box and octant slot assignment.
+      Aabb nbox;
+      for(uint32_t c : cands) { nbox.grow(bn[c].box); }
+      double pc[3];
+      for(int a = 0; a < 3; ++a) { pc[a] = 0.5 * (double(nbox.lo[a]) + nbox.hi[a]); }
+      int slot_of[8];
+      bool slot_used[8] = {false};
+      bool cand_done[8] = {false};
+      for(size_t k = 0; k < n; ++k) {
+        double best = std::numeric_limits<double>::infinity();
+        int bc = -1, bs = -1;
+        for(size_t c = 0; c < n; ++c) {
+          if(cand_done[c]) { continue; }
+          const Aabb& cb = bn[cands[c]].box;
+          double d[3];
+          for(int a = 0; a < 3; ++a) { d[a] = 0.5 * (double(cb.lo[a]) + cb.hi[a]) - pc[a]; }
+          for(int s = 0; s < 8; ++s) {
+            if(slot_used[s]) { continue; }
+            double cost = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) +
+                          ((s & 4) ? -d[2] : d[2]);
+            if(cost < best) { best = cost; bc = int(c); bs = s; }
+          }
+        }
+        cand_done[bc] = true;
+        slot_used[bs] = true;
+        slot_of[bc] = bs;
+      }
+
+      int cand_in_slot[8];
+      for(int s = 0; s < 8; ++s) { cand_in_slot[s] = -1; }
+      for(size_t c = 0; c < n; ++c) { cand_in_slot[slot_of[c]] = int(c); }
+
+      WideNode node;
+      std::memset(&node, 0, sizeof(node));
+      float clo[3][8], chi[3][8];
+      int nslots = 0;
+      for(int s = 0; s < 8; ++s) {
+        int c = cand_in_slot[s];
+        const Aabb& cb = c >= 0 ? bn[cands[c]].box : nbox;
+        for(int a = 0; a < 3; ++a) {
+          clo[a][s] = c >= 0 ? cb.lo[a] : nbox.lo[a];
+          chi[a][s] = c >= 0 ? cb.hi[a] : nbox.lo[a];
+        }
+        nslots = 8;
+      }
+      for(int a = 0; a < 3; ++a) {
+        if(!quantize_axis(nbox.lo[a], nbox.hi[a], clo[a], chi[a], nslots,
+                          node.p[a], node.e[a], node.qlo[a], node.qhi[a])) {
+          err = "BVH quantization failed (scene coordinates out of range)";
+          return false;
+        }
+      }
+
+      // Internal children first (contiguous, slot order), then leaf triangles.
+      uint32_t child_base = uint32_t(out.nodes.size());
+      uint32_t tri_base = uint32_t(out.tris.size());
+      node.child_base = child_base;
+      node.tri_base = tri_base;
+      uint32_t tri_off = 0;
+      std::vector<uint32_t> leaf_tris;
+      for(int s = 0; s < 8; ++s) {
+        int c = cand_in_slot[s];
+        if(c < 0) {
+          node.meta[s] = 0;
+          // empty slots get an inverted box so they never report a hit
+          for(int a = 0; a < 3; ++a) { node.qlo[a][s] = 255; node.qhi[a][s] = 0; }
+          continue;
+        }
+        uint32_t b = cands[c];
+        bool leaf = is_leaf(b) || bn[b].tri_total <= opts.max_leaf_tris;
+        if(!leaf) {
+          node.imask |= uint8_t(1u << s);
+          node.meta[s] = uint8_t(0x20 | (24 + s));
+          uint32_t wi = uint32_t(out.nodes.size());
+          out.nodes.emplace_back();
+          queue.push_back({b, wi, cur.depth + 1});
+        } else {
+          leaf_tris.clear();
+          collect_tris(b, leaf_tris);
+          uint32_t cnt = uint32_t(leaf_tris.size());
+          if(cnt == 0) {
+            node.meta[s] = 0;
+            for(int a = 0; a < 3; ++a) { node.qlo[a][s] = 255; node.qhi[a][s] = 0; }
+            continue;
+          }
+          if(cnt > 3 || tri_off + cnt > 24) {
+            err = "internal error: wide BVH leaf overflow";
+            return false;
+          }
+          node.meta[s] = uint8_t((((1u << cnt) - 1u) << 5) | tri_off);
+          for(uint32_t t : leaf_tris) {
+            LeafTri lt;
+            std::memset(&lt, 0, sizeof(lt));
+            const float* p0 = verts + 3 * size_t(tris[3 * size_t(t)]);
+            const float* p1 = verts + 3 * size_t(tris[3 * size_t(t) + 1]);
+            const float* p2 = verts + 3 * size_t(tris[3 * size_t(t) + 2]);
+            for(int a = 0; a < 3; ++a) {
+              lt.p0[a] = p0[a];
+              lt.e1[a] = p1[a] - p0[a];
+              lt.e2[a] = p2[a] - p0[a];
+            }
+            lt.id = t;
+            out.tris.push_back(lt);
+          }
+          tri_off += cnt;
+        }
+      }
+      out.nodes[cur.wide] = node;
+      if(cur.depth > kMaxWideDepth) {
+        err = "BVH too deep for the device traversal stack";
+        return false;
+      }
+    }
+    out.depth = max_depth;
+    for(int a = 0; a < 3; ++a) {
+      out.root_lo[a] = bn[0].box.lo[a];
+      out.root_hi[a] = bn[0].box.hi[a];
+    }
+    return true;
+  }
+};
+
+}  // namespace
+
+bool build_wide_bvh(const float* verts, uint32_t vert_count,
+                    const uint32_t* tris, uint32_t tri_count,
+                    const BuildOptions& opts, WideBvh& out, std::string& err) {
+  if(opts.max_leaf_tris < 1 || opts.max_leaf_tris > 3) {
+    err = "max_leaf_tris must be 1..3";
+    return false;
+  }
+  if(opts.width < 2 || opts.width > 8) {
+    err = "bvh_width must be 2..8";
+    return false;
+  }
+  std::vector<Prim> prims(tri_count);
+  for(uint32_t t = 0; t < tri_count; ++t) {
+    Prim& p = prims[t];
+    for(int k = 0; k < 3; ++k) {
+      uint32_t vi = tris[3 * size_t(t) + k];
+      if(vi >= vert_count) {
+        err = "triangle " + std::to_string(t) + " references vertex " +
+              std::to_string(vi) + " >= vert_count";
+        return false;
+      }
+      const float* v = verts + 3 * size_t(vi);
+      if(!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2])) {
+        err = "vertex " + std::to_string(vi) + " is not finite";
+        return false;
+      }
+      // keeps every quantization step and slab product finite on the device
+      if(std::fabs(v[0]) > 1e15f || std::fabs(v[1]) > 1e15f || std::fabs(v[2]) > 1e15f) {
+        err = "vertex " + std::to_string(vi) + " is out of range (|coord| > 1e15)";
+        return false;
+      }
+      p.box.grow(v);
+    }
+    for(int a = 0; a < 3; ++a) { p.c[a] = 0.5f * (p.box.lo[a] + p.box.hi[a]); }
+  }
+  BinaryBuilder bb(prims, opts);
+  if(tri_count > 0) { bb.build(); }
+  Collapser col{bb.nodes, bb.order_, verts, tris, opts, out, err};
+  return col.run();
+}
+
+}  // namespace dort_gpu

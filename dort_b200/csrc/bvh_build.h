@@ -1,0 +1,82 @@
+// Host-side BVH construction for the device scene.
+//
+// The reference builds a binary BVH per mesh with middle or SAH splits
+// (src/dort/bvh.cpp:9-416) and traverses it with a 64-entry stack of 32-byte
+// nodes (bvh.cpp:418-469).  The device scene instead uses a wide BVH (up to 8
+// children per node) with 8-bit quantized child boxes and octant-ordered
+// child slots, laid out for 128-bit loads:
+//
+//   WideNode (80 bytes = 5 x uint4, 16-byte aligned, always 3 x 32-byte
+//   sectors):
+//     float    p[3]        origin of the quantization grid
+//     uint8_t  e[3]        biased power-of-two exponents of the grid step
+//     uint8_t  imask       bit s set: slot s is an internal child
+//     uint32_t child_base  node index of the first internal child; internal
+//                          children are contiguous, ordered by slot
+//     uint32_t tri_base    index of the node's first triangle
+//     uint8_t  meta[8]     per slot: 0 = empty; internal: 0x20 | (24 + s);
+//                          leaf: (unary triangle count << 5) | tri offset
+//     uint8_t  qlo[3][8], qhi[3][8]   quantized child boxes
+//
+// Child boxes are quantized outward with one full grid step of margin on
+// every side, so that the device slab test (rounded float arithmetic) never
+// culls a child that contains a hit.
+//
+//   Triangle (48 bytes = 3 x float4, leaf order):
+//     (p0.xyz, original triangle index as bits), (e1.xyz, 0), (e2.xyz, 0)
+//   with e1 = p1 - p0 and e2 = p2 - p0 rounded exactly as the reference does
+//   inside Triangle::hit_p (triangle.cpp:18-19).
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace dort_gpu {
+
+struct alignas(16) WideNode {
+  float p[3];
+  uint8_t e[3];
+  uint8_t imask;
+  uint32_t child_base;
+  uint32_t tri_base;
+  uint8_t meta[8];
+  uint8_t qlo[3][8];
+  uint8_t qhi[3][8];
+};
+static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
+
+struct alignas(16) LeafTri {
+  float p0[3];
+  uint32_t id;
+  float e1[3];
+  float pad1;
+  float e2[3];
+  float pad2;
+};
+static_assert(sizeof(LeafTri) == 48, "LeafTri must be 48 bytes");
+
+struct BuildOptions {
+  uint32_t width = 8;          // children per node, 2..8
+  uint32_t max_leaf_tris = 3;  // triangles per leaf slot, 1..3
+  uint32_t bins = 32;          // SAH bins per axis
+  uint32_t threads = 0;        // 0: hardware concurrency
+};
+
+struct WideBvh {
+  std::vector<WideNode> nodes;
+  std::vector<LeafTri> tris;
+  uint32_t depth = 0;          // levels of wide nodes
+  double root_lo[3] = {0, 0, 0};
+  double root_hi[3] = {0, 0, 0};
+};
+
+// Maximum stack depth the device traversal supports; the builder guarantees
+// that no root-to-leaf path of the wide tree is deeper.
+constexpr uint32_t kMaxWideDepth = 64;
+
+// Builds the wide BVH; returns false (with a message) on invalid input.
+bool build_wide_bvh(const float* verts, uint32_t vert_count,
+                    const uint32_t* tris, uint32_t tri_count,
+                    const BuildOptions& opts, WideBvh& out, std::string& err);
+
+}  // namespace dort_gpu

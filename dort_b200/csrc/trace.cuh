@@ -1,0 +1,244 @@
+// Device ray queries over the wide BVH (bvh_build.h): closest hit and any
+// hit.  Shared by the ray-cast kernels and the path tracers.
+//
+// Replaces Bvh::traverse_elems (src/dort/bvh.cpp:418-469) with the callbacks
+// of MeshBvhPrimitive::intersect / intersect_p (mesh_bvh_primitive.cpp:13-45)
+// and the triangle tests TriangleUv::hit / Triangle::hit_p
+// (triangle.cpp:14-46, 102-134).
+//
+// Traversal: node groups (base index, 8 child-hit bits << 24 | internal-slot
+// mask) on a per-thread stack; child slots are visited in an order fixed by
+// the ray octant (slot bit index XOR octant), so no per-node sort is needed.
+// Child boxes are tested with fused multiply-adds on the quantized planes and
+// a relative widening of 2^-20 that covers the rounding of that arithmetic;
+// together with the one-step quantization margin the test never culls a box
+// containing a hit.
+//
+// Triangle test: the reference's Moller-Trumbore operations in the
+// reference's order with explicit round-to-nearest intrinsics (no fused
+// multiply-add, IEEE reciprocal), so (t, b1, b2) are bit-identical to the
+// reference computed on the same triangle.
+#pragma once
+#include <cstdint>
+#include <cstring>
+
+#include "common.h"
+
+// The traversal is compiled for the device and, with plain IEEE float
+// arithmetic (no contraction), for the host, so that the host can check the
+// tree and the traversal without a GPU.
+#ifdef __CUDA_ARCH__
+#define DG_MUL(a, b) __fmul_rn(a, b)
+#define DG_ADD(a, b) __fadd_rn(a, b)
+#define DG_SUB(a, b) __fsub_rn(a, b)
+#define DG_RCP(a) __frcp_rn(a)
+#define DG_U2F(u) __uint2float_rn(u)
+#define DG_CLZ(x) __clz(x)
+#define DG_POPC(x) __popc(x)
+#define DG_FFS(x) __ffs(x)
+#define DG_LDG(p) __ldg(p)
+#define DG_AS_FLOAT(u) __uint_as_float(u)
+#define DG_AS_UINT(f) __float_as_uint(f)
+#else
+namespace dort_gpu {
+inline float host_as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+inline uint32_t host_as_uint(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+}
+#define DG_MUL(a, b) ((a) * (b))
+#define DG_ADD(a, b) ((a) + (b))
+#define DG_SUB(a, b) ((a) - (b))
+#define DG_RCP(a) (1.f / (a))
+#define DG_U2F(u) (float(u))
+#define DG_CLZ(x) __builtin_clz(x)
+#define DG_POPC(x) __builtin_popcount(x)
+#define DG_FFS(x) __builtin_ffs(int(x))
+#define DG_LDG(p) (*(p))
+#define DG_AS_FLOAT(u) ::dort_gpu::host_as_float(u)
+#define DG_AS_UINT(f) ::dort_gpu::host_as_uint(f)
+#endif
+#define DG_HD __host__ __device__ __forceinline__
+
+namespace dort_gpu {
+
+constexpr uint32_t kMiss = 0xffffffffu;
+constexpr int kTraceStack = 64;   // == kMaxWideDepth (bvh_build.h)
+
+struct Hit {
+  float t, b1, b2;
+  uint32_t prim;   // original triangle index, kMiss if none
+};
+
+DG_HD float dot_rn(float ax, float ay, float az,
+                                        float bx, float by, float bz) {
+  // (a.x*b.x + a.y*b.y) + a.z*b.z, each product and sum rounded separately
+  return DG_ADD(DG_ADD(DG_MUL(ax, bx), DG_MUL(ay, by)), DG_MUL(az, bz));
+}
+
+// Moller-Trumbore as triangle.cpp:109-134 (also 18-42).
+DG_HD bool mt_exact(float4 a, float4 e1, float4 e2,
+                                         float ox, float oy, float oz,
+                                         float dx, float dy, float dz,
+                                         float t_min, float t_max,
+                                         float& out_t, float& out_b1, float& out_b2) {
+  // s1 = cross(dir, e2)
+  float s1x = DG_SUB(DG_MUL(dy, e2.z), DG_MUL(dz, e2.y));
+  float s1y = DG_SUB(DG_MUL(dz, e2.x), DG_MUL(dx, e2.z));
+  float s1z = DG_SUB(DG_MUL(dx, e2.y), DG_MUL(dy, e2.x));
+  float det = dot_rn(s1x, s1y, s1z, e1.x, e1.y, e1.z);
+  if(det == 0.f) { return false; }
+  float inv_det = DG_RCP(det);
+  // s = orig - p0
+  float sx = DG_SUB(ox, a.x), sy = DG_SUB(oy, a.y), sz = DG_SUB(oz, a.z);
+  float b1 = DG_MUL(inv_det, dot_rn(s1x, s1y, s1z, sx, sy, sz));
+  if(b1 < 0.f || b1 > 1.f) { return false; }
+  // s2 = cross(s, e1)
+  float s2x = DG_SUB(DG_MUL(sy, e1.z), DG_MUL(sz, e1.y));
+  float s2y = DG_SUB(DG_MUL(sz, e1.x), DG_MUL(sx, e1.z));
+  float s2z = DG_SUB(DG_MUL(sx, e1.y), DG_MUL(sy, e1.x));
+  float b2 = DG_MUL(inv_det, dot_rn(s2x, s2y, s2z, dx, dy, dz));
+  if(b2 < 0.f || DG_ADD(b1, b2) > 1.f) { return false; }
+  float t = DG_MUL(inv_det, dot_rn(s2x, s2y, s2z, e2.x, e2.y, e2.z));
+  if(t < t_min || t > t_max) { return false; }
+  out_t = t;
+  out_b1 = b1;
+  out_b2 = b2;
+  return true;
+}
+
+DG_HD float byte_to_float(uint32_t w, int j) {
+  return DG_U2F((w >> (8 * j)) & 0xffu);
+}
+
+// Widening factor for the slab test: 2^-20 relative (> 8 ulp).
+#define DORT_SLAB_WIDEN 9.5367431640625e-7f
+
+// Tests the 8 child boxes of one node; returns the hit mask: bits 24..31 =
+// internal children (bit 24 + (slot ^ oct_inv)), bits 0..23 = triangles
+// relative to the node's tri_base.
+DG_HD uint32_t node_hitmask(
+    const uint4& n0, const uint4& n1, const uint4& n2, const uint4& n3, const uint4& n4,
+    float ox, float oy, float oz, float ix, float iy, float iz,
+    float t_min, float t_max, uint32_t oct_inv4) {
+  float px = DG_AS_FLOAT(n0.x), py = DG_AS_FLOAT(n0.y), pz = DG_AS_FLOAT(n0.z);
+  float sx = DG_AS_FLOAT((n0.w & 0xffu) << 23);
+  float sy = DG_AS_FLOAT(((n0.w >> 8) & 0xffu) << 23);
+  float sz = DG_AS_FLOAT(((n0.w >> 16) & 0xffu) << 23);
+  float adj_ix = sx * ix, adj_iy = sy * iy, adj_iz = sz * iz;
+  float adj_ox = (px - ox) * ix, adj_oy = (py - oy) * iy, adj_oz = (pz - oz) * iz;
+
+  // near / far plane bytes per axis, by direction sign
+  const bool nx = ix < 0.f, ny = iy < 0.f, nz = iz < 0.f;
+  uint32_t near_x[2] = { nx ? n3.z : n2.x, nx ? n3.w : n2.y };
+  uint32_t far_x[2]  = { nx ? n2.x : n3.z, nx ? n2.y : n3.w };
+  uint32_t near_y[2] = { ny ? n4.x : n2.z, ny ? n4.y : n2.w };
+  uint32_t far_y[2]  = { ny ? n2.z : n4.x, ny ? n2.w : n4.y };
+  uint32_t near_z[2] = { nz ? n4.z : n3.x, nz ? n4.w : n3.y };
+  uint32_t far_z[2]  = { nz ? n3.x : n4.z, nz ? n3.y : n4.w };
+
+  uint32_t hitmask = 0;
+#pragma unroll
+  for(int h = 0; h < 2; ++h) {
+    uint32_t meta4 = h ? n1.w : n1.z;
+    uint32_t is_inner4 = (meta4 & (meta4 << 1)) & 0x10101010u;
+    uint32_t inner_mask4 = (is_inner4 >> 4) * 0xffu;
+    uint32_t bit_index4 = (meta4 ^ (oct_inv4 & inner_mask4)) & 0x1f1f1f1fu;
+    uint32_t child_bits4 = (meta4 >> 5) & 0x07070707u;
+#pragma unroll
+    for(int j = 0; j < 4; ++j) {
+      float tnx = fmaf(byte_to_float(near_x[h], j), adj_ix, adj_ox);
+      float tny = fmaf(byte_to_float(near_y[h], j), adj_iy, adj_oy);
+      float tnz = fmaf(byte_to_float(near_z[h], j), adj_iz, adj_oz);
+      float tfx = fmaf(byte_to_float(far_x[h], j), adj_ix, adj_ox);
+      float tfy = fmaf(byte_to_float(far_y[h], j), adj_iy, adj_oy);
+      float tfz = fmaf(byte_to_float(far_z[h], j), adj_iz, adj_oz);
+      float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, t_min));
+      float tfar = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
+      bool hit = fmaf(-fabsf(tnear), DORT_SLAB_WIDEN, tnear) <=
+                 fmaf(fabsf(tfar), DORT_SLAB_WIDEN, tfar);
+      if(hit) {
+        uint32_t bits = (child_bits4 >> (8 * j)) & 0xffu;
+        uint32_t bidx = (bit_index4 >> (8 * j)) & 0xffu;
+        hitmask |= bits << bidx;
+      }
+    }
+  }
+  return hitmask;
+}
+
+// Closest hit (ANY_HIT = false) or any hit (ANY_HIT = true) of one ray.
+// Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
+// triangle found to intersect.  `steps` (optional) counts node visits and
+// triangle tests.
+template<bool ANY_HIT>
+DG_HD Hit trace_ray(const TraceScene& sc,
+                                         float ox, float oy, float oz, float t_min,
+                                         float dx, float dy, float dz, float t_max) {
+  Hit best;
+  best.t = t_max;
+  best.b1 = 0.f;
+  best.b2 = 0.f;
+  best.prim = kMiss;
+  if(sc.node_count == 0) { return best; }
+
+  // Box-test reciprocals; zero components become tiny so no NaN appears.
+  const float tiny = 1e-20f;
+  float ix = 1.f / (fabsf(dx) < tiny ? copysignf(tiny, dx) : dx);
+  float iy = 1.f / (fabsf(dy) < tiny ? copysignf(tiny, dy) : dy);
+  float iz = 1.f / (fabsf(dz) < tiny ? copysignf(tiny, dz) : dz);
+  const uint32_t oct_inv = (ix < 0.f ? 0u : 1u) | (iy < 0.f ? 0u : 2u) | (iz < 0.f ? 0u : 4u);
+  const uint32_t oct_inv4 = oct_inv * 0x01010101u;
+
+  uint2 stack[kTraceStack];
+  int sp = 0;
+  // root group: internal bit 31 with an empty internal-slot mask -> node 0
+  uint2 group = make_uint2(0u, 0x80000000u);
+
+  for(;;) {
+    if((group.y & 0xff000000u) == 0u) {
+      if(sp == 0) { break; }
+      group = stack[--sp];
+    }
+    uint32_t bit = 31u - DG_CLZ(group.y & 0xff000000u);
+    group.y &= ~(1u << bit);
+    uint32_t slot = (bit - 24u) ^ oct_inv;
+    uint32_t node_idx = group.x + DG_POPC(group.y & 0xffu & ((1u << slot) - 1u));
+
+    const uint4* np = sc.nodes + 5 * size_t(node_idx);
+    uint4 n0 = DG_LDG(np), n1 = DG_LDG(np + 1), n2 = DG_LDG(np + 2);
+    uint4 n3 = DG_LDG(np + 3), n4 = DG_LDG(np + 4);
+    uint32_t hitmask = node_hitmask(n0, n1, n2, n3, n4, ox, oy, oz, ix, iy, iz,
+                                    t_min, best.t, oct_inv4);
+
+    uint32_t child_hits = hitmask & 0xff000000u;
+    if(child_hits) {
+      if(group.y & 0xff000000u) {
+        // sp < kTraceStack: each push descends one level and the builder
+        // bounds the depth by kMaxWideDepth.
+        stack[sp++] = group;
+      }
+      group = make_uint2(n1.x, child_hits | (n0.w >> 24));
+    }
+
+    uint32_t tri_hits = hitmask & 0x00ffffffu;
+    while(tri_hits) {
+      uint32_t b = DG_FFS(tri_hits) - 1u;
+      tri_hits &= tri_hits - 1u;
+      const float4* tp = sc.tris + 3 * size_t(n1.y + b);
+      float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
+      float t, b1, b2;
+      if(mt_exact(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2)) {
+        uint32_t id = DG_AS_UINT(a.w);
+        if(ANY_HIT) {
+          best.t = t; best.b1 = b1; best.b2 = b2; best.prim = id;
+          return best;
+        }
+        if(best.prim == kMiss || t < best.t || id > best.prim) {
+          best.t = t; best.b1 = b1; best.b2 = b2; best.prim = id;
+        }
+      }
+    }
+  }
+  return best;
+}
+
+}  // namespace dort_gpu

@@ -1,0 +1,184 @@
+/* dort_gpu.h -- C ABI of the B200 (sm_100a) path-tracing hot path.
+ *
+ * A drop-in for the reference renderer's (honzasp/dort) hot path:
+ *   - the ray query of the primitive tree: Primitive::intersect /
+ *     intersect_p (include/dort/primitive.hpp:26-33) as reached through
+ *     Scene::intersect / intersect_p (src/dort/scene.cpp:8-18),
+ *     MeshBvhPrimitive (src/dort/mesh_bvh_primitive.cpp:13-45),
+ *     Bvh::traverse_elems (src/dort/bvh.cpp:418-469) and
+ *     TriangleUv::hit / Triangle::hit_p (src/dort/triangle.cpp:14-46,102-173);
+ *   - the "pt" renderer: Renderer::render (include/dort/renderer.hpp:27) as
+ *     implemented by PathRenderer (src/dort/path_renderer.cpp:11-206) and
+ *     selected by renderer = "pt" in dort.render.make
+ *     (src/dort/lua_render.cpp:102-221).
+ *
+ * Conventions (all entry points):
+ *   - Every call returns an int status: DORT_OK (0) or a negative DORT_ERR_*.
+ *     dort_gpu_last_error() returns a thread-local message for the last
+ *     failing call on the calling thread.  No C++ exception crosses the ABI.
+ *   - The caller owns every host array; the library copies what it keeps.
+ *     Device memory created by *_create is owned by the handle until the
+ *     matching *_destroy.
+ *   - Entry points taking host pointers are synchronous.  *_device variants
+ *     take device pointers and a cudaStream_t (passed as void*, NULL = the
+ *     legacy default stream) and are asynchronous on that stream.
+ *   - A scene handle is not thread-safe; callers serialise access to it.
+ *
+ * Ray layout: 8 floats per ray = (orig.x, orig.y, orig.z, t_min,
+ *                                  dir.x,  dir.y,  dir.z,  t_max),
+ * the fields of dort::Ray (include/dort/geometry.hpp:172-186).
+ */
+#ifndef DORT_GPU_H
+#define DORT_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DORT_GPU_ABI_VERSION 1
+
+enum dort_status {
+  DORT_OK = 0,
+  DORT_ERR_INVALID = -1,      /* bad argument (null pointer, bad size, NaN vertex, ...) */
+  DORT_ERR_CUDA = -2,         /* a CUDA runtime call failed */
+  DORT_ERR_OOM = -3,          /* device or host allocation failed */
+  DORT_ERR_TIMEOUT = -4,      /* a bounded device-side wait gave up */
+  DORT_ERR_UNSUPPORTED = -5,  /* feature not available in this build */
+  DORT_ERR_DEVICE = -6        /* a kernel reported an internal error flag */
+};
+
+#define DORT_MISS 0xffffffffu
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* dort_gpu_last_error(void);
+
+/* ABI version of the loaded library (DORT_GPU_ABI_VERSION). */
+int dort_gpu_abi_version(void);
+
+/* ---- materials ------------------------------------------------------------
+ * Material kinds and their parameters; each follows one reference material:
+ *   LAMBERT    color = albedo                  lambert_material.cpp:5-35
+ *   MIRROR     color = albedo                  mirror_material.cpp:5-29
+ *   DIELECTRIC color = reflect tint,
+ *              color2 = transmit tint,
+ *              param[0] = ior (1.5 default)    dielectric_material.cpp:32-116
+ *   PHONG      color = diffuse albedo,
+ *              color2 = glossy albedo,
+ *              param[0] = exponent             phong_material.cpp:6-106
+ *   CONDUCTOR  color = normal-incidence reflectance F0 (Schlick),
+ *              param[0] = GGX alpha            (no reference counterpart)
+ * A material whose colors are all black scatters nothing (the reference adds
+ * no BxDF for a black albedo, lambert_material.cpp:29-35).
+ */
+enum dort_material_kind {
+  DORT_MAT_LAMBERT = 0,
+  DORT_MAT_MIRROR = 1,
+  DORT_MAT_DIELECTRIC = 2,
+  DORT_MAT_PHONG = 3,
+  DORT_MAT_CONDUCTOR = 4
+};
+
+typedef struct dort_material {
+  uint32_t kind;
+  float color[3];
+  float color2[3];
+  float param[4];
+} dort_material;
+
+/* ---- scene ----------------------------------------------------------------
+ * A flat triangle scene: the reference's primitive tree (triangles added with
+ * add_triangle / add_shape / add_*ply_mesh*, transforms baked into world
+ * space) flattened into one triangle array.
+ *
+ *   tri_material  per-triangle material index (NULL: all 0)
+ *   tri_emission  per-triangle RGB radiance (NULL: none); every triangle with
+ *                 non-black emission is one one-sided diffuse area light, as
+ *                 DiffuseLight on a triangle shape (diffuse_light.cpp:40-111),
+ *                 emitting to the side of cross(e2, e1) (triangle.cpp:73)
+ *   sky_*         background light: sky_width = sky_height = 0 and a
+ *                 non-black sky_const[] gives the constant InfiniteLight
+ *                 (infinite_light.cpp:5-65); a sky image (sky_width x
+ *                 sky_height RGB float, latitude-longitude) gives the
+ *                 EnvironmentLight (environment_light.cpp:6-158)
+ *   bvh_width     children per BVH node, 2..8 (0: 8)
+ */
+typedef struct dort_scene_desc {
+  uint32_t struct_size;            /* sizeof(dort_scene_desc) */
+  const float* verts;              /* vert_count * 3 */
+  uint32_t vert_count;
+  const uint32_t* tris;            /* tri_count * 3 vertex indices */
+  uint32_t tri_count;
+  const uint32_t* tri_material;    /* tri_count, or NULL */
+  const dort_material* materials;  /* material_count (>= 1 if tri_material) */
+  uint32_t material_count;
+  const float* tri_emission;       /* tri_count * 3, or NULL */
+  const float* sky_rgb;            /* sky_width * sky_height * 3, or NULL */
+  uint32_t sky_width;
+  uint32_t sky_height;
+  float sky_const[3];
+  float sky_to_world[9];           /* row-major rotation of the sky (identity if all 0) */
+  uint32_t bvh_width;
+  uint32_t reserved[7];
+} dort_scene_desc;
+
+typedef struct dort_scene dort_scene;
+
+/* Builds the acceleration structure on the host and uploads the scene to the
+ * current CUDA device.  Replaces the scene build of build_scene
+ * (lua_builder.cpp:113-146) and the Bvh constructor (bvh.cpp:9-55). */
+int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** out_scene);
+
+/* Frees the scene's device memory.  NULL is accepted. */
+int dort_gpu_scene_destroy(dort_scene* scene);
+
+/* Scene statistics: out[0] = BVH node count, out[1] = BVH depth,
+ * out[2] = triangle count, out[3] = emissive triangle count,
+ * out[4] = device bytes held, out[5] = host build milliseconds. */
+int dort_gpu_scene_stats(const dort_scene* scene, double out[8]);
+
+/* ---- ray casting ----------------------------------------------------------
+ * Closest hit (any_hit = 0), replacing MeshBvhPrimitive::intersect
+ * (mesh_bvh_primitive.cpp:13-32): out_prim[i] = hit triangle index or
+ * DORT_MISS; out_tb[3i..3i+2] = (t, b1, b2) of the hit (untouched on a miss).
+ * The triangle test is the reference's Moller-Trumbore arithmetic, rounded
+ * identically, so t, b1, b2 are bit-identical to the reference's for the same
+ * triangle.  Among hits at exactly equal t the larger triangle index wins.
+ *
+ * Any hit (any_hit = 1), replacing MeshBvhPrimitive::intersect_p
+ * (mesh_bvh_primitive.cpp:34-45): out_prim[i] = 1 if some triangle is hit
+ * with t in [t_min, t_max], else 0; out_tb may be NULL.
+ *
+ * Host-pointer form: rays, out_prim and out_tb are host arrays. */
+int dort_gpu_raycast(dort_scene* scene, const float* rays, size_t ray_count,
+                     int any_hit, uint32_t* out_prim, float* out_tb);
+
+/* Device-pointer form of dort_gpu_raycast on a caller stream. */
+int dort_gpu_raycast_device(dort_scene* scene, const float* d_rays,
+                            size_t ray_count, int any_hit, uint32_t* d_prim,
+                            float* d_tb, void* stream);
+
+/* Event-timed device ray cast: runs dort_gpu_raycast_device `repeat` times
+ * and writes the mean kernel milliseconds per launch (measured with CUDA
+ * events on the launch stream). */
+int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
+                           size_t ray_count, int any_hit, uint32_t* d_prim,
+                           float* d_tb, void* stream, int repeat,
+                           float* out_ms_per_launch);
+
+/* ---- diagnostics ----------------------------------------------------------
+ * No reference counterpart.  Builds the device scene's wide BVH on the host
+ * and runs the device traversal code compiled for the CPU, with the same
+ * outputs as dort_gpu_raycast; needs no GPU.  For checking the BVH builder
+ * and the traversal logic only -- the device entry points never use it.
+ * out_depth (optional) receives the wide BVH depth. */
+int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const float* rays,
+                                size_t ray_count, int any_hit, uint32_t* out_prim,
+                                float* out_tb, uint32_t* out_depth);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DORT_GPU_H */

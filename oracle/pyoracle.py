@@ -1,0 +1,181 @@
+"""ctypes bindings for the test oracle.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py, always as the checker or the timed CPU baseline,
+never by the product package.
+
+Two libraries:
+  * ``liboracle.so`` -- the C restatement in oracle/*.c (always present once
+    oracle/Makefile ran).
+  * ``_ref/libdort_ref.so`` -- the reference renderer's own sources compiled
+    with the harnesses in oracle/ref/ (present when the reference tree was
+    available at build time; the built file travels with the repository).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libdort_ref.so")
+
+_P = ctypes.c_void_p
+_u32 = ctypes.c_uint32
+_u64 = ctypes.c_uint64
+_i32 = ctypes.c_int
+
+
+def build(ref_dir: str | None = None) -> None:
+    """Compiles liboracle.so (and the reference harness when the reference
+    tree exists)."""
+    args = ["make", "-s", "-C", HERE]
+    if ref_dir:
+        args.append(f"REF={ref_dir}")
+    subprocess.run(args, check=True)
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.orc_bvh_build.restype = _P
+        L.orc_bvh_build.argtypes = [_P, _u32, _P, _u32, _i32, _u32, _u32]
+        L.orc_bvh_free.argtypes = [_P]
+        L.orc_bvh_node_count.restype = _u32
+        L.orc_bvh_node_count.argtypes = [_P]
+        L.orc_bvh_nodes.argtypes = [_P, _P, _P]
+        L.orc_raycast.argtypes = [_P, _P, _u64, _i32, _P, _P, _P, _P]
+        L.orc_raycast_brute.argtypes = [_P, _P, _u32, _P, _u64, _P, _P]
+        L.orc_triangle_hit.restype = _i32
+        L.orc_triangle_hit.argtypes = [_P, _P, _P, _P, _P]
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        R = ctypes.CDLL(REF_SO)
+        R.dref_scene_create.restype = _P
+        R.dref_scene_create.argtypes = [_P, _u32, _P, _u32, _i32, _u32, _u32, _u32, _P]
+        R.dref_scene_destroy.argtypes = [_P]
+        R.dref_raycast.restype = _i32
+        R.dref_raycast.argtypes = [_P, _P, _u64, _i32, _u32, _P, _P, _P, _P]
+        _ref = R
+    return _ref
+
+
+def _mesh_args(verts, tris):
+    verts = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1, 3)
+    tris = np.ascontiguousarray(tris, dtype=np.uint32).reshape(-1, 3)
+    return verts, tris
+
+
+class OracleBvh:
+    """The C restatement of the reference's binary BVH (bvh.cpp:9-469)."""
+
+    def __init__(self, verts, tris, split: str = "sah", leaf_size: int = 6,
+                 max_leaf_size: int = 32):
+        self.verts, self.tris = _mesh_args(verts, tris)
+        m = {"middle": 0, "sah": 1}[split]
+        self.h = lib().orc_bvh_build(_ptr(self.verts), len(self.verts),
+                                     _ptr(self.tris), len(self.tris), m,
+                                     leaf_size, max_leaf_size)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_bvh_free(self.h)
+            self.h = None
+
+    def node_count(self) -> int:
+        return lib().orc_bvh_node_count(self.h)
+
+    def nodes(self):
+        n = self.node_count()
+        boxes = np.zeros((n, 6), np.float32)
+        meta = np.zeros((n, 3), np.uint32)
+        lib().orc_bvh_nodes(self.h, _ptr(boxes), _ptr(meta))
+        return boxes, meta
+
+    def raycast(self, rays, any_hit: bool = False, counts: bool = False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        prim = np.zeros(n, np.uint32)
+        tb = np.zeros((n, 3), np.float32)
+        nodes = np.zeros(n, np.uint32) if counts else None
+        tests = np.zeros(n, np.uint32) if counts else None
+        lib().orc_raycast(self.h, _ptr(rays), n, int(any_hit), _ptr(prim),
+                          _ptr(tb), _ptr(nodes), _ptr(tests))
+        if counts:
+            return prim, tb, nodes, tests
+        return prim, tb
+
+
+def brute_raycast(verts, tris, rays):
+    verts, tris = _mesh_args(verts, tris)
+    rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+    prim = np.zeros(len(rays), np.uint32)
+    tb = np.zeros((len(rays), 3), np.float32)
+    lib().orc_raycast_brute(_ptr(verts), _ptr(tris), len(tris), _ptr(rays),
+                            len(rays), _ptr(prim), _ptr(tb))
+    return prim, tb
+
+
+def triangle_hit(p0, p1, p2, ray):
+    a = [np.ascontiguousarray(x, dtype=np.float32) for x in (p0, p1, p2, ray)]
+    tb = np.zeros(3, np.float32)
+    ok = lib().orc_triangle_hit(*[_ptr(x) for x in a], _ptr(tb))
+    return bool(ok), tb
+
+
+class RefBvh:
+    """The reference's own Bvh<> + Triangle code (compiled from its sources)."""
+
+    def __init__(self, verts, tris, split: str = "sah", leaf_size: int = 6,
+                 max_leaf_size: int = 32, threads: int = 1):
+        self.verts, self.tris = _mesh_args(verts, tris)
+        m = {"middle": 0, "sah": 1}[split]
+        bt = ctypes.c_double(0.0)
+        self.h = ref().dref_scene_create(_ptr(self.verts), len(self.verts),
+                                         _ptr(self.tris), len(self.tris), m,
+                                         leaf_size, max_leaf_size, threads,
+                                         ctypes.byref(bt))
+        self.build_s = bt.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().dref_scene_destroy(self.h)
+            self.h = None
+
+    def raycast(self, rays, any_hit: bool = False, threads: int = 1,
+                counts: bool = False):
+        rays = np.ascontiguousarray(rays, dtype=np.float32).reshape(-1, 8)
+        n = len(rays)
+        prim = np.zeros(n, np.uint32)
+        tb = np.zeros((n, 3), np.float32)
+        tests = np.zeros(n, np.uint32) if counts else None
+        ts = ctypes.c_double(0.0)
+        ref().dref_raycast(self.h, _ptr(rays), n, int(any_hit), threads,
+                           _ptr(prim), _ptr(tb), _ptr(tests), ctypes.byref(ts))
+        self.trace_s = ts.value
+        if counts:
+            return prim, tb, tests
+        return prim, tb
