@@ -38,8 +38,9 @@ class _DescHolder:
 
 
 def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None,
-               sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_to_world=None,
-               bvh_width: int = 8) -> _DescHolder:
+               sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
+               sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
+               bvh_width: int = 8, **_ignored) -> _DescHolder:
     h = _DescHolder()
     d = h.desc
     verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
@@ -67,8 +68,9 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
         d.sky_rgb = h.arr(sky, np.float32)
         d.sky_height, d.sky_width = sky.shape[0], sky.shape[1]
     d.sky_const = (ctypes.c_float * 3)(*sky_const)
-    if sky_to_world is not None:
-        d.sky_to_world = (ctypes.c_float * 9)(*np.asarray(sky_to_world, np.float32).ravel())
+    d.sky_scale = (ctypes.c_float * 3)(*sky_scale)
+    d.sky_up = (ctypes.c_float * 3)(*sky_up)
+    d.sky_fwd = (ctypes.c_float * 3)(*sky_fwd)
     d.bvh_width = bvh_width
     return h
 
@@ -116,6 +118,18 @@ class Scene:
             self.handle, ctypes.c_void_p(d_rays), n, int(any_hit), ctypes.c_void_p(d_prim),
             ctypes.c_void_p(d_tb) if d_tb else None, ctypes.c_void_p(stream)))
 
+    def render(self, params: _abi.RenderParams):
+        """dort_gpu_render: returns (image [h, w, 3] float32, stats dict)."""
+        out = np.zeros((params.height, params.width, 3), np.float32)
+        st = (ctypes.c_double * 4)()
+        _abi.check(_abi.lib().dort_gpu_render(self.handle, ctypes.byref(params), _ptr(out), st))
+        return out, {"rays": st[0], "samples": st[1], "ms": st[2], "dropped": st[3]}
+
+    def render_device(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
+        _abi.check(_abi.lib().dort_gpu_render_device(self.handle, ctypes.byref(params),
+                                                     ctypes.c_void_p(d_out),
+                                                     ctypes.c_void_p(stream)))
+
     def raycast_timed(self, d_rays: int, n: int, d_prim: int, d_tb: int | None,
                       any_hit: bool = False, stream: int = 0, repeat: int = 1) -> float:
         ms = ctypes.c_float(0.0)
@@ -124,6 +138,48 @@ class Scene:
             ctypes.c_void_p(d_tb) if d_tb else None, ctypes.c_void_p(stream), repeat,
             ctypes.byref(ms)))
         return ms.value
+
+
+def render_params(camera: dict, width: int, height: int, iterations: int = 1,
+                  min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
+                  sample_all_lights: bool = False, direct_strategy: str = "mis",
+                  seed: int = 42) -> _abi.RenderParams:
+    """dort.render.make parameters (lua_render.cpp:102-145) with its defaults."""
+    p = _abi.RenderParams()
+    p.struct_size = ctypes.sizeof(_abi.RenderParams)
+    p.width, p.height, p.iterations = width, height, iterations
+    p.min_depth, p.max_depth = min_depth, max_depth
+    p.only_direct, p.sample_all_lights = int(only_direct), int(sample_all_lights)
+    p.direct_strategy = {"mis": 0, "bsdf": 1, "light": 2}[direct_strategy]
+    p.seed = seed
+    c = p.camera
+    c.origin = (ctypes.c_float * 3)(*camera["origin"])
+    c.right = (ctypes.c_float * 3)(*camera["right"])
+    c.up = (ctypes.c_float * 3)(*camera["up"])
+    c.forward = (ctypes.c_float * 3)(*camera["forward"])
+    c.fov = camera["fov"]
+    return p
+
+
+def scene_from_dict(d: dict, **kw) -> "Scene":
+    """Scene from the dict form used by dort_b200.scenes generators."""
+    keys = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
+            "sky_scale", "sky_up", "sky_fwd")
+    args = {k: d[k] for k in keys if k in d and d[k] is not None}
+    args.update(kw)
+    return Scene(d["verts"], d["tris"], **args)
+
+
+def host_check_render(d: dict, params: _abi.RenderParams, rows=None):
+    """Runs the device path sampler compiled for the host (diagnostic)."""
+    keys = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
+            "sky_scale", "sky_up", "sky_fwd")
+    h = scene_desc(d["verts"], d["tris"], **{k: d[k] for k in keys if k in d and d[k] is not None})
+    out = np.zeros((params.height, params.width, 3), np.float32)
+    r0, r1 = rows if rows else (0, params.height)
+    _abi.check(_abi.lib().dort_gpu_host_check_render(ctypes.byref(h.desc), ctypes.byref(params),
+                                                     r0, r1, _ptr(out)))
+    return out
 
 
 def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8):

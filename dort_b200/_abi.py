@@ -42,9 +42,26 @@ class SceneDesc(ctypes.Structure):
         ("tri_emission", c_p),
         ("sky_rgb", c_p), ("sky_width", c_u32), ("sky_height", c_u32),
         ("sky_const", c_f * 3),
-        ("sky_to_world", c_f * 9),
+        ("sky_scale", c_f * 3),
+        ("sky_up", c_f * 3),
+        ("sky_fwd", c_f * 3),
         ("bvh_width", c_u32),
         ("reserved", c_u32 * 7),
+    ]
+
+
+class Camera(ctypes.Structure):
+    _fields_ = [("origin", c_f * 3), ("right", c_f * 3), ("up", c_f * 3),
+                ("forward", c_f * 3), ("fov", c_f)]
+
+
+class RenderParams(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", c_u32), ("width", c_u32), ("height", c_u32),
+        ("iterations", c_u32), ("min_depth", c_u32), ("max_depth", c_u32),
+        ("only_direct", c_u32), ("sample_all_lights", c_u32),
+        ("direct_strategy", c_u32), ("pad0", c_u32), ("seed", ctypes.c_uint64),
+        ("camera", Camera), ("reserved", c_u32 * 8),
     ]
 
 
@@ -86,6 +103,15 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_host_check_raycast.restype = c_i32
         L.dort_gpu_host_check_raycast.argtypes = [ctypes.POINTER(SceneDesc), c_p, c_size,
                                                   c_i32, c_p, c_p, ctypes.POINTER(c_u32)]
+        L.dort_gpu_render.restype = c_i32
+        L.dort_gpu_render.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p,
+                                      ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_render_device.restype = c_i32
+        L.dort_gpu_render_device.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p, c_p]
+        L.dort_gpu_host_check_render.restype = c_i32
+        L.dort_gpu_host_check_render.argtypes = [ctypes.POINTER(SceneDesc),
+                                                 ctypes.POINTER(RenderParams), c_u32, c_u32,
+                                                 c_p]
         _lib = L
     return _lib
 

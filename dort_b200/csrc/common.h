@@ -5,7 +5,10 @@
 #include <cstdint>
 #include <string>
 
+#include <vector>
+
 #include "../../include/dort_gpu.h"
+#include "pt_scene.h"
 
 namespace dort_gpu {
 
@@ -23,28 +26,20 @@ int fail(int code, const std::string& msg);
     }                                                                        \
   } while(0)
 
-// Device view of the ray-query part of a scene.
-struct TraceScene {
-  const uint4* nodes;   // 5 x uint4 per WideNode (bvh_build.h)
-  const float4* tris;   // 3 x float4 per LeafTri
-  uint32_t node_count;
-  uint32_t tri_count;
-};
-
 }  // namespace dort_gpu
 
 // Host-side scene handle behind the opaque dort_scene.
 struct dort_scene {
   int device = 0;
   dort_gpu::TraceScene trace{};
+  dort_gpu::PtScene pt{};               // device view for the path tracers
   uint32_t depth = 0;
   uint32_t tri_count = 0;
   uint32_t emissive_count = 0;
   size_t device_bytes = 0;
   double build_ms = 0.0;
-  void* d_nodes = nullptr;
-  void* d_tris = nullptr;
-  uint32_t* d_work = nullptr;          // persistent-kernel work counters (scratch)
+  std::vector<void*> allocations;       // every device buffer owned by the scene
+  uint32_t* d_work = nullptr;           // work counters of persistent kernels (scratch)
   // staging for the host-pointer entry points (grow-only)
   void* d_stage = nullptr;
   size_t stage_bytes = 0;

@@ -1,0 +1,288 @@
+// The plain per-pixel path tracer ("megakernel"): one thread runs whole
+// paths for one pixel over a slice of its samples, keeps the sums in
+// registers and writes one (sum RGB, kept count) record per (slice, pixel);
+// a resolve kernel adds the slices in a fixed order and divides, so the image
+// is deterministic and needs no atomics.
+//
+// Replaces PathRenderer::render (path_renderer.cpp:11-21) and the tiling of
+// Renderer::iteration_tiled (renderer.cpp:26-86); each path is pt_sample
+// (pt.cuh).
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "pt.cuh"
+#include "scene_build.h"
+
+namespace dort_gpu {
+
+constexpr int kPtBlock = 128;
+
+// Film position of sample `s` of pixel (x, y): the pixel centre on
+// iteration 0, uniform jitter afterwards (path_renderer.cpp:17).
+DG_HD void film_pos(const PtParams& pp, uint32_t pixel, uint32_t x, uint32_t y, uint32_t s,
+                    float& fx, float& fy) {
+  if(s == 0) {
+    fx = float(x) + 0.5f;
+    fy = float(y) + 0.5f;
+  } else {
+    Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
+    fx = float(x) + j.a;
+    fy = float(y) + j.b;
+  }
+}
+
+DG_HD bool keep_sample(V3 L) {
+  // renderer.cpp:36-41: only finite, non-negative samples reach the film
+  return isfinite(L.x) && isfinite(L.y) && isfinite(L.z) && L.x >= 0.f && L.y >= 0.f &&
+         L.z >= 0.f;
+}
+
+__global__ void __launch_bounds__(kPtBlock)
+pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
+              uint32_t per_slice, float4* __restrict__ partial,
+              unsigned long long* __restrict__ ray_count) {
+  const uint32_t npix = pp.width * pp.height;
+  const uint64_t tid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  uint32_t rays = 0;
+  if(tid < uint64_t(per_slice) * slices) {
+    // 8x4 pixel tiles per warp keep primary rays of a warp coherent; the
+    // grid covers whole tiles, threads past the image edge idle
+    uint32_t slice = uint32_t(tid / per_slice);
+    uint32_t local = uint32_t(tid % per_slice);
+    uint32_t tiles_x = (pp.width + 7) / 8;
+    uint32_t tile = local / 32, lane = local % 32;
+    uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+    uint32_t x = tx * 8 + lane % 8, y = ty * 4 + lane / 8;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    if(x < pp.width && y < pp.height) {
+      uint32_t pixel = y * pp.width + x;
+      uint32_t s0 = slice * spp_per_slice;
+      uint32_t s1 = min(pp.spp, s0 + spp_per_slice);
+      NoTape tape;
+      for(uint32_t s = s0; s < s1; ++s) {
+        float fx, fy;
+        film_pos(pp, pixel, x, y, s, fx, fy);
+        PathResult r = pt_sample(sc, pp, pixel, s, fx, fy, tape);
+        rays += r.rays;
+        if(keep_sample(r.L)) {
+          acc.x += r.L.x;
+          acc.y += r.L.y;
+          acc.z += r.L.z;
+          acc.w += 1.f;
+        }
+      }
+      partial[size_t(slice) * npix + pixel] = acc;
+    }
+  }
+  // one atomic per warp for the ray statistics
+  for(int o = 16; o > 0; o >>= 1) { rays += __shfl_down_sync(0xffffffffu, rays, o); }
+  if((threadIdx.x & 31) == 0 && rays) { atomicAdd(ray_count, (unsigned long long)rays); }
+}
+
+__global__ void pt_resolve(const float4* __restrict__ partial, uint32_t slices, uint32_t npix,
+                           float* __restrict__ out_rgb, unsigned long long* __restrict__ kept) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t k = 0;
+  if(p < npix) {
+    float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+    for(uint32_t s = 0; s < slices; ++s) {
+      float4 v = partial[size_t(s) * npix + p];
+      a.x += v.x; a.y += v.y; a.z += v.z; a.w += v.w;
+    }
+    float inv = a.w != 0.f ? 1.f / a.w : 0.f;
+    out_rgb[3 * size_t(p)] = a.w != 0.f ? a.x * inv : 0.f;
+    out_rgb[3 * size_t(p) + 1] = a.w != 0.f ? a.y * inv : 0.f;
+    out_rgb[3 * size_t(p) + 2] = a.w != 0.f ? a.z * inv : 0.f;
+    k = uint32_t(a.w);
+  }
+  for(int o = 16; o > 0; o >>= 1) { k += __shfl_down_sync(0xffffffffu, k, o); }
+  if((threadIdx.x & 31) == 0 && k) { atomicAdd(kept, (unsigned long long)k); }
+}
+
+bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
+  if(rp->struct_size != sizeof(dort_render_params)) {
+    err = "dort_render_params.struct_size mismatch (ABI version)";
+    return false;
+  }
+  if(rp->width == 0 || rp->height == 0 || rp->width > 16384 || rp->height > 16384) {
+    err = "width and height must be 1..16384";
+    return false;
+  }
+  if(rp->iterations == 0 || rp->iterations > (1u << 20)) {
+    err = "iterations must be 1..2^20";
+    return false;
+  }
+  if(rp->max_depth > 1000) { err = "max_depth must be <= 1000"; return false; }
+  if(rp->direct_strategy > 2) { err = "direct_strategy must be 0 (mis), 1 (bsdf) or 2 (light)"; return false; }
+  std::memset(&pp, 0, sizeof(pp));
+  const dort_camera& c = rp->camera;
+  for(int a = 0; a < 3; ++a) {
+    pp.origin[a] = c.origin[a];
+    pp.right[a] = c.right[a];
+    pp.up[a] = c.up[a];
+    pp.forward[a] = c.forward[a];
+  }
+  // lua_camera.cpp:63-64 clamps the field of view to [1e-2, pi]
+  float fov = c.fov;
+  if(!(fov >= 1e-2f)) { fov = 1e-2f; }
+  if(fov > kPi) { fov = kPi; }
+  pp.proj_dim = 2.f * tanf(0.5f * fov);
+  pp.width = rp->width;
+  pp.height = rp->height;
+  pp.spp = rp->iterations;
+  pp.min_depth = rp->min_depth;
+  pp.max_depth = rp->max_depth;
+  pp.only_direct = rp->only_direct;
+  pp.sample_all_lights = rp->sample_all_lights;
+  pp.strategy = rp->direct_strategy;
+  pp.seed = rp->seed;
+  return true;
+}
+
+// Scratch for the megakernel: per-(slice, pixel) partial sums plus counters,
+// grown on demand and kept with the scene.
+static int ensure_scratch(dort_scene* s, size_t bytes, void** out) {
+  if(s->stage_bytes < bytes) {
+    if(s->d_stage) { cudaFree(s->d_stage); s->d_stage = nullptr; s->stage_bytes = 0; }
+    if(cudaMalloc(&s->d_stage, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DORT_ERR_OOM, "cudaMalloc of render scratch failed");
+    }
+    s->stage_bytes = bytes;
+  }
+  *out = s->d_stage;
+  return DORT_OK;
+}
+
+int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
+                  unsigned long long* d_counters) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint32_t npix = pp.width * pp.height;
+  // enough (pixel, slice) threads for ~4 waves of 1024 threads per SM
+  uint64_t target = uint64_t(sms) * 1024 * 4;
+  uint32_t slices = uint32_t(std::min<uint64_t>(pp.spp, std::max<uint64_t>(1, target / npix)));
+  uint32_t per = (pp.spp + slices - 1) / slices;
+  slices = (pp.spp + per - 1) / per;
+  // tiles of 8x4 pixels: the thread grid covers the padded tile area
+  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  uint32_t per_slice = tiles * 32;
+  size_t partial_bytes = size_t(slices) * npix * sizeof(float4);
+  void* scratch = nullptr;
+  int rc = ensure_scratch(s, partial_bytes, &scratch);
+  if(rc != DORT_OK) { return rc; }
+  float4* partial = static_cast<float4*>(scratch);
+  uint64_t threads = uint64_t(slices) * per_slice;
+  uint32_t blocks = uint32_t((threads + kPtBlock - 1) / kPtBlock);
+  pt_megakernel<<<blocks, kPtBlock, 0, st>>>(s->pt, pp, slices, per, per_slice, partial,
+                                             d_counters);
+  DG_CUDA(cudaGetLastError());
+  pt_resolve<<<(npix + 255) / 256, 256, 0, st>>>(partial, slices, npix, d_out, d_counters + 1);
+  DG_CUDA(cudaGetLastError());
+  return DORT_OK;
+}
+
+}  // namespace dort_gpu
+
+using namespace dort_gpu;
+
+extern "C" int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
+                                      float* d_out_rgb, void* stream) {
+  clear_error();
+  if(!scene || !params || !d_out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  DG_CUDA(cudaMemsetAsync(scene->d_work, 0, 2 * sizeof(unsigned long long), st));
+  return launch_render(scene, pp, d_out_rgb, st,
+                       reinterpret_cast<unsigned long long*>(scene->d_work));
+}
+
+extern "C" int dort_gpu_render(dort_scene* scene, const dort_render_params* params,
+                               float* out_rgb, double* out_stats) {
+  clear_error();
+  if(!scene || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  size_t npix = size_t(pp.width) * pp.height;
+  float* d_out = nullptr;
+  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
+  }
+  cudaStream_t st = 0;
+  unsigned long long* ctr = reinterpret_cast<unsigned long long*>(scene->d_work);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  int rc = DORT_OK;
+  if(cudaMemsetAsync(ctr, 0, 2 * sizeof(unsigned long long), st) != cudaSuccess) {
+    rc = fail(DORT_ERR_CUDA, "cudaMemsetAsync failed");
+  }
+  if(rc == DORT_OK) {
+    cudaEventRecord(e0, st);
+    rc = launch_render(scene, pp, d_out, st, ctr);
+    cudaEventRecord(e1, st);
+  }
+  unsigned long long counters[2] = {0, 0};
+  if(rc == DORT_OK) {
+    if(cudaMemcpyAsync(out_rgb, d_out, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st) !=
+           cudaSuccess ||
+       cudaMemcpyAsync(counters, ctr, sizeof(counters), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = fail(DORT_ERR_CUDA, std::string("render failed: ") + cudaGetErrorString(cudaGetLastError()));
+    }
+  }
+  float ms = 0.f;
+  if(rc == DORT_OK) { cudaEventElapsedTime(&ms, e0, e1); }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_out);
+  if(rc == DORT_OK && out_stats) {
+    out_stats[0] = double(counters[0]);
+    out_stats[1] = double(counters[1]);
+    out_stats[2] = ms;
+    out_stats[3] = double(uint64_t(npix) * pp.spp - counters[1]);
+  }
+  return rc;
+}
+
+extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
+                                          const dort_render_params* params,
+                                          uint32_t row_begin, uint32_t row_end,
+                                          float* out_rgb) {
+  clear_error();
+  if(!desc || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  HostScene hs;
+  std::string err;
+  if(!build_host_scene(desc, hs, err)) { return fail(DORT_ERR_INVALID, err); }
+  PtParams pp;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(row_end > pp.height) { row_end = pp.height; }
+  PtScene sc = host_view(hs);
+  NoTape tape;
+  for(uint32_t y = row_begin; y < row_end; ++y) {
+    for(uint32_t x = 0; x < pp.width; ++x) {
+      uint32_t pixel = y * pp.width + x;
+      double acc[3] = {0, 0, 0};
+      double w = 0;
+      for(uint32_t s = 0; s < pp.spp; ++s) {
+        float fx, fy;
+        film_pos(pp, pixel, x, y, s, fx, fy);
+        PathResult r = pt_sample(sc, pp, pixel, s, fx, fy, tape);
+        if(keep_sample(r.L)) {
+          acc[0] += r.L.x; acc[1] += r.L.y; acc[2] += r.L.z;
+          w += 1;
+        }
+      }
+      float* o = out_rgb + 3 * size_t(pixel);
+      for(int a = 0; a < 3; ++a) { o[a] = w != 0 ? float(acc[a] / w) : 0.f; }
+    }
+  }
+  return DORT_OK;
+}

@@ -1,0 +1,89 @@
+// Device view of a renderable scene and of the render parameters.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/dort_gpu.h"
+
+namespace dort_gpu {
+
+// Device view of the ray-query part of a scene.
+struct TraceScene {
+  const uint4* nodes;   // 5 x uint4 per WideNode (bvh_build.h)
+  const float4* tris;   // 3 x float4 per LeafTri
+  uint32_t node_count;
+  uint32_t tri_count;
+};
+
+// BxDF flag bits as the reference's BxdfFlags (include/dort/bsdf.hpp:8-28).
+enum : uint32_t {
+  F_REFL = 1, F_TRANS = 2, F_DIFF = 4, F_GLOSSY = 8, F_DELTA = 16,
+  F_MODES = F_REFL | F_TRANS, F_LOBES = F_DIFF | F_GLOSSY | F_DELTA,
+  F_ALL = F_MODES | F_LOBES,
+};
+
+// Resolved material: which single BxDF the reference's Material::add_bxdfs
+// would add (every material in scope adds at most one), with its constants.
+struct DevMaterial {
+  uint32_t kind;      // DORT_MAT_* ; bxdf_flags == 0: no BxDF (black)
+  uint32_t bxdf_flags;
+  float c[3];         // lambert/mirror albedo; dielectric reflect tint;
+                      // phong diffuse; conductor F0
+  float c2[3];        // dielectric transmit tint; phong glossy
+  float p0;           // dielectric ior_inside; phong exponent; conductor alpha
+  float p1;           // phong: glossy sampling weight
+  float p2, p3;
+};
+
+enum : uint32_t { LIGHT_TRI = 0, LIGHT_INFINITE = 1, LIGHT_ENV = 2 };
+
+struct DevLight {
+  uint32_t kind;
+  uint32_t tri;       // LIGHT_TRI: original triangle index
+  float L[3];         // radiance (LIGHT_ENV: unused)
+  float area;         // LIGHT_TRI: triangle area
+  float p0[3], e1[3], e2[3];
+  float nn[3];        // normalize(cross(e2, e1))
+};
+
+// Latitude-longitude environment map (EnvironmentLight,
+// environment_light.cpp:6-158) with its piecewise-constant 2-D distribution
+// (piecewise_distrib_2d.cpp).
+struct DevEnv {
+  const float* rgb;          // w * h * 3
+  const float* marginal_cdf; // h + 1
+  const float* cond_cdf;     // (w + 1) * h
+  const float* pdfs;         // w * h
+  uint32_t w, h;
+  float scale[3];
+  float up[3], s[3], t[3];
+};
+
+struct PtScene {
+  TraceScene trace;
+  const float4* shade;       // 3 per original triangle: (p0, material), (p1, light+1), (p2, 0)
+  const DevMaterial* mats;
+  uint32_t mat_count;
+  const float* tri_albedo;   // optional per-triangle albedo override (tri_count * 3)
+  const float* tri_emission; // optional per-triangle emission override (tri_count * 3)
+  const DevLight* lights;
+  uint32_t light_count;
+  const float* light_cdf;    // light_count + 1
+  uint32_t bg_count;
+  uint32_t bg_light[2];      // indices into lights of the background lights
+  DevEnv env;
+};
+
+struct PtParams {
+  float origin[3], right[3], up[3], forward[3];
+  float proj_dim;            // 2 tan(fov / 2)
+  uint32_t width, height;
+  uint32_t spp;              // iterations
+  uint32_t min_depth, max_depth;
+  uint32_t only_direct, sample_all_lights;
+  uint32_t strategy;         // 0 mis, 1 bsdf, 2 light
+  uint64_t seed;
+};
+
+}  // namespace dort_gpu

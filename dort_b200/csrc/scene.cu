@@ -5,6 +5,7 @@
 
 #include "bvh_build.h"
 #include "common.h"
+#include "scene_build.h"
 
 namespace dort_gpu {
 
@@ -26,79 +27,96 @@ extern "C" const char* dort_gpu_last_error(void) { return g_last_error.c_str(); 
 extern "C" int dort_gpu_abi_version(void) { return DORT_GPU_ABI_VERSION; }
 
 static void scene_free_device(dort_scene* s) {
-  if(s->d_nodes) { cudaFree(s->d_nodes); }
-  if(s->d_tris) { cudaFree(s->d_tris); }
-  if(s->d_work) { cudaFree(s->d_work); }
+  for(void* p : s->allocations) { cudaFree(p); }
+  s->allocations.clear();
   if(s->d_stage) { cudaFree(s->d_stage); }
-  s->d_nodes = s->d_tris = s->d_stage = nullptr;
+  s->d_stage = nullptr;
+  s->stage_bytes = 0;
   s->d_work = nullptr;
+}
+
+// Copies a host vector into a new device buffer owned by the scene.
+template<class T>
+static int upload(dort_scene* s, const std::vector<T>& v, const T** out) {
+  *out = nullptr;
+  if(v.empty()) { return DORT_OK; }
+  void* d = nullptr;
+  size_t bytes = v.size() * sizeof(T);
+  if(cudaMalloc(&d, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DORT_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
+  }
+  s->allocations.push_back(d);
+  s->device_bytes += bytes;
+  DG_CUDA(cudaMemcpy(d, v.data(), bytes, cudaMemcpyHostToDevice));
+  *out = static_cast<const T*>(d);
+  return DORT_OK;
+}
+
+static int scene_upload(dort_scene* s, const HostScene& hs) {
+  int rc;
+  const WideNode* nodes;
+  const LeafTri* tris;
+  if((rc = upload(s, hs.bvh.nodes, &nodes)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.bvh.tris, &tris)) != DORT_OK) { return rc; }
+  s->trace.nodes = reinterpret_cast<const uint4*>(nodes);
+  s->trace.tris = reinterpret_cast<const float4*>(tris);
+  s->trace.node_count = uint32_t(hs.bvh.nodes.size());
+  s->trace.tri_count = uint32_t(hs.bvh.tris.size());
+
+  PtScene& pt = s->pt;
+  std::memset(&pt, 0, sizeof(pt));
+  pt.trace = s->trace;
+  if((rc = upload(s, hs.shade, &pt.shade)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.mats, &pt.mats)) != DORT_OK) { return rc; }
+  pt.mat_count = uint32_t(hs.mats.size());
+  if((rc = upload(s, hs.lights, &pt.lights)) != DORT_OK) { return rc; }
+  pt.light_count = uint32_t(hs.lights.size());
+  if((rc = upload(s, hs.light_cdf, &pt.light_cdf)) != DORT_OK) { return rc; }
+  pt.bg_count = hs.bg_count;
+  pt.bg_light[0] = hs.bg_light[0];
+  pt.bg_light[1] = hs.bg_light[1];
+  pt.env = hs.env;
+  if((rc = upload(s, hs.env_rgb, &pt.env.rgb)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.env_marginal, &pt.env.marginal_cdf)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.env_cond, &pt.env.cond_cdf)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.env_pdfs, &pt.env.pdfs)) != DORT_OK) { return rc; }
+
+  void* w = nullptr;
+  if(cudaMalloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DORT_ERR_OOM, "cudaMalloc of work counters failed");
+  }
+  s->allocations.push_back(w);
+  s->device_bytes += 64 * sizeof(uint32_t);
+  s->d_work = static_cast<uint32_t*>(w);
+  return DORT_OK;
 }
 
 extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** out_scene) {
   clear_error();
   if(!desc || !out_scene) { return fail(DORT_ERR_INVALID, "null argument"); }
   *out_scene = nullptr;
-  if(desc->struct_size != sizeof(dort_scene_desc)) {
-    return fail(DORT_ERR_INVALID, "dort_scene_desc.struct_size mismatch (ABI version)");
-  }
-  if(desc->tri_count > 0 && (!desc->verts || !desc->tris)) {
-    return fail(DORT_ERR_INVALID, "verts and tris are required when tri_count > 0");
-  }
-  if(desc->tri_count > (1u << 30)) {
-    return fail(DORT_ERR_INVALID, "tri_count exceeds 2^30");
-  }
 
   auto t0 = std::chrono::steady_clock::now();
-  BuildOptions opts;
-  opts.width = desc->bvh_width ? desc->bvh_width : 8;
-  WideBvh bvh;
+  HostScene hs;
   std::string err;
-  if(!build_wide_bvh(desc->verts, desc->vert_count, desc->tris, desc->tri_count,
-                     opts, bvh, err)) {
-    return fail(DORT_ERR_INVALID, err);
-  }
+  if(!build_host_scene(desc, hs, err)) { return fail(DORT_ERR_INVALID, err); }
   auto t1 = std::chrono::steady_clock::now();
 
   dort_scene* s = new dort_scene();
   cudaGetDevice(&s->device);
   s->tri_count = desc->tri_count;
-  s->depth = bvh.depth;
+  s->depth = hs.bvh.depth;
+  s->emissive_count = hs.emissive_count;
   s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-
-  size_t node_bytes = bvh.nodes.size() * sizeof(WideNode);
-  size_t tri_bytes = bvh.tris.size() * sizeof(LeafTri);
-  auto cleanup_fail = [&](int code, const std::string& msg) {
+  int rc = scene_upload(s, hs);
+  if(rc != DORT_OK) {
+    std::string msg = g_last_error;
     scene_free_device(s);
     delete s;
-    return fail(code, msg);
-  };
-  if(node_bytes) {
-    if(cudaMalloc(&s->d_nodes, node_bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return cleanup_fail(DORT_ERR_OOM, "cudaMalloc of BVH nodes failed");
-    }
-    if(cudaMemcpy(s->d_nodes, bvh.nodes.data(), node_bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
-      return cleanup_fail(DORT_ERR_CUDA, "copy of BVH nodes failed");
-    }
+    return fail(rc, msg);
   }
-  if(tri_bytes) {
-    if(cudaMalloc(&s->d_tris, tri_bytes) != cudaSuccess) {
-      cudaGetLastError();
-      return cleanup_fail(DORT_ERR_OOM, "cudaMalloc of triangles failed");
-    }
-    if(cudaMemcpy(s->d_tris, bvh.tris.data(), tri_bytes, cudaMemcpyHostToDevice) != cudaSuccess) {
-      return cleanup_fail(DORT_ERR_CUDA, "copy of triangles failed");
-    }
-  }
-  if(cudaMalloc(&s->d_work, 64 * sizeof(uint32_t)) != cudaSuccess) {
-    cudaGetLastError();
-    return cleanup_fail(DORT_ERR_OOM, "cudaMalloc of work counters failed");
-  }
-  s->trace.nodes = static_cast<const uint4*>(s->d_nodes);
-  s->trace.tris = static_cast<const float4*>(s->d_tris);
-  s->trace.node_count = uint32_t(bvh.nodes.size());
-  s->trace.tri_count = uint32_t(bvh.tris.size());
-  s->device_bytes = node_bytes + tri_bytes + 64 * sizeof(uint32_t);
   *out_scene = s;
   return DORT_OK;
 }

@@ -1,0 +1,314 @@
+// Host-side scene assembly (see scene_build.h).
+//
+// Follows what the reference's builder and lights compute before rendering:
+//   - materials resolve to the single BxDF their add_bxdfs would add
+//     (lambert_material.cpp:27-35, mirror_material.cpp:24-29,
+//     dielectric_material.cpp:105-116, phong_material.cpp:98-106);
+//   - every emissive triangle becomes one DiffuseLight (diffuse_light.cpp),
+//     background lights follow in the order InfiniteLight, EnvironmentLight;
+//   - the light choice CDF is DiscreteDistrib1d over approximate_power()
+//     averages (scene.cpp:20-28, discrete_distrib_1d.cpp:4-20), with the
+//     scene radius of build_scene (lua_builder.cpp:124-126);
+//   - the environment map's 2-D distribution is PiecewiseDistrib2d over
+//     |average(texel) * clamp(cos theta, 0, 1)| (environment_light.cpp:6-30,
+//     piecewise_distrib_2d.cpp:4-35).
+#include "scene_build.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+namespace dort_gpu {
+namespace {
+
+struct F3 { float x, y, z; };
+F3 f3(const float* p) { return {p[0], p[1], p[2]}; }
+F3 sub(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+F3 crs(F3 a, F3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+float dt(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+float len(F3 a) { return std::sqrt(dt(a, a)); }
+F3 nrm(F3 a) { float k = 1.f / len(a); return {a.x * k, a.y * k, a.z * k}; }
+float avg3(const float* c) { return (1.f / 3.f) * (c[0] + c[1] + c[2]); }
+bool black3(const float* c) { return c[0] == 0.f && c[1] == 0.f && c[2] == 0.f; }
+
+bool resolve_material(const dort_material& in, DevMaterial& m, std::string& err) {
+  std::memset(&m, 0, sizeof(m));
+  m.kind = in.kind;
+  for(int i = 0; i < 3; ++i) { m.c[i] = in.color[i]; m.c2[i] = in.color2[i]; }
+  for(int i = 0; i < 3; ++i) {
+    if(!std::isfinite(in.color[i]) || !std::isfinite(in.color2[i]) ||
+       in.color[i] < 0.f || in.color2[i] < 0.f) {
+      err = "material colors must be finite and non-negative";
+      return false;
+    }
+  }
+  switch(in.kind) {
+    case DORT_MAT_LAMBERT:
+      m.bxdf_flags = black3(m.c) ? 0 : (F_REFL | F_DIFF);
+      return true;
+    case DORT_MAT_MIRROR:
+      m.bxdf_flags = black3(m.c) ? 0 : (F_DELTA | F_REFL);
+      return true;
+    case DORT_MAT_DIELECTRIC: {
+      float ior = in.param[0] > 0.f ? in.param[0] : 1.5f;
+      m.p0 = ior;
+      m.bxdf_flags = (black3(m.c) && black3(m.c2)) ? 0 : (F_DELTA | F_REFL | F_TRANS);
+      return true;
+    }
+    case DORT_MAT_PHONG: {
+      float s[3] = {m.c[0] + m.c2[0], m.c[1] + m.c2[1], m.c[2] + m.c2[2]};
+      float mx = std::max(s[0], std::max(s[1], s[2]));
+      if(mx > 1.f) {
+        float darken = 1.f / mx;
+        for(int i = 0; i < 3; ++i) { m.c[i] *= darken; m.c2[i] *= darken; }
+      }
+      m.p0 = in.param[0];
+      if(!black3(m.c2)) {
+        float dw = avg3(m.c), gw = avg3(m.c2);
+        float sum = dw + gw;
+        m.p1 = sum != 0.f ? gw / sum : 0.f;
+        m.bxdf_flags = F_REFL | F_DIFF | F_GLOSSY;
+      } else if(!black3(m.c)) {
+        m.kind = DORT_MAT_LAMBERT;
+        m.bxdf_flags = F_REFL | F_DIFF;
+      } else {
+        m.bxdf_flags = 0;
+      }
+      return true;
+    }
+    case DORT_MAT_CONDUCTOR:
+      m.p0 = std::max(in.param[0], 1e-3f);
+      m.bxdf_flags = black3(m.c) ? 0 : (F_REFL | F_GLOSSY);
+      return true;
+    default:
+      err = "unknown material kind " + std::to_string(in.kind);
+      return false;
+  }
+}
+
+// DiscreteDistrib1d (discrete_distrib_1d.cpp:4-20)
+std::vector<float> make_cdf(const std::vector<float>& xs) {
+  std::vector<float> cdf;
+  float sum = 0.f;
+  for(float x : xs) { cdf.push_back(sum); sum += x; }
+  cdf.push_back(sum);
+  float inv = sum == 0.f ? 0.f : 1.f / sum;
+  for(float& c : cdf) { c *= inv; }
+  return cdf;
+}
+
+}  // namespace
+
+bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& err) {
+  if(desc->struct_size != sizeof(dort_scene_desc)) {
+    err = "dort_scene_desc.struct_size mismatch (ABI version)";
+    return false;
+  }
+  uint32_t n = desc->tri_count;
+  if(n > 0 && (!desc->verts || !desc->tris)) {
+    err = "verts and tris are required when tri_count > 0";
+    return false;
+  }
+  if(n > (1u << 30)) { err = "tri_count exceeds 2^30"; return false; }
+  if(desc->tri_material && (!desc->materials || desc->material_count == 0)) {
+    err = "tri_material given without materials";
+    return false;
+  }
+
+  // materials (material 0 is a white Lambert when none are given)
+  hs.mats.clear();
+  if(desc->materials && desc->material_count > 0) {
+    for(uint32_t i = 0; i < desc->material_count; ++i) {
+      DevMaterial m;
+      if(!resolve_material(desc->materials[i], m, err)) { return false; }
+      hs.mats.push_back(m);
+    }
+  } else {
+    dort_material def;
+    std::memset(&def, 0, sizeof(def));
+    def.kind = DORT_MAT_LAMBERT;
+    def.color[0] = def.color[1] = def.color[2] = 0.5f;
+    DevMaterial m;
+    resolve_material(def, m, err);
+    hs.mats.push_back(m);
+  }
+
+  BuildOptions opts;
+  opts.width = desc->bvh_width ? desc->bvh_width : 8;
+  if(!build_wide_bvh(desc->verts, desc->vert_count, desc->tris, n, opts, hs.bvh, err)) {
+    return false;
+  }
+
+  // per-triangle shading records and area lights
+  hs.shade.assign(3 * size_t(n), make_float4(0.f, 0.f, 0.f, 0.f));
+  hs.lights.clear();
+  std::vector<float> powers;
+  hs.emissive_count = 0;
+  float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for(uint32_t t = 0; t < n; ++t) {
+    const float* p[3];
+    for(int k = 0; k < 3; ++k) {
+      p[k] = desc->verts + 3 * size_t(desc->tris[3 * size_t(t) + k]);
+      for(int a = 0; a < 3; ++a) {
+        lo[a] = std::min(lo[a], p[k][a]);
+        hi[a] = std::max(hi[a], p[k][a]);
+      }
+    }
+    uint32_t mat = desc->tri_material ? desc->tri_material[t] : 0;
+    if(mat >= hs.mats.size()) {
+      err = "triangle " + std::to_string(t) + " has material " + std::to_string(mat) +
+            " >= material_count";
+      return false;
+    }
+    uint32_t light = 0;
+    if(desc->tri_emission) {
+      const float* le = desc->tri_emission + 3 * size_t(t);
+      for(int a = 0; a < 3; ++a) {
+        if(!std::isfinite(le[a]) || le[a] < 0.f) {
+          err = "triangle emission must be finite and non-negative";
+          return false;
+        }
+      }
+      if(!black3(le)) {
+        DevLight l;
+        std::memset(&l, 0, sizeof(l));
+        l.kind = LIGHT_TRI;
+        l.tri = t;
+        for(int a = 0; a < 3; ++a) { l.L[a] = le[a]; }
+        F3 p0 = f3(p[0]), e1 = sub(f3(p[1]), p0), e2 = sub(f3(p[2]), p0);
+        l.area = 0.5f * len(crs(e1, e2));      // Triangle::area (triangle.cpp:56-60)
+        F3 nn = nrm(crs(e2, e1));
+        l.p0[0] = p0.x; l.p0[1] = p0.y; l.p0[2] = p0.z;
+        l.e1[0] = e1.x; l.e1[1] = e1.y; l.e1[2] = e1.z;
+        l.e2[0] = e2.x; l.e2[1] = e2.y; l.e2[2] = e2.z;
+        l.nn[0] = nn.x; l.nn[1] = nn.y; l.nn[2] = nn.z;
+        float pw[3] = {l.area * le[0], l.area * le[1], l.area * le[2]};
+        powers.push_back(avg3(pw));
+        hs.lights.push_back(l);
+        light = uint32_t(hs.lights.size());
+        hs.emissive_count += 1;
+      }
+    }
+    uint32_t matbits, lightbits;
+    std::memcpy(&matbits, &mat, 4);
+    std::memcpy(&lightbits, &light, 4);
+    float mf, lf;
+    std::memcpy(&mf, &matbits, 4);
+    std::memcpy(&lf, &lightbits, 4);
+    hs.shade[3 * size_t(t)] = make_float4(p[0][0], p[0][1], p[0][2], mf);
+    hs.shade[3 * size_t(t) + 1] = make_float4(p[1][0], p[1][1], p[1][2], lf);
+    hs.shade[3 * size_t(t) + 2] = make_float4(p[2][0], p[2][1], p[2][2], 0.f);
+  }
+  // Scene::radius = bounds.radius() (box.hpp:36-38)
+  F3 ext = n > 0 ? F3{hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]} : F3{0.f, 0.f, 0.f};
+  hs.radius = len(ext) * 0.5f;
+  float r2pi = 3.14159265358979323846f * hs.radius * hs.radius;
+
+  hs.bg_count = 0;
+  if(!black3(desc->sky_const)) {
+    DevLight l;
+    std::memset(&l, 0, sizeof(l));
+    l.kind = LIGHT_INFINITE;
+    for(int a = 0; a < 3; ++a) { l.L[a] = desc->sky_const[a]; }
+    float pw[3] = {r2pi * l.L[0], r2pi * l.L[1], r2pi * l.L[2]};
+    powers.push_back(avg3(pw));
+    hs.lights.push_back(l);
+    hs.bg_light[hs.bg_count++] = uint32_t(hs.lights.size() - 1);
+  }
+  hs.env_rgb.clear();
+  std::memset(&hs.env, 0, sizeof(hs.env));
+  if(desc->sky_rgb && desc->sky_width > 0 && desc->sky_height > 0) {
+    uint32_t w = desc->sky_width, h = desc->sky_height;
+    if(size_t(w) * h > (size_t(1) << 26)) { err = "sky image too large"; return false; }
+    hs.env_rgb.assign(desc->sky_rgb, desc->sky_rgb + 3 * size_t(w) * h);
+    for(float v : hs.env_rgb) {
+      if(!std::isfinite(v) || v < 0.f) { err = "sky image must be finite and non-negative"; return false; }
+    }
+    float scale[3] = {1.f, 1.f, 1.f};
+    if(!black3(desc->sky_scale)) { for(int a = 0; a < 3; ++a) { scale[a] = desc->sky_scale[a]; } }
+    F3 up = black3(desc->sky_up) ? F3{0.f, 1.f, 0.f} : f3(desc->sky_up);
+    F3 fwd = black3(desc->sky_fwd) ? F3{1.f, 0.f, 0.f} : f3(desc->sky_fwd);
+    // EnvironmentLight constructor (environment_light.cpp:6-31)
+    F3 upn = nrm(up);
+    F3 tt = nrm(crs(up, fwd));
+    F3 ss = crs(upn, tt);
+    std::vector<float> values(size_t(w) * h);
+    double vs[3] = {0, 0, 0};
+    float vsum[3] = {0.f, 0.f, 0.f};
+    float vweight = 0.f;
+    (void)vs;
+    for(uint32_t y = 0; y < h; ++y) {
+      float theta = (float(y) + 0.5f) / float(h) * 3.14159265358979323846f;
+      float ct = std::min(std::max(std::cos(theta), 0.f), 1.f);
+      for(uint32_t x = 0; x < w; ++x) {
+        const float* px = &hs.env_rgb[3 * (size_t(y) * w + x)];
+        values[size_t(y) * w + x] = std::fabs(avg3(px) * ct);
+        for(int a = 0; a < 3; ++a) { vsum[a] += px[a] * ct; }
+        vweight += ct;
+      }
+    }
+    // PiecewiseDistrib2d (piecewise_distrib_2d.cpp:4-35)
+    hs.env_pdfs.assign(size_t(w) * h, 0.f);
+    hs.env_marginal.assign(h + 1, 0.f);
+    hs.env_cond.assign(size_t(w + 1) * h, 0.f);
+    float sum = 0.f;
+    for(uint32_t y = 0; y < h; ++y) {
+      float ysum = 0.f;
+      hs.env_cond[size_t(w + 1) * y] = 0.f;
+      for(uint32_t x = 0; x < w; ++x) {
+        ysum += values[size_t(y) * w + x];
+        hs.env_cond[size_t(w + 1) * y + x + 1] = ysum;
+      }
+      float inv = 1.f / ysum;
+      for(uint32_t x = 0; x <= w; ++x) { hs.env_cond[size_t(w + 1) * y + x] *= inv; }
+      sum += ysum;
+      hs.env_marginal[y + 1] = sum;
+    }
+    float inv_sum = 1.f / sum;
+    for(uint32_t y = 0; y <= h; ++y) { hs.env_marginal[y] *= inv_sum; }
+    for(size_t i = 0; i < values.size(); ++i) { hs.env_pdfs[i] = values[i] * inv_sum; }
+    hs.env.w = w;
+    hs.env.h = h;
+    for(int a = 0; a < 3; ++a) { hs.env.scale[a] = scale[a]; }
+    hs.env.up[0] = upn.x; hs.env.up[1] = upn.y; hs.env.up[2] = upn.z;
+    hs.env.s[0] = ss.x; hs.env.s[1] = ss.y; hs.env.s[2] = ss.z;
+    hs.env.t[0] = tt.x; hs.env.t[1] = tt.y; hs.env.t[2] = tt.z;
+    DevLight l;
+    std::memset(&l, 0, sizeof(l));
+    l.kind = LIGHT_ENV;
+    float ar[3];
+    for(int a = 0; a < 3; ++a) { ar[a] = scale[a] * vsum[a] / vweight; }
+    float pw[3] = {r2pi * ar[0], r2pi * ar[1], r2pi * ar[2]};
+    powers.push_back(avg3(pw));
+    hs.lights.push_back(l);
+    hs.bg_light[hs.bg_count++] = uint32_t(hs.lights.size() - 1);
+  }
+  hs.light_cdf = make_cdf(powers);
+  return true;
+}
+
+PtScene host_view(const HostScene& hs) {
+  PtScene sc;
+  std::memset(&sc, 0, sizeof(sc));
+  sc.trace.nodes = reinterpret_cast<const uint4*>(hs.bvh.nodes.data());
+  sc.trace.tris = reinterpret_cast<const float4*>(hs.bvh.tris.data());
+  sc.trace.node_count = uint32_t(hs.bvh.nodes.size());
+  sc.trace.tri_count = uint32_t(hs.bvh.tris.size());
+  sc.shade = hs.shade.data();
+  sc.mats = hs.mats.data();
+  sc.mat_count = uint32_t(hs.mats.size());
+  sc.lights = hs.lights.data();
+  sc.light_count = uint32_t(hs.lights.size());
+  sc.light_cdf = hs.light_cdf.data();
+  sc.bg_count = hs.bg_count;
+  sc.bg_light[0] = hs.bg_light[0];
+  sc.bg_light[1] = hs.bg_light[1];
+  sc.env = hs.env;
+  sc.env.rgb = hs.env_rgb.empty() ? nullptr : hs.env_rgb.data();
+  sc.env.marginal_cdf = hs.env_marginal.empty() ? nullptr : hs.env_marginal.data();
+  sc.env.cond_cdf = hs.env_cond.empty() ? nullptr : hs.env_cond.data();
+  sc.env.pdfs = hs.env_pdfs.empty() ? nullptr : hs.env_pdfs.data();
+  return sc;
+}
+
+}  // namespace dort_gpu

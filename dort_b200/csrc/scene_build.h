@@ -1,0 +1,33 @@
+// Host-side assembly of a renderable scene from a dort_scene_desc: the wide
+// BVH plus the shading tables the path tracer reads.  The same host arrays are
+// uploaded for the device and used directly by the host checks.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "bvh_build.h"
+#include "pt_scene.h"
+
+namespace dort_gpu {
+
+struct HostScene {
+  WideBvh bvh;
+  std::vector<float4> shade;         // 3 per triangle
+  std::vector<DevMaterial> mats;
+  std::vector<DevLight> lights;
+  std::vector<float> light_cdf;
+  uint32_t bg_count = 0;
+  uint32_t bg_light[2] = {0, 0};
+  std::vector<float> env_rgb, env_marginal, env_cond, env_pdfs;
+  DevEnv env{};
+  uint32_t emissive_count = 0;
+  float radius = 0.f;
+};
+
+// Validates the description and builds everything; false + message on error.
+bool build_host_scene(const dort_scene_desc* desc, HostScene& out, std::string& err);
+
+// Device-view structures pointing at the host arrays (host checks only).
+PtScene host_view(const HostScene& hs);
+
+}  // namespace dort_gpu

@@ -159,3 +159,214 @@ def raycast_workload(n_tris: int, n_rays: int, seed_tris: int = 1,
     diffuse = diffuse_rays(verts, tris, n_rays - len(coherent), cast, seed_rays)
     rays = np.ascontiguousarray(np.concatenate([coherent, diffuse]))
     return verts, tris, rays
+
+
+# ---- cameras -----------------------------------------------------------------
+
+def look_at_camera(eye, look, up, fov: float, flip_y: bool = True):
+    """Pinhole camera as dort.camera.make_pinhole with transform
+    look_at(eye, look, up) * scale(1, -1, 1) (transform.cpp:146-162): returns
+    {"origin", "right", "up", "forward", "fov"} with the columns of the
+    camera-to-world matrix (the y column already flipped)."""
+    f32 = np.float32
+    eye = np.asarray(eye, f32)
+    d = np.asarray(look, f32) - eye
+    d = d / np.linalg.norm(d)
+    upn = np.asarray(up, f32) / np.linalg.norm(np.asarray(up, f32))
+    right = np.cross(upn, d)
+    right = right / np.linalg.norm(right)
+    upv = np.cross(d, right)
+    if flip_y:
+        upv = -upv
+    return {"origin": eye.astype(f32), "right": right.astype(f32), "up": upv.astype(f32),
+            "forward": d.astype(f32), "fov": float(fov)}
+
+
+def camera_rays(cam, width: int, height: int):
+    """Pixel-centre rays of PinholeCamera::sample_ray_importance
+    (pinhole_camera.cpp:13-31), t in [0, inf)."""
+    f32 = np.float32
+    proj = f32(2.0) * f32(np.tan(0.5 * cam["fov"]))
+    xs = (np.arange(width, dtype=f32) + f32(0.5)) / f32(width) - f32(0.5)
+    ys = (np.arange(height, dtype=f32) + f32(0.5)) / f32(height) - f32(0.5)
+    X, Y = np.meshgrid(xs, ys)
+    if width > height:
+        Y = Y * f32(height) / f32(width)
+    else:
+        X = X * f32(width) / f32(height)
+    px, py = X * proj, Y * proj
+    d = (px[..., None] * cam["right"] + py[..., None] * cam["up"] + cam["forward"]).astype(f32)
+    d = d / np.linalg.norm(d, axis=-1, keepdims=True)
+    rays = np.zeros((height, width, 8), f32)
+    rays[..., 0:3] = cam["origin"]
+    rays[..., 4:7] = d
+    rays[..., 7] = np.inf
+    return rays.reshape(-1, 8)
+
+
+# ---- Cornell box ---------------------------------------------------------------
+
+def _cube_tris():
+    """Unit cube [-1, 1]^3 (cube_shape.cpp) as 12 triangles, normals
+    cross(e2, e1) pointing outward."""
+    c = np.array([[x, y, z] for x in (-1, 1) for y in (-1, 1) for z in (-1, 1)], np.float64)
+    faces = []
+    for a in range(3):
+        for s in (-1, 1):
+            idx = [i for i in range(8) if c[i, a] == s]
+            # order the 4 corners around the face
+            b, cc = [k for k in range(3) if k != a]
+            ang = np.arctan2(c[idx, cc], c[idx, b])
+            idx = [idx[k] for k in np.argsort(ang)]
+            for tri in ((idx[0], idx[1], idx[2]), (idx[0], idx[2], idx[3])):
+                p0, p1, p2 = c[list(tri)]
+                n = np.cross(p2 - p0, p1 - p0)
+                if np.dot(n, p0) < 0:
+                    tri = (tri[0], tri[2], tri[1])
+                faces.append(tri)
+    return c, np.array(faces, np.uint32)
+
+
+def _rot_y(angle):
+    # rotate_y (transform.cpp:105-115)
+    cs, sn = np.cos(angle), np.sin(angle)
+    return np.array([[cs, 0.0, sn], [0.0, 1.0, 0.0], [-sn, 0.0, cs]])
+
+
+def cornell_box(white=(0.75, 0.75, 0.75), red=(0.63, 0.06, 0.05),
+                green=(0.14, 0.45, 0.09), light_radiance=(17.0, 12.0, 4.0),
+                light_size=0.5):
+    """The Cornell box of the reference's test scenes (test/test_box.lua:40-105,
+    scale s = 0.01): 10 wall triangles, two rotated boxes (12 triangles each)
+    and a light_size^2 quad light (2 emissive triangles) just below the
+    ceiling.  Materials: 0 white, 1 red, 2 green, 3 black (light)."""
+    s = 0.01
+    P = np.array([[552.8, 0, 0], [0, 0, 0], [0, 0, 559.2], [549.6, 0, 559.2],
+                  [556, 548.8, 0], [556, 548.8, 559.2], [0, 548.8, 559.2], [0, 548.8, 0]],
+                 np.float64) * s
+    V = [0, 1, 2, 0, 2, 3, 4, 5, 6, 4, 6, 7, 6, 5, 3, 6, 3, 2, 7, 6, 2, 7, 2, 1,
+         0, 3, 5, 0, 5, 4]
+    verts = [P]
+    tris = [np.array(V, np.uint32).reshape(-1, 3)]
+    # floor, ceiling, back wall: white; left wall (x = 0): green; right: red
+    mats = [0, 0, 0, 0, 0, 0, 2, 2, 1, 1]
+    cube_v, cube_t = _cube_tris()
+    for trans, ang, scl in (((185, 82.5, 169), -0.29, (165 / 2, 165 / 2, 165 / 2)),
+                            ((368, 165, 351), -1.27, (165 / 2, 330 / 2, 165 / 2))):
+        v = (cube_v * (np.array(scl) * s)) @ _rot_y(ang).T + np.array(trans) * s
+        tris.append(cube_t + sum(len(x) for x in verts))
+        verts.append(v)
+        mats += [0] * 12
+    cx, cz, y = 278 * s, 279.5 * s, 548.8 * s - 1 * s
+    h = light_size / 2
+    L = np.array([[cx + h, y, cz - h], [cx + h, y, cz + h], [cx - h, y, cz + h],
+                  [cx - h, y, cz - h]])
+    base = sum(len(x) for x in verts)
+    verts.append(L)
+    tris.append(np.array([[2, 1, 0], [3, 2, 0]], np.uint32) + base)
+    mats += [3, 3]
+    verts = np.concatenate(verts).astype(np.float32)
+    tris = np.concatenate(tris).astype(np.uint32)
+    emission = np.zeros((len(tris), 3), np.float32)
+    emission[-2:] = light_radiance
+    materials = [
+        {"kind": 0, "color": white}, {"kind": 0, "color": red},
+        {"kind": 0, "color": green}, {"kind": 0, "color": (0.0, 0.0, 0.0)},
+    ]
+    cam = look_at_camera((278 * s, 273 * s, -800 * s), (278 * s, 273 * s, 0.0),
+                         (0.0, 1.0, 0.0), 0.686)
+    return {"verts": verts, "tris": tris, "tri_material": np.array(mats, np.uint32),
+            "materials": materials, "tri_emission": emission, "camera": cam}
+
+
+def cornell_variant(kind: str = "diff", light: str = "area"):
+    """Cornell box variants after the reference's test scenes
+    (test/test_box.lua:110-140): "diff" all Lambert, "glos" Phong boxes and
+    right wall, "delt" mirror right box + glass left box + mirror left wall;
+    light "area" (quad light), "infi" (constant sky, open box) or "both"."""
+    c = cornell_box()
+    mats = c["materials"]
+    if kind == "glos":
+        # phong_material { albedo = a, exponent = 50 }: glossy albedo
+        # defaults to the diffuse one (lua_material.cpp:166-176)
+        mats.append({"kind": 3, "color": (0.5, 0.5, 0.5), "color2": (0.5, 0.5, 0.5),
+                     "param": (50.0,)})
+        mats.append({"kind": 3, "color": (0.5, 0.0, 0.0), "color2": (0.5, 0.0, 0.0),
+                     "param": (50.0,)})
+        tm = c["tri_material"]
+        tm[10:34] = len(mats) - 2          # both boxes glossy white
+        tm[8:10] = len(mats) - 1           # right wall glossy red
+    elif kind == "delt":
+        mats.append({"kind": 1, "color": (1.0, 1.0, 1.0)})
+        mats.append({"kind": 2, "color": (1.0, 1.0, 1.0), "color2": (1.0, 1.0, 1.0),
+                     "param": (1.3,)})
+        tm = c["tri_material"]
+        tm[22:34] = len(mats) - 2          # right box mirror
+        tm[10:22] = len(mats) - 1          # left box glass
+        tm[6:8] = len(mats) - 2            # left wall mirror
+    if light in ("infi", "both"):
+        c["sky_const"] = (1.0, 1.0, 1.0)
+    if light == "infi":
+        c["tri_emission"] = np.zeros_like(c["tri_emission"])
+        # open box: drop the back wall so the sky is visible
+        keep = np.ones(len(c["tris"]), bool)
+        keep[4:6] = False
+        c["tris"] = c["tris"][keep]
+        c["tri_material"] = c["tri_material"][keep]
+        c["tri_emission"] = c["tri_emission"][keep]
+    return c
+
+
+def procedural_sky(width: int = 256, height: int = 128, seed: int = 3):
+    """Latitude-longitude HDR sky (row 0 = zenith): a vertical gradient plus a
+    sun lobe; float32 [height, width, 3]."""
+    v = (np.arange(height, dtype=np.float64) + 0.5) / height          # theta / pi
+    u = (np.arange(width, dtype=np.float64) + 0.5) / width
+    theta = v * np.pi
+    phi = (u - 0.5) * 2.0 * np.pi
+    T, P = np.meshgrid(theta, phi, indexing="ij")
+    up = np.cos(T)
+    sky = np.stack([0.35 + 0.5 * np.clip(up, 0, 1), 0.45 + 0.55 * np.clip(up, 0, 1),
+                    0.7 + 0.6 * np.clip(up, 0, 1)], -1)
+    ground = np.array([0.25, 0.22, 0.2])
+    sky = np.where(up[..., None] < 0.0, ground, sky)
+    rng = np.random.default_rng(seed)
+    sun_t, sun_p = 0.3 + 0.1 * rng.random(), (rng.random() - 0.5) * np.pi
+    d = np.stack([np.sin(T) * np.cos(P), np.cos(T), np.sin(T) * np.sin(P)], -1)
+    s = np.array([np.sin(sun_t) * np.cos(sun_p), np.cos(sun_t), np.sin(sun_t) * np.sin(sun_p)])
+    cosang = d @ s
+    sun = 40.0 * np.exp((cosang - 1.0) * 400.0)
+    sky = sky + sun[..., None] * np.array([1.0, 0.9, 0.7])
+    return sky.astype(np.float32)
+
+
+def env_test_scene(seed: int = 11, conductor: bool = False):
+    """A small scene lit only by the procedural sky: a ground quad and a few
+    random boxes of Lambert / mirror / glass / Phong (/ GGX conductor, which
+    has no reference counterpart, when ``conductor``)."""
+    rng = np.random.default_rng(seed)
+    verts = [np.array([[-3, 0, -3], [3, 0, -3], [3, 0, 3], [-3, 0, 3]], np.float64)]
+    tris = [np.array([[0, 2, 1], [0, 3, 2]], np.uint32)]
+    mats = [0, 0]
+    cube_v, cube_t = _cube_tris()
+    for k in range(6):
+        sc = 0.25 + 0.3 * rng.random(3)
+        pos = np.array([rng.uniform(-1.8, 1.8), sc[1], rng.uniform(-1.8, 1.8)])
+        v = (cube_v * sc) @ _rot_y(rng.uniform(0, 3)).T + pos
+        tris.append(cube_t + sum(len(x) for x in verts))
+        verts.append(v)
+        mats += [1 + k % 5] * 12
+    materials = [
+        {"kind": 0, "color": (0.6, 0.6, 0.6)},
+        {"kind": 0, "color": (0.7, 0.3, 0.2)},
+        {"kind": 1, "color": (0.9, 0.9, 0.9)},
+        {"kind": 2, "color": (1.0, 1.0, 1.0), "color2": (1.0, 1.0, 1.0), "param": (1.5,)},
+        {"kind": 3, "color": (0.3, 0.3, 0.5), "color2": (0.4, 0.4, 0.4), "param": (30.0,)},
+        {"kind": 4, "color": (0.9, 0.7, 0.4), "param": (0.2,)} if conductor
+        else {"kind": 0, "color": (0.2, 0.5, 0.3)},
+    ]
+    cam = look_at_camera((0.0, 2.5, -6.0), (0.0, 0.5, 0.0), (0.0, 1.0, 0.0), 0.9)
+    return {"verts": np.concatenate(verts).astype(np.float32),
+            "tris": np.concatenate(tris).astype(np.uint32),
+            "tri_material": np.array(mats, np.uint32), "materials": materials,
+            "tri_emission": None, "sky_rgb": procedural_sky(), "camera": cam}

@@ -98,11 +98,13 @@ typedef struct dort_material {
  *                 non-black emission is one one-sided diffuse area light, as
  *                 DiffuseLight on a triangle shape (diffuse_light.cpp:40-111),
  *                 emitting to the side of cross(e2, e1) (triangle.cpp:73)
- *   sky_*         background light: sky_width = sky_height = 0 and a
- *                 non-black sky_const[] gives the constant InfiniteLight
- *                 (infinite_light.cpp:5-65); a sky image (sky_width x
- *                 sky_height RGB float, latitude-longitude) gives the
- *                 EnvironmentLight (environment_light.cpp:6-158)
+ *   sky_*         background lights: a non-black sky_const[] gives the
+ *                 constant InfiniteLight (infinite_light.cpp:5-65); a sky
+ *                 image (sky_width x sky_height RGB float, latitude-longitude,
+ *                 row 0 = zenith) gives the EnvironmentLight
+ *                 (environment_light.cpp:6-158) with radiance scale
+ *                 sky_scale (0,0,0 = 1,1,1), up and forward vectors sky_up /
+ *                 sky_fwd (0 = +y / +x)
  *   bvh_width     children per BVH node, 2..8 (0: 8)
  */
 typedef struct dort_scene_desc {
@@ -119,7 +121,9 @@ typedef struct dort_scene_desc {
   uint32_t sky_width;
   uint32_t sky_height;
   float sky_const[3];
-  float sky_to_world[9];           /* row-major rotation of the sky (identity if all 0) */
+  float sky_scale[3];
+  float sky_up[3];
+  float sky_fwd[3];
   uint32_t bvh_width;
   uint32_t reserved[7];
 } dort_scene_desc;
@@ -168,6 +172,53 @@ int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
                            float* d_tb, void* stream, int repeat,
                            float* out_ms_per_launch);
 
+/* ---- rendering ------------------------------------------------------------
+ * The "pt" renderer: PathRenderer (path_renderer.cpp:11-206) behind
+ * Renderer::render (renderer.hpp:27), with the parameters of
+ * dort.render.make (lua_render.cpp:102-145).  The film uses the default box
+ * filter of radius 0.5 (each sample lands in its own pixel); non-finite or
+ * negative samples are dropped as Renderer::iteration_tiled does
+ * (renderer.cpp:36-41); a pixel is sum(L) / count of its kept samples
+ * (Film::to_image, film.cpp:90-108).  Iteration 0 samples pixel centres,
+ * later iterations jitter uniformly (path_renderer.cpp:15-20).
+ *
+ * Camera: PinholeCamera (pinhole_camera.cpp:13-31) with the columns of its
+ * camera-to-world transform (origin, and the images of the camera x, y, z
+ * axes) and the field of view in radians. */
+typedef struct dort_camera {
+  float origin[3];
+  float right[3];
+  float up[3];
+  float forward[3];
+  float fov;
+} dort_camera;
+
+enum dort_direct_strategy { DORT_DIRECT_MIS = 0, DORT_DIRECT_BSDF = 1, DORT_DIRECT_LIGHT = 2 };
+
+typedef struct dort_render_params {
+  uint32_t struct_size;        /* sizeof(dort_render_params) */
+  uint32_t width, height;      /* x_res, y_res */
+  uint32_t iterations;         /* samples per pixel */
+  uint32_t min_depth, max_depth;
+  uint32_t only_direct;
+  uint32_t sample_all_lights;
+  uint32_t direct_strategy;    /* dort_direct_strategy */
+  uint32_t pad0;
+  uint64_t seed;
+  dort_camera camera;
+  uint32_t reserved[8];
+} dort_render_params;
+
+/* Renders into out_rgb (host, width * height * 3 floats, row-major, row 0 at
+ * the top).  out_stats (optional, 4 doubles): rays traced, samples kept,
+ * kernel milliseconds, samples dropped. */
+int dort_gpu_render(dort_scene* scene, const dort_render_params* params,
+                    float* out_rgb, double* out_stats);
+
+/* Device-pointer form on a caller stream; d_out_rgb is device memory. */
+int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
+                           float* d_out_rgb, void* stream);
+
 /* ---- diagnostics ----------------------------------------------------------
  * No reference counterpart.  Builds the device scene's wide BVH on the host
  * and runs the device traversal code compiled for the CPU, with the same
@@ -177,6 +228,12 @@ int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
 int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const float* rays,
                                 size_t ray_count, int any_hit, uint32_t* out_prim,
                                 float* out_tb, uint32_t* out_depth);
+
+/* No reference counterpart.  Runs the device path-sampling code compiled for
+ * the CPU over the pixels [row_begin, row_end) of the image (small images
+ * only); writes those rows of out_rgb.  For checking without a GPU. */
+int dort_gpu_host_check_render(const dort_scene_desc* desc, const dort_render_params* params,
+                               uint32_t row_begin, uint32_t row_end, float* out_rgb);
 
 #ifdef __cplusplus
 }

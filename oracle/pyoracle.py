@@ -179,3 +179,62 @@ class RefBvh:
         if counts:
             return prim, tb, tests
         return prim, tb
+
+
+def pack_materials(materials) -> np.ndarray:
+    """Material dicts -> rows of 11 floats (kind, color[3], color2[3], param[4])."""
+    rows = []
+    for m in materials:
+        p = list(m.get("param", ())) + [0.0] * 4
+        rows.append([float(m.get("kind", 0)), *m.get("color", (0, 0, 0)),
+                     *m.get("color2", (0, 0, 0)), *p[:4]])
+    return np.ascontiguousarray(np.array(rows, np.float32).reshape(-1, 11))
+
+
+def pack_camera(cam) -> np.ndarray:
+    return np.ascontiguousarray(np.concatenate(
+        [cam["origin"], cam["right"], cam["up"], cam["forward"]]).astype(np.float32))
+
+
+def ref_pt_render(scene: dict, width: int, height: int, iterations: int,
+                  min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
+                  sample_all_lights: bool = False, strategy: str = "mis", seed: int = 42,
+                  split: str = "middle", threads: int | None = None):
+    """Renders with the reference's own PathRenderer (dort.render.make with
+    renderer = "pt"); returns (image [h, w, 3] f32, seconds)."""
+    R = ref()
+    if not hasattr(R, "_pt_ready"):
+        R.dref_pt_render.restype = _i32
+        R.dref_pt_render.argtypes = [_P, _u32, _P, _u32, _P, _P, _u32, _P, _P, _P, _u32,
+                                     _u32, _P, _P, ctypes.c_float, _u32, _u32, _u32, _u32,
+                                     _u32, _i32, _i32, _i32, _u32, _i32, _u32, _P, _P]
+        R._pt_ready = True
+    v = np.ascontiguousarray(scene["verts"], np.float32)
+    t = np.ascontiguousarray(scene["tris"], np.uint32)
+    tm = np.ascontiguousarray(scene.get("tri_material", np.zeros(len(t), np.uint32)), np.uint32)
+    mats = pack_materials(scene["materials"])
+    em = scene.get("tri_emission")
+    em = None if em is None else np.ascontiguousarray(em, np.float32)
+    bg = scene.get("sky_const")
+    bg = None if bg is None else np.ascontiguousarray(bg, np.float32)
+    env = scene.get("sky_rgb")
+    env_frame = None
+    ew = eh = 0
+    if env is not None:
+        env = np.ascontiguousarray(env, np.float32)
+        eh, ew = env.shape[0], env.shape[1]
+        env_frame = np.ascontiguousarray(np.concatenate([
+            np.asarray(scene.get("sky_scale", (1, 1, 1)), np.float32),
+            np.asarray(scene.get("sky_up", (0, 1, 0)), np.float32),
+            np.asarray(scene.get("sky_fwd", (1, 0, 0)), np.float32)]))
+    cam = pack_camera(scene["camera"])
+    out = np.zeros((height, width, 3), np.float32)
+    secs = ctypes.c_double(0.0)
+    strat = {"mis": 0, "bsdf": 1, "light": 2}[strategy]
+    R.dref_pt_render(_ptr(v), len(v), _ptr(t), len(t), _ptr(tm), _ptr(mats), len(mats),
+                     _ptr(em), _ptr(bg), _ptr(env), ew, eh, _ptr(env_frame), _ptr(cam),
+                     ctypes.c_float(scene["camera"]["fov"]), width, height, iterations,
+                     min_depth, max_depth, int(only_direct), int(sample_all_lights), strat,
+                     seed, {"middle": 0, "sah": 1}[split], threads or os.cpu_count() or 1,
+                     _ptr(out), ctypes.byref(secs))
+    return out, secs.value
