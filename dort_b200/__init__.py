@@ -125,6 +125,22 @@ class Scene:
         _abi.check(_abi.lib().dort_gpu_render(self.handle, ctypes.byref(params), _ptr(out), st))
         return out, {"rays": st[0], "samples": st[1], "ms": st[2], "dropped": st[3]}
 
+    def render_wavefront(self, params: _abi.RenderParams, tuning: dict | None = None):
+        """dort_gpu_render_wavefront: returns (image, stats dict)."""
+        out = np.zeros((params.height, params.width, 3), np.float32)
+        st = (ctypes.c_double * 4)()
+        t = wavefront_tuning(**tuning) if tuning else None
+        _abi.check(_abi.lib().dort_gpu_render_wavefront(
+            self.handle, ctypes.byref(params), ctypes.byref(t) if t else None, _ptr(out), st))
+        return out, {"rays": st[0], "ms": st[2], "waves": st[3]}
+
+    def render_wavefront_device(self, params: _abi.RenderParams, d_out: int, stream: int = 0,
+                                tuning: dict | None = None):
+        t = wavefront_tuning(**tuning) if tuning else None
+        _abi.check(_abi.lib().dort_gpu_render_wavefront_device(
+            self.handle, ctypes.byref(params), ctypes.byref(t) if t else None,
+            ctypes.c_void_p(d_out), ctypes.c_void_p(stream)))
+
     def render_device(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
         _abi.check(_abi.lib().dort_gpu_render_device(self.handle, ctypes.byref(params),
                                                      ctypes.c_void_p(d_out),
@@ -159,6 +175,14 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     c.forward = (ctypes.c_float * 3)(*camera["forward"])
     c.fov = camera["fov"]
     return p
+
+
+def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
+                     shade_block: int = 0) -> _abi.WavefrontTuning:
+    t = _abi.WavefrontTuning()
+    t.struct_size = ctypes.sizeof(_abi.WavefrontTuning)
+    t.queue_capacity, t.trace_block, t.shade_block = queue_capacity, trace_block, shade_block
+    return t
 
 
 def scene_from_dict(d: dict, **kw) -> "Scene":

@@ -65,6 +65,11 @@ class RenderParams(ctypes.Structure):
     ]
 
 
+class WavefrontTuning(ctypes.Structure):
+    _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
+                ("shade_block", c_u32), ("reserved", c_u32 * 4)]
+
+
 class DortError(RuntimeError):
     """A C-ABI call returned a negative status."""
 
@@ -112,6 +117,13 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_host_check_render.argtypes = [ctypes.POINTER(SceneDesc),
                                                  ctypes.POINTER(RenderParams), c_u32, c_u32,
                                                  c_p]
+        L.dort_gpu_render_wavefront.restype = c_i32
+        L.dort_gpu_render_wavefront.argtypes = [c_p, ctypes.POINTER(RenderParams),
+                                                ctypes.POINTER(WavefrontTuning), c_p,
+                                                ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_render_wavefront_device.restype = c_i32
+        L.dort_gpu_render_wavefront_device.argtypes = [c_p, ctypes.POINTER(RenderParams),
+                                                       ctypes.POINTER(WavefrontTuning), c_p, c_p]
         _lib = L
     return _lib
 

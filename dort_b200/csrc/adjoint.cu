@@ -1,0 +1,295 @@
+// Adjoint of the path tracer: gradients of an image loss with respect to
+// per-triangle Lambert albedo and per-triangle emitted radiance, by path
+// replay backpropagation (Vicini, Speierer, Jakob, "Path Replay
+// Backpropagation", SIGGRAPH 2021).  No path vertex is stored: every sample
+// is traced twice from its counter-based random numbers,
+//   pass 1: the sample value L (as the forward render computes it);
+//   pass 2: the same path again, with an observer that keeps the sum A of
+//           the terms seen so far and attributes derivatives:
+//     - a Lambert vertex on triangle t: every later term of the sample is
+//       linear in that vertex's albedo, so dL/d(albedo_t) += (L - A) / albedo_t
+//       (per channel);
+//     - an emission term throughput * Le of light triangle t:
+//       dL/d(Le_t) += throughput;
+//     - a direct-lighting term c from light triangle t: dL/d(Le_t) += c / Le_t.
+// Sampling decisions (light choice, Russian roulette probabilities, MIS
+// weights) are held fixed, which keeps the gradient estimate unbiased.  The
+// image gradient dLoss/dI weights each sample by dLoss/dI(pixel) / spp, and
+// gradients are accumulated with float atomics.
+//
+// No reference counterpart: the reference renderer has no derivatives.
+#include <cstring>
+#include <string>
+
+#include "common.h"
+#include "pt.cuh"
+#include "scene_build.h"
+
+namespace dort_gpu {
+
+bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err);
+int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
+                  unsigned long long* d_counters);
+
+// The observer only runs on the device (atomics); its host instantiation of
+// the shared path code is never called.
+#ifdef __CUDA_ARCH__
+#define ADJ_ADD(p, v) atomicAdd((p), (v))
+#else
+#define ADJ_ADD(p, v) (*(p) += (v))
+#endif
+
+struct AdjointTape {
+  V3 L;          // sample value from pass 1
+  V3 acc;        // terms seen so far
+  V3 adj;        // dLoss/dI(pixel) / spp
+  float* d_albedo;
+  float* d_emission;
+  const float* tri_emission;
+
+  DG_HD void emission(uint32_t tri, V3 thr, V3 Le) {
+    acc = acc + thr * Le;
+    if(d_emission && !is_black(Le)) {
+      float* g = d_emission + 3 * size_t(tri);
+      ADJ_ADD(g, adj.x * thr.x);
+      ADJ_ADD(g + 1, adj.y * thr.y);
+      ADJ_ADD(g + 2, adj.z * thr.z);
+    }
+  }
+  DG_HD void background(V3 c) { acc = acc + c; }
+  DG_HD void vertex(uint32_t tri, const DevMaterial& m) {
+    if(!d_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags) { return; }
+    V3 rem = L - acc;
+    float* g = d_albedo + 3 * size_t(tri);
+    if(m.c[0] > 0.f) { ADJ_ADD(g, adj.x * rem.x / m.c[0]); }
+    if(m.c[1] > 0.f) { ADJ_ADD(g + 1, adj.y * rem.y / m.c[1]); }
+    if(m.c[2] > 0.f) { ADJ_ADD(g + 2, adj.z * rem.z / m.c[2]); }
+  }
+  DG_HD void direct(uint32_t light_tri, V3 c) {
+    acc = acc + c;
+    if(d_emission && light_tri != kMiss) {
+      const float* le = tri_emission + 3 * size_t(light_tri);
+      float* g = d_emission + 3 * size_t(light_tri);
+      if(le[0] > 0.f) { ADJ_ADD(g, adj.x * c.x / le[0]); }
+      if(le[1] > 0.f) { ADJ_ADD(g + 1, adj.y * c.y / le[1]); }
+      if(le[2] > 0.f) { ADJ_ADD(g + 2, adj.z * c.z / le[2]); }
+    }
+  }
+};
+
+constexpr int kAdjBlock = 128;
+
+__global__ void __launch_bounds__(kAdjBlock)
+adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
+               uint32_t per_slice, const float* __restrict__ dl_dimage,
+               float* __restrict__ d_albedo, float* __restrict__ d_emission) {
+  const uint64_t tid = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if(tid >= uint64_t(per_slice) * slices) { return; }
+  uint32_t slice = uint32_t(tid / per_slice);
+  uint32_t local = uint32_t(tid % per_slice);
+  uint32_t tiles_x = (pp.width + 7) / 8;
+  uint32_t tile = local / 32, lane = local % 32;
+  uint32_t x = (tile % tiles_x) * 8 + lane % 8, y = (tile / tiles_x) * 4 + lane / 8;
+  if(x >= pp.width || y >= pp.height) { return; }
+  uint32_t pixel = y * pp.width + x;
+  float inv_spp = 1.f / float(pp.spp);
+  V3 adj = v3(dl_dimage[3 * size_t(pixel)], dl_dimage[3 * size_t(pixel) + 1],
+              dl_dimage[3 * size_t(pixel) + 2]) * inv_spp;
+  if(is_black(adj)) { return; }
+  uint32_t s0 = slice * spp_per_slice;
+  uint32_t s1 = min(pp.spp, s0 + spp_per_slice);
+  for(uint32_t s = s0; s < s1; ++s) {
+    float fx, fy;
+    if(s == 0) {
+      fx = float(x) + 0.5f;
+      fy = float(y) + 0.5f;
+    } else {
+      Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
+      fx = float(x) + j.a;
+      fy = float(y) + j.b;
+    }
+    NoTape none;
+    PathResult r1 = pt_sample(sc, pp, pixel, s, fx, fy, none);
+    V3 L = r1.L;
+    // samples the film drops have no gradient (renderer.cpp:36-41)
+    if(!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) || L.x < 0.f || L.y < 0.f ||
+       L.z < 0.f) {
+      continue;
+    }
+    AdjointTape tape;
+    tape.L = L;
+    tape.acc = v3(0.f, 0.f, 0.f);
+    tape.adj = adj;
+    tape.d_albedo = d_albedo;
+    tape.d_emission = d_emission;
+    tape.tri_emission = sc.tri_emission;
+    pt_sample(sc, pp, pixel, s, fx, fy, tape);
+  }
+}
+
+__global__ void l2_loss_grad(const float* __restrict__ img, const float* __restrict__ target,
+                             uint32_t n, float* __restrict__ grad, double* __restrict__ loss) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  double l = 0.0;
+  if(i < n) {
+    float d = img[i] - target[i];
+    grad[i] = 2.f * d;
+    l = double(d) * double(d);
+  }
+  for(int o = 16; o > 0; o >>= 1) { l += __shfl_down_sync(0xffffffffu, l, o); }
+  if((threadIdx.x & 31) == 0 && l != 0.0) { atomicAdd(loss, l); }
+}
+
+// Per-triangle parameter overrides held by the scene: one device buffer each,
+// allocated on first use and overwritten by later calls; NULL clears.
+static int set_tri_params(dort_scene* s, const float* albedo, const float* emission) {
+  size_t n = size_t(s->tri_count) * 3;
+  size_t bytes = n * sizeof(float);
+  for(size_t i = 0; albedo && i < n; ++i) {
+    if(!std::isfinite(albedo[i]) || albedo[i] < 0.f) {
+      return fail(DORT_ERR_INVALID, "tri_albedo must be finite and non-negative");
+    }
+  }
+  for(size_t i = 0; emission && i < n; ++i) {
+    if(!std::isfinite(emission[i]) || emission[i] < 0.f) {
+      return fail(DORT_ERR_INVALID, "tri_emission must be finite and non-negative");
+    }
+  }
+  auto put = [&](const float* src, float** buf, const float** view) -> int {
+    if(!src) { *view = nullptr; return DORT_OK; }
+    if(!*buf) {
+      void* d = nullptr;
+      if(cudaMalloc(&d, bytes ? bytes : 4) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DORT_ERR_OOM, "cudaMalloc of triangle parameters failed");
+      }
+      s->allocations.push_back(d);
+      s->device_bytes += bytes;
+      *buf = static_cast<float*>(d);
+    }
+    DG_CUDA(cudaMemcpy(*buf, src, bytes, cudaMemcpyHostToDevice));
+    *view = *buf;
+    return DORT_OK;
+  };
+  int rc = put(albedo, &s->d_tri_albedo, &s->pt.tri_albedo);
+  if(rc != DORT_OK) { return rc; }
+  return put(emission, &s->d_tri_emission, &s->pt.tri_emission);
+}
+
+}  // namespace dort_gpu
+
+using namespace dort_gpu;
+
+extern "C" int dort_gpu_adjoint_forward(dort_scene* scene, const dort_render_params* params,
+                                        const float* tri_albedo, const float* tri_emission,
+                                        float* out_image) {
+  clear_error();
+  if(!scene || !params || !out_image) { return fail(DORT_ERR_INVALID, "null argument"); }
+  int rc = set_tri_params(scene, tri_albedo, tri_emission);
+  if(rc != DORT_OK) { return rc; }
+  return dort_gpu_render(scene, params, out_image, nullptr);
+}
+
+extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_params* params,
+                                         const float* tri_albedo, const float* tri_emission,
+                                         const float* dl_dimage, float* d_albedo,
+                                         float* d_emission) {
+  clear_error();
+  if(!scene || !params || !dl_dimage || (!d_albedo && !d_emission)) {
+    return fail(DORT_ERR_INVALID, "null argument");
+  }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  int rc = set_tri_params(scene, tri_albedo, tri_emission);
+  if(rc != DORT_OK) { return rc; }
+  if(d_emission && !scene->pt.tri_emission) {
+    return fail(DORT_ERR_INVALID, "emission gradients need tri_emission");
+  }
+  size_t npix = size_t(pp.width) * pp.height;
+  size_t tbytes = size_t(scene->tri_count) * 3 * sizeof(float);
+  float *d_img = nullptr, *d_ga = nullptr, *d_ge = nullptr;
+  auto cleanup = [&]() {
+    if(d_img) { cudaFree(d_img); }
+    if(d_ga) { cudaFree(d_ga); }
+    if(d_ge) { cudaFree(d_ge); }
+  };
+  if(cudaMalloc(&d_img, npix * 3 * sizeof(float)) != cudaSuccess ||
+     (d_albedo && cudaMalloc(&d_ga, tbytes ? tbytes : 4) != cudaSuccess) ||
+     (d_emission && cudaMalloc(&d_ge, tbytes ? tbytes : 4) != cudaSuccess)) {
+    cudaGetLastError();
+    cleanup();
+    return fail(DORT_ERR_OOM, "cudaMalloc for the adjoint failed");
+  }
+  cudaStream_t st = 0;
+  bool ok = cudaMemcpyAsync(d_img, dl_dimage, npix * 3 * sizeof(float),
+                            cudaMemcpyHostToDevice, st) == cudaSuccess;
+  if(d_ga) { ok = ok && cudaMemsetAsync(d_ga, 0, tbytes, st) == cudaSuccess; }
+  if(d_ge) { ok = ok && cudaMemsetAsync(d_ge, 0, tbytes, st) == cudaSuccess; }
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  uint64_t target = uint64_t(sms) * 1024 * 4;
+  uint32_t slices = uint32_t(std::min<uint64_t>(pp.spp, std::max<uint64_t>(1, target / npix)));
+  uint32_t per = (pp.spp + slices - 1) / slices;
+  slices = (pp.spp + per - 1) / per;
+  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  uint32_t per_slice = tiles * 32;
+  uint64_t threads = uint64_t(slices) * per_slice;
+  if(ok) {
+    adjoint_replay<<<uint32_t((threads + kAdjBlock - 1) / kAdjBlock), kAdjBlock, 0, st>>>(
+        scene->pt, pp, slices, per, per_slice, d_img, d_ga, d_ge);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  if(ok && d_albedo) {
+    ok = cudaMemcpyAsync(d_albedo, d_ga, tbytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  }
+  if(ok && d_emission) {
+    ok = cudaMemcpyAsync(d_emission, d_ge, tbytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  }
+  ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+  cleanup();
+  if(!ok) {
+    return fail(DORT_ERR_CUDA, std::string("adjoint failed: ") +
+                               cudaGetErrorString(cudaGetLastError()));
+  }
+  return DORT_OK;
+}
+
+extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t count,
+                                double* out_loss, float* out_grad) {
+  clear_error();
+  if(!image || !target || !out_loss || !out_grad) {
+    return fail(DORT_ERR_INVALID, "null argument");
+  }
+  if(count > 0xffffffffull) { return fail(DORT_ERR_INVALID, "count exceeds 2^32 - 1"); }
+  float *d_a = nullptr, *d_b = nullptr, *d_g = nullptr;
+  double* d_l = nullptr;
+  size_t bytes = count * sizeof(float);
+  bool ok = cudaMalloc(&d_a, bytes ? bytes : 4) == cudaSuccess &&
+            cudaMalloc(&d_b, bytes ? bytes : 4) == cudaSuccess &&
+            cudaMalloc(&d_g, bytes ? bytes : 4) == cudaSuccess &&
+            cudaMalloc(&d_l, sizeof(double)) == cudaSuccess;
+  cudaStream_t st = 0;
+  ok = ok && cudaMemcpyAsync(d_a, image, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(d_b, target, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
+  ok = ok && cudaMemsetAsync(d_l, 0, sizeof(double), st) == cudaSuccess;
+  if(ok && count) {
+    l2_loss_grad<<<uint32_t((count + 255) / 256), 256, 0, st>>>(d_a, d_b, uint32_t(count), d_g,
+                                                                  d_l);
+    ok = cudaGetLastError() == cudaSuccess;
+  }
+  ok = ok && cudaMemcpyAsync(out_grad, d_g, bytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(out_loss, d_l, sizeof(double), cudaMemcpyDeviceToHost, st) ==
+                 cudaSuccess;
+  ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+  if(d_a) { cudaFree(d_a); }
+  if(d_b) { cudaFree(d_b); }
+  if(d_g) { cudaFree(d_g); }
+  if(d_l) { cudaFree(d_l); }
+  if(!ok) {
+    cudaGetLastError();
+    return fail(DORT_ERR_CUDA, "l2 loss failed");
+  }
+  return DORT_OK;
+}

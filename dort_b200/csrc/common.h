@@ -12,6 +12,8 @@
 
 namespace dort_gpu {
 
+struct Wavefront;
+
 // Thread-local message behind dort_gpu_last_error().
 void set_error(const std::string& msg);
 void clear_error();
@@ -39,6 +41,9 @@ struct dort_scene {
   size_t device_bytes = 0;
   double build_ms = 0.0;
   std::vector<void*> allocations;       // every device buffer owned by the scene
+  dort_gpu::Wavefront* wavefront = nullptr;  // wavefront queues + frame graph (lazy)
+  float* d_tri_albedo = nullptr;        // per-triangle overrides (adjoint), lazy
+  float* d_tri_emission = nullptr;
   uint32_t* d_work = nullptr;           // work counters of persistent kernels (scratch)
   // staging for the host-pointer entry points (grow-only)
   void* d_stage = nullptr;

@@ -580,12 +580,19 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
 
 // ---- the path ---------------------------------------------------------------------
 
-// Optional observer of path events, used by the adjoint to re-trace a path
-// and attribute derivatives; the forward renderer passes a no-op.
+// Observer of the terms a path adds to its sample value, in path order; the
+// adjoint replays a path with an observer that attributes derivatives, the
+// forward renderers pass this no-op.
+//   emission(light tri, throughput, Le)  adds throughput * Le
+//   background(c)                        adds c
+//   vertex(tri, material)                a scattering vertex starts; every
+//                                        later term is linear in its BSDF
+//   direct(light tri or kMiss, c)        adds c (a direct-lighting term)
 struct NoTape {
-  DG_HD void emission(uint32_t, V3, V3) {}            // (tri, throughput-weighted factor, Le)
-  DG_HD void scatter(uint32_t, V3) {}                 // (tri, factor by which albedo multiplied)
-  DG_HD void direct(uint32_t, uint32_t, V3) {}        // (tri of surface, light tri, contribution)
+  DG_HD void emission(uint32_t, V3, V3) {}
+  DG_HD void background(V3) {}
+  DG_HD void vertex(uint32_t, const DevMaterial&) {}
+  DG_HD void direct(uint32_t, V3) {}
 };
 
 struct PathResult {
@@ -606,11 +613,10 @@ DG_HD void camera_ray(const PtParams& pp, float fx, float fy, V3& o, V3& d) {
 }
 
 // Direct lighting from one light (estimate_direct, path_renderer.cpp:135-206).
-template<class Tape>
 DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& l,
                          const SurfaceHit& g, const DevMaterial& m, V3 wo,
                          float u_bsdf, float v_bsdf, float c_bsdf, float u_l, float v_l,
-                         uint32_t& rays, Tape& tape) {
+                         uint32_t& rays) {
   const uint32_t req = F_ALL & ~F_DELTA;
   bool use_bsdf = pp.strategy != 2;   // area and background lights only; no delta lights
   bool use_light = pp.strategy != 1;
@@ -641,9 +647,7 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
           float lp = light_pivot_pdf(sc, l, bs.w, g.p);
           w = bs.pdf / (bs.pdf + lp);
         }
-        V3 c = bs.f * L * (w * fabsf(dot(g.n, bs.w)) / bs.pdf);
-        tape.direct(g.tri, l.kind == LIGHT_TRI ? l.tri : kMiss, c);
-        sum = sum + c;
+        sum = sum + bs.f * L * (w * fabsf(dot(g.n, bs.w)) / bs.pdf);
       }
     }
   }
@@ -661,9 +665,7 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
             float bp = bsdf_pdf(m, g.frame, ls.wi, wo, req);
             w = ls.pdf / (ls.pdf + bp);
           }
-          V3 c = f * ls.L * (w * fabsf(dot(g.n, ls.wi)) / ls.pdf);
-          tape.direct(g.tri, l.kind == LIGHT_TRI ? l.tri : kMiss, c);
-          sum = sum + c;
+          sum = sum + f * ls.L * (w * fabsf(dot(g.n, ls.wi)) / ls.pdf);
         }
       }
     }
@@ -701,7 +703,9 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
         }
       } else {
         for(uint32_t k = 0; k < sc.bg_count; ++k) {
-          sum = sum + thr * background_radiance(sc, sc.lights[sc.bg_light[k]], d);
+          V3 c = thr * background_radiance(sc, sc.lights[sc.bg_light[k]], d);
+          tape.background(c);
+          sum = sum + c;
         }
       }
     }
@@ -715,27 +719,30 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
     Rand4 r1 = rand4(pp.seed, pixel, sample, blk + 1);
     Rand4 r2 = rand4(pp.seed, pixel, sample, blk + 2);
 
+    tape.vertex(g.tri, m);
     if(bounces >= pp.min_depth && bxdf_matches(m.bxdf_flags, req_nd)) {
       // sample_direct_lighting (path_renderer.cpp:113-132)
-      V3 direct = v3(0.f, 0.f, 0.f);
       if(pp.sample_all_lights) {
         for(uint32_t li = 0; li < sc.light_count; ++li) {
           uint32_t b2 = all_lights_block(bounces, li, sc.light_count);
           Rand4 a = rand4(pp.seed, pixel, sample, b2);
           Rand4 b = rand4(pp.seed, pixel, sample, b2 + 1);
-          direct = direct + estimate_direct(sc, pp, sc.lights[li], g, m, wo, a.a, a.b, a.c,
-                                            b.a, b.b, res.rays, tape);
+          const DevLight& l = sc.lights[li];
+          V3 c = estimate_direct(sc, pp, l, g, m, wo, a.a, a.b, a.c, b.a, b.b, res.rays) * thr;
+          tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
+          sum = sum + c;
         }
       } else if(sc.light_count > 0) {
         uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, r0.a);
         float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
         if(lpdf != 0.f) {
-          V3 e = estimate_direct(sc, pp, sc.lights[li], g, m, wo, r0.b, r0.c, r0.d, r1.a,
-                                 r1.b, res.rays, tape);
-          direct = e * (1.f / lpdf);
+          const DevLight& l = sc.lights[li];
+          V3 e = estimate_direct(sc, pp, l, g, m, wo, r0.b, r0.c, r0.d, r1.a, r1.b, res.rays);
+          V3 c = e * (1.f / lpdf) * thr;
+          tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
+          sum = sum + c;
         }
       }
-      sum = sum + direct * thr;
     }
 
     uint32_t req = (pp.only_direct || bounces == pp.max_depth) ? (F_MODES | F_DELTA) : F_ALL;
@@ -743,7 +750,6 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
     if(is_black(bs.f) || bs.pdf == 0.f) { break; }
     V3 contrib = bs.f * (fabsf(dot(bs.w, g.n)) / bs.pdf);
     last_delta = (bs.flags & F_DELTA) != 0;
-    tape.scatter(g.tri, contrib);
     thr = thr * contrib;
     if(bounces == pp.max_depth && !last_delta) {
       break;

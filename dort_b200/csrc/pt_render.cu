@@ -286,3 +286,105 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
   }
   return DORT_OK;
 }
+
+// ---- wavefront entry points -------------------------------------------------
+
+#include "wavefront.h"
+
+static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTuning& tn,
+                        std::string& err) {
+  uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  uint64_t total = tiles * 32 * pp.spp;
+  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 21));
+  tn.trace_block = 128;
+  tn.shade_block = 128;
+  tn.pad = 0;
+  if(t) {
+    if(t->struct_size != sizeof(dort_wavefront_tuning)) {
+      err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
+      return false;
+    }
+    if(t->queue_capacity) { tn.capacity = t->queue_capacity; }
+    if(t->trace_block) { tn.trace_block = t->trace_block; }
+    if(t->shade_block) { tn.shade_block = t->shade_block; }
+  }
+  tn.capacity = (tn.capacity + 31u) & ~31u;
+  if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
+    err = "queue_capacity must be 32..2^26";
+    return false;
+  }
+  for(uint32_t b : {tn.trace_block, tn.shade_block}) {
+    if(b < 32 || b > 1024 || b % 32 != 0) {
+      err = "block sizes must be multiples of 32 in 32..1024";
+      return false;
+    }
+  }
+  return true;
+}
+
+extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
+                                                const dort_render_params* params,
+                                                const dort_wavefront_tuning* tuning,
+                                                float* d_out_rgb, void* stream) {
+  clear_error();
+  if(!scene || !params || !d_out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.sample_all_lights) {
+    return fail(DORT_ERR_UNSUPPORTED, "the wavefront renderer does not do sample_all_lights; "
+                                      "use dort_gpu_render");
+  }
+  WfTuning tn;
+  if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
+  return wavefront_render(scene, pp, tn, d_out_rgb, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_params* params,
+                                         const dort_wavefront_tuning* tuning, float* out_rgb,
+                                         double* out_stats) {
+  clear_error();
+  if(!scene || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  size_t npix = size_t(pp.width) * pp.height;
+  float* d_out = nullptr;
+  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
+  }
+  cudaStream_t st = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, st);
+  int rc = dort_gpu_render_wavefront_device(scene, params, tuning, d_out, st);
+  cudaEventRecord(e1, st);
+  uint64_t rays = 0;
+  uint32_t waves = 0, error = 0;
+  if(rc == DORT_OK) {
+    if(cudaMemcpyAsync(out_rgb, d_out, npix * 3 * sizeof(float), cudaMemcpyDeviceToHost, st) !=
+           cudaSuccess ||
+       cudaStreamSynchronize(st) != cudaSuccess) {
+      rc = fail(DORT_ERR_CUDA, std::string("wavefront render failed: ") +
+                               cudaGetErrorString(cudaGetLastError()));
+    }
+  }
+  if(rc == DORT_OK) { rc = wavefront_counters(scene, &rays, &waves, &error, st); }
+  if(rc == DORT_OK && error) {
+    rc = fail(DORT_ERR_TIMEOUT, "wavefront frame exceeded its wave limit");
+  }
+  float ms = 0.f;
+  if(rc == DORT_OK) { cudaEventElapsedTime(&ms, e0, e1); }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(d_out);
+  if(rc == DORT_OK && out_stats) {
+    out_stats[0] = double(rays);
+    out_stats[1] = 0.0;
+    out_stats[2] = ms;
+    out_stats[3] = double(waves);
+  }
+  return rc;
+}

@@ -6,6 +6,7 @@
 #include "bvh_build.h"
 #include "common.h"
 #include "scene_build.h"
+#include "wavefront.h"
 
 namespace dort_gpu {
 
@@ -27,6 +28,7 @@ extern "C" const char* dort_gpu_last_error(void) { return g_last_error.c_str(); 
 extern "C" int dort_gpu_abi_version(void) { return DORT_GPU_ABI_VERSION; }
 
 static void scene_free_device(dort_scene* s) {
+  if(s->wavefront) { wavefront_destroy(s->wavefront); s->wavefront = nullptr; }
   for(void* p : s->allocations) { cudaFree(p); }
   s->allocations.clear();
   if(s->d_stage) { cudaFree(s->d_stage); }

@@ -1,0 +1,25 @@
+// Wavefront path tracer (wavefront.cu): host-side entry points.
+#pragma once
+#include <cstdint>
+
+#include "pt_scene.h"
+
+struct dort_scene;
+
+namespace dort_gpu {
+
+struct WfTuning {
+  uint32_t capacity;      // paths in flight
+  uint32_t trace_block;   // threads per block of extend / shadow / neeb
+  uint32_t shade_block;   // threads per block of shade
+  uint32_t pad;
+};
+
+struct Wavefront;
+void wavefront_destroy(Wavefront* wf);
+int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
+                     cudaStream_t st);
+int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                       cudaStream_t st);
+
+}  // namespace dort_gpu

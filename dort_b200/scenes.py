@@ -370,3 +370,123 @@ def env_test_scene(seed: int = 11, conductor: bool = False):
             "tris": np.concatenate(tris).astype(np.uint32),
             "tri_material": np.array(mats, np.uint32), "materials": materials,
             "tri_emission": None, "sky_rgb": procedural_sky(), "camera": cam}
+
+
+# ---- the 1080p wavefront workload ------------------------------------------------
+
+def _hash3(ix, iy, iz, seed):
+    """Integer lattice hash -> [0, 1) (a 32-bit multiply-xorshift mix)."""
+    h = (ix.astype(np.uint64) * np.uint64(73856093)) ^ (iy.astype(np.uint64) * np.uint64(19349663)) \
+        ^ (iz.astype(np.uint64) * np.uint64(83492791)) ^ np.uint64(seed * 2654435761 % (1 << 32))
+    h = h & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(16)
+    h = (h * np.uint64(0x7FEB352D)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(15)
+    h = (h * np.uint64(0x846CA68B)) & np.uint64(0xFFFFFFFF)
+    h ^= h >> np.uint64(16)
+    return (h.astype(np.float64) / 4294967296.0)
+
+
+def value_noise(p, seed):
+    """Trilinear value noise in [-1, 1] at points p [n, 3] (smoothstep fade)."""
+    f = np.floor(p)
+    t = p - f
+    t = t * t * (3.0 - 2.0 * t)
+    i = f.astype(np.int64) + (1 << 20)
+    out = np.zeros(len(p))
+    for dx in (0, 1):
+        for dy in (0, 1):
+            for dz in (0, 1):
+                w = (t[:, 0] if dx else 1 - t[:, 0]) * (t[:, 1] if dy else 1 - t[:, 1]) * \
+                    (t[:, 2] if dz else 1 - t[:, 2])
+                out += w * _hash3(i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz, seed)
+    return out * 2.0 - 1.0
+
+
+def fbm(p, seed, octaves=6, base_freq=2.0):
+    total = np.zeros(len(p))
+    amp, freq, norm = 1.0, base_freq, 0.0
+    for o in range(octaves):
+        total += amp * value_noise(p * freq, seed + o)
+        norm += amp
+        amp *= 0.5
+        freq *= 2.0
+    return total / norm
+
+
+def icosphere(freq: int):
+    """Geodesic sphere: each icosahedron face split into freq^2 triangles,
+    vertices projected to the unit sphere.  Vertices are shared within a face
+    (not across faces).  Returns (verts [V,3] f64, tris [20 freq^2, 3])."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    V = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t],
+                  [0, -1, -t], [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]],
+                 np.float64)
+    F = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9],
+                  [5, 11, 4], [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2],
+                  [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10],
+                  [8, 6, 7], [9, 8, 1]])
+    n = freq
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    mask = ii + jj <= n
+    ii, jj = ii[mask], jj[mask]
+    idx = -np.ones((n + 1, n + 1), np.int64)
+    idx[ii, jj] = np.arange(len(ii))
+    # local triangles of the barycentric grid
+    a_i, a_j = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = a_i + a_j < n
+    t_up = np.stack([idx[a_i[up], a_j[up]], idx[a_i[up] + 1, a_j[up]], idx[a_i[up], a_j[up] + 1]], 1)
+    dn = a_i + a_j < n - 1
+    t_dn = np.stack([idx[a_i[dn] + 1, a_j[dn]], idx[a_i[dn] + 1, a_j[dn] + 1],
+                     idx[a_i[dn], a_j[dn] + 1]], 1)
+    local = np.concatenate([t_up, t_dn])
+    npts = len(ii)
+    verts, tris = [], []
+    for f_i, (a, b, c) in enumerate(F):
+        wa = (n - ii - jj) / n
+        wb = ii / n
+        wc = jj / n
+        p = wa[:, None] * V[a] + wb[:, None] * V[b] + wc[:, None] * V[c]
+        p /= np.linalg.norm(p, axis=1, keepdims=True)
+        verts.append(p)
+        tris.append(local + f_i * npts)
+    return np.concatenate(verts), np.concatenate(tris).astype(np.uint32)
+
+
+def wavefront_scene(freq: int = 316, sky_w: int = 1024, sky_h: int = 512, seed: int = 3,
+                    n_materials: int = 96, conductor: bool = True):
+    """The 1080p wavefront workload: a geodesic icosphere of frequency `freq`
+    (20 freq^2 triangles; 1,997,120 at 316) displaced along the normal by fBm
+    (amplitude 0.1, 6 octaves), on a 2-triangle ground plane, lit by a
+    procedural sky_w x sky_h HDR sky.  Materials are a seeded mix of Lambert
+    (albedo U(0.2, 0.8)), GGX conductor (alpha U(0.05, 0.5)) and dielectric
+    (ior 1.5), assigned per surface patch."""
+    rng = np.random.default_rng(seed)
+    v, t = icosphere(freq)
+    disp = 0.1 * fbm(v * 1.5, seed, octaves=6)
+    v = v * (1.0 + disp)[:, None]
+    v = v + np.array([0.0, 1.15, 0.0])
+    # materials: table of n_materials entries, one per patch of ~256 triangles
+    mats = []
+    for k in range(n_materials):
+        r = k % 3 if conductor else k % 2 * 2
+        if r == 0:
+            mats.append({"kind": 0, "color": tuple(rng.uniform(0.2, 0.8, 3))})
+        elif r == 1:
+            mats.append({"kind": 4, "color": tuple(rng.uniform(0.5, 0.95, 3)),
+                         "param": (float(rng.uniform(0.05, 0.5)),)})
+        else:
+            mats.append({"kind": 2, "color": (1.0, 1.0, 1.0), "color2": (1.0, 1.0, 1.0),
+                         "param": (1.5,)})
+    patch = np.arange(len(t)) // 256
+    tri_mat = _hash3(patch, patch * 7 + 1, patch * 13 + 2, seed) * n_materials
+    tri_mat = np.minimum(tri_mat.astype(np.uint32), n_materials - 1)
+    ground_v = np.array([[-20, 0, -20], [20, 0, -20], [20, 0, 20], [-20, 0, 20]], np.float64)
+    ground_t = np.array([[0, 2, 1], [0, 3, 2]], np.uint32) + len(v)
+    mats.append({"kind": 0, "color": (0.45, 0.42, 0.4)})
+    verts = np.concatenate([v, ground_v]).astype(np.float32)
+    tris = np.concatenate([t, ground_t]).astype(np.uint32)
+    tri_mat = np.concatenate([tri_mat, np.full(2, len(mats) - 1, np.uint32)])
+    cam = look_at_camera((0.0, 1.6, -4.2), (0.0, 1.05, 0.0), (0.0, 1.0, 0.0), 0.75)
+    return {"verts": verts, "tris": tris, "tri_material": tri_mat, "materials": mats,
+            "tri_emission": None, "sky_rgb": procedural_sky(sky_w, sky_h, seed), "camera": cam}

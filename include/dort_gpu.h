@@ -219,6 +219,59 @@ int dort_gpu_render(dort_scene* scene, const dort_render_params* params,
 int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
                            float* d_out_rgb, void* stream);
 
+/* ---- wavefront ------------------------------------------------------------
+ * No single reference counterpart: the same "pt" estimator as dort_gpu_render
+ * (same parameters, same random numbers per pixel and sample, so the same
+ * paths), executed as a wavefront of generate / extend / shade / shadow
+ * stages over device-resident path queues with path regeneration, looped
+ * inside one CUDA graph per frame.  sample_all_lights is not supported here
+ * (DORT_ERR_UNSUPPORTED); use dort_gpu_render for it. */
+typedef struct dort_wavefront_tuning {
+  uint32_t struct_size;        /* sizeof(dort_wavefront_tuning) */
+  uint32_t queue_capacity;     /* paths in flight (0: auto) */
+  uint32_t trace_block;        /* threads per block, trace stages (0: auto) */
+  uint32_t shade_block;        /* threads per block, shade stage (0: auto) */
+  uint32_t reserved[4];
+} dort_wavefront_tuning;
+
+/* out_stats (optional, 4 doubles): rays traced, samples kept, kernel
+ * milliseconds, waves.  tuning may be NULL (automatic). */
+int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_params* params,
+                              const dort_wavefront_tuning* tuning, float* out_rgb,
+                              double* out_stats);
+
+/* Device-pointer form on a caller stream. */
+int dort_gpu_render_wavefront_device(dort_scene* scene, const dort_render_params* params,
+                                     const dort_wavefront_tuning* tuning, float* d_out_rgb,
+                                     void* stream);
+
+/* ---- adjoint --------------------------------------------------------------
+ * No reference counterpart.  Differentiable rendering of the "pt" estimator
+ * with respect to per-triangle Lambert albedo and per-triangle emitted
+ * radiance, by path replay backpropagation (every sample is re-traced from its
+ * random numbers; nothing per vertex is stored).
+ *
+ * tri_albedo (tri_count * 3, or NULL) replaces the albedo of every triangle
+ * whose material is Lambert; tri_emission (tri_count * 3, or NULL) replaces
+ * the radiance of the scene's emissive triangles (the set of lights is fixed
+ * when the scene is created).  Both stay in effect for later renders of the
+ * scene until replaced; NULL removes an override.
+ *
+ * forward:  renders the image (as dort_gpu_render) with the overrides.
+ * backward: given dLoss/dImage (width * height * 3, host), writes
+ *           d_albedo[t*3+c] = dLoss/d albedo and d_emission[t*3+c] =
+ *           dLoss/d Le (host, tri_count * 3 each; either may be NULL), for
+ *           the same parameters and seed as the forward call.
+ * loss_l2:  loss = sum (image - target)^2 and its image gradient, on the GPU. */
+int dort_gpu_adjoint_forward(dort_scene* scene, const dort_render_params* params,
+                             const float* tri_albedo, const float* tri_emission,
+                             float* out_image);
+int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_params* params,
+                              const float* tri_albedo, const float* tri_emission,
+                              const float* dl_dimage, float* d_albedo, float* d_emission);
+int dort_gpu_loss_l2(const float* image, const float* target, size_t count,
+                     double* out_loss, float* out_grad);
+
 /* ---- diagnostics ----------------------------------------------------------
  * No reference counterpart.  Builds the device scene's wide BVH on the host
  * and runs the device traversal code compiled for the CPU, with the same
