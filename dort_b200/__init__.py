@@ -141,6 +141,42 @@ class Scene:
             self.handle, ctypes.byref(params), ctypes.byref(t) if t else None,
             ctypes.c_void_p(d_out), ctypes.c_void_p(stream)))
 
+    def wavefront_stage_times(self, params: _abi.RenderParams, tuning: dict | None = None):
+        """Per-stage milliseconds of one frame run wave by wave (measurement)."""
+        ms = (ctypes.c_double * 6)()
+        rays = ctypes.c_double(0.0)
+        t = wavefront_tuning(**tuning) if tuning else None
+        _abi.check(_abi.lib().dort_gpu_wavefront_stage_times(
+            self.handle, ctypes.byref(params), ctypes.byref(t) if t else None, ms,
+            ctypes.byref(rays)))
+        names = ["regen", "extend", "shade", "shadow", "neeb"]
+        out = {n: ms[i] for i, n in enumerate(names)}
+        out["waves"] = ms[5]
+        out["rays"] = rays.value
+        return out
+
+    def adjoint_forward(self, params: _abi.RenderParams, tri_albedo=None, tri_emission=None):
+        """dort_gpu_adjoint_forward: image with per-triangle overrides."""
+        out = np.zeros((params.height, params.width, 3), np.float32)
+        a = None if tri_albedo is None else np.ascontiguousarray(tri_albedo, np.float32)
+        e = None if tri_emission is None else np.ascontiguousarray(tri_emission, np.float32)
+        _abi.check(_abi.lib().dort_gpu_adjoint_forward(self.handle, ctypes.byref(params),
+                                                       _ptr(a), _ptr(e), _ptr(out)))
+        return out
+
+    def adjoint_backward(self, params: _abi.RenderParams, dl_dimage, tri_albedo=None,
+                         tri_emission=None, want_albedo=True, want_emission=True):
+        """dort_gpu_adjoint_backward: (d_albedo, d_emission), tri_count x 3 each."""
+        g = np.ascontiguousarray(dl_dimage, np.float32)
+        a = None if tri_albedo is None else np.ascontiguousarray(tri_albedo, np.float32)
+        e = None if tri_emission is None else np.ascontiguousarray(tri_emission, np.float32)
+        da = np.zeros((self.tri_count, 3), np.float32) if want_albedo else None
+        de = np.zeros((self.tri_count, 3), np.float32) if want_emission else None
+        _abi.check(_abi.lib().dort_gpu_adjoint_backward(self.handle, ctypes.byref(params),
+                                                        _ptr(a), _ptr(e), _ptr(g), _ptr(da),
+                                                        _ptr(de)))
+        return da, de
+
     def render_device(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
         _abi.check(_abi.lib().dort_gpu_render_device(self.handle, ctypes.byref(params),
                                                      ctypes.c_void_p(d_out),
@@ -204,6 +240,16 @@ def host_check_render(d: dict, params: _abi.RenderParams, rows=None):
     _abi.check(_abi.lib().dort_gpu_host_check_render(ctypes.byref(h.desc), ctypes.byref(params),
                                                      r0, r1, _ptr(out)))
     return out
+
+
+def loss_l2(image, target):
+    """dort_gpu_loss_l2: (sum (image - target)^2, its image gradient)."""
+    a = np.ascontiguousarray(image, np.float32)
+    b = np.ascontiguousarray(target, np.float32)
+    g = np.zeros_like(a)
+    loss = ctypes.c_double(0.0)
+    _abi.check(_abi.lib().dort_gpu_loss_l2(_ptr(a), _ptr(b), a.size, ctypes.byref(loss), _ptr(g)))
+    return loss.value, g
 
 
 def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8):

@@ -124,6 +124,18 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_render_wavefront_device.restype = c_i32
         L.dort_gpu_render_wavefront_device.argtypes = [c_p, ctypes.POINTER(RenderParams),
                                                        ctypes.POINTER(WavefrontTuning), c_p, c_p]
+        L.dort_gpu_wavefront_stage_times.restype = c_i32
+        L.dort_gpu_wavefront_stage_times.argtypes = [c_p, ctypes.POINTER(RenderParams),
+                                                     ctypes.POINTER(WavefrontTuning),
+                                                     ctypes.POINTER(ctypes.c_double),
+                                                     ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_adjoint_forward.restype = c_i32
+        L.dort_gpu_adjoint_forward.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p, c_p, c_p]
+        L.dort_gpu_adjoint_backward.restype = c_i32
+        L.dort_gpu_adjoint_backward.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p, c_p, c_p,
+                                                c_p, c_p]
+        L.dort_gpu_loss_l2.restype = c_i32
+        L.dort_gpu_loss_l2.argtypes = [c_p, c_p, c_size, ctypes.POINTER(ctypes.c_double), c_p]
         _lib = L
     return _lib
 

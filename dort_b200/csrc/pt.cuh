@@ -624,8 +624,13 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
   if(use_bsdf) {
     BsdfSample bs = bsdf_sample(m, g.frame, wo, req, u_bsdf, v_bsdf, c_bsdf);
     if(!(bs.pdf == 0.f || is_black(bs.f))) {
-      Hit h = trace_ray<false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
-                               INFINITY);
+      // A background light counts only if the ray escapes, so whether anything
+      // is hit is all that matters: an any-hit query gives the same answer.
+      Hit h = l.kind == LIGHT_TRI
+          ? trace_ray<false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
+                             INFINITY)
+          : trace_ray<true>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
+                            INFINITY);
       rays += 1;
       V3 L = v3(0.f, 0.f, 0.f);
       if(h.prim != kMiss && l.kind == LIGHT_TRI) {

@@ -388,3 +388,32 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
   }
   return rc;
 }
+
+extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* params,
+                                              const dort_wavefront_tuning* tuning,
+                                              double out_ms[6], double* out_rays) {
+  clear_error();
+  if(!scene || !params || !out_ms) { return fail(DORT_ERR_INVALID, "null argument"); }
+  PtParams pp;
+  std::string err;
+  if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.sample_all_lights) { return fail(DORT_ERR_UNSUPPORTED, "sample_all_lights"); }
+  WfTuning tn;
+  if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
+  size_t npix = size_t(pp.width) * pp.height;
+  float* d_out = nullptr;
+  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
+  }
+  int rc = wavefront_stage_times(scene, pp, tn, d_out, 0, out_ms);
+  cudaFree(d_out);
+  if(rc == DORT_OK && out_rays) {
+    uint64_t rays = 0;
+    uint32_t waves = 0, error = 0;
+    rc = wavefront_counters(scene, &rays, &waves, &error, 0);
+    *out_rays = double(rays);
+    out_ms[5] = double(waves);
+  }
+  return rc;
+}

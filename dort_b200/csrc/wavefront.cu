@@ -35,12 +35,17 @@ namespace dort_gpu {
 
 enum : uint32_t { SLOT_FREE = 0, SLOT_ACTIVE = 1, SLOT_FINISHED = 2 };
 
-// device counters (one cache line each would be nicer; these are few)
+// Device counters.  Queues that are produced in one wave and consumed in the
+// next are double-buffered; buffer b of wave w is (w + b) & 1.
 enum : uint32_t {
-  C_ACTIVE = 0, C_SHADOW = 1, C_NEEB = 2, C_LIVE = 3, C_WAVES = 4, C_ERROR = 5,
-  C_NEXT_LO = 8,   // 64-bit next-sample counter at [8..9]
-  C_RAYS_LO = 10,  // 64-bit ray counter at [10..11]
-  C_COUNT = 16
+  C_ACT0 = 0, C_ACT1 = 1,      // active queue lengths (per buffer)
+  C_FIN0 = 2, C_FIN1 = 3,      // finished queue lengths (per buffer)
+  C_SHADOW = 4, C_NEEB = 5,    // this wave's shadow / BSDF-strategy queues
+  C_LIVE = 6, C_WAVES = 7, C_ERROR = 8,
+  C_F_EXT = 9, C_F_SHADE = 10, C_F_SH = 11, C_F_NB = 12,   // work-fetch cursors
+  C_NEXT_LO = 16,   // 64-bit next-sample counter at [16..17]
+  C_RAYS_LO = 18,   // 64-bit ray counter at [18..19]
+  C_COUNT = 32
 };
 
 DG_HD uint32_t f2u(float f) { return DG_AS_UINT(f); }
@@ -56,6 +61,13 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
   if(lane == leader) { base = atomicAdd(counter, __popc(mask)); }
   base = __shfl_sync(mask, base, leader);
   return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// Next 32 work items for this warp from a fetch cursor (lane 0 advances it).
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor) {
+  uint32_t base = 0;
+  if((threadIdx.x & 31u) == 0) { base = atomicAdd(cursor, 32u); }
+  return __shfl_sync(0xffffffffu, base, 0);
 }
 
 // Maps a global sample id to (pixel, x, y, sample): sample-major order, 8x4
@@ -81,7 +93,8 @@ struct WfDev {
   float4* sum;     // radiance sum
   uint4* meta;     // pixel, sample, bounces | last_delta << 31, state
   float4* hit;     // t, b1, b2, prim
-  uint32_t* active;
+  uint32_t* active[2];
+  uint32_t* finished[2];
   uint32_t* sh_slot;
   float4* sh_o;    // o.xyz, t_min
   float4* sh_d;    // d.xyz, t_max
@@ -97,48 +110,59 @@ struct WfDev {
   uint32_t max_waves;
 };
 
+__device__ __forceinline__ uint32_t wave_of(const WfDev& w) {
+  return *(volatile uint32_t*)(w.ctr + C_WAVES);
+}
+
 __global__ void wf_init(WfDev w, uint32_t npix) {
   uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < w.capacity; i += stride) {
     w.meta[i] = make_uint4(0u, 0u, 0u, SLOT_FREE);
+    w.finished[0][i] = uint32_t(i);    // every slot starts on the free list
   }
   for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npix; i += stride) {
     w.film[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  if(blockIdx.x == 0 && threadIdx.x < C_COUNT) { w.ctr[threadIdx.x] = 0u; }
+  if(blockIdx.x == 0 && threadIdx.x < C_COUNT) {
+    w.ctr[threadIdx.x] = threadIdx.x == C_FIN0 ? w.capacity : 0u;
+  }
 }
 
+// Finished paths of the last wave go to the film; their slots (and, in the
+// first wave, every slot) take the next samples and join this wave's active
+// queue behind the paths that continue.
 __global__ void wf_regen(PtScene sc, PtParams pp, WfDev w) {
-  uint32_t stride = gridDim.x * blockDim.x;
+  const uint32_t wave = wave_of(w);
+  const uint32_t cur = wave & 1u;
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_FIN0 + cur);
+  const uint32_t* fin = w.finished[cur];
+  uint32_t* act = w.active[cur];
   uint64_t* next = reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
-  // grid-stride over whole warps so that the warp-level append sees 32 lanes
-  uint32_t cap_pad = (w.capacity + 31u) & ~31u;
-  for(uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x; slot < cap_pad; slot += stride) {
-    bool valid = slot < w.capacity;
-    uint4 m = valid ? w.meta[slot] : make_uint4(0u, 0u, 0u, SLOT_ACTIVE + 7u);
-    if(m.w == SLOT_FINISHED) {
+  uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t n_pad = (n + 31u) & ~31u;
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+    bool valid = i < n;
+    uint32_t slot = valid ? fin[i] : 0u;
+    uint4 m = valid ? w.meta[slot] : make_uint4(0u, 0u, 0u, SLOT_ACTIVE);
+    if(valid && m.w == SLOT_FINISHED) {
       float4 s = w.sum[slot];
-      V3 L = v3(s.x, s.y, s.z);
       // renderer.cpp:36-41: only finite, non-negative samples reach the film
-      bool keep = isfinite(L.x) && isfinite(L.y) && isfinite(L.z) && L.x >= 0.f &&
-                  L.y >= 0.f && L.z >= 0.f;
-      if(keep) {
-        float4* f = w.film + m.x;
-        atomicAdd(&f->x, L.x);
-        atomicAdd(&f->y, L.y);
-        atomicAdd(&f->z, L.z);
-        atomicAdd(&f->w, 1.f);
-      }
+      bool keep = isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && s.x >= 0.f &&
+                  s.y >= 0.f && s.z >= 0.f;
+      if(keep) { atomicAdd(w.film + m.x, make_float4(s.x, s.y, s.z, 1.f)); }
       atomicSub(w.ctr + C_LIVE, 1u);
       m.w = SLOT_FREE;
     }
-    bool want_new = m.w == SLOT_FREE;
+    bool want_new = valid && m.w == SLOT_FREE;
     uint32_t nmask = __ballot_sync(0xffffffffu, want_new);
     uint64_t sid = ~0ull;
     if(want_new) {
       uint32_t lane = threadIdx.x & 31u, leader = __ffs(nmask) - 1u;
       unsigned long long base = 0;
-      if(lane == leader) { base = atomicAdd(reinterpret_cast<unsigned long long*>(next), (unsigned long long)__popc(nmask)); }
+      if(lane == leader) {
+        base = atomicAdd(reinterpret_cast<unsigned long long*>(next),
+                         (unsigned long long)__popc(nmask));
+      }
       base = __shfl_sync(nmask, base, leader);
       sid = base + __popc(nmask & ((1u << lane) - 1u));
     }
@@ -166,37 +190,52 @@ __global__ void wf_regen(PtScene sc, PtParams pp, WfDev w) {
         fresh = true;
       }
     }
-    if(valid && (want_new || fresh)) { w.meta[slot] = m; }
+    if(want_new) { w.meta[slot] = m; }
     if(fresh) { atomicAdd(w.ctr + C_LIVE, 1u); }
-    bool active = valid && m.w == SLOT_ACTIVE;
-    uint32_t at = warp_append(w.ctr + C_ACTIVE, active);
-    if(active) { w.active[at] = slot; }
+    // a slot whose sample fell outside the image goes back on the next free
+    // list so that it keeps taking samples
+    bool retry = want_new && !fresh && sid < w.total_samples;
+    uint32_t at = warp_append(w.ctr + C_ACT0 + cur, fresh);
+    if(fresh) { act[at] = slot; }
+    uint32_t rt = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), retry);
+    if(retry) { w.finished[cur ^ 1u][rt] = slot; }
   }
 }
 
 __global__ void wf_extend(PtScene sc, WfDev w) {
-  uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACTIVE);
-  uint32_t stride = gridDim.x * blockDim.x;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    uint32_t slot = w.active[i];
-    float4 o = w.ray_o[slot], d = w.ray_d[slot];
-    Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
-    w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
+  const uint32_t cur = wave_of(w) & 1u;
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t* act = w.active[cur];
+  for(;;) {
+    uint32_t base = warp_fetch(w.ctr + C_F_EXT);
+    if(base >= n) { break; }
+    uint32_t i = base + (threadIdx.x & 31u);
+    if(i < n) {
+      uint32_t slot = act[i];
+      float4 o = w.ray_o[slot], d = w.ray_d[slot];
+      Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
+    }
   }
 }
 
 __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
-  uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACTIVE);
-  uint32_t stride = gridDim.x * blockDim.x;
-  uint32_t n_pad = (n + 31u) & ~31u;
+  const uint32_t cur = wave_of(w) & 1u;
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t* act = w.active[cur];
+  uint32_t* act_next = w.active[cur ^ 1u];
+  uint32_t* fin_next = w.finished[cur ^ 1u];
   const uint32_t req_nd = F_ALL & ~F_DELTA;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
+  for(;;) {
+    uint32_t base = warp_fetch(w.ctr + C_F_SHADE);
+    if(base >= n) { break; }
+    uint32_t i = base + (threadIdx.x & 31u);
     bool valid = i < n;
-    bool push_sh = false, push_nb = false;
+    bool push_sh = false, push_nb = false, cont = false, done = false;
     float4 sh_o, sh_d, sh_c, nb_o, nb_d, nb_f;
     uint32_t slot = 0;
     if(valid) {
-      slot = w.active[i];
+      slot = act[i];
       float4 ro = w.ray_o[slot], rd = w.ray_d[slot];
       float4 t4 = w.thr[slot], s4 = w.sum[slot];
       uint4 m = w.meta[slot];
@@ -298,7 +337,13 @@ __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
       m.z = bounces | (last_delta ? 0x80000000u : 0u);
       m.w = finished ? SLOT_FINISHED : SLOT_ACTIVE;
       w.meta[slot] = m;
+      cont = !finished;
+      done = finished;
     }
+    uint32_t ci = warp_append(w.ctr + C_ACT0 + (cur ^ 1u), cont);
+    if(cont) { act_next[ci] = slot; }
+    uint32_t fi = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), done);
+    if(done) { fin_next[fi] = slot; }
     uint32_t si = warp_append(w.ctr + C_SHADOW, push_sh);
     if(push_sh) {
       w.sh_slot[si] = slot;
@@ -317,33 +362,47 @@ __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
 }
 
 __global__ void wf_shadow(PtScene sc, WfDev w) {
-  uint32_t n = *(volatile uint32_t*)(w.ctr + C_SHADOW);
-  uint32_t stride = gridDim.x * blockDim.x;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    float4 o = w.sh_o[i], d = w.sh_d[i];
-    Hit h = trace_ray<true>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w);
-    if(h.prim == kMiss) {
-      uint32_t slot = w.sh_slot[i];
-      float4 c = w.sh_c[i];
-      float4 s = w.sum[slot];
-      w.sum[slot] = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.f);
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_SHADOW);
+  for(;;) {
+    uint32_t base = warp_fetch(w.ctr + C_F_SH);
+    if(base >= n) { break; }
+    uint32_t i = base + (threadIdx.x & 31u);
+    if(i < n) {
+      float4 o = w.sh_o[i], d = w.sh_d[i];
+      Hit h = trace_ray<true>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w);
+      if(h.prim == kMiss) {
+        uint32_t slot = w.sh_slot[i];
+        float4 c = w.sh_c[i];
+        float4 s = w.sum[slot];
+        w.sum[slot] = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.f);
+      }
     }
   }
 }
 
+__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i);
+#define neeb_one neeb_one_impl
+
 __global__ void wf_neeb(PtScene sc, WfDev w) {
-  uint32_t n = *(volatile uint32_t*)(w.ctr + C_NEEB);
-  uint32_t stride = gridDim.x * blockDim.x;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_NEEB);
+  for(;;) {
+    uint32_t base = warp_fetch(w.ctr + C_F_NB);
+    if(base >= n) { break; }
+    uint32_t i = base + (threadIdx.x & 31u);
+    if(i < n) { neeb_one(sc, w, i); }
+  }
+}
+
+__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i) {
     float4 o = w.nb_o[i], d = w.nb_d[i], f = w.nb_f[i];
     uint32_t lw = f2u(f.w);
     const DevLight& l = sc.lights[lw & 0x7fffffffu];
     bool use_mis = (lw >> 31) != 0;
-    Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
     V3 L = v3(0.f, 0.f, 0.f);
     V3 p = v3(o.x, o.y, o.z), wi = v3(d.x, d.y, d.z);
-    if(h.prim != kMiss && l.kind == LIGHT_TRI) {
-      if(h.prim == l.tri) {
+    if(l.kind == LIGHT_TRI) {
+      Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      if(h.prim != kMiss && h.prim == l.tri) {
         const float4* sh = sc.shade + 3 * size_t(h.prim);
         float4 a = sh[0], b = sh[1], c = sh[2];
         V3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
@@ -352,8 +411,10 @@ __global__ void wf_neeb(PtScene sc, WfDev w) {
         V3 ln = normalize(cross(p2 - p0, p1 - p0));
         L = area_eval_radiance(sc, l, lp, ln, p);
       }
-    } else if(h.prim == kMiss && l.kind != LIGHT_TRI) {
-      L = background_radiance(sc, l, wi);
+    } else {
+      // background light: only escaping rays count, an any-hit query decides
+      Hit h = trace_ray<true>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      if(h.prim == kMiss) { L = background_radiance(sc, l, wi); }
     }
     if(!is_black(L)) {
       float wgt = 1.f;
@@ -366,26 +427,36 @@ __global__ void wf_neeb(PtScene sc, WfDev w) {
       float4 s = w.sum[slot];
       w.sum[slot] = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.f);
     }
-  }
 }
 
-__global__ void wf_control(WfDev w, cudaGraphConditionalHandle handle) {
-  // single thread: account the wave, reset the queues, decide whether to loop
-  uint32_t a = w.ctr[C_ACTIVE], s = w.ctr[C_SHADOW], b = w.ctr[C_NEEB];
+// Single thread: account the wave, retire its queues, decide whether to loop.
+__device__ __forceinline__ bool wf_end_wave(WfDev& w) {
+  uint32_t wave = w.ctr[C_WAVES];
+  uint32_t cur = wave & 1u;
+  uint32_t a = w.ctr[C_ACT0 + cur], s = w.ctr[C_SHADOW], b = w.ctr[C_NEEB];
   unsigned long long* rays = reinterpret_cast<unsigned long long*>(w.ctr + C_RAYS_LO);
   *rays += (unsigned long long)a + s + b;
-  w.ctr[C_ACTIVE] = 0u;
+  w.ctr[C_ACT0 + cur] = 0u;     // consumed; the next wave fills the other buffer
+  w.ctr[C_FIN0 + cur] = 0u;
   w.ctr[C_SHADOW] = 0u;
   w.ctr[C_NEEB] = 0u;
-  uint32_t waves = ++w.ctr[C_WAVES];
+  w.ctr[C_F_EXT] = 0u;
+  w.ctr[C_F_SHADE] = 0u;
+  w.ctr[C_F_SH] = 0u;
+  w.ctr[C_F_NB] = 0u;
+  w.ctr[C_WAVES] = wave + 1u;
   uint64_t next = *reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
   bool more = w.ctr[C_LIVE] > 0u || next < w.total_samples;
-  if(more && waves >= w.max_waves) {
+  if(more && wave + 1u >= w.max_waves) {
     // bounded: a frame never loops forever; the host reports the error
     w.ctr[C_ERROR] = 1u;
     more = false;
   }
-  cudaGraphSetConditional(handle, more ? 1u : 0u);
+  return more;
+}
+
+__global__ void wf_control(WfDev w, cudaGraphConditionalHandle handle) {
+  cudaGraphSetConditional(handle, wf_end_wave(w) ? 1u : 0u);
 }
 
 __global__ void wf_resolve(WfDev w, uint32_t npix, float* __restrict__ out) {
@@ -436,8 +507,9 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t Q = capacity;
   size_t f4 = al(Q * sizeof(float4)), u4 = al(Q * sizeof(uint4)), u1 = al(Q * sizeof(uint32_t));
-  size_t bytes = 4 * f4 + u4 + f4 /*hit*/ + u1 /*active*/ + u1 + 3 * f4 /*shadow*/ +
-                 u1 + 3 * f4 /*neeb*/ + al(size_t(npix) * sizeof(float4)) + al(C_COUNT * 4);
+  size_t bytes = 4 * f4 + u4 + f4 /*hit*/ + 4 * u1 /*active, finished*/ + u1 +
+                 3 * f4 /*shadow*/ + u1 + 3 * f4 /*neeb*/ +
+                 al(size_t(npix) * sizeof(float4)) + al(C_COUNT * 4);
   if(cudaMalloc(&wf->mem, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of wavefront queues failed (" +
@@ -452,7 +524,10 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.sum = reinterpret_cast<float4*>(take(f4));
   d.meta = reinterpret_cast<uint4*>(take(u4));
   d.hit = reinterpret_cast<float4*>(take(f4));
-  d.active = reinterpret_cast<uint32_t*>(take(u1));
+  d.active[0] = reinterpret_cast<uint32_t*>(take(u1));
+  d.active[1] = reinterpret_cast<uint32_t*>(take(u1));
+  d.finished[0] = reinterpret_cast<uint32_t*>(take(u1));
+  d.finished[1] = reinterpret_cast<uint32_t*>(take(u1));
   d.sh_slot = reinterpret_cast<uint32_t*>(take(u1));
   d.sh_o = reinterpret_cast<float4*>(take(f4));
   d.sh_d = reinterpret_cast<float4*>(take(f4));
@@ -499,7 +574,7 @@ static int wf_build_graph(Wavefront* wf, const PtScene& sc, const PtParams& pp,
   cudaGraph_t body = cp.conditional.phGraph_out[0];
 
   int b_trace = int(tn.trace_block), b_shade = int(tn.shade_block);
-  int g_regen = (int(wf->capacity) + 255) / 256;
+  int g_regen = grid_for(reinterpret_cast<const void*>(&wf_regen), 256);
   int g_ext = grid_for(reinterpret_cast<const void*>(&wf_extend), b_trace);
   int g_sha = grid_for(reinterpret_cast<const void*>(&wf_shade), b_shade);
   int g_shw = grid_for(reinterpret_cast<const void*>(&wf_shadow), b_trace);
@@ -552,6 +627,73 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   DG_CUDA(cudaGraphLaunch(wf->exec, st));
   wf_resolve<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, d_out);
   DG_CUDA(cudaGetLastError());
+  return DORT_OK;
+}
+
+// The same frame as wavefront_render, run wave by wave from the host without
+// the graph, with CUDA events around every stage; for measurement only.
+__global__ void wf_control_host(WfDev w, uint32_t* more_flag) {
+  *more_flag = wf_end_wave(w) ? 1u : 0u;
+}
+
+int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
+                          float* d_out, cudaStream_t st, double ms[6]) {
+  if(!s->wavefront) { s->wavefront = new Wavefront(); }
+  Wavefront* wf = s->wavefront;
+  uint32_t npix = pp.width * pp.height;
+  int rc = wf_alloc(wf, tn.capacity, npix);
+  if(rc != DORT_OK) { return rc; }
+  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  wf->dev.total_samples = uint64_t(tiles) * 32 * pp.spp;
+  wf->dev.max_waves = uint32_t(std::min<uint64_t>(
+      0x7fffffffull, (wf->dev.total_samples / std::max(1u, tn.capacity) + 2) *
+                     (uint64_t(pp.max_depth) + 3) + 64));
+  const PtScene& sc = s->pt;
+  int b_trace = int(tn.trace_block), b_shade = int(tn.shade_block);
+  int g_regen = grid_for(reinterpret_cast<const void*>(&wf_regen), 256);
+  int g_ext = grid_for(reinterpret_cast<const void*>(&wf_extend), b_trace);
+  int g_sha = grid_for(reinterpret_cast<const void*>(&wf_shade), b_shade);
+  int g_shw = grid_for(reinterpret_cast<const void*>(&wf_shadow), b_trace);
+  int g_nb = grid_for(reinterpret_cast<const void*>(&wf_neeb), b_trace);
+  uint32_t* more = nullptr;
+  DG_CUDA(cudaMallocHost(&more, sizeof(uint32_t)));
+  cudaEvent_t ev[6];
+  for(auto& e : ev) { cudaEventCreate(&e); }
+  for(int k = 0; k < 6; ++k) { ms[k] = 0.0; }
+  wf_init<<<(std::max(tn.capacity, npix) + 255) / 256, 256, 0, st>>>(wf->dev, npix);
+  bool ok = cudaGetLastError() == cudaSuccess;
+  for(uint32_t wave = 0; ok && wave < wf->dev.max_waves + 1; ++wave) {
+    cudaEventRecord(ev[0], st);
+    wf_regen<<<g_regen, 256, 0, st>>>(sc, pp, wf->dev);
+    cudaEventRecord(ev[1], st);
+    wf_extend<<<g_ext, b_trace, 0, st>>>(sc, wf->dev);
+    cudaEventRecord(ev[2], st);
+    wf_shade<<<g_sha, b_shade, 0, st>>>(sc, pp, wf->dev);
+    cudaEventRecord(ev[3], st);
+    wf_shadow<<<g_shw, b_trace, 0, st>>>(sc, wf->dev);
+    cudaEventRecord(ev[4], st);
+    wf_neeb<<<g_nb, b_trace, 0, st>>>(sc, wf->dev);
+    cudaEventRecord(ev[5], st);
+    wf_control_host<<<1, 1, 0, st>>>(wf->dev, more);
+    ok = cudaStreamSynchronize(st) == cudaSuccess;
+    for(int k = 0; ok && k < 5; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
+      ms[k] += t;
+    }
+    if(!*more) { break; }
+  }
+  if(ok) {
+    wf_resolve<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, d_out);
+    ok = cudaStreamSynchronize(st) == cudaSuccess;
+  }
+  for(auto& e : ev) { cudaEventDestroy(e); }
+  cudaFreeHost(more);
+  ms[5] = 0.0;
+  if(!ok) {
+    return fail(DORT_ERR_CUDA, std::string("staged wavefront failed: ") +
+                               cudaGetErrorString(cudaGetLastError()));
+  }
   return DORT_OK;
 }
 

@@ -19,6 +19,8 @@ struct Wavefront;
 void wavefront_destroy(Wavefront* wf);
 int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
                      cudaStream_t st);
+int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
+                          float* d_out, cudaStream_t st, double ms[6]);
 int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
                        cudaStream_t st);
 

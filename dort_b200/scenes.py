@@ -490,3 +490,37 @@ def wavefront_scene(freq: int = 316, sky_w: int = 1024, sky_h: int = 512, seed: 
     cam = look_at_camera((0.0, 1.6, -4.2), (0.0, 1.05, 0.0), (0.0, 1.0, 0.0), 0.75)
     return {"verts": verts, "tris": tris, "tri_material": tri_mat, "materials": mats,
             "tri_emission": None, "sky_rgb": procedural_sky(sky_w, sky_h, seed), "camera": cam}
+
+
+def adjoint_scene(n_tris: int = 500_000, seed: int = 5):
+    """The adjoint workload: a random-triangle soup (the ray-cast generator,
+    seed 5) with per-triangle RGB albedo U(0.1, 0.9), plus 8 emissive
+    triangles in a ring above the soup, facing down.  Returns the scene dict
+    plus "tri_albedo" and the emissive triangles' indices in "lights"."""
+    rng = np.random.default_rng(seed)
+    verts, tris = random_triangles(n_tris, seed=seed, sigma=0.02)
+    albedo = rng.uniform(0.1, 0.9, (n_tris, 3)).astype(np.float32)
+    lv, lt = [], []
+    base = len(verts)
+    for k in range(8):
+        ang = 2 * np.pi * k / 8
+        c = np.array([0.5 + 0.55 * np.cos(ang), 1.45, 0.5 + 0.55 * np.sin(ang)])
+        a, b = 0.22, 0.18
+        # cross(e2, e1) must point down (-y): p0, p1 = p0 + (0,0,b), p2 = p0 + (a,0,0)
+        p0 = c + np.array([-a / 2, 0.0, -b / 2])
+        lv += [p0, p0 + np.array([0.0, 0.0, b]), p0 + np.array([a, 0.0, 0.0])]
+        lt.append([base + 3 * k, base + 3 * k + 1, base + 3 * k + 2])
+    verts = np.concatenate([verts, np.array(lv, np.float32)]).astype(np.float32)
+    tris = np.concatenate([tris, np.array(lt, np.uint32)]).astype(np.uint32)
+    n = len(tris)
+    emission = np.zeros((n, 3), np.float32)
+    cols = rng.uniform(0.5, 1.0, (8, 3)) * 30.0
+    emission[n_tris:] = cols
+    tri_albedo = np.concatenate([albedo, np.zeros((8, 3), np.float32)])
+    mats = [{"kind": 0, "color": (0.5, 0.5, 0.5)}, {"kind": 0, "color": (0.0, 0.0, 0.0)}]
+    tri_mat = np.zeros(n, np.uint32)
+    tri_mat[n_tris:] = 1
+    cam = look_at_camera((0.5, 1.0, -1.4), (0.5, 0.45, 0.5), (0.0, 1.0, 0.0), 0.9)
+    return {"verts": verts, "tris": tris, "tri_material": tri_mat, "materials": mats,
+            "tri_emission": emission, "tri_albedo": tri_albedo,
+            "lights": np.arange(n_tris, n, dtype=np.int64), "camera": cam}

@@ -245,6 +245,14 @@ int dort_gpu_render_wavefront_device(dort_scene* scene, const dort_render_params
                                      const dort_wavefront_tuning* tuning, float* d_out_rgb,
                                      void* stream);
 
+/* Measurement entry: renders the same frame wave by wave from the host
+ * (without the graph) with CUDA events around each stage; out_ms[0..4] =
+ * total milliseconds of regen, extend, shade, shadow, neeb; out_ms[5] = waves;
+ * out_rays = rays traced. */
+int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* params,
+                                   const dort_wavefront_tuning* tuning, double out_ms[6],
+                                   double* out_rays);
+
 /* ---- adjoint --------------------------------------------------------------
  * No reference counterpart.  Differentiable rendering of the "pt" estimator
  * with respect to per-triangle Lambert albedo and per-triangle emitted

@@ -238,3 +238,65 @@ def ref_pt_render(scene: dict, width: int, height: int, iterations: int,
                      seed, {"middle": 0, "sah": 1}[split], threads or os.cpu_count() or 1,
                      _ptr(out), ctypes.byref(secs))
     return out, secs.value
+
+
+class RefPtScene:
+    """A scene built once by the reference (for repeated timed renders)."""
+
+    def __init__(self, scene: dict, split: str = "middle", threads: int = 1):
+        R = ref()
+        if not hasattr(R, "_pts_ready"):
+            R.dref_pt_scene_create.restype = _P
+            R.dref_pt_scene_create.argtypes = [_P, _u32, _P, _u32, _P, _P, _u32, _P, _P, _P,
+                                               _u32, _u32, _P, _i32, _u32, _P]
+            R.dref_pt_scene_destroy.argtypes = [_P]
+            R.dref_pt_scene_render.restype = _i32
+            R.dref_pt_scene_render.argtypes = [_P, _P, ctypes.c_float, _u32, _u32, _u32, _u32,
+                                               _u32, _i32, _i32, _i32, _u32, _u32, _P, _P]
+            R._pts_ready = True
+        self.keep = []
+
+        def arr(a, dt):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dt)
+            self.keep.append(a)
+            return a
+        v = arr(scene["verts"], np.float32)
+        t = arr(scene["tris"], np.uint32)
+        tm = arr(scene.get("tri_material"), np.uint32)
+        mats = arr(pack_materials(scene["materials"]), np.float32)
+        em = arr(scene.get("tri_emission"), np.float32)
+        bg = arr(scene.get("sky_const"), np.float32)
+        env = arr(scene.get("sky_rgb"), np.float32)
+        ew = eh = 0
+        frame = None
+        if env is not None:
+            eh, ew = env.shape[0], env.shape[1]
+            frame = arr(np.concatenate([
+                np.asarray(scene.get("sky_scale", (1, 1, 1)), np.float32),
+                np.asarray(scene.get("sky_up", (0, 1, 0)), np.float32),
+                np.asarray(scene.get("sky_fwd", (1, 0, 0)), np.float32)]), np.float32)
+        bs = ctypes.c_double(0.0)
+        self.h = R.dref_pt_scene_create(_ptr(v), len(v), _ptr(t), len(t), _ptr(tm), _ptr(mats),
+                                        len(mats), _ptr(em), _ptr(bg), _ptr(env), ew, eh,
+                                        _ptr(frame), {"middle": 0, "sah": 1}[split], threads,
+                                        ctypes.byref(bs))
+        self.build_s = bs.value
+        self.camera = scene["camera"]
+
+    def render(self, width, height, iterations, min_depth=0, max_depth=5, seed=42,
+               strategy="mis", threads=1):
+        cam = pack_camera(self.camera)
+        out = np.zeros((height, width, 3), np.float32)
+        secs = ctypes.c_double(0.0)
+        ref().dref_pt_scene_render(self.h, _ptr(cam), ctypes.c_float(self.camera["fov"]), width,
+                                   height, iterations, min_depth, max_depth, 0, 0,
+                                   {"mis": 0, "bsdf": 1, "light": 2}[strategy], seed, threads,
+                                   _ptr(out), ctypes.byref(secs))
+        return out, secs.value
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            ref().dref_pt_scene_destroy(self.h)
+            self.h = None

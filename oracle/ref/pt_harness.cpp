@@ -94,22 +94,21 @@ namespace {
   }
 }
 
-extern "C" int dref_pt_render(
+struct RefPtScene {
+  std::shared_ptr<Scene> scene;
+  std::shared_ptr<Mesh> mesh;
+};
+
+extern "C" void* dref_pt_scene_create(
     const float* verts, uint32_t vert_count, const uint32_t* tris, uint32_t tri_count,
     const uint32_t* tri_mat, const float* mats, uint32_t mat_count,
     const float* tri_emission,
     const float* bg_const, const float* env_rgb, uint32_t env_w, uint32_t env_h,
     const float* env_frame /* scale.rgb, up.xyz, fwd.xyz */,
-    const float* cam /* origin, right, up, forward (12 floats) */, float fov,
-    uint32_t width, uint32_t height, uint32_t iterations,
-    uint32_t min_depth, uint32_t max_depth, int only_direct, int sample_all_lights,
-    int strategy /* 0 mis, 1 bsdf, 2 light */, uint32_t seed, int split_method,
-    uint32_t threads, float* out_rgb, double* out_seconds)
+    int split_method, uint32_t threads, double* out_build_s)
 {
   auto pool = pool_for(threads);
-  CtxG ctx;
-  ctx.pool = pool;
-
+  auto t0 = std::chrono::steady_clock::now();
   auto mesh = std::make_shared<Mesh>();
   for(uint32_t i = 0; i < vert_count; ++i) {
     mesh->points.push_back(Point(verts[3*i], verts[3*i + 1], verts[3*i + 2]));
@@ -176,7 +175,29 @@ extern "C" int dref_pt_render(
     if(light->flags & LIGHT_BACKGROUND) { scene->background_lights.push_back(light); }
   }
   scene->meshes.push_back(mesh);
+  auto t1 = std::chrono::steady_clock::now();
+  if(out_build_s) { *out_build_s = std::chrono::duration<double>(t1 - t0).count(); }
+  auto* h = new RefPtScene();
+  h->scene = scene;
+  h->mesh = mesh;
+  return h;
+}
 
+extern "C" void dref_pt_scene_destroy(void* handle) {
+  delete static_cast<RefPtScene*>(handle);
+}
+
+extern "C" int dref_pt_scene_render(void* handle,
+    const float* cam /* origin, right, up, forward (12 floats) */, float fov,
+    uint32_t width, uint32_t height, uint32_t iterations,
+    uint32_t min_depth, uint32_t max_depth, int only_direct, int sample_all_lights,
+    int strategy /* 0 mis, 1 bsdf, 2 light */, uint32_t seed,
+    uint32_t threads, float* out_rgb, double* out_seconds)
+{
+  auto* h = static_cast<RefPtScene*>(handle);
+  auto pool = pool_for(threads);
+  CtxG ctx;
+  ctx.pool = pool;
   Mat4x4 m(1.f);
   for(int r = 0; r < 3; ++r) {
     m.cols[0][r] = cam[3 + r];
@@ -185,7 +206,6 @@ extern "C" int dref_pt_render(
     m.cols[3][r] = cam[r];
   }
   auto camera = std::make_shared<PinholeCamera>(Transform(m, Mat4x4(1.f)), fov);
-
   auto film = std::make_shared<Film>(width, height,
       std::make_shared<BoxFilter>(Vec2(0.5f, 0.5f)));
   std::shared_ptr<Sampler> sampler =
@@ -193,15 +213,13 @@ extern "C" int dref_pt_render(
   PathRenderer::DirectStrategy ds = strategy == 1 ? PathRenderer::DirectStrategy::SAMPLE_BSDF
     : strategy == 2 ? PathRenderer::DirectStrategy::SAMPLE_LIGHT
     : PathRenderer::DirectStrategy::MIS;
-  PathRenderer renderer(scene, film, sampler, camera, iterations, min_depth, max_depth,
+  PathRenderer renderer(h->scene, film, sampler, camera, iterations, min_depth, max_depth,
       only_direct != 0, sample_all_lights != 0, ds);
-
   NoProgress progress;
   auto t0 = std::chrono::steady_clock::now();
   renderer.render(ctx, progress);
   auto t1 = std::chrono::steady_clock::now();
   if(out_seconds) { *out_seconds = std::chrono::duration<double>(t1 - t0).count(); }
-
   Image<PixelRgbFloat> img = film->to_image<PixelRgbFloat>();
   for(uint32_t y = 0; y < height; ++y) {
     for(uint32_t x = 0; x < width; ++x) {
@@ -211,4 +229,24 @@ extern "C" int dref_pt_render(
     }
   }
   return 0;
+}
+
+extern "C" int dref_pt_render(
+    const float* verts, uint32_t vert_count, const uint32_t* tris, uint32_t tri_count,
+    const uint32_t* tri_mat, const float* mats, uint32_t mat_count,
+    const float* tri_emission,
+    const float* bg_const, const float* env_rgb, uint32_t env_w, uint32_t env_h,
+    const float* env_frame,
+    const float* cam, float fov,
+    uint32_t width, uint32_t height, uint32_t iterations,
+    uint32_t min_depth, uint32_t max_depth, int only_direct, int sample_all_lights,
+    int strategy, uint32_t seed, int split_method,
+    uint32_t threads, float* out_rgb, double* out_seconds)
+{
+  void* h = dref_pt_scene_create(verts, vert_count, tris, tri_count, tri_mat, mats, mat_count,
+      tri_emission, bg_const, env_rgb, env_w, env_h, env_frame, split_method, threads, nullptr);
+  int rc = dref_pt_scene_render(h, cam, fov, width, height, iterations, min_depth, max_depth,
+      only_direct, sample_all_lights, strategy, seed, threads, out_rgb, out_seconds);
+  dref_pt_scene_destroy(h);
+  return rc;
 }

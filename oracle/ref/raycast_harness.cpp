@@ -13,8 +13,11 @@
 // (mesh_bvh_primitive.hpp:9-16: Element = vertex-array offset, bounds =
 // Triangle(mesh, idx).bounds()) and replays MeshBvhPrimitive::intersect /
 // intersect_p (mesh_bvh_primitive.cpp:13-45) while recording the index.
+#include <atomic>
 #include <chrono>
 #include <cstring>
+#include <thread>
+#include <vector>
 #include "dort/bvh.hpp"
 #include "dort/mesh.hpp"
 #include "dort/shape.hpp"
@@ -85,9 +88,13 @@ void* dref_scene_create(const float* verts, uint32_t vert_count,
   opts.leaf_size = leaf_size;
   opts.max_leaf_size = max_leaf_size;
 
+  // The reference's ThreadPool is only safe with one worker: with more, a
+  // thread can read a finished loop's flags after its owner returned
+  // (thread_pool.cpp:112-148) and crash.  The build runs on one worker.
+  (void)threads;
   double t0 = now_s();
   scene->bvh = std::make_unique<dort::Bvh<HarnessTraits>>(
-      std::move(elems), &scene->mesh, opts, pool_with(threads));
+      std::move(elems), &scene->mesh, opts, pool_with(1));
   if(out_build_s) { *out_build_s = now_s() - t0; }
   return scene;
 }
@@ -105,12 +112,14 @@ int dref_raycast(void* handle, const float* rays, uint64_t ray_count,
     uint32_t* out_tests, double* out_trace_s)
 {
   auto* scene = static_cast<RefScene*>(handle);
-  auto& pool = pool_with(threads);
   const uint64_t chunk = 4096;
   uint32_t jobs = uint32_t((ray_count + chunk - 1) / chunk);
 
-  double t0 = now_s();
-  dort::parallel_for(pool, jobs, [&](uint32_t job) {
+  // Rays are spread over plain threads of this harness (see the note on the
+  // reference's ThreadPool in dref_scene_create); each ray runs the
+  // reference's own traversal.
+  std::atomic<uint32_t> next_job{0};
+  auto run_job = [&](uint32_t job) {
     uint64_t begin = uint64_t(job) * chunk;
     uint64_t end = std::min(ray_count, begin + chunk);
     for(uint64_t i = begin; i < end; ++i) {
@@ -162,7 +171,18 @@ int dref_raycast(void* handle, const float* rays, uint64_t ray_count,
       }
       if(out_tests) { out_tests[i] = tests; }
     }
-  });
+  };
+  double t0 = now_s();
+  uint32_t nthreads = threads > 0 ? threads : 1;
+  std::vector<std::thread> workers;
+  for(uint32_t t = 0; t < nthreads; ++t) {
+    workers.emplace_back([&]() {
+      for(uint32_t job = next_job.fetch_add(1); job < jobs; job = next_job.fetch_add(1)) {
+        run_job(job);
+      }
+    });
+  }
+  for(auto& w : workers) { w.join(); }
   if(out_trace_s) { *out_trace_s = now_s() - t0; }
   return 0;
 }

@@ -82,7 +82,7 @@ def main():
         arrays[f"{name}_tris"] = t.astype(np.uint32)
         arrays[f"{name}_rays"] = rays
         for split in ("middle", "sah"):
-            rb = po.RefBvh(v, t, split, threads=2)
+            rb = po.RefBvh(v, t, split, threads=1)
             prim, tb, tests = rb.raycast(rays, counts=True)
             anyh, _ = rb.raycast(rays, any_hit=True)
             tb[prim == 0xFFFFFFFF] = 0.0
