@@ -177,6 +177,11 @@ class Scene:
                                                         _ptr(de)))
         return da, de
 
+    def render_device_noalloc(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
+        """dort_gpu_render_device_noalloc: no device allocation in the call."""
+        _abi.check(_abi.lib().dort_gpu_render_device_noalloc(
+            self.handle, ctypes.byref(params), ctypes.c_void_p(d_out), ctypes.c_void_p(stream)))
+
     def render_device(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
         _abi.check(_abi.lib().dort_gpu_render_device(self.handle, ctypes.byref(params),
                                                      ctypes.c_void_p(d_out),

@@ -136,6 +136,9 @@ def lib() -> ctypes.CDLL:
                                                 c_p, c_p]
         L.dort_gpu_loss_l2.restype = c_i32
         L.dort_gpu_loss_l2.argtypes = [c_p, c_p, c_size, ctypes.POINTER(ctypes.c_double), c_p]
+        L.dort_gpu_render_device_noalloc.restype = c_i32
+        L.dort_gpu_render_device_noalloc.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p,
+                                                     c_p]
         _lib = L
     return _lib
 

@@ -219,6 +219,19 @@ int dort_gpu_render(dort_scene* scene, const dort_render_params* params,
 int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
                            float* d_out_rgb, void* stream);
 
+/* No reference counterpart.  dort_gpu_render_device for callers that must not
+ * allocate GPU memory during a render (a frame recorded into a CUDA graph, a
+ * host application that owns every device allocation under a fixed budget, a
+ * real-time loop that cannot absorb cudaFree's device synchronisation).  Same
+ * kernels and result; the scratch is a fixed 16 MiB array that the library
+ * holds on every GPU it is loaded on, so this call allocates nothing.  Images
+ * above 1,048,560 pixels are rejected (DORT_ERR_INVALID).  All calls on a
+ * device share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * address (cudaGetSymbolAddress); make it before any stream capture. */
+int dort_gpu_render_device_noalloc(dort_scene* scene, const dort_render_params* params,
+                                   float* d_out_rgb, void* stream);
+
 /* ---- wavefront ------------------------------------------------------------
  * No single reference counterpart: the same "pt" estimator as dort_gpu_render
  * (same parameters, same random numbers per pixel and sample, so the same
