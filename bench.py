@@ -565,6 +565,8 @@ def run_dort_pt(args):
                        "rays_per_frame": rays_per_frame,
                        "mrays_per_s": rays_per_frame * args.steps * world / (ms_max / 1e3) / 1e6,
                        "queue_capacity": tuning["queue_capacity"],
+                       "stage_ms_per_frame": {k: round(stages[k], 3) for k in
+                                              ("regen", "extend", "shade", "shadow", "neeb")},
                        "l2": "frame state (queues 1 GB, image 25 MB) larger than L2"},
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 0,
@@ -609,13 +611,146 @@ def run_reference_pt(args):
     print(json.dumps(line), flush=True)
 
 
+# ---- batch workload -----------------------------------------------------------------
+
+BATCH_WORKLOAD = ("batch: 64 seeded jobs, random-triangle soups of 10k-500k tris (log-uniform) "
+                  "with one quad light, resolution 64-1024 per axis (log-uniform), spp 16-512, "
+                  "depth 8-16, one wavefront launch (one CUDA graph) for all jobs")
+
+
+def run_dort_batch(args):
+    import torch
+    import dort_b200 as db
+    from dort_b200 import scenes
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    t0 = time.time()
+    specs = scenes.batch_jobs(count=64, seed=4 + 1000 * rank)
+    jobs = []
+    for k, (sd, w, h, spp, depth) in enumerate(specs):
+        sc = db.scene_from_dict(sd)
+        jobs.append((sc, db.render_params(sd["camera"], w, h, spp, max_depth=depth, seed=k)))
+    samples = sum(w * h * spp for (_, w, h, spp, _) in specs)
+    log(f"[rank {rank}] 64 scenes ready in {time.time() - t0:.1f}s, {samples / 1e9:.2f}G samples")
+    b = db.Batch(jobs, {"queue_capacity": 1 << 22})
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        b.render(stream.cuda_stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        b.render(stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(pg)
+    ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
+    clk = clocks.stop()
+    st = b.stats()
+    value = world * samples * args.steps / (ms / 1e3)
+    # the plain per-pixel megakernel, one launch per job
+    outs = [torch.empty(p.width * p.height * 3, dtype=torch.float32, device="cuda")
+            for _, p in jobs]
+    for (sc, p), o in zip(jobs, outs):
+        sc.render_device(p, o.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for (sc, p), o in zip(jobs, outs):
+        sc.render_device(p, o.data_ptr(), stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    mega_ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
+    if rank == 0:
+        line = {
+            "metric": "batched samples/s, wavefront batch vs per-job megakernel", "value": value,
+            "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": BATCH_WORKLOAD, "jobs": len(jobs), "samples": samples,
+                       "megakernel_samples_per_s": world * samples / (mega_ms / 1e3),
+                       "batch_over_megakernel": (mega_ms / (ms / args.steps)),
+                       "rays_per_batch": st["rays"], "waves": st["waves"]},
+            "roofline": None, "cpu_baseline": None,
+            "e2e": None, "gpu_launches": args.steps * int(st["waves"] * 6 + 2), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+# ---- adjoint workload ---------------------------------------------------------------
+
+ADJ_WORKLOAD = ("adjoint: 512x512, 64 spp, depth 6, 500k random tris with per-triangle RGB "
+                "albedo U(0.1,0.9) and 8 emissive tris; L2 loss vs a seeded target; forward "
+                "render + path-replay backward for albedo and emission gradients")
+
+
+def run_dort_adjoint(args):
+    import torch
+    import dort_b200 as db
+    from dort_b200 import scenes
+
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    sd = scenes.adjoint_scene()
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], 512, 512, 64, max_depth=6, seed=1 + rank)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    rng = np.random.default_rng(9)
+    target = sc.adjoint_forward(p, np.clip(alb * rng.uniform(0.8, 1.2, alb.shape), 0, 1)
+                                .astype(np.float32), em)
+
+    def step():
+        img = sc.adjoint_forward(p, alb, em)
+        loss, g = db.loss_l2(img, target)
+        return sc.adjoint_backward(p, g, alb, em)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
+    dt = max_over_ranks(pg, time.perf_counter() - t0)
+    clk = clocks.stop()
+    if rank == 0:
+        ms = dt / args.steps * 1e3
+        line = {
+            "metric": "adjoint ms (forward + backward, host arrays)", "value": ms, "unit": "ms",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": ADJ_WORKLOAD, "tris": int(len(sd["tris"]))},
+            "roofline": None, "cpu_baseline": None,
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": int(2 * alb.nbytes * 2 +
+                                                                          512 * 512 * 12 * 2),
+                    "d2h_bytes_per_step": int(alb.nbytes * 2 + 512 * 512 * 12)},
+            "gpu_launches": args.steps * 4, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    sc.close()
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=0, help="timed steps (default: 5 for pt1080p, 100 for raycast)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dort", choices=["dort", "reference"])
-    ap.add_argument("--workload", default="pt1080p", choices=["pt1080p", "raycast"])
+    ap.add_argument("--workload", default="pt1080p",
+                    choices=["pt1080p", "raycast", "batch", "adjoint"])
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
@@ -623,17 +758,24 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.steps <= 0:
-        args.steps = 5 if args.workload == "pt1080p" else 100
+        args.steps = {"pt1080p": 5, "raycast": 100, "batch": 2, "adjoint": 5}[args.workload]
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return
-        if args.workload == "pt1080p":
+        if args.workload in ("raycast",):
+            run_reference(args)
+        elif args.workload == "pt1080p":
             run_reference_pt(args)
         else:
-            run_reference(args)
+            print(json.dumps({"impl": "reference", "unavailable":
+                              f"the reference has no {args.workload} renderer"}), flush=True)
         return
     if args.workload == "pt1080p":
         run_dort_pt(args)
+    elif args.workload == "batch":
+        run_dort_batch(args)
+    elif args.workload == "adjoint":
+        run_dort_adjoint(args)
     else:
         run_dort(args)
 

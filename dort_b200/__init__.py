@@ -247,6 +247,46 @@ def host_check_render(d: dict, params: _abi.RenderParams, rows=None):
     return out
 
 
+class Batch:
+    """Many frames rendered by one wavefront (dort_gpu_batch_*).  jobs is a
+    list of (Scene, RenderParams); the scenes must outlive the batch."""
+
+    def __init__(self, jobs, tuning: dict | None = None):
+        arr = (_abi.BatchJob * len(jobs))()
+        for i, (sc, p) in enumerate(jobs):
+            arr[i].scene = sc.handle
+            arr[i].params = p
+        self._scenes = [sc for sc, _ in jobs]
+        self._params = [p for _, p in jobs]
+        t = wavefront_tuning(**tuning) if tuning else None
+        h = ctypes.c_void_p()
+        _abi.check(_abi.lib().dort_gpu_batch_create(arr, len(jobs), ctypes.byref(t) if t else None,
+                                                    ctypes.byref(h)))
+        self.handle = h
+
+    def render(self, stream: int = 0):
+        _abi.check(_abi.lib().dort_gpu_batch_render(self.handle, ctypes.c_void_p(stream)))
+
+    def image(self, job: int):
+        p = self._params[job]
+        out = np.zeros((p.height, p.width, 3), np.float32)
+        _abi.check(_abi.lib().dort_gpu_batch_image(self.handle, job, _ptr(out)))
+        return out
+
+    def stats(self) -> dict:
+        out = (ctypes.c_double * 4)()
+        _abi.check(_abi.lib().dort_gpu_batch_stats(self.handle, out))
+        return {"rays": out[0], "waves": out[1], "error": out[2], "samples": out[3]}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _abi.lib().dort_gpu_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
 def loss_l2(image, target):
     """dort_gpu_loss_l2: (sum (image - target)^2, its image gradient)."""
     a = np.ascontiguousarray(image, np.float32)

@@ -9,7 +9,9 @@ import ctypes
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "libdort_gpu.so")
+# DORT_GPU_LIBRARY selects another build of the same library (e.g. an
+# installed copy); the default is the in-tree build.
+LIB_PATH = os.environ.get("DORT_GPU_LIBRARY") or os.path.join(PKG, "libdort_gpu.so")
 
 c_u32 = ctypes.c_uint32
 c_i32 = ctypes.c_int
@@ -68,6 +70,10 @@ class RenderParams(ctypes.Structure):
 class WavefrontTuning(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
                 ("shade_block", c_u32), ("reserved", c_u32 * 4)]
+
+
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", c_p), ("params", RenderParams)]
 
 
 class DortError(RuntimeError):
@@ -139,6 +145,19 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_render_device_noalloc.restype = c_i32
         L.dort_gpu_render_device_noalloc.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p,
                                                      c_p]
+        L.dort_gpu_batch_create.restype = c_i32
+        L.dort_gpu_batch_create.argtypes = [ctypes.POINTER(BatchJob), c_u32,
+                                            ctypes.POINTER(WavefrontTuning), ctypes.POINTER(c_p)]
+        L.dort_gpu_batch_render.restype = c_i32
+        L.dort_gpu_batch_render.argtypes = [c_p, c_p]
+        L.dort_gpu_batch_image.restype = c_i32
+        L.dort_gpu_batch_image.argtypes = [c_p, c_u32, c_p]
+        L.dort_gpu_batch_image_device.restype = c_i32
+        L.dort_gpu_batch_image_device.argtypes = [c_p, c_u32, ctypes.POINTER(c_p)]
+        L.dort_gpu_batch_stats.restype = c_i32
+        L.dort_gpu_batch_stats.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_batch_destroy.restype = c_i32
+        L.dort_gpu_batch_destroy.argtypes = [c_p]
         _lib = L
     return _lib
 

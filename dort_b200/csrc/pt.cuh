@@ -627,9 +627,9 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
       // A background light counts only if the ray escapes, so whether anything
       // is hit is all that matters: an any-hit query gives the same answer.
       Hit h = l.kind == LIGHT_TRI
-          ? trace_ray<false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
+          ? trace_ray<false, false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
                              INFINITY)
-          : trace_ray<true>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
+          : trace_ray<true, false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
                             INFINITY);
       rays += 1;
       V3 L = v3(0.f, 0.f, 0.f);
@@ -661,7 +661,7 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
     if(!(ls.pdf == 0.f || is_black(ls.L))) {
       V3 f = bsdf_eval(m, g.frame, ls.wi, wo, req);
       if(!is_black(f)) {
-        Hit h = trace_ray<true>(sc.trace, ls.o.x, ls.o.y, ls.o.z, ls.tmin, ls.d.x, ls.d.y,
+        Hit h = trace_ray<true, false>(sc.trace, ls.o.x, ls.o.y, ls.o.z, ls.tmin, ls.d.x, ls.d.y,
                                 ls.d.z, ls.tmax);
         rays += 1;
         if(h.prim == kMiss) {
@@ -693,7 +693,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
   bool last_delta = false;
   const uint32_t req_nd = F_ALL & ~F_DELTA;
   for(;;) {
-    Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, tmin, d.x, d.y, d.z, INFINITY);
+    Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, tmin, d.x, d.y, d.z, INFINITY);
     res.rays += 1;
     bool hit = h.prim != kMiss;
     SurfaceHit g;

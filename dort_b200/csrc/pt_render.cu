@@ -417,3 +417,118 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
   }
   return rc;
 }
+
+// ---- batches ------------------------------------------------------------------
+
+struct dort_batch {
+  dort_gpu::WavefrontBatch* impl = nullptr;
+  uint64_t total_samples = 0;
+};
+
+extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_count,
+                                     const dort_wavefront_tuning* tuning,
+                                     dort_batch** out_batch) {
+  clear_error();
+  if(!jobs || !out_batch || job_count == 0) { return fail(DORT_ERR_INVALID, "null argument"); }
+  if(job_count > 65536) { return fail(DORT_ERR_INVALID, "job_count exceeds 65536"); }
+  *out_batch = nullptr;
+  std::vector<PtScene> scenes(job_count);
+  std::vector<PtParams> params(job_count);
+  uint64_t total = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  for(uint32_t j = 0; j < job_count; ++j) {
+    if(!jobs[j].scene) { return fail(DORT_ERR_INVALID, "job " + std::to_string(j) + ": null scene"); }
+    if(jobs[j].scene->device != dev) {
+      return fail(DORT_ERR_INVALID, "job " + std::to_string(j) + ": scene on another device");
+    }
+    std::string err;
+    if(!make_params(&jobs[j].params, params[j], err)) {
+      return fail(DORT_ERR_INVALID, "job " + std::to_string(j) + ": " + err);
+    }
+    if(params[j].sample_all_lights) {
+      return fail(DORT_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": sample_all_lights");
+    }
+    scenes[j] = jobs[j].scene->pt;
+    total += uint64_t(params[j].width) * params[j].height * params[j].spp;
+  }
+  WfTuning tn;
+  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 22));
+  tn.trace_block = 128;
+  tn.shade_block = 128;
+  tn.pad = 0;
+  if(tuning) {
+    if(tuning->struct_size != sizeof(dort_wavefront_tuning)) {
+      return fail(DORT_ERR_INVALID, "dort_wavefront_tuning.struct_size mismatch (ABI version)");
+    }
+    if(tuning->queue_capacity) { tn.capacity = tuning->queue_capacity; }
+    if(tuning->trace_block) { tn.trace_block = tuning->trace_block; }
+    if(tuning->shade_block) { tn.shade_block = tuning->shade_block; }
+  }
+  tn.capacity = (tn.capacity + 31u) & ~31u;
+  if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
+    return fail(DORT_ERR_INVALID, "queue_capacity must be 32..2^26");
+  }
+  for(uint32_t b : {tn.trace_block, tn.shade_block}) {
+    if(b < 32 || b > 1024 || b % 32 != 0) {
+      return fail(DORT_ERR_INVALID, "block sizes must be multiples of 32 in 32..1024");
+    }
+  }
+  auto* batch = new dort_batch();
+  int rc = wavefront_batch_create(scenes.data(), params.data(), job_count, tn, &batch->impl);
+  if(rc != DORT_OK) {
+    delete batch;
+    return rc;
+  }
+  batch->total_samples = total;
+  *out_batch = batch;
+  return DORT_OK;
+}
+
+extern "C" int dort_gpu_batch_render(dort_batch* batch, void* stream) {
+  clear_error();
+  if(!batch) { return fail(DORT_ERR_INVALID, "null argument"); }
+  return wavefront_batch_render(batch->impl, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int dort_gpu_batch_image_device(dort_batch* batch, uint32_t job,
+                                           const float** out_d_rgb) {
+  clear_error();
+  if(!batch || !out_d_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  uint32_t npix = 0;
+  return wavefront_batch_image(batch->impl, job, out_d_rgb, &npix);
+}
+
+extern "C" int dort_gpu_batch_image(dort_batch* batch, uint32_t job, float* out_rgb) {
+  clear_error();
+  if(!batch || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
+  const float* d = nullptr;
+  uint32_t npix = 0;
+  int rc = wavefront_batch_image(batch->impl, job, &d, &npix);
+  if(rc != DORT_OK) { return rc; }
+  DG_CUDA(cudaMemcpy(out_rgb, d, size_t(npix) * 3 * sizeof(float), cudaMemcpyDeviceToHost));
+  return DORT_OK;
+}
+
+extern "C" int dort_gpu_batch_stats(dort_batch* batch, double out[4]) {
+  clear_error();
+  if(!batch || !out) { return fail(DORT_ERR_INVALID, "null argument"); }
+  DG_CUDA(cudaDeviceSynchronize());
+  uint64_t rays = 0;
+  uint32_t waves = 0, error = 0;
+  int rc = wavefront_batch_counters(batch->impl, &rays, &waves, &error, 0);
+  if(rc != DORT_OK) { return rc; }
+  out[0] = double(rays);
+  out[1] = double(waves);
+  out[2] = double(error);
+  out[3] = double(batch->total_samples);
+  return DORT_OK;
+}
+
+extern "C" int dort_gpu_batch_destroy(dort_batch* batch) {
+  clear_error();
+  if(!batch) { return DORT_OK; }
+  wavefront_batch_destroy(batch->impl);
+  delete batch;
+  return DORT_OK;
+}

@@ -39,6 +39,9 @@
 #define DG_LDG(p) __ldg(p)
 #define DG_AS_FLOAT(u) __uint_as_float(u)
 #define DG_AS_UINT(f) __float_as_uint(f)
+#define DG_BYTE_F(w, j) __uint2float_rn(((w) >> (8 * (j))) & 0xffu)
+#define DG_FMA(a, b, c) fmaf(a, b, c)
+#define DG_RCP_FAST(a) __frcp_rn(a)
 #else
 namespace dort_gpu {
 inline float host_as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
@@ -55,6 +58,9 @@ inline uint32_t host_as_uint(float f) { uint32_t u; std::memcpy(&u, &f, 4); retu
 #define DG_LDG(p) (*(p))
 #define DG_AS_FLOAT(u) ::dort_gpu::host_as_float(u)
 #define DG_AS_UINT(f) ::dort_gpu::host_as_uint(f)
+#define DG_BYTE_F(w, j) (float(((w) >> (8 * (j))) & 0xffu))
+#define DG_FMA(a, b, c) std::fma(a, b, c)
+#define DG_RCP_FAST(a) (1.f / (a))
 #endif
 #define DG_HD __host__ __device__ __forceinline__
 
@@ -105,8 +111,38 @@ DG_HD bool mt_exact(float4 a, float4 e1, float4 e2,
   return true;
 }
 
+// Byte j of w as a float: on the device the byte is placed in the mantissa of
+// 2^23 with one byte permute and the 2^23 is subtracted (exact), which keeps
+// the conversions off the multi-function unit.
+// Moller-Trumbore with fused multiply-adds, for the path tracers (which need
+// the reference's estimator, not its rounding).
+DG_HD bool mt_fast(float4 a, float4 e1, float4 e2, float ox, float oy, float oz,
+                   float dx, float dy, float dz, float t_min, float t_max,
+                   float& out_t, float& out_b1, float& out_b2) {
+  float s1x = DG_FMA(dy, e2.z, -dz * e2.y);
+  float s1y = DG_FMA(dz, e2.x, -dx * e2.z);
+  float s1z = DG_FMA(dx, e2.y, -dy * e2.x);
+  float det = DG_FMA(s1x, e1.x, DG_FMA(s1y, e1.y, s1z * e1.z));
+  if(det == 0.f) { return false; }
+  float inv_det = DG_RCP_FAST(det);
+  float sx = ox - a.x, sy = oy - a.y, sz = oz - a.z;
+  float b1 = inv_det * DG_FMA(s1x, sx, DG_FMA(s1y, sy, s1z * sz));
+  if(b1 < 0.f || b1 > 1.f) { return false; }
+  float s2x = DG_FMA(sy, e1.z, -sz * e1.y);
+  float s2y = DG_FMA(sz, e1.x, -sx * e1.z);
+  float s2z = DG_FMA(sx, e1.y, -sy * e1.x);
+  float b2 = inv_det * DG_FMA(s2x, dx, DG_FMA(s2y, dy, s2z * dz));
+  if(b2 < 0.f || b1 + b2 > 1.f) { return false; }
+  float t = inv_det * DG_FMA(s2x, e2.x, DG_FMA(s2y, e2.y, s2z * e2.z));
+  if(t < t_min || t > t_max) { return false; }
+  out_t = t;
+  out_b1 = b1;
+  out_b2 = b2;
+  return true;
+}
+
 DG_HD float byte_to_float(uint32_t w, int j) {
-  return DG_U2F((w >> (8 * j)) & 0xffu);
+  return DG_BYTE_F(w, j);
 }
 
 // Widening factor for the slab test: 2^-20 relative (> 8 ulp).
@@ -169,7 +205,7 @@ DG_HD uint32_t node_hitmask(
 // Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
 // triangle found to intersect.  `steps` (optional) counts node visits and
 // triangle tests.
-template<bool ANY_HIT>
+template<bool ANY_HIT, bool EXACT_MT = true>
 DG_HD Hit trace_ray(const TraceScene& sc,
                                          float ox, float oy, float oz, float t_min,
                                          float dx, float dy, float dz, float t_max) {
@@ -226,7 +262,10 @@ DG_HD Hit trace_ray(const TraceScene& sc,
       const float4* tp = sc.tris + 3 * size_t(n1.y + b);
       float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
       float t, b1, b2;
-      if(mt_exact(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2)) {
+      bool h = EXACT_MT
+          ? mt_exact(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2)
+          : mt_fast(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2);
+      if(h) {
         uint32_t id = DG_AS_UINT(a.w);
         if(ANY_HIT) {
           best.t = t; best.b1 = b1; best.b2 = b2; best.prim = id;

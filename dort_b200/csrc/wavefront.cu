@@ -43,10 +43,16 @@ enum : uint32_t {
   C_SHADOW = 4, C_NEEB = 5,    // this wave's shadow / BSDF-strategy queues
   C_LIVE = 6, C_WAVES = 7, C_ERROR = 8,
   C_F_EXT = 9, C_F_SHADE = 10, C_F_SH = 11, C_F_NB = 12,   // work-fetch cursors
+  C_KQ0 = 20,       // [20..25]: lengths of the shade queues by material kind
   C_NEXT_LO = 16,   // 64-bit next-sample counter at [16..17]
   C_RAYS_LO = 18,   // 64-bit ray counter at [18..19]
   C_COUNT = 32
 };
+
+// Shade queues: paths are sorted by what they hit (material kind 0..4, or a
+// miss) so that the warps of the shade stage run one BSDF's code.
+constexpr uint32_t kShadeQueues = 6;
+constexpr uint32_t kMissQueue = 5;
 
 DG_HD uint32_t f2u(float f) { return DG_AS_UINT(f); }
 DG_HD float u2f(uint32_t u) { return DG_AS_FLOAT(u); }
@@ -70,31 +76,37 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor) {
   return __shfl_sync(0xffffffffu, base, 0);
 }
 
-// Maps a global sample id to (pixel, x, y, sample): sample-major order, 8x4
-// pixel tiles, so consecutive ids are coherent primary rays.
-__device__ __forceinline__ void sample_to_pixel(const PtParams& pp, uint64_t sid,
-                                                uint32_t& pixel, uint32_t& x, uint32_t& y,
-                                                uint32_t& s) {
+// Work is handed out in units of kChunk consecutive samples of one pixel:
+// the path slot that takes a unit traces its samples one after the other and
+// adds their sum to the film once.  Unit ids run chunk-major over 8x4 pixel
+// tiles, so consecutive units are neighbouring pixels (coherent primary rays).
+constexpr uint32_t kChunk = 4;
+
+__device__ __forceinline__ void unit_to_pixel(const PtParams& pp, uint64_t uid, uint32_t& pixel,
+                                              uint32_t& x, uint32_t& y, uint32_t& s0) {
   uint32_t tiles_x = (pp.width + 7) / 8;
   uint32_t tiles = tiles_x * ((pp.height + 3) / 4);
-  uint64_t per_sample = uint64_t(tiles) * 32;
-  s = uint32_t(sid / per_sample);
-  uint32_t local = uint32_t(sid % per_sample);
+  uint64_t per_chunk = uint64_t(tiles) * 32;
+  uint32_t c = uint32_t(uid / per_chunk);
+  uint32_t local = uint32_t(uid % per_chunk);
   uint32_t tile = local / 32, lane = local % 32;
   x = (tile % tiles_x) * 8 + lane % 8;
   y = (tile / tiles_x) * 4 + lane / 8;
   pixel = y * pp.width + x;
+  s0 = c * kChunk;
 }
 
 struct WfDev {
   float4* ray_o;   // o.xyz, t_min
   float4* ray_d;   // d.xyz, -
   float4* thr;     // throughput
-  float4* sum;     // radiance sum
-  uint4* meta;     // pixel, sample, bounces | last_delta << 31, state
+  float4* sum;     // radiance sum of the current path
+  float4* acc;     // kept samples of the slot's unit: sum rgb, count
+  uint4* meta;     // pixel, sample, bounces | last_delta << 31, state | job << 8
   float4* hit;     // t, b1, b2, prim
   uint32_t* active[2];
   uint32_t* finished[2];
+  uint32_t* kq[kShadeQueues];   // shade queues by hit kind
   uint32_t* sh_slot;
   float4* sh_o;    // o.xyz, t_min
   float4* sh_d;    // d.xyz, t_max
@@ -106,8 +118,49 @@ struct WfDev {
   float4* film;    // sum rgb, kept count
   uint32_t* ctr;
   uint32_t capacity;
-  uint64_t total_samples;
+  uint64_t total_samples;   // work units (see kChunk) of all jobs
   uint32_t max_waves;
+};
+
+// Where a path's scene and render parameters come from.  A single frame
+// passes them as kernel arguments; a batch of frames (many scenes, each with
+// its own resolution, spp and depth) reads a device table of jobs, and every
+// path carries its job index in the high bits of meta.w.
+struct SingleJob {
+  static constexpr bool kBatched = false;
+  PtScene sc;
+  PtParams pp;
+  __device__ __forceinline__ uint32_t job_of_sample(uint64_t) const { return 0; }
+  __device__ __forceinline__ uint64_t sample_begin(uint32_t) const { return 0; }
+  __device__ __forceinline__ const PtScene& scene(uint32_t) const { return sc; }
+  __device__ __forceinline__ const PtParams& params(uint32_t) const { return pp; }
+  __device__ __forceinline__ uint32_t film_offset(uint32_t) const { return 0; }
+};
+
+struct WfJob {
+  PtScene sc;
+  PtParams pp;
+  uint64_t sample_begin;   // first global work-unit id of the job
+  uint32_t film_offset;    // first pixel of the job in the batch film
+  uint32_t pad;
+};
+
+struct JobTable {
+  static constexpr bool kBatched = true;
+  const WfJob* jobs;
+  uint32_t count;
+  __device__ __forceinline__ uint32_t job_of_sample(uint64_t sid) const {
+    uint32_t lo = 0, hi = count;         // last job with sample_begin <= sid
+    while(lo + 1 < hi) {
+      uint32_t mid = (lo + hi) / 2;
+      if(jobs[mid].sample_begin <= sid) { lo = mid; } else { hi = mid; }
+    }
+    return lo;
+  }
+  __device__ __forceinline__ uint64_t sample_begin(uint32_t j) const { return jobs[j].sample_begin; }
+  __device__ __forceinline__ const PtScene& scene(uint32_t j) const { return jobs[j].sc; }
+  __device__ __forceinline__ const PtParams& params(uint32_t j) const { return jobs[j].pp; }
+  __device__ __forceinline__ uint32_t film_offset(uint32_t j) const { return jobs[j].film_offset; }
 };
 
 __device__ __forceinline__ uint32_t wave_of(const WfDev& w) {
@@ -128,81 +181,128 @@ __global__ void wf_init(WfDev w, uint32_t npix) {
   }
 }
 
-// Finished paths of the last wave go to the film; their slots (and, in the
-// first wave, every slot) take the next samples and join this wave's active
-// queue behind the paths that continue.
-__global__ void wf_regen(PtScene sc, PtParams pp, WfDev w) {
-  const uint32_t wave = wave_of(w);
-  const uint32_t cur = wave & 1u;
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_FIN0 + cur);
-  const uint32_t* fin = w.finished[cur];
-  uint32_t* act = w.active[cur];
+// Starts sample s of `pixel` in `slot`: camera ray, unit throughput.
+__device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_t slot,
+                                           uint32_t pixel, uint32_t s) {
+  uint32_t x = pixel % pp.width, y = pixel / pp.width;
+  float fx, fy;
+  if(s == 0) {
+    fx = float(x) + 0.5f;
+    fy = float(y) + 0.5f;
+  } else {
+    Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
+    fx = float(x) + j.a;
+    fy = float(y) + j.b;
+  }
+  V3 o, d;
+  camera_ray(pp, fx, fy, o, d);
+  w.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
+  w.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.f);
+  w.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+  w.sum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+// Builds this wave's active queue.  It walks the previous wave's active queue
+// in order: continuing paths stay; a finished path's sample joins its slot's
+// unit sum and the slot starts the unit's next sample in the same place, or,
+// when the unit is done, adds the unit to the film and takes a new unit.  Then
+// it walks the free list (every slot in the first wave; slots whose unit fell
+// outside the image later).  Keeping the queue order keeps neighbouring
+// pixels' primary rays next to each other whatever order the shade stage ran
+// the paths in.
+template<class J>
+__device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32_t slot,
+                                           uint32_t cur, bool from_free) {
   uint64_t* next = reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
-  uint32_t stride = gridDim.x * blockDim.x;
-  uint32_t n_pad = (n + 31u) & ~31u;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_pad; i += stride) {
-    bool valid = i < n;
-    uint32_t slot = valid ? fin[i] : 0u;
-    uint4 m = valid ? w.meta[slot] : make_uint4(0u, 0u, 0u, SLOT_ACTIVE);
-    if(valid && m.w == SLOT_FINISHED) {
-      float4 s = w.sum[slot];
-      // renderer.cpp:36-41: only finite, non-negative samples reach the film
-      bool keep = isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && s.x >= 0.f &&
-                  s.y >= 0.f && s.z >= 0.f;
-      if(keep) { atomicAdd(w.film + m.x, make_float4(s.x, s.y, s.z, 1.f)); }
+  uint32_t* act = w.active[cur];
+  uint4 m = valid ? w.meta[slot] : make_uint4(0u, 0u, 0u, SLOT_FREE + 7u);
+  bool keep = valid && (m.w & 0xffu) == SLOT_ACTIVE && !from_free;
+  bool started = false;
+  if(valid && (m.w & 0xffu) == SLOT_FINISHED) {
+    const uint32_t job = m.w >> 8;
+    const PtParams& pp = jobs.params(job);
+    float4 s = w.sum[slot];
+    float4 a = w.acc[slot];
+    // renderer.cpp:36-41: only finite, non-negative samples reach the film
+    if(isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && s.x >= 0.f && s.y >= 0.f &&
+       s.z >= 0.f) {
+      a = make_float4(a.x + s.x, a.y + s.y, a.z + s.z, a.w + 1.f);
+    }
+    uint32_t next_s = m.y + 1u;
+    uint32_t unit_end = min(pp.spp, (m.y / kChunk + 1u) * kChunk);
+    if(next_s < unit_end) {
+      w.acc[slot] = a;
+      start_path(w, pp, slot, m.x, next_s);
+      m = make_uint4(m.x, next_s, 0u, SLOT_ACTIVE | (job << 8));
+      started = true;
+    } else {
+      if(a.w > 0.f || a.x != 0.f || a.y != 0.f || a.z != 0.f) {
+        atomicAdd(w.film + jobs.film_offset(job) + m.x, a);
+      }
       atomicSub(w.ctr + C_LIVE, 1u);
       m.w = SLOT_FREE;
     }
-    bool want_new = valid && m.w == SLOT_FREE;
-    uint32_t nmask = __ballot_sync(0xffffffffu, want_new);
-    uint64_t sid = ~0ull;
-    if(want_new) {
-      uint32_t lane = threadIdx.x & 31u, leader = __ffs(nmask) - 1u;
-      unsigned long long base = 0;
-      if(lane == leader) {
-        base = atomicAdd(reinterpret_cast<unsigned long long*>(next),
-                         (unsigned long long)__popc(nmask));
-      }
-      base = __shfl_sync(nmask, base, leader);
-      sid = base + __popc(nmask & ((1u << lane) - 1u));
+  }
+  bool want_new = valid && (m.w & 0xffu) == SLOT_FREE;
+  uint32_t nmask = __ballot_sync(0xffffffffu, want_new);
+  uint64_t uid = ~0ull;
+  if(want_new) {
+    uint32_t lane = threadIdx.x & 31u, leader = __ffs(nmask) - 1u;
+    unsigned long long base = 0;
+    if(lane == leader) {
+      base = atomicAdd(reinterpret_cast<unsigned long long*>(next),
+                       (unsigned long long)__popc(nmask));
     }
-    bool fresh = false;
-    if(want_new && sid < w.total_samples) {
-      uint32_t pixel, x, y, s;
-      sample_to_pixel(pp, sid, pixel, x, y, s);
-      if(x < pp.width && y < pp.height) {
-        float fx, fy;
-        if(s == 0) {
-          fx = float(x) + 0.5f;
-          fy = float(y) + 0.5f;
-        } else {
-          Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
-          fx = float(x) + j.a;
-          fy = float(y) + j.b;
-        }
-        V3 o, d;
-        camera_ray(pp, fx, fy, o, d);
-        w.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
-        w.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.f);
-        w.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
-        w.sum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-        m = make_uint4(pixel, s, 0u, SLOT_ACTIVE);
-        fresh = true;
-      }
+    base = __shfl_sync(nmask, base, leader);
+    uid = base + __popc(nmask & ((1u << lane) - 1u));
+  }
+  if(want_new && uid < w.total_samples) {
+    uint32_t job = jobs.job_of_sample(uid);
+    const PtParams& pp = jobs.params(job);
+    uint32_t pixel, x, y, s0;
+    unit_to_pixel(pp, uid - jobs.sample_begin(job), pixel, x, y, s0);
+    if(x < pp.width && y < pp.height) {
+      w.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+      start_path(w, pp, slot, pixel, s0);
+      m = make_uint4(pixel, s0, 0u, SLOT_ACTIVE | (job << 8));
+      started = true;
+      atomicAdd(w.ctr + C_LIVE, 1u);
     }
-    if(want_new) { w.meta[slot] = m; }
-    if(fresh) { atomicAdd(w.ctr + C_LIVE, 1u); }
-    // a slot whose sample fell outside the image goes back on the next free
-    // list so that it keeps taking samples
-    bool retry = want_new && !fresh && sid < w.total_samples;
-    uint32_t at = warp_append(w.ctr + C_ACT0 + cur, fresh);
-    if(fresh) { act[at] = slot; }
-    uint32_t rt = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), retry);
-    if(retry) { w.finished[cur ^ 1u][rt] = slot; }
+  }
+  if(valid && (started || want_new)) { w.meta[slot] = m; }
+  // a slot whose unit fell outside the image goes on the next free list so
+  // that it keeps taking units
+  bool retry = want_new && !started && uid < w.total_samples;
+  bool put = keep || started;
+  uint32_t at = warp_append(w.ctr + C_ACT0 + cur, put);
+  if(put) { act[at] = slot; }
+  uint32_t rt = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), retry);
+  if(retry) { w.finished[cur ^ 1u][rt] = slot; }
+}
+
+template<class J>
+__global__ void wf_regen(J jobs, WfDev w) {
+  const uint32_t wave = wave_of(w);
+  const uint32_t cur = wave & 1u, prev = cur ^ 1u;
+  const uint32_t n_prev = *(volatile uint32_t*)(w.ctr + C_ACT0 + prev);
+  const uint32_t n_free = *(volatile uint32_t*)(w.ctr + C_FIN0 + cur);
+  const uint32_t* old = w.active[prev];
+  const uint32_t* fre = w.finished[cur];
+  uint32_t stride = gridDim.x * blockDim.x;
+  uint32_t np = (n_prev + 31u) & ~31u;
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+    bool valid = i < n_prev;
+    regen_slot(jobs, w, valid, valid ? old[i] : 0u, cur, false);
+  }
+  uint32_t nf = (n_free + 31u) & ~31u;
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += stride) {
+    bool valid = i < n_free;
+    regen_slot(jobs, w, valid, valid ? fre[i] : 0u, cur, true);
   }
 }
 
-__global__ void wf_extend(PtScene sc, WfDev w) {
+template<class J>
+__global__ void wf_extend(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
   const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
   const uint32_t* act = w.active[cur];
@@ -210,35 +310,62 @@ __global__ void wf_extend(PtScene sc, WfDev w) {
     uint32_t base = warp_fetch(w.ctr + C_F_EXT);
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
+    uint32_t slot = 0, kind = kShadeQueues;
     if(i < n) {
-      uint32_t slot = act[i];
+      slot = act[i];
+      uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
+      const PtScene& sc = jobs.scene(job);
       float4 o = w.ray_o[slot], d = w.ray_d[slot];
-      Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
       w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
+      kind = kMissQueue;
+      if(h.prim != kMiss) {
+        uint32_t mat = f2u(__ldg(&sc.shade[3 * size_t(h.prim)].w));
+        kind = __ldg(&sc.mats[mat].kind);
+      }
+    }
+#pragma unroll
+    for(uint32_t k = 0; k < kShadeQueues; ++k) {
+      bool mine = kind == k;
+      uint32_t at = warp_append(w.ctr + C_KQ0 + k, mine);
+      if(mine) { w.kq[k][at] = slot; }
     }
   }
 }
 
-__global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
+template<class J>
+__global__ void wf_shade(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
-  const uint32_t* act = w.active[cur];
-  uint32_t* act_next = w.active[cur ^ 1u];
-  uint32_t* fin_next = w.finished[cur ^ 1u];
+  uint32_t qn[kShadeQueues];
+  uint32_t n = 0;
+#pragma unroll
+  for(uint32_t k = 0; k < kShadeQueues; ++k) {
+    qn[k] = *(volatile uint32_t*)(w.ctr + C_KQ0 + k);
+    n += qn[k];
+  }
   const uint32_t req_nd = F_ALL & ~F_DELTA;
   for(;;) {
     uint32_t base = warp_fetch(w.ctr + C_F_SHADE);
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     bool valid = i < n;
-    bool push_sh = false, push_nb = false, cont = false, done = false;
-    float4 sh_o, sh_d, sh_c, nb_o, nb_d, nb_f;
+    bool push_sh = false, push_sh2 = false, push_nb = false, cont = false, done = false;
+    float4 sh_o, sh_d, sh_c, sh2_o, sh2_d, sh2_c, nb_o, nb_d, nb_f;
     uint32_t slot = 0;
     if(valid) {
-      slot = act[i];
+      // index i of the concatenated shade queues
+      uint32_t k = 0, off = i;
+#pragma unroll
+      for(uint32_t q = 0; q + 1 < kShadeQueues; ++q) {
+        if(k == q && off >= qn[q]) { off -= qn[q]; k = q + 1; }
+      }
+      slot = w.kq[k][off];
       float4 ro = w.ray_o[slot], rd = w.ray_d[slot];
       float4 t4 = w.thr[slot], s4 = w.sum[slot];
       uint4 m = w.meta[slot];
+      const uint32_t job = m.w >> 8;
+      const PtScene& sc = jobs.scene(job);
+      const PtParams& pp = jobs.params(job);
       float4 h4 = w.hit[slot];
       Hit h;
       h.t = h4.x; h.b1 = h4.y; h.b2 = h4.z; h.prim = f2u(h4.w);
@@ -279,13 +406,33 @@ __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
             if(use_bsdf) {
               BsdfSample bs = bsdf_sample(mt, g.frame, wo, req_nd, r0.b, r0.c, r0.d);
               if(!(bs.pdf == 0.f || is_black(bs.f))) {
-                // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf,
-                // L and w known once the ray is traced
+                // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf
                 V3 fac = thr * (bs.f * (fabsf(dot(g.n, bs.w)) / bs.pdf)) * (1.f / lpdf);
-                push_nb = true;
-                nb_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
-                nb_d = make_float4(bs.w.x, bs.w.y, bs.w.z, bs.pdf);
-                nb_f = make_float4(fac.x, fac.y, fac.z, u2f(li | (use_light ? 0x80000000u : 0u)));
+                if(l.kind == LIGHT_TRI) {
+                  // L and w are known once the closest hit is
+                  push_nb = true;
+                  nb_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
+                  nb_d = make_float4(bs.w.x, bs.w.y, bs.w.z, bs.pdf);
+                  nb_f = make_float4(fac.x, fac.y, fac.z,
+                                     u2f(li | (use_light ? 0x80000000u : 0u)));
+                } else {
+                  // a background light counts only if the ray escapes: L and
+                  // w depend on the direction alone, so the ray is an any-hit
+                  // query with its contribution computed here
+                  V3 L = background_radiance(sc, l, bs.w);
+                  if(!is_black(L)) {
+                    float wgt = 1.f;
+                    if(use_light) {
+                      float lp = light_pivot_pdf(sc, l, bs.w, g.p);
+                      wgt = bs.pdf / (bs.pdf + lp);
+                    }
+                    V3 c = fac * L * wgt;
+                    push_sh2 = true;
+                    sh2_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
+                    sh2_d = make_float4(bs.w.x, bs.w.y, bs.w.z, INFINITY);
+                    sh2_c = make_float4(c.x, c.y, c.z, 0.f);
+                  }
+                }
               }
             }
             if(use_light) {
@@ -335,21 +482,26 @@ __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
       }
       w.sum[slot] = make_float4(sum.x, sum.y, sum.z, 0.f);
       m.z = bounces | (last_delta ? 0x80000000u : 0u);
-      m.w = finished ? SLOT_FINISHED : SLOT_ACTIVE;
+      m.w = (finished ? SLOT_FINISHED : SLOT_ACTIVE) | (job << 8);
       w.meta[slot] = m;
       cont = !finished;
       done = finished;
     }
-    uint32_t ci = warp_append(w.ctr + C_ACT0 + (cur ^ 1u), cont);
-    if(cont) { act_next[ci] = slot; }
-    uint32_t fi = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), done);
-    if(done) { fin_next[fi] = slot; }
+    (void)cont;
+    (void)done;
     uint32_t si = warp_append(w.ctr + C_SHADOW, push_sh);
     if(push_sh) {
       w.sh_slot[si] = slot;
       w.sh_o[si] = sh_o;
       w.sh_d[si] = sh_d;
       w.sh_c[si] = sh_c;
+    }
+    uint32_t si2 = warp_append(w.ctr + C_SHADOW, push_sh2);
+    if(push_sh2) {
+      w.sh_slot[si2] = slot;
+      w.sh_o[si2] = sh2_o;
+      w.sh_d[si2] = sh2_d;
+      w.sh_c[si2] = sh2_c;
     }
     uint32_t ni = warp_append(w.ctr + C_NEEB, push_nb);
     if(push_nb) {
@@ -361,35 +513,45 @@ __global__ void wf_shade(PtScene sc, PtParams pp, WfDev w) {
   }
 }
 
-__global__ void wf_shadow(PtScene sc, WfDev w) {
+template<class J>
+__global__ void wf_shadow(J jobs, WfDev w) {
   const uint32_t n = *(volatile uint32_t*)(w.ctr + C_SHADOW);
   for(;;) {
     uint32_t base = warp_fetch(w.ctr + C_F_SH);
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     if(i < n) {
+      uint32_t slot = w.sh_slot[i];
+      uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
+      const PtScene& sc = jobs.scene(job);
       float4 o = w.sh_o[i], d = w.sh_d[i];
-      Hit h = trace_ray<true>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w);
+      Hit h = trace_ray<true, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w);
       if(h.prim == kMiss) {
-        uint32_t slot = w.sh_slot[i];
+        // a path can own two entries (light and BSDF strategy for a
+        // background light), so the additions are atomic
         float4 c = w.sh_c[i];
-        float4 s = w.sum[slot];
-        w.sum[slot] = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.f);
+        float* sp = &w.sum[slot].x;
+        atomicAdd(sp, c.x);
+        atomicAdd(sp + 1, c.y);
+        atomicAdd(sp + 2, c.z);
       }
     }
   }
 }
 
 __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i);
-#define neeb_one neeb_one_impl
 
-__global__ void wf_neeb(PtScene sc, WfDev w) {
+template<class J>
+__global__ void wf_neeb(J jobs, WfDev w) {
   const uint32_t n = *(volatile uint32_t*)(w.ctr + C_NEEB);
   for(;;) {
     uint32_t base = warp_fetch(w.ctr + C_F_NB);
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
-    if(i < n) { neeb_one(sc, w, i); }
+    if(i < n) {
+      uint32_t job = J::kBatched ? (w.meta[w.nb_slot[i]].w >> 8) : 0u;
+      neeb_one_impl(jobs.scene(job), w, i);
+    }
   }
 }
 
@@ -401,7 +563,7 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
     V3 L = v3(0.f, 0.f, 0.f);
     V3 p = v3(o.x, o.y, o.z), wi = v3(d.x, d.y, d.z);
     if(l.kind == LIGHT_TRI) {
-      Hit h = trace_ray<false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
       if(h.prim != kMiss && h.prim == l.tri) {
         const float4* sh = sc.shade + 3 * size_t(h.prim);
         float4 a = sh[0], b = sh[1], c = sh[2];
@@ -413,7 +575,7 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
       }
     } else {
       // background light: only escaping rays count, an any-hit query decides
-      Hit h = trace_ray<true>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      Hit h = trace_ray<true, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
       if(h.prim == kMiss) { L = background_radiance(sc, l, wi); }
     }
     if(!is_black(L)) {
@@ -436,7 +598,9 @@ __device__ __forceinline__ bool wf_end_wave(WfDev& w) {
   uint32_t a = w.ctr[C_ACT0 + cur], s = w.ctr[C_SHADOW], b = w.ctr[C_NEEB];
   unsigned long long* rays = reinterpret_cast<unsigned long long*>(w.ctr + C_RAYS_LO);
   *rays += (unsigned long long)a + s + b;
-  w.ctr[C_ACT0 + cur] = 0u;     // consumed; the next wave fills the other buffer
+  // this wave's active queue stays for the next regen; the lists this wave's
+  // regen read are consumed
+  w.ctr[C_ACT0 + (cur ^ 1u)] = 0u;
   w.ctr[C_FIN0 + cur] = 0u;
   w.ctr[C_SHADOW] = 0u;
   w.ctr[C_NEEB] = 0u;
@@ -444,6 +608,7 @@ __device__ __forceinline__ bool wf_end_wave(WfDev& w) {
   w.ctr[C_F_SHADE] = 0u;
   w.ctr[C_F_SH] = 0u;
   w.ctr[C_F_NB] = 0u;
+  for(uint32_t k = 0; k < kShadeQueues; ++k) { w.ctr[C_KQ0 + k] = 0u; }
   w.ctr[C_WAVES] = wave + 1u;
   uint64_t next = *reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
   bool more = w.ctr[C_LIVE] > 0u || next < w.total_samples;
@@ -483,6 +648,7 @@ struct Wavefront {
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   PtParams pp_cached{};
+  const void* jobs_cached = nullptr;
   WfTuning tune_cached{};
   bool valid = false;
 };
@@ -507,8 +673,9 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t Q = capacity;
   size_t f4 = al(Q * sizeof(float4)), u4 = al(Q * sizeof(uint4)), u1 = al(Q * sizeof(uint32_t));
-  size_t bytes = 4 * f4 + u4 + f4 /*hit*/ + 4 * u1 /*active, finished*/ + u1 +
-                 3 * f4 /*shadow*/ + u1 + 3 * f4 /*neeb*/ +
+  size_t f4x2 = al(2 * Q * sizeof(float4)), u1x2 = al(2 * Q * sizeof(uint32_t));
+  size_t bytes = 5 * f4 + u4 + f4 /*hit*/ + (4 + kShadeQueues) * u1 /*queues*/ + u1x2 +
+                 3 * f4x2 /*shadow, two per path*/ + u1 + 3 * f4 /*neeb*/ +
                  al(size_t(npix) * sizeof(float4)) + al(C_COUNT * 4);
   if(cudaMalloc(&wf->mem, bytes) != cudaSuccess) {
     cudaGetLastError();
@@ -522,16 +689,18 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.ray_d = reinterpret_cast<float4*>(take(f4));
   d.thr = reinterpret_cast<float4*>(take(f4));
   d.sum = reinterpret_cast<float4*>(take(f4));
+  d.acc = reinterpret_cast<float4*>(take(f4));
   d.meta = reinterpret_cast<uint4*>(take(u4));
   d.hit = reinterpret_cast<float4*>(take(f4));
   d.active[0] = reinterpret_cast<uint32_t*>(take(u1));
   d.active[1] = reinterpret_cast<uint32_t*>(take(u1));
   d.finished[0] = reinterpret_cast<uint32_t*>(take(u1));
   d.finished[1] = reinterpret_cast<uint32_t*>(take(u1));
-  d.sh_slot = reinterpret_cast<uint32_t*>(take(u1));
-  d.sh_o = reinterpret_cast<float4*>(take(f4));
-  d.sh_d = reinterpret_cast<float4*>(take(f4));
-  d.sh_c = reinterpret_cast<float4*>(take(f4));
+  for(uint32_t k = 0; k < kShadeQueues; ++k) { d.kq[k] = reinterpret_cast<uint32_t*>(take(u1)); }
+  d.sh_slot = reinterpret_cast<uint32_t*>(take(u1x2));
+  d.sh_o = reinterpret_cast<float4*>(take(f4x2));
+  d.sh_d = reinterpret_cast<float4*>(take(f4x2));
+  d.sh_c = reinterpret_cast<float4*>(take(f4x2));
   d.nb_slot = reinterpret_cast<uint32_t*>(take(u1));
   d.nb_o = reinterpret_cast<float4*>(take(f4));
   d.nb_d = reinterpret_cast<float4*>(take(f4));
@@ -553,14 +722,41 @@ static int grid_for(const void* kernel, int block) {
   return sms * std::max(per_sm, 1);
 }
 
-static int wf_build_graph(Wavefront* wf, const PtScene& sc, const PtParams& pp,
-                          const WfTuning& tn) {
+struct WfGrids {
+  int regen, ext, sha, shw, nb;
+};
+
+template<class J>
+static WfGrids wf_grids(const WfTuning& tn) {
+  WfGrids g;
+  g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), 256);
+  g.ext = grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
+  g.sha = grid_for(reinterpret_cast<const void*>(&wf_shade<J>), int(tn.shade_block));
+  g.shw = grid_for(reinterpret_cast<const void*>(&wf_shadow<J>), int(tn.trace_block));
+  g.nb = grid_for(reinterpret_cast<const void*>(&wf_neeb<J>), int(tn.trace_block));
+  return g;
+}
+
+template<class J>
+static void wf_launch_wave(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
+                           cudaStream_t st) {
+  int bt = int(tn.trace_block), bs = int(tn.shade_block);
+  wf_regen<J><<<g.regen, 256, 0, st>>>(jobs, dev);
+  wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
+  wf_shade<J><<<g.sha, bs, 0, st>>>(jobs, dev);
+  wf_shadow<J><<<g.shw, bt, 0, st>>>(jobs, dev);
+  wf_neeb<J><<<g.nb, bt, 0, st>>>(jobs, dev);
+}
+
+template<class J>
+static int wf_build_graph(Wavefront* wf, const J& jobs, const WfTuning& tn) {
   if(!wf->capture_stream) {
     DG_CUDA(cudaStreamCreateWithFlags(&wf->capture_stream, cudaStreamNonBlocking));
   }
   cudaStream_t st = wf->capture_stream;
   if(wf->exec) { cudaGraphExecDestroy(wf->exec); wf->exec = nullptr; }
   if(wf->graph) { cudaGraphDestroy(wf->graph); wf->graph = nullptr; }
+  wf->valid = false;
   DG_CUDA(cudaGraphCreate(&wf->graph, 0));
   cudaGraphConditionalHandle handle;
   DG_CUDA(cudaGraphConditionalHandleCreate(&handle, wf->graph, 1, cudaGraphCondAssignDefault));
@@ -572,21 +768,10 @@ static int wf_build_graph(Wavefront* wf, const PtScene& sc, const PtParams& pp,
   cudaGraphNode_t cnode;
   DG_CUDA(cudaGraphAddNode(&cnode, wf->graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-
-  int b_trace = int(tn.trace_block), b_shade = int(tn.shade_block);
-  int g_regen = grid_for(reinterpret_cast<const void*>(&wf_regen), 256);
-  int g_ext = grid_for(reinterpret_cast<const void*>(&wf_extend), b_trace);
-  int g_sha = grid_for(reinterpret_cast<const void*>(&wf_shade), b_shade);
-  int g_shw = grid_for(reinterpret_cast<const void*>(&wf_shadow), b_trace);
-  int g_nb = grid_for(reinterpret_cast<const void*>(&wf_neeb), b_trace);
-
+  WfGrids g = wf_grids<J>(tn);
   DG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
-  wf_regen<<<g_regen, 256, 0, st>>>(sc, pp, wf->dev);
-  wf_extend<<<g_ext, b_trace, 0, st>>>(sc, wf->dev);
-  wf_shade<<<g_sha, b_shade, 0, st>>>(sc, pp, wf->dev);
-  wf_shadow<<<g_shw, b_trace, 0, st>>>(sc, wf->dev);
-  wf_neeb<<<g_nb, b_trace, 0, st>>>(sc, wf->dev);
+  wf_launch_wave<J>(jobs, wf->dev, tn, g, st);
   wf_control<<<1, 1, 0, st>>>(wf->dev, handle);
   cudaGraph_t captured = nullptr;
   cudaError_t ce = cudaStreamEndCapture(st, &captured);
@@ -594,14 +779,24 @@ static int wf_build_graph(Wavefront* wf, const PtScene& sc, const PtParams& pp,
     return fail(DORT_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(ce));
   }
   DG_CUDA(cudaGraphInstantiate(&wf->exec, wf->graph, 0));
-  wf->pp_cached = pp;
   wf->tune_cached = tn;
   wf->valid = true;
   return DORT_OK;
 }
 
-static bool same_params(const PtParams& a, const PtParams& b) {
-  return std::memcmp(&a, &b, sizeof(PtParams)) == 0;
+static uint32_t wave_bound(uint64_t total_units, uint32_t capacity, uint32_t max_depth) {
+  // each slot runs at most ceil(units / capacity) + 1 units of kChunk samples
+  // of at most max_depth + 2 waves each
+  return uint32_t(std::min<uint64_t>(
+      0x7fffffffull, (total_units / std::max(1u, capacity) + 2) * kChunk *
+                     (uint64_t(max_depth) + 3) + 64));
+}
+
+// Work units of a frame (kChunk samples of one pixel each, padded to whole
+// 8x4 tiles).
+static uint64_t padded_samples(const PtParams& pp) {
+  uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  return tiles * 32 * ((pp.spp + kChunk - 1) / kChunk);
 }
 
 int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
@@ -611,15 +806,16 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   uint32_t npix = pp.width * pp.height;
   int rc = wf_alloc(wf, tn.capacity, npix);
   if(rc != DORT_OK) { return rc; }
-  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  wf->dev.total_samples = uint64_t(tiles) * 32 * pp.spp;
-  wf->dev.max_waves = uint32_t(std::min<uint64_t>(
-      0x7fffffffull, (wf->dev.total_samples / std::max(1u, tn.capacity) + 2) *
-                     (uint64_t(pp.max_depth) + 3) + 64));
-  if(!wf->valid || !same_params(wf->pp_cached, pp) ||
+  wf->dev.total_samples = padded_samples(pp);
+  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth);
+  if(!wf->valid || wf->jobs_cached != nullptr ||
+     std::memcmp(&wf->pp_cached, &pp, sizeof(PtParams)) != 0 ||
      std::memcmp(&wf->tune_cached, &tn, sizeof(WfTuning)) != 0) {
-    rc = wf_build_graph(wf, s->pt, pp, tn);
+    SingleJob jobs{s->pt, pp};
+    rc = wf_build_graph(wf, jobs, tn);
     if(rc != DORT_OK) { return rc; }
+    wf->pp_cached = pp;
+    wf->jobs_cached = nullptr;
   }
   // the graph holds the kernel arguments, including total_samples and max_waves
   wf_init<<<(std::max(tn.capacity, npix) + 255) / 256, 256, 0, st>>>(wf->dev, npix);
@@ -643,18 +839,11 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   uint32_t npix = pp.width * pp.height;
   int rc = wf_alloc(wf, tn.capacity, npix);
   if(rc != DORT_OK) { return rc; }
-  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  wf->dev.total_samples = uint64_t(tiles) * 32 * pp.spp;
-  wf->dev.max_waves = uint32_t(std::min<uint64_t>(
-      0x7fffffffull, (wf->dev.total_samples / std::max(1u, tn.capacity) + 2) *
-                     (uint64_t(pp.max_depth) + 3) + 64));
-  const PtScene& sc = s->pt;
-  int b_trace = int(tn.trace_block), b_shade = int(tn.shade_block);
-  int g_regen = grid_for(reinterpret_cast<const void*>(&wf_regen), 256);
-  int g_ext = grid_for(reinterpret_cast<const void*>(&wf_extend), b_trace);
-  int g_sha = grid_for(reinterpret_cast<const void*>(&wf_shade), b_shade);
-  int g_shw = grid_for(reinterpret_cast<const void*>(&wf_shadow), b_trace);
-  int g_nb = grid_for(reinterpret_cast<const void*>(&wf_neeb), b_trace);
+  wf->dev.total_samples = padded_samples(pp);
+  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth);
+  SingleJob jobs{s->pt, pp};
+  WfGrids g = wf_grids<SingleJob>(tn);
+  int bt = int(tn.trace_block), bs = int(tn.shade_block);
   uint32_t* more = nullptr;
   DG_CUDA(cudaMallocHost(&more, sizeof(uint32_t)));
   cudaEvent_t ev[6];
@@ -664,15 +853,15 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   bool ok = cudaGetLastError() == cudaSuccess;
   for(uint32_t wave = 0; ok && wave < wf->dev.max_waves + 1; ++wave) {
     cudaEventRecord(ev[0], st);
-    wf_regen<<<g_regen, 256, 0, st>>>(sc, pp, wf->dev);
+    wf_regen<SingleJob><<<g.regen, 256, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[1], st);
-    wf_extend<<<g_ext, b_trace, 0, st>>>(sc, wf->dev);
+    wf_extend<SingleJob><<<g.ext, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[2], st);
-    wf_shade<<<g_sha, b_shade, 0, st>>>(sc, pp, wf->dev);
+    wf_shade<SingleJob><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[3], st);
-    wf_shadow<<<g_shw, b_trace, 0, st>>>(sc, wf->dev);
+    wf_shadow<SingleJob><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[4], st);
-    wf_neeb<<<g_nb, b_trace, 0, st>>>(sc, wf->dev);
+    wf_neeb<SingleJob><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);
     wf_control_host<<<1, 1, 0, st>>>(wf->dev, more);
     ok = cudaStreamSynchronize(st) == cudaSuccess;
@@ -690,6 +879,8 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   for(auto& e : ev) { cudaEventDestroy(e); }
   cudaFreeHost(more);
   ms[5] = 0.0;
+  // the graph cache no longer matches the queues' state; rebuild next time
+  wf->valid = false;
   if(!ok) {
     return fail(DORT_ERR_CUDA, std::string("staged wavefront failed: ") +
                                cudaGetErrorString(cudaGetLastError()));
@@ -697,16 +888,134 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   return DORT_OK;
 }
 
-int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
-                       cudaStream_t st) {
-  if(!s->wavefront || !s->wavefront->mem) { return fail(DORT_ERR_INVALID, "no wavefront state"); }
+int wavefront_counters_of(Wavefront* wf, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                          cudaStream_t st) {
+  if(!wf || !wf->mem) { return fail(DORT_ERR_INVALID, "no wavefront state"); }
   uint32_t c[C_COUNT];
-  DG_CUDA(cudaMemcpyAsync(c, s->wavefront->dev.ctr, sizeof(c), cudaMemcpyDeviceToHost, st));
+  DG_CUDA(cudaMemcpyAsync(c, wf->dev.ctr, sizeof(c), cudaMemcpyDeviceToHost, st));
   DG_CUDA(cudaStreamSynchronize(st));
   *rays = uint64_t(c[C_RAYS_LO]) | (uint64_t(c[C_RAYS_LO + 1]) << 32);
   *waves = c[C_WAVES];
   *error = c[C_ERROR];
   return DORT_OK;
+}
+
+int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                       cudaStream_t st) {
+  return wavefront_counters_of(s->wavefront, rays, waves, error, st);
+}
+
+// ---- batches of frames ------------------------------------------------------------
+
+__global__ void wf_resolve_batch(WfDev w, const WfJob* jobs, uint32_t job_count,
+                                 uint32_t total_pix, float* __restrict__ out) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if(p >= total_pix) { return; }
+  float4 a = w.film[p];
+  float inv = a.w != 0.f ? 1.f / a.w : 0.f;
+  out[3 * size_t(p)] = a.w != 0.f ? a.x * inv : 0.f;
+  out[3 * size_t(p) + 1] = a.w != 0.f ? a.y * inv : 0.f;
+  out[3 * size_t(p) + 2] = a.w != 0.f ? a.z * inv : 0.f;
+  (void)jobs;
+  (void)job_count;
+}
+
+struct WavefrontBatch {
+  Wavefront wf;
+  WfJob* d_jobs = nullptr;
+  float* d_images = nullptr;
+  uint32_t job_count = 0;
+  uint32_t total_pix = 0;
+  uint64_t total_samples = 0;
+  uint32_t max_depth = 0;
+  WfTuning tn{};
+  std::vector<uint32_t> film_offset;
+  std::vector<uint32_t> npix;
+};
+
+void wavefront_batch_destroy(WavefrontBatch* b) {
+  if(!b) { return; }
+  wf_release(&b->wf);
+  if(b->d_jobs) { cudaFree(b->d_jobs); }
+  if(b->d_images) { cudaFree(b->d_images); }
+  delete b;
+}
+
+int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32_t n,
+                           const WfTuning& tn, WavefrontBatch** out) {
+  auto* b = new WavefrontBatch();
+  std::vector<WfJob> jobs(n);
+  uint64_t sample = 0;
+  uint32_t pix = 0;
+  for(uint32_t j = 0; j < n; ++j) {
+    std::memset(&jobs[j], 0, sizeof(WfJob));
+    jobs[j].sc = scenes[j];
+    jobs[j].pp = params[j];
+    jobs[j].sample_begin = sample;
+    jobs[j].film_offset = pix;
+    b->film_offset.push_back(pix);
+    b->npix.push_back(params[j].width * params[j].height);
+    sample += padded_samples(params[j]);
+    uint64_t np = uint64_t(pix) + uint64_t(params[j].width) * params[j].height;
+    if(np > 0x7fffffffull) {
+      delete b;
+      return fail(DORT_ERR_INVALID, "batch exceeds 2^31 pixels");
+    }
+    pix = uint32_t(np);
+    b->max_depth = std::max(b->max_depth, params[j].max_depth);
+  }
+  b->job_count = n;
+  b->total_pix = pix;
+  b->total_samples = sample;
+  b->tn = tn;
+  int rc = wf_alloc(&b->wf, tn.capacity, pix);
+  if(rc == DORT_OK && (cudaMalloc(&b->d_jobs, n * sizeof(WfJob)) != cudaSuccess ||
+                       cudaMalloc(&b->d_images, size_t(pix) * 3 * sizeof(float)) != cudaSuccess)) {
+    cudaGetLastError();
+    rc = fail(DORT_ERR_OOM, "cudaMalloc for the batch failed");
+  }
+  if(rc == DORT_OK &&
+     cudaMemcpy(b->d_jobs, jobs.data(), n * sizeof(WfJob), cudaMemcpyHostToDevice) != cudaSuccess) {
+    rc = fail(DORT_ERR_CUDA, "copy of the batch job table failed");
+  }
+  if(rc == DORT_OK) {
+    b->wf.dev.total_samples = b->total_samples;
+    b->wf.dev.max_waves = wave_bound(b->total_samples, tn.capacity, b->max_depth);
+    JobTable table{b->d_jobs, n};
+    rc = wf_build_graph(&b->wf, table, tn);
+    b->wf.jobs_cached = b->d_jobs;
+  }
+  if(rc != DORT_OK) {
+    wavefront_batch_destroy(b);
+    return rc;
+  }
+  *out = b;
+  return DORT_OK;
+}
+
+int wavefront_batch_render(WavefrontBatch* b, cudaStream_t st) {
+  Wavefront* wf = &b->wf;
+  wf_init<<<(std::max(wf->capacity, b->total_pix) + 255) / 256, 256, 0, st>>>(wf->dev,
+                                                                              b->total_pix);
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaGraphLaunch(wf->exec, st));
+  wf_resolve_batch<<<(b->total_pix + 255) / 256, 256, 0, st>>>(wf->dev, b->d_jobs,
+                                                               b->job_count, b->total_pix,
+                                                               b->d_images);
+  DG_CUDA(cudaGetLastError());
+  return DORT_OK;
+}
+
+int wavefront_batch_image(WavefrontBatch* b, uint32_t job, const float** d_rgb, uint32_t* npix) {
+  if(job >= b->job_count) { return fail(DORT_ERR_INVALID, "job index out of range"); }
+  *d_rgb = b->d_images + 3 * size_t(b->film_offset[job]);
+  *npix = b->npix[job];
+  return DORT_OK;
+}
+
+int wavefront_batch_counters(WavefrontBatch* b, uint64_t* rays, uint32_t* waves,
+                             uint32_t* error, cudaStream_t st) {
+  return wavefront_counters_of(&b->wf, rays, waves, error, st);
 }
 
 }  // namespace dort_gpu

@@ -1,6 +1,7 @@
 // Wavefront path tracer (wavefront.cu): host-side entry points.
 #pragma once
 #include <cstdint>
+#include <vector>
 
 #include "pt_scene.h"
 
@@ -21,6 +22,14 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
                      cudaStream_t st);
 int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
                           float* d_out, cudaStream_t st, double ms[6]);
+struct WavefrontBatch;
+int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32_t n,
+                           const WfTuning& tn, WavefrontBatch** out);
+void wavefront_batch_destroy(WavefrontBatch* b);
+int wavefront_batch_render(WavefrontBatch* b, cudaStream_t st);
+int wavefront_batch_image(WavefrontBatch* b, uint32_t job, const float** d_rgb, uint32_t* npix);
+int wavefront_batch_counters(WavefrontBatch* b, uint64_t* rays, uint32_t* waves,
+                             uint32_t* error, cudaStream_t st);
 int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
                        cudaStream_t st);
 

@@ -524,3 +524,43 @@ def adjoint_scene(n_tris: int = 500_000, seed: int = 5):
     return {"verts": verts, "tris": tris, "tri_material": tri_mat, "materials": mats,
             "tri_emission": emission, "tri_albedo": tri_albedo,
             "lights": np.arange(n_tris, n, dtype=np.int64), "camera": cam}
+
+
+def soup_with_light(n_tris: int, seed: int):
+    """A random-triangle soup (the ray-cast generator) with Lambert albedo
+    0.6 and one 2-triangle quad light above it, facing down (the batched
+    workload's scene)."""
+    verts, tris = random_triangles(n_tris, seed=seed, sigma=0.02)
+    base = len(verts)
+    L = np.array([[0.7, 1.4, 0.3], [0.7, 1.4, 0.7], [0.3, 1.4, 0.7], [0.3, 1.4, 0.3]], np.float32)
+    verts = np.concatenate([verts, L]).astype(np.float32)
+    # (2,1,0), (3,2,0) as the Cornell light: cross(e2, e1) points down
+    lt = np.array([[base + 2, base + 1, base], [base + 3, base + 2, base]], np.uint32)
+    tris = np.concatenate([tris, lt]).astype(np.uint32)
+    em = np.zeros((len(tris), 3), np.float32)
+    em[-2:] = (12.0, 11.0, 10.0)
+    tm = np.zeros(len(tris), np.uint32)
+    tm[-2:] = 1
+    mats = [{"kind": 0, "color": (0.6, 0.6, 0.6)}, {"kind": 0, "color": (0.0, 0.0, 0.0)}]
+    cam = look_at_camera((0.5, 0.8, -1.3), (0.5, 0.45, 0.5), (0.0, 1.0, 0.0), 0.9)
+    return {"verts": verts, "tris": tris, "tri_material": tm, "materials": mats,
+            "tri_emission": em, "camera": cam}
+
+
+def batch_jobs(count: int = 64, seed: int = 4, min_tris: int = 10_000, max_tris: int = 500_000,
+               min_res: int = 64, max_res: int = 1024, min_spp: int = 16, max_spp: int = 512,
+               min_depth: int = 8, max_depth: int = 16):
+    """The batched workload: `count` seeded jobs, job k a soup_with_light of
+    log-uniform triangle count (seed 4 + k), resolution log-uniform per axis,
+    spp uniform in [min_spp, max_spp], depth uniform in [min_depth,
+    max_depth].  Returns a list of (scene dict, width, height, spp, depth)."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(count):
+        n = int(np.exp(rng.uniform(np.log(min_tris), np.log(max_tris))))
+        w = int(np.exp(rng.uniform(np.log(min_res), np.log(max_res))))
+        h = int(np.exp(rng.uniform(np.log(min_res), np.log(max_res))))
+        spp = int(rng.integers(min_spp, max_spp + 1))
+        depth = int(rng.integers(min_depth, max_depth + 1))
+        jobs.append((soup_with_light(n, seed + k), w, h, spp, depth))
+    return jobs

@@ -258,6 +258,32 @@ int dort_gpu_render_wavefront_device(dort_scene* scene, const dort_render_params
                                      const dort_wavefront_tuning* tuning, float* d_out_rgb,
                                      void* stream);
 
+/* Batched rendering: many frames -- different scenes, resolutions, spp and
+ * depths -- rendered together by one wavefront (one CUDA graph launch): the
+ * path queues mix samples of all jobs, so short jobs do not leave the GPU
+ * idle.  A batch snapshots each job's scene (which must stay alive and on the
+ * current device) and parameters when it is created; it owns its queues,
+ * film and images until destroyed.  sample_all_lights is not supported. */
+typedef struct dort_batch_job {
+  dort_scene* scene;
+  dort_render_params params;
+} dort_batch_job;
+
+typedef struct dort_batch dort_batch;
+
+int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_count,
+                          const dort_wavefront_tuning* tuning, dort_batch** out_batch);
+/* Renders every job (asynchronous on `stream`). */
+int dort_gpu_batch_render(dort_batch* batch, void* stream);
+/* Copies job `job`'s image (width * height * 3 floats) to host memory (waits). */
+int dort_gpu_batch_image(dort_batch* batch, uint32_t job, float* out_rgb);
+/* Device pointer of job `job`'s image inside the batch. */
+int dort_gpu_batch_image_device(dort_batch* batch, uint32_t job, const float** out_d_rgb);
+/* out[0] = rays traced, out[1] = waves, out[2] = 1 if the wave bound was hit,
+ * out[3] = total samples (waits for the last render). */
+int dort_gpu_batch_stats(dort_batch* batch, double out[4]);
+int dort_gpu_batch_destroy(dort_batch* batch);
+
 /* Measurement entry: renders the same frame wave by wave from the host
  * (without the graph) with CUDA events around each stage; out_ms[0..4] =
  * total milliseconds of regen, extend, shade, shadow, neeb; out_ms[5] = waves;
