@@ -11,11 +11,20 @@ import ctypes
 import numpy as np
 
 from . import _abi
-from ._abi import (DortError, MISS, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_LAMBERT,
-                   MAT_MIRROR, MAT_PHONG)
+from ._abi import (CAMERA_ORTHO, CAMERA_PINHOLE, CAMERA_THIN_LENS, DortError, LIGHT_DIRECTIONAL,
+                   LIGHT_POINT, MISS, MAT_CONDUCTOR, MAT_DIELECTRIC, MAT_LAMBERT, MAT_MIRROR,
+                   MAT_OREN_NAYAR, MAT_PHONG, SHAPE_CUBE, SHAPE_CYLINDER, SHAPE_DISK,
+                   SHAPE_SPHERE)
 
 __all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
-           "MAT_LAMBERT", "MAT_MIRROR", "MAT_DIELECTRIC", "MAT_PHONG", "MAT_CONDUCTOR"]
+           "MAT_LAMBERT", "MAT_MIRROR", "MAT_DIELECTRIC", "MAT_PHONG", "MAT_CONDUCTOR",
+           "MAT_OREN_NAYAR", "SHAPE_SPHERE", "SHAPE_DISK", "SHAPE_CUBE", "SHAPE_CYLINDER",
+           "LIGHT_POINT", "LIGHT_DIRECTIONAL", "CAMERA_PINHOLE", "CAMERA_ORTHO",
+           "CAMERA_THIN_LENS"]
+
+# optional scene-dict keys passed through to scene_desc
+SCENE_KEYS = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
+              "sky_scale", "sky_up", "sky_fwd", "shapes", "lights")
 
 
 def _ptr(a):
@@ -40,7 +49,10 @@ class _DescHolder:
 def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None,
                sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
                sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
-               bvh_width: int = 8, **_ignored) -> _DescHolder:
+               bvh_width: int = 8, shapes=None, lights=None, **_ignored) -> _DescHolder:
+    """SceneDesc for the arrays given.  `shapes`: dicts with kind (SHAPE_*),
+    material, param (up to 4), to_world (3x4) and emission (RGB); `lights`:
+    dicts with kind (LIGHT_POINT / LIGHT_DIRECTIONAL), rgb and vec."""
     h = _DescHolder()
     d = h.desc
     verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
@@ -72,6 +84,32 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
     d.sky_up = (ctypes.c_float * 3)(*sky_up)
     d.sky_fwd = (ctypes.c_float * 3)(*sky_fwd)
     d.bvh_width = bvh_width
+    if shapes:
+        arr = (_abi.Shape * len(shapes))()
+        for i, sh in enumerate(shapes):
+            arr[i].kind = sh["kind"]
+            arr[i].material = sh.get("material", 0)
+            p = list(sh.get("param", ())) + [0.0] * 4
+            arr[i].param = (ctypes.c_float * 4)(*p[:4])
+            m = np.asarray(sh.get("to_world", np.eye(4)[:3]), np.float64).reshape(-1)[:12]
+            arr[i].to_world = (ctypes.c_float * 12)(*m.tolist())
+            arr[i].emission = (ctypes.c_float * 3)(*sh.get("emission", (0.0, 0.0, 0.0)))
+            if sh.get("light_to_world") is not None:
+                lm = np.asarray(sh["light_to_world"], np.float64).reshape(-1)[:12]
+                arr[i].light_to_world = (ctypes.c_float * 12)(*lm.tolist())
+                arr[i].flags |= _abi.SHAPE_LIGHT_TRANSFORM
+        h.keep.append(arr)
+        d.shapes = ctypes.cast(arr, ctypes.c_void_p)
+        d.shape_count = len(shapes)
+    if lights:
+        arr = (_abi.Light * len(lights))()
+        for i, li in enumerate(lights):
+            arr[i].kind = li["kind"]
+            arr[i].rgb = (ctypes.c_float * 3)(*li["rgb"])
+            arr[i].vec = (ctypes.c_float * 3)(*li["vec"])
+        h.keep.append(arr)
+        d.lights = ctypes.cast(arr, ctypes.c_void_p)
+        d.light_count = len(lights)
     return h
 
 
@@ -214,7 +252,11 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     c.right = (ctypes.c_float * 3)(*camera["right"])
     c.up = (ctypes.c_float * 3)(*camera["up"])
     c.forward = (ctypes.c_float * 3)(*camera["forward"])
-    c.fov = camera["fov"]
+    c.fov = camera.get("fov", 0.0)
+    c.kind = camera.get("kind", _abi.CAMERA_PINHOLE)
+    c.lens_radius = camera.get("lens_radius", 0.0)
+    c.focal_distance = camera.get("focal_distance", 0.0)
+    c.dimension = camera.get("dimension", 0.0)
     return p
 
 
@@ -228,18 +270,15 @@ def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
 
 def scene_from_dict(d: dict, **kw) -> "Scene":
     """Scene from the dict form used by dort_b200.scenes generators."""
-    keys = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
-            "sky_scale", "sky_up", "sky_fwd")
-    args = {k: d[k] for k in keys if k in d and d[k] is not None}
+    args = {k: d[k] for k in SCENE_KEYS if k in d and d[k] is not None}
     args.update(kw)
     return Scene(d["verts"], d["tris"], **args)
 
 
 def host_check_render(d: dict, params: _abi.RenderParams, rows=None):
     """Runs the device path sampler compiled for the host (diagnostic)."""
-    keys = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
-            "sky_scale", "sky_up", "sky_fwd")
-    h = scene_desc(d["verts"], d["tris"], **{k: d[k] for k in keys if k in d and d[k] is not None})
+    h = scene_desc(d["verts"], d["tris"],
+                   **{k: d[k] for k in SCENE_KEYS if k in d and d[k] is not None})
     out = np.zeros((params.height, params.width, 3), np.float32)
     r0, r1 = rows if rows else (0, params.height)
     _abi.check(_abi.lib().dort_gpu_host_check_render(ctypes.byref(h.desc), ctypes.byref(params),

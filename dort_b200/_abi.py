@@ -26,12 +26,27 @@ STATUS_NAMES = {
 }
 MISS = 0xFFFFFFFF
 
-MAT_LAMBERT, MAT_MIRROR, MAT_DIELECTRIC, MAT_PHONG, MAT_CONDUCTOR = range(5)
+MAT_LAMBERT, MAT_MIRROR, MAT_DIELECTRIC, MAT_PHONG, MAT_CONDUCTOR, MAT_OREN_NAYAR = range(6)
+SHAPE_SPHERE, SHAPE_DISK, SHAPE_CUBE, SHAPE_CYLINDER = 1, 2, 3, 4
+SHAPE_LIGHT_TRANSFORM = 1
+LIGHT_POINT, LIGHT_DIRECTIONAL = 1, 2
+CAMERA_PINHOLE, CAMERA_ORTHO, CAMERA_THIN_LENS = 0, 1, 2
+ABI_VERSION = 2
 
 
 class Material(ctypes.Structure):
     _fields_ = [("kind", c_u32), ("color", c_f * 3), ("color2", c_f * 3),
                 ("param", c_f * 4)]
+
+
+class Shape(ctypes.Structure):
+    _fields_ = [("kind", c_u32), ("material", c_u32), ("param", c_f * 4),
+                ("to_world", c_f * 12), ("emission", c_f * 3), ("flags", c_u32),
+                ("light_to_world", c_f * 12)]
+
+
+class Light(ctypes.Structure):
+    _fields_ = [("kind", c_u32), ("rgb", c_f * 3), ("vec", c_f * 3), ("reserved", c_u32)]
 
 
 class SceneDesc(ctypes.Structure):
@@ -48,13 +63,18 @@ class SceneDesc(ctypes.Structure):
         ("sky_up", c_f * 3),
         ("sky_fwd", c_f * 3),
         ("bvh_width", c_u32),
-        ("reserved", c_u32 * 7),
+        ("shape_count", c_u32),
+        ("shapes", c_p),
+        ("lights", c_p),
+        ("light_count", c_u32),
+        ("reserved", c_u32 * 5),
     ]
 
 
 class Camera(ctypes.Structure):
     _fields_ = [("origin", c_f * 3), ("right", c_f * 3), ("up", c_f * 3),
-                ("forward", c_f * 3), ("fov", c_f)]
+                ("forward", c_f * 3), ("fov", c_f), ("kind", c_u32),
+                ("lens_radius", c_f), ("focal_distance", c_f), ("dimension", c_f)]
 
 
 class RenderParams(ctypes.Structure):
@@ -98,6 +118,9 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_last_error.restype = ctypes.c_char_p
         L.dort_gpu_last_error.argtypes = []
         L.dort_gpu_abi_version.restype = c_i32
+        if L.dort_gpu_abi_version() != ABI_VERSION:
+            raise RuntimeError(f"{LIB_PATH} has ABI version {L.dort_gpu_abi_version()}, "
+                               f"expected {ABI_VERSION}: rebuild it")
         L.dort_gpu_scene_create.restype = c_i32
         L.dort_gpu_scene_create.argtypes = [ctypes.POINTER(SceneDesc), ctypes.POINTER(c_p)]
         L.dort_gpu_scene_destroy.restype = c_i32

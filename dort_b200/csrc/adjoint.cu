@@ -46,10 +46,11 @@ struct AdjointTape {
   float* d_albedo;
   float* d_emission;
   const float* tri_emission;
+  uint32_t tri_count;   // prims at or above it are analytic shapes (no gradient)
 
   DG_HD void emission(uint32_t tri, V3 thr, V3 Le) {
     acc = acc + thr * Le;
-    if(d_emission && !is_black(Le)) {
+    if(d_emission && !is_black(Le) && tri < tri_count) {
       float* g = d_emission + 3 * size_t(tri);
       ADJ_ADD(g, adj.x * thr.x);
       ADJ_ADD(g + 1, adj.y * thr.y);
@@ -58,7 +59,7 @@ struct AdjointTape {
   }
   DG_HD void background(V3 c) { acc = acc + c; }
   DG_HD void vertex(uint32_t tri, const DevMaterial& m) {
-    if(!d_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags) { return; }
+    if(!d_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags || tri >= tri_count) { return; }
     V3 rem = L - acc;
     float* g = d_albedo + 3 * size_t(tri);
     if(m.c[0] > 0.f) { ADJ_ADD(g, adj.x * rem.x / m.c[0]); }
@@ -123,6 +124,7 @@ adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
     tape.d_albedo = d_albedo;
     tape.d_emission = d_emission;
     tape.tri_emission = sc.tri_emission;
+    tape.tri_count = sc.shape_base;
     pt_sample(sc, pp, pixel, s, fx, fy, tape);
   }
 }

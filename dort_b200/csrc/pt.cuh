@@ -7,13 +7,20 @@
 //     material in scope adds -- LambertBrdf (lambert_material.cpp:5-35),
 //     MirrorBrdf (mirror_material.cpp:5-29), DielectricBxdf
 //     (dielectric_material.cpp:32-116, fresnel.cpp:5-47), PhongBrdf
-//     (phong_material.cpp:6-106) and a GGX conductor built on the reference's
-//     GGX distribution (microfacet.cpp:19-86; the conductor itself has no
-//     reference counterpart);
-//   - lights: DiffuseLight on a triangle (diffuse_light.cpp:40-111,
-//     shape.cpp:4-26, triangle.cpp:62-80), InfiniteLight
-//     (infinite_light.cpp:5-65), EnvironmentLight (environment_light.cpp);
-//   - camera: PinholeCamera::sample_ray_importance (pinhole_camera.cpp:13-31);
+//     (phong_material.cpp:6-106), OrenNayarBrdf (oren_nayar_material.cpp:5-72)
+//     and a GGX conductor built on the reference's GGX distribution
+//     (microfacet.cpp:19-86; the conductor itself has no reference
+//     counterpart);
+//   - geometry: the triangle BVH (trace.cuh) plus analytic shapes
+//     (shapes.cuh);
+//   - lights: DiffuseLight on a triangle, sphere or disk (diffuse_light.cpp:40-111,
+//     shape.cpp:4-26, triangle.cpp:62-80, sphere_shape.cpp:74-121),
+//     PointLight (point_light.cpp:19-31), DirectionalLight
+//     (directional_light.cpp:28-42), InfiniteLight (infinite_light.cpp:5-65),
+//     EnvironmentLight (environment_light.cpp);
+//   - cameras: PinholeCamera, OrthoCamera and ThinLensCamera
+//     ::sample_ray_importance (pinhole_camera.cpp:13-31, ortho_camera.cpp:13-26,
+//     thin_lens_camera.cpp:15-33);
 //   - light choice: DiscreteDistrib1d over approximate powers
 //     (discrete_distrib_1d.cpp, scene.cpp:20-28).
 // Random numbers come from Philox keyed by (seed, pixel, sample, block); see
@@ -24,70 +31,10 @@
 #include "philox.cuh"
 #include "pt_scene.h"
 #include "trace.cuh"
+#include "pt_math.cuh"
+#include "shapes.cuh"
 
 namespace dort_gpu {
-
-constexpr float kPi = 3.14159265358979323846f;
-constexpr float kInvPi = 0.31830988618379067154f;
-constexpr float kTwoPi = 6.28318530717958647692f;
-constexpr float kInvTwoPi = 0.15915494309189533577f;
-constexpr float kInvFourPi = 0.07957747154594766788f;
-
-struct V3 { float x, y, z; };
-DG_HD V3 v3(float x, float y, float z) { V3 r; r.x = x; r.y = y; r.z = z; return r; }
-DG_HD V3 v3p(const float* p) { return v3(p[0], p[1], p[2]); }
-DG_HD V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-DG_HD V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-DG_HD V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
-DG_HD V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-DG_HD V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
-DG_HD V3 operator*(V3 a, V3 b) { return v3(a.x * b.x, a.y * b.y, a.z * b.z); }
-DG_HD float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-DG_HD V3 cross(V3 a, V3 b) {
-  return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
-}
-DG_HD float length_sq(V3 a) { return dot(a, a); }
-DG_HD float length(V3 a) { return sqrtf(length_sq(a)); }
-DG_HD V3 normalize(V3 a) { return a * (1.f / length(a)); }
-DG_HD bool is_black(V3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
-DG_HD float average(V3 a) { return (1.f / 3.f) * (a.x + a.y + a.z); }
-DG_HD float sq(float a) { return a * a; }
-DG_HD float clampf(float v, float lo, float hi) { return v > hi ? hi : (v < lo ? lo : v); }
-
-// geometry.cpp:4-11
-DG_HD void coordinate_system(V3 v0, V3& v1, V3& v2) {
-  if(fabsf(v0.x) > fabsf(v0.y)) {
-    v1 = normalize(v3(-v0.z, 0.f, v0.x));
-  } else {
-    v1 = normalize(v3(0.f, -v0.z, v0.y));
-  }
-  v2 = cross(v0, v1);
-}
-
-// monte_carlo.cpp
-DG_HD V3 cosine_hemisphere_sample(float u1, float u2) {
-  float r = sqrtf(u1);
-  float th = kTwoPi * u2;
-  float x = cosf(th) * r, y = sinf(th) * r;
-  float z = sqrtf(fmaxf(0.f, 1.f - x * x - y * y));
-  return v3(x, y, z);
-}
-DG_HD float cosine_hemisphere_pdf(float cos_theta) { return fabsf(cos_theta * kInvPi); }
-DG_HD V3 uniform_sphere_sample(float u1, float u2) {
-  float z = 1.f - 2.f * u1;
-  float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-  float phi = kTwoPi * u2;
-  return v3(cosf(phi) * r, sinf(phi) * r, z);
-}
-DG_HD V3 power_cosine_hemisphere_sample(float u1, float u2, float e) {
-  float phi = kTwoPi * u1;
-  float ct = powf(u2, 1.f / (1.f + e));
-  float st = sqrtf(1.f - ct * ct);
-  return v3(cosf(phi) * st, sinf(phi) * st, ct);
-}
-DG_HD float power_cosine_hemisphere_pdf(float ct, float e) {
-  return (e + 1.f) * powf(ct, e) * kInvTwoPi;
-}
 
 // ---- BSDF -------------------------------------------------------------------
 
@@ -163,6 +110,29 @@ DG_HD float conductor_pdf(const DevMaterial& m, V3 wi, V3 wo) {
   return ggx_d(h, m.p0) * fabsf(h.z) / (4.f * dwo);
 }
 
+// OrenNayarBrdf::eval_f (oren_nayar_material.cpp:5-38); m.p0 = sigma^2 terms
+// A and B precomputed as p1, p2.
+DG_HD V3 oren_nayar_f(const DevMaterial& m, V3 wi, V3 wo) {
+  float ci = fabsf(wi.z), co = fabsf(wo.z);
+  if(ci == 0.f || co == 0.f) { return v3(0.f, 0.f, 0.f); }
+  float a = m.p1, b = m.p2;
+  if(ci >= 0.99f || co >= 0.99f) { return v3p(m.c) * (kInvPi * a); }
+  // Bsdf::sin_theta / sin_phi / cos_phi (bsdf.hpp:220-247)
+  float si = sqrtf(fmaxf(0.f, 1.f - wi.z * wi.z));
+  float so = sqrtf(fmaxf(0.f, 1.f - wo.z * wo.z));
+  float spi = wi.y / si, cpi = wi.x / si, spo = wo.y / so, cpo = wo.x / so;
+  float cos_dphi = cpi * cpo + spi * spo;
+  float sin_alpha, tan_beta;
+  if(ci >= co) {
+    sin_alpha = so;
+    tan_beta = si / ci;
+  } else {
+    sin_alpha = si;
+    tan_beta = so / co;
+  }
+  return v3p(m.c) * (kInvPi * (a + b * fmaxf(0.f, cos_dphi) * sin_alpha * tan_beta));
+}
+
 // Bxdf::eval_f for the resolved BxDF of `m` (local directions).
 DG_HD V3 bxdf_eval(const DevMaterial& m, V3 wi, V3 wo, uint32_t request) {
   switch(m.kind) {
@@ -182,6 +152,8 @@ DG_HD V3 bxdf_eval(const DevMaterial& m, V3 wi, V3 wo, uint32_t request) {
     }
     case DORT_MAT_CONDUCTOR:
       return conductor_f(m, wi, wo);
+    case DORT_MAT_OREN_NAYAR:
+      return oren_nayar_f(m, wi, wo);
     default:
       return v3(0.f, 0.f, 0.f);   // mirror, dielectric: delta only
   }
@@ -209,6 +181,8 @@ DG_HD float bxdf_pdf(const DevMaterial& m, V3 wg, V3 wf, uint32_t request) {
     }
     case DORT_MAT_CONDUCTOR:
       return conductor_pdf(m, wg, wf);
+    case DORT_MAT_OREN_NAYAR:
+      return cosine_hemisphere_pdf(wg.z);
     default:
       return 0.f;
   }
@@ -251,11 +225,21 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
       if(wf.z == 0.f) { return zero; }
       return v3p(m.c) * (1.f / fabsf(wf.z));
     }
+    case DORT_MAT_OREN_NAYAR: {
+      // OrenNayarBrdf::sample_symmetric_f (oren_nayar_material.cpp:40-50)
+      wg = cosine_hemisphere_sample(u, v);
+      pdf = cosine_hemisphere_pdf(wg.z);
+      wg.z = copysignf(wg.z, wf.z);
+      flags = F_REFL | F_DIFF;
+      return oren_nayar_f(m, wf, wg);
+    }
     case DORT_MAT_DIELECTRIC: {
-      // dielectric_material.cpp:33-99 with fix_is_light = false, not thin
+      // dielectric_material.cpp:33-99 with fix_is_light = false; m.p0 =
+      // ior_inside, m.p1 = ior_outside, m.p2 != 0: thin slab; get_iors (:101-111)
       bool s_refl = request & F_REFL, s_trans = request & F_TRANS;
+      bool thin = m.p2 != 0.f;
       float ir, it;
-      if(wf.z >= 0.f) { ir = 1.f; it = m.p0; } else { ir = m.p0; it = 1.f; }
+      if(thin || wf.z >= 0.f) { ir = m.p1; it = m.p0; } else { ir = m.p0; it = m.p1; }
       float cr = fabsf(wf.z);
       V3 w_reflect = v3(-wf.x, -wf.y, wf.z);
       V3 w_trans;
@@ -268,7 +252,8 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
       }
       float ct = fabsf(w_trans.z);
       float fr = fresnel_dielectric(cr, ct, ir, it);
-      float r = fr, t = 1.f - r;
+      float r = thin ? 1.f - sq(1.f - fr) / (1.f - sq(fr)) : fr;
+      float t = 1.f - r;
       bool reflect = uc <= r && s_refl;
       bool transmit = uc > r && s_trans;
       float rp = s_trans ? r : 1.f;
@@ -278,6 +263,11 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
         pdf = rp;
         wg = w_reflect;
         return v3p(m.c) * (r / cr);
+      } else if(transmit && thin) {
+        flags = F_DELTA | F_TRANS;
+        pdf = tp;
+        wg = -wf;
+        return v3p(m.c2) * (t / cr);
       } else if(transmit) {
         flags = F_DELTA | F_TRANS;
         pdf = tp;
@@ -373,16 +363,70 @@ DG_HD float bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo, uint32
 
 // ---- scene access ---------------------------------------------------------------
 
+// Scene::intersect / intersect_p (scene.cpp:8-18) over the flat scene: the
+// triangle BVH, then the analytic shapes (a short list, each tested in its own
+// space against the closest t so far).  A shape hit has prim = shape_base +
+// its index and b1 = the cube face.
+template<bool ANY_HIT>
+DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
+  Hit h = trace_ray<ANY_HIT, false>(sc.trace, o.x, o.y, o.z, t_min, d.x, d.y, d.z, t_max);
+  if(sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
+  float best = h.prim == kMiss ? t_max : h.t;
+  for(uint32_t k = 0; k < sc.shape_count; ++k) {
+    const DevShape& s = sc.shapes[k];
+    V3 ol = xf_point(s.inv, o), dl = xf_vec(s.inv, d);
+    float t;
+    uint32_t face;
+    if(shape_hit<ANY_HIT>(s, ol, dl, t_min, best, t, face)) {
+      h.t = t;
+      h.b1 = float(face);
+      h.b2 = 0.f;
+      h.prim = sc.shape_base + k;
+      if(ANY_HIT) { return h; }
+      best = t;
+    }
+  }
+  return h;
+}
+
+// Material index of a hit primitive.
+DG_HD uint32_t prim_material(const PtScene& sc, uint32_t prim) {
+  if(prim >= sc.shape_base) { return sc.shapes[prim - sc.shape_base].mat; }
+  return DG_AS_UINT(DG_LDG(&sc.shade[3 * size_t(prim)].w));
+}
+
 struct SurfaceHit {
-  V3 p, n;          // point, unit geometric normal (cross(e2, e1))
+  V3 p, n;          // point, unit geometric normal (triangles: cross(e2, e1))
   Frame frame;
-  float eps;        // ray epsilon |1e-3 t|
-  uint32_t tri;
+  float eps;        // ray epsilon (triangles |1e-3 t|)
+  uint32_t tri;     // hit prim (a shape's is >= shape_base)
   uint32_t mat;
   uint32_t light;   // light index + 1, 0 if not emissive
 };
 
-DG_HD SurfaceHit surface_at(const PtScene& sc, const Hit& h) {
+// DiffGeom of an analytic shape hit (the shape's hit, transformed by
+// Transform::apply(DiffGeom), transform.cpp:15-25).  The BSDF frame is any
+// frame around the normal: every BxDF here is isotropic.
+DG_HD SurfaceHit shape_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+  SurfaceHit s;
+  const DevShape& sh = sc.shapes[h.prim - sc.shape_base];
+  V3 ol = xf_point(sh.inv, o), dl = xf_vec(sh.inv, d);
+  V3 pl = ol + dl * h.t;
+  V3 nl = shape_local_normal(sh, pl, uint32_t(h.b1));
+  s.p = xf_point(sh.m, pl);
+  s.n = normalize(xf_normal(sh.inv, nl));
+  s.eps = shape_ray_epsilon(sh, h.t);
+  s.tri = h.prim;
+  s.mat = sh.mat;
+  s.light = sh.light;
+  s.frame.n = s.n;
+  coordinate_system(s.n, s.frame.s, s.frame.t);
+  return s;
+}
+
+// Surface at the closest hit h of the ray (o, d).
+DG_HD SurfaceHit surface_at(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+  if(h.prim >= sc.shape_base) { return shape_surface(sc, h, o, d); }
   SurfaceHit s;
   const float4* sh = sc.shade + 3 * size_t(h.prim);
   float4 a = DG_LDG(sh), b = DG_LDG(sh + 1), c = DG_LDG(sh + 2);
@@ -409,7 +453,7 @@ DG_HD SurfaceHit surface_at(const PtScene& sc, const Hit& h) {
 // Material of a hit, with the optional per-triangle albedo override.
 DG_HD DevMaterial material_at(const PtScene& sc, const SurfaceHit& s) {
   DevMaterial m = sc.mats[s.mat];
-  if(sc.tri_albedo && m.bxdf_flags) {
+  if(sc.tri_albedo && m.bxdf_flags && s.tri < sc.shape_base) {
     const float* a = sc.tri_albedo + 3 * size_t(s.tri);
     m.c[0] = a[0]; m.c[1] = a[1]; m.c[2] = a[2];
     if(m.kind == DORT_MAT_LAMBERT && a[0] == 0.f && a[1] == 0.f && a[2] == 0.f) {
@@ -510,10 +554,22 @@ DG_HD V3 background_radiance(const PtScene& sc, const DevLight& l, V3 dir) {
   return env_radiance_uv(sc.env, du, dv);
 }
 
+DG_HD bool light_is_area(const DevLight& l) { return l.kind == LIGHT_TRI || l.kind == LIGHT_SHAPE; }
+DG_HD bool light_is_background(const DevLight& l) {
+  return l.kind == LIGHT_INFINITE || l.kind == LIGHT_ENV;
+}
+
 // Light::pivot_radiance_pdf
 DG_HD float light_pivot_pdf(const PtScene& sc, const DevLight& l, V3 wi, V3 pivot) {
   if(l.kind == LIGHT_INFINITE) { return kInvFourPi; }
   if(l.kind == LIGHT_ENV) { return env_dir_pdf(sc.env, wi); }
+  if(l.kind == LIGHT_POINT) { return length_sq(v3p(l.p0) - pivot); }   // point_light.cpp:50-52
+  if(l.kind == LIGHT_DIR) { return 1.f; }                              // directional_light.cpp:60-62
+  if(l.kind == LIGHT_SHAPE) {
+    // DiffuseLight::pivot_radiance_pdf (diffuse_light.cpp:104-110), in shape space
+    const DevShape& sh = sc.light_shapes[l.tri];
+    return shape_pivot_pdf(sh, xf_point(sh.inv, pivot), normalize(xf_vec(sh.inv, wi)));
+  }
   // Shape::point_pivot_pdf (shape.cpp:15-26) on the light's triangle
   V3 w = normalize(wi);
   float4 a = make_float4(l.p0[0], l.p0[1], l.p0[2], 0.f);
@@ -558,6 +614,43 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmin = pivot_eps;
     s.tmax = dist - 1e-3f;
     s.L = dot(wi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+  } else if(l.kind == LIGHT_SHAPE) {
+    // DiffuseLight::sample_pivot_radiance (diffuse_light.cpp:40-68): sampled
+    // in shape space, emitting to the side of the shape's normal
+    const DevShape& sh = sc.light_shapes[l.tri];
+    V3 pl = xf_point(sh.inv, pivot);
+    V3 n;
+    float eps;
+    V3 ptl = shape_sample_pivot(sh, pl, u, v, n, s.pdf, eps);
+    V3 swi = normalize(ptl - pl);
+    V3 pt = xf_point(sh.m, ptl);
+    float dist = length(pt - pivot);
+    s.wi = normalize(pt - pivot);
+    s.o = pivot;
+    s.d = (pt - pivot) * (1.f / dist);
+    s.tmin = pivot_eps;
+    s.tmax = dist - eps;
+    s.L = dot(swi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+  } else if(l.kind == LIGHT_POINT) {
+    // PointLight::sample_pivot_radiance (point_light.cpp:19-31)
+    V3 pt = v3p(l.p0);
+    float dist = length(pt - pivot);
+    s.wi = normalize(pt - pivot);
+    s.pdf = length_sq(pt - pivot);
+    s.o = pivot;
+    s.d = (pt - pivot) * (1.f / dist);
+    s.tmin = pivot_eps;
+    s.tmax = dist;
+    s.L = v3p(l.L);
+  } else if(l.kind == LIGHT_DIR) {
+    // DirectionalLight::sample_pivot_radiance (directional_light.cpp:28-42)
+    s.wi = -v3p(l.nn);
+    s.pdf = 1.f;
+    s.o = pivot;
+    s.d = normalize(s.wi);
+    s.tmin = pivot_eps;
+    s.tmax = INFINITY;
+    s.L = v3p(l.L);
   } else {
     V3 wi;
     if(l.kind == LIGHT_INFINITE) {
@@ -600,9 +693,46 @@ struct PathResult {
   uint32_t rays;   // closest-hit + shadow rays traced
 };
 
-DG_HD void camera_ray(const PtParams& pp, float fx, float fy, V3& o, V3& d) {
-  // PinholeCamera::sample_ray_importance (pinhole_camera.cpp:13-31)
+// Radiance that area light `li` sends along a BSDF-strategy ray from p whose
+// closest hit is h: only a hit on the light's own primitive counts
+// (estimate_direct_from_bsdf, path_renderer.cpp:158-166).
+DG_HD V3 area_light_hit_radiance(const PtScene& sc, uint32_t li, const Hit& h, V3 p, V3 wi) {
+  if(h.prim == kMiss) { return v3(0.f, 0.f, 0.f); }
+  SurfaceHit g = surface_at(sc, h, p, wi);
+  if(g.light != li + 1) { return v3(0.f, 0.f, 0.f); }
+  return area_eval_radiance(sc, sc.lights[li], g.p, g.n, p);
+}
+
+// Camera ray of film position (fx, fy) for sample `sample` of `pixel`; the
+// thin lens draws its lens point from the camera block of the sample.
+DG_HD void camera_ray(const PtParams& pp, uint32_t pixel, uint32_t sample, float fx, float fy,
+                      V3& o, V3& d) {
   float w = float(pp.width), h = float(pp.height);
+  if(pp.camera == CAMERA_ORTHO) {
+    // OrthoCamera::sample_ray_importance / get_plane_pos (ortho_camera.cpp:13-26,84-88)
+    float k = pp.ortho_dim / fmaxf(w, h);
+    float px = (fx - 0.5f * w) * k, py = (fy - 0.5f * h) * k;
+    o = v3p(pp.origin) + v3p(pp.right) * px + v3p(pp.up) * py;
+    d = normalize(v3p(pp.forward));
+    return;
+  }
+  if(pp.camera == CAMERA_THIN_LENS) {
+    // ThinLensCamera::sample_ray_importance, get_focus_point, sample_lens_point
+    // (thin_lens_camera.cpp:15-33,100-114)
+    float k = pp.proj_dim / fmaxf(w, h);
+    float px = (fx - 0.5f * w) * k, py = (fy - 0.5f * h) * k;
+    V3 focus = v3(px * pp.focal_distance, py * pp.focal_distance, pp.focal_distance);
+    Rand4 r = rand4(pp.seed, pixel, sample, kBlockCamera);
+    float lx, ly;
+    uniform_disk_sample(r.c, r.d, lx, ly);
+    V3 R = v3p(pp.right), U = v3p(pp.up), F = v3p(pp.forward), O = v3p(pp.origin);
+    V3 wf = O + R * focus.x + U * focus.y + F * focus.z;
+    V3 wl = O + R * (lx * pp.lens_radius) + U * (ly * pp.lens_radius);
+    o = wl;
+    d = normalize(wf - wl);
+    return;
+  }
+  // PinholeCamera::sample_ray_importance (pinhole_camera.cpp:13-31)
   float cx = fx / w - 0.5f, cy = fy / h - 0.5f;
   float nx, ny;
   if(w > h) { nx = cx; ny = cy * h / w; } else { nx = cx * w / h; ny = cy; }
@@ -613,12 +743,14 @@ DG_HD void camera_ray(const PtParams& pp, float fx, float fy, V3& o, V3& d) {
 }
 
 // Direct lighting from one light (estimate_direct, path_renderer.cpp:135-206).
-DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& l,
+DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, uint32_t li,
                          const SurfaceHit& g, const DevMaterial& m, V3 wo,
                          float u_bsdf, float v_bsdf, float c_bsdf, float u_l, float v_l,
                          uint32_t& rays) {
   const uint32_t req = F_ALL & ~F_DELTA;
-  bool use_bsdf = pp.strategy != 2;   // area and background lights only; no delta lights
+  const DevLight& l = sc.lights[li];
+  // the BSDF strategy only for area and background lights (:138-140)
+  bool use_bsdf = pp.strategy != 2 && (light_is_area(l) || light_is_background(l));
   bool use_light = pp.strategy != 1;
   V3 sum = v3(0.f, 0.f, 0.f);
   if(use_bsdf) {
@@ -626,24 +758,14 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
     if(!(bs.pdf == 0.f || is_black(bs.f))) {
       // A background light counts only if the ray escapes, so whether anything
       // is hit is all that matters: an any-hit query gives the same answer.
-      Hit h = l.kind == LIGHT_TRI
-          ? trace_ray<false, false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
-                             INFINITY)
-          : trace_ray<true, false>(sc.trace, g.p.x, g.p.y, g.p.z, g.eps, bs.w.x, bs.w.y, bs.w.z,
-                            INFINITY);
+      bool area = light_is_area(l);
+      Hit h = area ? scene_trace<false>(sc, g.p, g.eps, bs.w, INFINITY)
+                   : scene_trace<true>(sc, g.p, g.eps, bs.w, INFINITY);
       rays += 1;
       V3 L = v3(0.f, 0.f, 0.f);
-      if(h.prim != kMiss && l.kind == LIGHT_TRI) {
-        if(h.prim == l.tri) {
-          const float4* sh = sc.shade + 3 * size_t(h.prim);
-          float4 a = DG_LDG(sh), b = DG_LDG(sh + 1), c = DG_LDG(sh + 2);
-          V3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
-          float b0 = 1.f - h.b1 - h.b2;
-          V3 lp = b0 * p0 + h.b1 * p1 + h.b2 * p2;
-          V3 ln = normalize(cross(p2 - p0, p1 - p0));
-          L = area_eval_radiance(sc, l, lp, ln, g.p);
-        }
-      } else if(h.prim == kMiss && l.kind != LIGHT_TRI) {
+      if(area) {
+        L = area_light_hit_radiance(sc, li, h, g.p, bs.w);
+      } else if(h.prim == kMiss) {
         L = background_radiance(sc, l, bs.w);
       }
       if(!is_black(L)) {
@@ -661,8 +783,7 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, const DevLight& 
     if(!(ls.pdf == 0.f || is_black(ls.L))) {
       V3 f = bsdf_eval(m, g.frame, ls.wi, wo, req);
       if(!is_black(f)) {
-        Hit h = trace_ray<true, false>(sc.trace, ls.o.x, ls.o.y, ls.o.z, ls.tmin, ls.d.x, ls.d.y,
-                                ls.d.z, ls.tmax);
+        Hit h = scene_trace<true>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
         rays += 1;
         if(h.prim == kMiss) {
           float w = 1.f;
@@ -685,7 +806,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
   PathResult res;
   res.rays = 0;
   V3 o, d;
-  camera_ray(pp, fx, fy, o, d);
+  camera_ray(pp, pixel, sample, fx, fy, o, d);
   float tmin = 0.f;
   V3 sum = v3(0.f, 0.f, 0.f);
   V3 thr = v3(1.f, 1.f, 1.f);
@@ -693,11 +814,11 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
   bool last_delta = false;
   const uint32_t req_nd = F_ALL & ~F_DELTA;
   for(;;) {
-    Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, tmin, d.x, d.y, d.z, INFINITY);
+    Hit h = scene_trace<false>(sc, o, tmin, d, INFINITY);
     res.rays += 1;
     bool hit = h.prim != kMiss;
     SurfaceHit g;
-    if(hit) { g = surface_at(sc, h); }
+    if(hit) { g = surface_at(sc, h, o, d); }
     if((bounces == 0 || last_delta) && bounces >= pp.min_depth && bounces <= pp.max_depth) {
       if(hit) {
         if(g.light) {
@@ -733,7 +854,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
           Rand4 a = rand4(pp.seed, pixel, sample, b2);
           Rand4 b = rand4(pp.seed, pixel, sample, b2 + 1);
           const DevLight& l = sc.lights[li];
-          V3 c = estimate_direct(sc, pp, l, g, m, wo, a.a, a.b, a.c, b.a, b.b, res.rays) * thr;
+          V3 c = estimate_direct(sc, pp, li, g, m, wo, a.a, a.b, a.c, b.a, b.b, res.rays) * thr;
           tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
           sum = sum + c;
         }
@@ -742,7 +863,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
         float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
         if(lpdf != 0.f) {
           const DevLight& l = sc.lights[li];
-          V3 e = estimate_direct(sc, pp, l, g, m, wo, r0.b, r0.c, r0.d, r1.a, r1.b, res.rays);
+          V3 e = estimate_direct(sc, pp, li, g, m, wo, r0.b, r0.c, r0.d, r1.a, r1.b, res.rays);
           V3 c = e * (1.f / lpdf) * thr;
           tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
           sum = sum + c;

@@ -7,6 +7,7 @@
 // Replaces PathRenderer::render (path_renderer.cpp:11-21) and the tiling of
 // Renderer::iteration_tiled (renderer.cpp:26-86); each path is pt_sample
 // (pt.cuh).
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -124,11 +125,32 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
     pp.up[a] = c.up[a];
     pp.forward[a] = c.forward[a];
   }
-  // lua_camera.cpp:63-64 clamps the field of view to [1e-2, pi]
+  // lua_camera.cpp:63-64 clamps the pinhole's field of view to [1e-2, pi]
   float fov = c.fov;
-  if(!(fov >= 1e-2f)) { fov = 1e-2f; }
-  if(fov > kPi) { fov = kPi; }
+  if(c.kind == DORT_CAMERA_PINHOLE) {
+    if(!(fov >= 1e-2f)) { fov = 1e-2f; }
+    if(fov > kPi) { fov = kPi; }
+  } else if(c.kind == DORT_CAMERA_THIN_LENS) {
+    if(!(fov > 0.f && fov < kPi)) { err = "thin lens fov must be in (0, pi)"; return false; }
+    if(!(c.lens_radius >= 0.f) || !std::isfinite(c.lens_radius) ||
+       !(c.focal_distance > 0.f) || !std::isfinite(c.focal_distance)) {
+      err = "thin lens needs lens_radius >= 0 and focal_distance > 0";
+      return false;
+    }
+  } else if(c.kind == DORT_CAMERA_ORTHO) {
+    if(!(c.dimension > 0.f) || !std::isfinite(c.dimension)) {
+      err = "orthographic camera needs dimension > 0";
+      return false;
+    }
+  } else {
+    err = "unknown camera kind " + std::to_string(c.kind);
+    return false;
+  }
+  pp.camera = c.kind;
   pp.proj_dim = 2.f * tanf(0.5f * fov);
+  pp.lens_radius = c.lens_radius;
+  pp.focal_distance = c.focal_distance;
+  pp.ortho_dim = c.dimension;
   pp.width = rp->width;
   pp.height = rp->height;
   pp.spp = rp->iterations;

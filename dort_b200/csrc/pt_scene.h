@@ -36,15 +36,32 @@ struct DevMaterial {
   float p2, p3;
 };
 
-enum : uint32_t { LIGHT_TRI = 0, LIGHT_INFINITE = 1, LIGHT_ENV = 2 };
+enum : uint32_t {
+  LIGHT_TRI = 0, LIGHT_INFINITE = 1, LIGHT_ENV = 2,
+  LIGHT_SHAPE = 3,    // DiffuseLight on an analytic shape (sphere or disk)
+  LIGHT_POINT = 4, LIGHT_DIR = 5,
+};
 
 struct DevLight {
   uint32_t kind;
-  uint32_t tri;       // LIGHT_TRI: original triangle index
-  float L[3];         // radiance (LIGHT_ENV: unused)
-  float area;         // LIGHT_TRI: triangle area
-  float p0[3], e1[3], e2[3];
-  float nn[3];        // normalize(cross(e2, e1))
+  uint32_t tri;       // LIGHT_TRI: original triangle index; LIGHT_SHAPE: light_shapes index
+  float L[3];         // radiance (point: intensity; LIGHT_ENV: unused)
+  float area;         // LIGHT_TRI: triangle area; LIGHT_SHAPE: area in shape space
+  float p0[3], e1[3], e2[3];   // LIGHT_POINT: p0 = position
+  float nn[3];        // LIGHT_TRI: normalize(cross(e2, e1)); LIGHT_DIR: unit direction
+};
+
+enum : uint32_t { SHAPE_SPHERE = 1, SHAPE_DISK = 2, SHAPE_CUBE = 3, SHAPE_CYLINDER = 4 };
+
+// Analytic shape primitive: shape parameters, material, optional area light
+// and the shape-to-world transform with its inverse (3x4 row-major each).
+struct DevShape {
+  uint32_t kind;
+  uint32_t mat;
+  uint32_t light;     // light index + 1, 0 if not emissive
+  float r, z0, z1;    // sphere: r; disk: r, z0; cylinder: r, z0 = z_min, z1 = z_max
+  float m[12];        // shape to world
+  float inv[12];      // world to shape
 };
 
 // Latitude-longitude environment map (EnvironmentLight,
@@ -73,11 +90,21 @@ struct PtScene {
   uint32_t bg_count;
   uint32_t bg_light[2];      // indices into lights of the background lights
   DevEnv env;
+  const DevShape* shapes;    // analytic shapes; hit prim = shape_base + index
+  uint32_t shape_count;
+  uint32_t shape_base;       // number of triangles
+  const DevShape* light_shapes;  // the shapes of LIGHT_SHAPE lights, under the
+                                 // lights' own transforms
 };
+
+enum : uint32_t { CAMERA_PINHOLE = 0, CAMERA_ORTHO = 1, CAMERA_THIN_LENS = 2 };
 
 struct PtParams {
   float origin[3], right[3], up[3], forward[3];
-  float proj_dim;            // 2 tan(fov / 2)
+  float proj_dim;            // 2 tan(fov / 2) (pinhole, thin lens)
+  uint32_t camera;           // CAMERA_*
+  float lens_radius, focal_distance;
+  float ortho_dim;           // orthographic image plane dimension
   uint32_t width, height;
   uint32_t spp;              // iterations
   uint32_t min_depth, max_depth;

@@ -83,6 +83,10 @@ static int scene_upload(dort_scene* s, const HostScene& hs) {
   if((rc = upload(s, hs.env_marginal, &pt.env.marginal_cdf)) != DORT_OK) { return rc; }
   if((rc = upload(s, hs.env_cond, &pt.env.cond_cdf)) != DORT_OK) { return rc; }
   if((rc = upload(s, hs.env_pdfs, &pt.env.pdfs)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.shapes, &pt.shapes)) != DORT_OK) { return rc; }
+  pt.shape_count = uint32_t(hs.shapes.size());
+  pt.shape_base = hs.shape_base;
+  if((rc = upload(s, hs.light_shapes, &pt.light_shapes)) != DORT_OK) { return rc; }
 
   void* w = nullptr;
   if(cudaMalloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {

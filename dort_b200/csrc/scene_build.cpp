@@ -4,8 +4,13 @@
 //   - materials resolve to the single BxDF their add_bxdfs would add
 //     (lambert_material.cpp:27-35, mirror_material.cpp:24-29,
 //     dielectric_material.cpp:105-116, phong_material.cpp:98-106);
-//   - every emissive triangle becomes one DiffuseLight (diffuse_light.cpp),
-//     background lights follow in the order InfiniteLight, EnvironmentLight;
+//   - every emissive triangle and every emissive analytic shape becomes one
+//     DiffuseLight (diffuse_light.cpp), then the delta lights (PointLight,
+//     DirectionalLight) in the caller's order, then the background lights in
+//     the order InfiniteLight, EnvironmentLight;
+//   - the scene bounds are the union of the triangles' boxes and the shapes'
+//     boxes taken through their transforms (Transform::apply(Box),
+//     transform.cpp:27-40);
 //   - the light choice CDF is DiscreteDistrib1d over approximate_power()
 //     averages (scene.cpp:20-28, discrete_distrib_1d.cpp:4-20), with the
 //     scene radius of build_scene (lua_builder.cpp:124-126);
@@ -50,9 +55,35 @@ bool resolve_material(const dort_material& in, DevMaterial& m, std::string& err)
       m.bxdf_flags = black3(m.c) ? 0 : (F_DELTA | F_REFL);
       return true;
     case DORT_MAT_DIELECTRIC: {
-      float ior = in.param[0] > 0.f ? in.param[0] : 1.5f;
-      m.p0 = ior;
-      m.bxdf_flags = (black3(m.c) && black3(m.c2)) ? 0 : (F_DELTA | F_REFL | F_TRANS);
+      // param[0] = ior_inside (0: 1.5), param[1] = ior_outside (0: 1),
+      // param[2] != 0: thin; DielectricMaterial::add_bxdfs adds nothing for a
+      // non-positive ior or black tints (dielectric_material.cpp:105-116)
+      float ior_in = in.param[0] != 0.f ? in.param[0] : 1.5f;
+      float ior_out = in.param[1] != 0.f ? in.param[1] : 1.f;
+      m.p0 = ior_in;
+      m.p1 = ior_out;
+      m.p2 = in.param[2] != 0.f ? 1.f : 0.f;
+      bool none = (black3(m.c) && black3(m.c2)) || !(ior_in > 0.f) || !(ior_out > 0.f);
+      m.bxdf_flags = none ? 0 : (F_DELTA | F_REFL | F_TRANS);
+      return true;
+    }
+    case DORT_MAT_OREN_NAYAR: {
+      // OrenNayarMaterial::add_bxdfs (oren_nayar_material.cpp:60-71): Lambert
+      // for sigma = 0; A and B of OrenNayarBrdf::eval_f (:9-11)
+      float sigma = in.param[0];
+      if(!std::isfinite(sigma)) { err = "oren_nayar sigma must be finite"; return false; }
+      if(black3(m.c)) {
+        m.bxdf_flags = 0;
+      } else if(sigma == 0.f) {
+        m.kind = DORT_MAT_LAMBERT;
+        m.bxdf_flags = F_REFL | F_DIFF;
+      } else {
+        float s2 = sigma * sigma;
+        m.p0 = sigma;
+        m.p1 = 1.f - 0.5f * s2 / (s2 + 0.33f);
+        m.p2 = 0.45f * s2 / (s2 + 0.09f);
+        m.bxdf_flags = F_REFL | F_DIFF;
+      }
       return true;
     }
     case DORT_MAT_PHONG: {
@@ -95,6 +126,45 @@ std::vector<float> make_cdf(const std::vector<float>& xs) {
   float inv = sum == 0.f ? 0.f : 1.f / sum;
   for(float& c : cdf) { c *= inv; }
   return cdf;
+}
+
+// Inverse of a 3x4 affine transform; false if singular.
+bool invert_affine(const float* m, float* inv) {
+  double a = m[0], b = m[1], c = m[2], d = m[4], e = m[5], f = m[6], g = m[8], h = m[9],
+         i = m[10];
+  double A = e * i - f * h, B = -(d * i - f * g), C = d * h - e * g;
+  double det = a * A + b * B + c * C;
+  if(!(std::fabs(det) > 1e-30) || !std::isfinite(det)) { return false; }
+  double r[9] = {A, -(b * i - c * h), b * f - c * e,
+                 B, a * i - c * g, -(a * f - c * d),
+                 C, -(a * h - b * g), a * e - b * d};
+  for(int k = 0; k < 9; ++k) { r[k] /= det; }
+  double t[3] = {m[3], m[7], m[11]};
+  for(int row = 0; row < 3; ++row) {
+    inv[4 * row] = float(r[3 * row]);
+    inv[4 * row + 1] = float(r[3 * row + 1]);
+    inv[4 * row + 2] = float(r[3 * row + 2]);
+    inv[4 * row + 3] = float(-(r[3 * row] * t[0] + r[3 * row + 1] * t[1] + r[3 * row + 2] * t[2]));
+  }
+  return true;
+}
+
+// Shape-space bounding box (the shapes' bounds()).
+void shape_local_bounds(const DevShape& s, float lo[3], float hi[3]) {
+  switch(s.kind) {
+    case SHAPE_SPHERE:
+      for(int a = 0; a < 3; ++a) { lo[a] = -s.r; hi[a] = s.r; }
+      break;
+    case SHAPE_DISK:
+      lo[0] = lo[1] = -s.r; hi[0] = hi[1] = s.r; lo[2] = hi[2] = s.z0;
+      break;
+    case SHAPE_CUBE:
+      for(int a = 0; a < 3; ++a) { lo[a] = -1.f; hi[a] = 1.f; }
+      break;
+    default:   // cylinder
+      lo[0] = lo[1] = -s.r; hi[0] = hi[1] = s.r; lo[2] = s.z0; hi[2] = s.z1;
+      break;
+  }
 }
 
 }  // namespace
@@ -199,10 +269,146 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
     hs.shade[3 * size_t(t) + 1] = make_float4(p[1][0], p[1][1], p[1][2], lf);
     hs.shade[3 * size_t(t) + 2] = make_float4(p[2][0], p[2][1], p[2][2], 0.f);
   }
+  // analytic shapes (ShapePrimitive) and their area lights
+  hs.shapes.clear();
+  hs.light_shapes.clear();
+  hs.shape_base = n;
+  if(desc->shape_count > 0 && !desc->shapes) { err = "shapes is NULL with shape_count > 0"; return false; }
+  if(desc->shape_count > kMaxShapes) {
+    err = "at most " + std::to_string(kMaxShapes) + " analytic shapes (they are tested as a list)";
+    return false;
+  }
+  for(uint32_t k = 0; k < desc->shape_count; ++k) {
+    const dort_shape& in = desc->shapes[k];
+    DevShape sh;
+    std::memset(&sh, 0, sizeof(sh));
+    sh.kind = in.kind;
+    if(in.kind < DORT_SHAPE_SPHERE || in.kind > DORT_SHAPE_CYLINDER) {
+      err = "shape " + std::to_string(k) + " has unknown kind " + std::to_string(in.kind);
+      return false;
+    }
+    if(in.material >= hs.mats.size()) {
+      err = "shape " + std::to_string(k) + " has material >= material_count";
+      return false;
+    }
+    sh.mat = in.material;
+    for(int a = 0; a < 4; ++a) {
+      if(!std::isfinite(in.param[a])) { err = "shape parameters must be finite"; return false; }
+    }
+    sh.r = in.param[0];
+    sh.z0 = in.param[1];
+    sh.z1 = in.param[2];
+    if(in.kind != DORT_SHAPE_CUBE && !(sh.r > 0.f)) { err = "shape radius must be positive"; return false; }
+    if(in.kind == DORT_SHAPE_CYLINDER && !(sh.z1 > sh.z0)) {
+      err = "cylinder needs z_max > z_min";
+      return false;
+    }
+    for(int a = 0; a < 12; ++a) {
+      if(!std::isfinite(in.to_world[a])) { err = "shape transform must be finite"; return false; }
+      sh.m[a] = in.to_world[a];
+    }
+    if(!invert_affine(sh.m, sh.inv)) {
+      err = "shape " + std::to_string(k) + " has a singular transform";
+      return false;
+    }
+    // Transform::apply(Box) (transform.cpp:27-40): centre and half extents
+    float blo[3], bhi[3];
+    shape_local_bounds(sh, blo, bhi);
+    for(int row = 0; row < 3; ++row) {
+      float mid = sh.m[4 * row + 3], rad = 0.f;
+      for(int c = 0; c < 3; ++c) {
+        mid += sh.m[4 * row + c] * 0.5f * (blo[c] + bhi[c]);
+        rad += std::fabs(sh.m[4 * row + c] * 0.5f * (bhi[c] - blo[c]));
+      }
+      lo[row] = std::min(lo[row], mid - rad);
+      hi[row] = std::max(hi[row], mid + rad);
+    }
+    for(int a = 0; a < 3; ++a) {
+      if(!std::isfinite(in.emission[a]) || in.emission[a] < 0.f) {
+        err = "shape emission must be finite and non-negative";
+        return false;
+      }
+    }
+    if(!black3(in.emission)) {
+      if(in.kind != DORT_SHAPE_SPHERE && in.kind != DORT_SHAPE_DISK) {
+        err = "only spheres and disks can be area lights";
+        return false;
+      }
+      DevShape ls = sh;
+      if(in.flags & DORT_SHAPE_LIGHT_TRANSFORM) {
+        for(int a = 0; a < 12; ++a) {
+          if(!std::isfinite(in.light_to_world[a])) {
+            err = "shape light transform must be finite";
+            return false;
+          }
+          ls.m[a] = in.light_to_world[a];
+        }
+        if(!invert_affine(ls.m, ls.inv)) {
+          err = "shape " + std::to_string(k) + " has a singular light transform";
+          return false;
+        }
+      }
+      DevLight l;
+      std::memset(&l, 0, sizeof(l));
+      l.kind = LIGHT_SHAPE;
+      l.tri = uint32_t(hs.light_shapes.size());
+      for(int a = 0; a < 3; ++a) { l.L[a] = in.emission[a]; }
+      // DiffuseLight: area = shape->area() in shape space; approximate_power
+      // = area * radiance (diffuse_light.cpp:5-12,118-120)
+      float r = sh.r;
+      l.area = in.kind == DORT_SHAPE_SPHERE ? 4.f * 3.14159265358979323846f * r * r
+                                            : 3.14159265358979323846f * r * r;
+      float pw[3] = {l.area * l.L[0], l.area * l.L[1], l.area * l.L[2]};
+      powers.push_back(avg3(pw));
+      hs.lights.push_back(l);
+      sh.light = uint32_t(hs.lights.size());
+      ls.light = sh.light;
+      hs.light_shapes.push_back(ls);
+      hs.emissive_count += 1;
+    }
+    hs.shapes.push_back(sh);
+  }
+
   // Scene::radius = bounds.radius() (box.hpp:36-38)
-  F3 ext = n > 0 ? F3{hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]} : F3{0.f, 0.f, 0.f};
+  bool any = n > 0 || desc->shape_count > 0;
+  F3 ext = any ? F3{hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]} : F3{0.f, 0.f, 0.f};
   hs.radius = len(ext) * 0.5f;
   float r2pi = 3.14159265358979323846f * hs.radius * hs.radius;
+
+  // delta lights
+  if(desc->light_count > 0 && !desc->lights) { err = "lights is NULL with light_count > 0"; return false; }
+  for(uint32_t k = 0; k < desc->light_count; ++k) {
+    const dort_light& in = desc->lights[k];
+    for(int a = 0; a < 3; ++a) {
+      if(!std::isfinite(in.rgb[a]) || in.rgb[a] < 0.f || !std::isfinite(in.vec[a])) {
+        err = "delta light values must be finite (and colors non-negative)";
+        return false;
+      }
+    }
+    DevLight l;
+    std::memset(&l, 0, sizeof(l));
+    for(int a = 0; a < 3; ++a) { l.L[a] = in.rgb[a]; }
+    float pw[3];
+    if(in.kind == DORT_LIGHT_POINT) {
+      // PointLight: approximate_power = 4 pi intensity (point_light.cpp:59-61)
+      l.kind = LIGHT_POINT;
+      for(int a = 0; a < 3; ++a) { l.p0[a] = in.vec[a]; pw[a] = 4.f * 3.14159265358979323846f * l.L[a]; }
+    } else if(in.kind == DORT_LIGHT_DIRECTIONAL) {
+      // DirectionalLight: normalized direction; approximate_power = pi r^2 L
+      // (directional_light.cpp:5-12,66-68)
+      F3 dir = f3(in.vec);
+      if(!(len(dir) > 0.f)) { err = "directional light needs a non-zero direction"; return false; }
+      dir = nrm(dir);
+      l.kind = LIGHT_DIR;
+      l.nn[0] = dir.x; l.nn[1] = dir.y; l.nn[2] = dir.z;
+      for(int a = 0; a < 3; ++a) { pw[a] = r2pi * l.L[a]; }
+    } else {
+      err = "light " + std::to_string(k) + " has unknown kind " + std::to_string(in.kind);
+      return false;
+    }
+    powers.push_back(avg3(pw));
+    hs.lights.push_back(l);
+  }
 
   hs.bg_count = 0;
   if(!black3(desc->sky_const)) {
@@ -308,6 +514,10 @@ PtScene host_view(const HostScene& hs) {
   sc.env.marginal_cdf = hs.env_marginal.empty() ? nullptr : hs.env_marginal.data();
   sc.env.cond_cdf = hs.env_cond.empty() ? nullptr : hs.env_cond.data();
   sc.env.pdfs = hs.env_pdfs.empty() ? nullptr : hs.env_pdfs.data();
+  sc.shapes = hs.shapes.empty() ? nullptr : hs.shapes.data();
+  sc.shape_count = uint32_t(hs.shapes.size());
+  sc.shape_base = hs.shape_base;
+  sc.light_shapes = hs.light_shapes.empty() ? nullptr : hs.light_shapes.data();
   return sc;
 }
 

@@ -19,10 +19,16 @@ struct HostScene {
   uint32_t bg_count = 0;
   uint32_t bg_light[2] = {0, 0};
   std::vector<float> env_rgb, env_marginal, env_cond, env_pdfs;
+  std::vector<DevShape> shapes;
+  std::vector<DevShape> light_shapes;
+  uint32_t shape_base = 0;
   DevEnv env{};
   uint32_t emissive_count = 0;
   float radius = 0.f;
 };
+
+// Analytic shapes are intersected as a list after the BVH.
+constexpr uint32_t kMaxShapes = 4096;
 
 // Validates the description and builds everything; false + message on error.
 bool build_host_scene(const dort_scene_desc* desc, HostScene& out, std::string& err);

@@ -195,7 +195,7 @@ __device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_
     fy = float(y) + j.b;
   }
   V3 o, d;
-  camera_ray(pp, fx, fy, o, d);
+  camera_ray(pp, pixel, s, fx, fy, o, d);
   w.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
   w.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.f);
   w.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
@@ -316,12 +316,14 @@ __global__ void wf_extend(J jobs, WfDev w) {
       uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
       const PtScene& sc = jobs.scene(job);
       float4 o = w.ray_o[slot], d = w.ray_d[slot];
-      Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      Hit h = scene_trace<false>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), INFINITY);
       w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
       kind = kMissQueue;
       if(h.prim != kMiss) {
-        uint32_t mat = f2u(__ldg(&sc.shade[3 * size_t(h.prim)].w));
+        uint32_t mat = prim_material(sc, h.prim);
         kind = __ldg(&sc.mats[mat].kind);
+        // Oren-Nayar shares the Lambert queue (the queues only group work)
+        if(kind >= kMissQueue) { kind = DORT_MAT_LAMBERT; }
       }
     }
 #pragma unroll
@@ -375,7 +377,7 @@ __global__ void wf_shade(J jobs, WfDev w) {
       bool last_delta = (m.z >> 31) != 0;
       bool hit = h.prim != kMiss;
       SurfaceHit g;
-      if(hit) { g = surface_at(sc, h); }
+      if(hit) { g = surface_at(sc, h, o, d); }
       if((bounces == 0 || last_delta) && bounces >= pp.min_depth && bounces <= pp.max_depth) {
         if(hit) {
           if(g.light) {
@@ -402,13 +404,16 @@ __global__ void wf_shade(J jobs, WfDev w) {
           float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
           if(lpdf != 0.f) {
             const DevLight& l = sc.lights[li];
-            bool use_bsdf = pp.strategy != 2, use_light = pp.strategy != 1;
+            // the BSDF strategy only for area and background lights
+            // (path_renderer.cpp:138-140)
+            bool use_bsdf = pp.strategy != 2 && (light_is_area(l) || light_is_background(l));
+            bool use_light = pp.strategy != 1;
             if(use_bsdf) {
               BsdfSample bs = bsdf_sample(mt, g.frame, wo, req_nd, r0.b, r0.c, r0.d);
               if(!(bs.pdf == 0.f || is_black(bs.f))) {
                 // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf
                 V3 fac = thr * (bs.f * (fabsf(dot(g.n, bs.w)) / bs.pdf)) * (1.f / lpdf);
-                if(l.kind == LIGHT_TRI) {
+                if(light_is_area(l)) {
                   // L and w are known once the closest hit is
                   push_nb = true;
                   nb_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
@@ -525,7 +530,7 @@ __global__ void wf_shadow(J jobs, WfDev w) {
       uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
       const PtScene& sc = jobs.scene(job);
       float4 o = w.sh_o[i], d = w.sh_d[i];
-      Hit h = trace_ray<true, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, d.w);
+      Hit h = scene_trace<true>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), d.w);
       if(h.prim == kMiss) {
         // a path can own two entries (light and BSDF strategy for a
         // background light), so the additions are atomic
@@ -558,24 +563,17 @@ __global__ void wf_neeb(J jobs, WfDev w) {
 __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i) {
     float4 o = w.nb_o[i], d = w.nb_d[i], f = w.nb_f[i];
     uint32_t lw = f2u(f.w);
-    const DevLight& l = sc.lights[lw & 0x7fffffffu];
+    const uint32_t li = lw & 0x7fffffffu;
+    const DevLight& l = sc.lights[li];
     bool use_mis = (lw >> 31) != 0;
     V3 L = v3(0.f, 0.f, 0.f);
     V3 p = v3(o.x, o.y, o.z), wi = v3(d.x, d.y, d.z);
-    if(l.kind == LIGHT_TRI) {
-      Hit h = trace_ray<false, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
-      if(h.prim != kMiss && h.prim == l.tri) {
-        const float4* sh = sc.shade + 3 * size_t(h.prim);
-        float4 a = sh[0], b = sh[1], c = sh[2];
-        V3 p0 = v3(a.x, a.y, a.z), p1 = v3(b.x, b.y, b.z), p2 = v3(c.x, c.y, c.z);
-        float b0 = 1.f - h.b1 - h.b2;
-        V3 lp = b0 * p0 + h.b1 * p1 + h.b2 * p2;
-        V3 ln = normalize(cross(p2 - p0, p1 - p0));
-        L = area_eval_radiance(sc, l, lp, ln, p);
-      }
+    if(light_is_area(l)) {
+      Hit h = scene_trace<false>(sc, p, o.w, wi, INFINITY);
+      L = area_light_hit_radiance(sc, li, h, p, wi);
     } else {
       // background light: only escaping rays count, an any-hit query decides
-      Hit h = trace_ray<true, false>(sc.trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
+      Hit h = scene_trace<true>(sc, p, o.w, wi, INFINITY);
       if(h.prim == kMiss) { L = background_radiance(sc, l, wi); }
     }
     if(!is_black(L)) {

@@ -38,7 +38,7 @@
 extern "C" {
 #endif
 
-#define DORT_GPU_ABI_VERSION 1
+#define DORT_GPU_ABI_VERSION 2
 
 enum dort_status {
   DORT_OK = 0,
@@ -70,6 +70,11 @@ int dort_gpu_abi_version(void);
  *              param[0] = exponent             phong_material.cpp:6-106
  *   CONDUCTOR  color = normal-incidence reflectance F0 (Schlick),
  *              param[0] = GGX alpha            (no reference counterpart)
+ *   OREN_NAYAR color = albedo,
+ *              param[0] = sigma (0: Lambert)   oren_nayar_material.cpp:5-72
+ * DIELECTRIC also takes param[1] = ior_outside (0: 1.0) and param[2] != 0 for
+ * the thin-slab variant (dielectric_material.cpp:59-61,75-80,93-103); a
+ * non-positive ior_inside or ior_outside scatters nothing (:108).
  * A material whose colors are all black scatters nothing (the reference adds
  * no BxDF for a black albedo, lambert_material.cpp:29-35).
  */
@@ -78,7 +83,8 @@ enum dort_material_kind {
   DORT_MAT_MIRROR = 1,
   DORT_MAT_DIELECTRIC = 2,
   DORT_MAT_PHONG = 3,
-  DORT_MAT_CONDUCTOR = 4
+  DORT_MAT_CONDUCTOR = 4,
+  DORT_MAT_OREN_NAYAR = 5
 };
 
 typedef struct dort_material {
@@ -88,10 +94,62 @@ typedef struct dort_material {
   float param[4];
 } dort_material;
 
+/* ---- analytic shapes and delta lights ---------------------------------------
+ * An analytic shape is a ShapePrimitive (primitive.cpp:28-58) of one of the
+ * reference's quadric / box shapes, placed by an affine shape-to-world
+ * transform (3x4, row-major: world = M[:, 0:3] * local + M[:, 3]); the shape
+ * is intersected in its own space, as the reference does:
+ *   SPHERE    param[0] = radius                      sphere_shape.cpp
+ *   DISK      param[0] = radius, param[1] = z        disk_shape.cpp
+ *   CUBE      [-1, 1]^3                              cube_shape.cpp
+ *   CYLINDER  param[0] = radius, param[1..2] = z_min, z_max (no caps)
+ *                                                    cylinder_shape.cpp
+ * A non-black `emission` makes the shape a DiffuseLight (diffuse_light.cpp),
+ * spheres and disks only.  The light samples and weights its shape under
+ * its own transform: `to_world`, or `light_to_world` when flags has
+ * DORT_SHAPE_LIGHT_TRANSFORM.  The two differ when a script gives the light
+ * and its primitive different transforms, as dort.builder.add_diffuse_light
+ * does under a non-identity builder transform (builder_ext.lua:38-48 sets the
+ * light's transform again on top of the builder's, lua_builder.cpp:227-232).
+ *
+ * Delta lights (point_light.cpp, directional_light.cpp):
+ *   POINT        rgb = intensity, vec = world position
+ *   DIRECTIONAL  rgb = radiance,  vec = direction the light travels in
+ */
+enum dort_shape_kind {
+  DORT_SHAPE_SPHERE = 1,
+  DORT_SHAPE_DISK = 2,
+  DORT_SHAPE_CUBE = 3,
+  DORT_SHAPE_CYLINDER = 4
+};
+
+#define DORT_SHAPE_LIGHT_TRANSFORM 1u
+
+typedef struct dort_shape {
+  uint32_t kind;
+  uint32_t material;
+  float param[4];
+  float to_world[12];
+  float emission[3];
+  uint32_t flags;
+  float light_to_world[12];
+} dort_shape;
+
+enum dort_light_kind { DORT_LIGHT_POINT = 1, DORT_LIGHT_DIRECTIONAL = 2 };
+
+typedef struct dort_light {
+  uint32_t kind;
+  float rgb[3];
+  float vec[3];
+  uint32_t reserved;
+} dort_light;
+
 /* ---- scene ----------------------------------------------------------------
- * A flat triangle scene: the reference's primitive tree (triangles added with
+ * A flat scene: the reference's primitive tree (triangles added with
  * add_triangle / add_shape / add_*ply_mesh*, transforms baked into world
- * space) flattened into one triangle array.
+ * space) flattened into one triangle array, plus analytic shapes and delta
+ * lights.  Hit ids of shapes follow the triangles: shape k is prim
+ * tri_count + k.
  *
  *   tri_material  per-triangle material index (NULL: all 0)
  *   tri_emission  per-triangle RGB radiance (NULL: none); every triangle with
@@ -125,7 +183,11 @@ typedef struct dort_scene_desc {
   float sky_up[3];
   float sky_fwd[3];
   uint32_t bvh_width;
-  uint32_t reserved[7];
+  uint32_t shape_count;
+  const dort_shape* shapes;        /* shape_count, or NULL */
+  const dort_light* lights;        /* light_count delta lights, or NULL */
+  uint32_t light_count;
+  uint32_t reserved[5];
 } dort_scene_desc;
 
 typedef struct dort_scene dort_scene;
@@ -182,15 +244,31 @@ int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
  * (Film::to_image, film.cpp:90-108).  Iteration 0 samples pixel centres,
  * later iterations jitter uniformly (path_renderer.cpp:15-20).
  *
- * Camera: PinholeCamera (pinhole_camera.cpp:13-31) with the columns of its
- * camera-to-world transform (origin, and the images of the camera x, y, z
- * axes) and the field of view in radians. */
+ * Camera: the columns of its camera-to-world transform (origin, and the
+ * images of the camera x, y, z axes) and its kind:
+ *   PINHOLE    fov in radians              pinhole_camera.cpp:13-31
+ *   ORTHO      dimension (image plane width of the longer side)
+ *                                          ortho_camera.cpp:13-26,72-93
+ *   THIN_LENS  fov, lens_radius, focal_distance
+ *                                          thin_lens_camera.cpp:15-33,100-116
+ * Every kind has importance / ray pdf = 1, so a sample's value is the
+ * path's radiance (path_renderer.cpp:110). */
+enum dort_camera_kind {
+  DORT_CAMERA_PINHOLE = 0,
+  DORT_CAMERA_ORTHO = 1,
+  DORT_CAMERA_THIN_LENS = 2
+};
+
 typedef struct dort_camera {
   float origin[3];
   float right[3];
   float up[3];
   float forward[3];
   float fov;
+  uint32_t kind;
+  float lens_radius;
+  float focal_distance;
+  float dimension;
 } dort_camera;
 
 enum dort_direct_strategy { DORT_DIRECT_MIS = 0, DORT_DIRECT_BSDF = 1, DORT_DIRECT_LIGHT = 2 };

@@ -300,3 +300,27 @@ class RefPtScene:
         if getattr(self, "h", None):
             ref().dref_pt_scene_destroy(self.h)
             self.h = None
+
+
+def ref_scene_render(scene: dict, params) -> tuple[np.ndarray, float]:
+    """Renders a scene dict (the form dort_b200.scene_desc takes: triangles,
+    analytic shapes, delta lights, sky) with the reference's own PathRenderer,
+    single-threaded; `params` is a dort_b200 RenderParams (camera kind
+    included).  Returns (image [h, w, 3] f32, seconds).  The ctypes structures
+    of the product's C ABI only describe the input here; nothing of the
+    product library runs."""
+    import sys
+    sys.path.insert(0, os.path.dirname(HERE))
+    from dort_b200 import SCENE_KEYS, scene_desc
+    R = ref()
+    if not hasattr(R, "_scene_ready"):
+        R.dref_scene_render.restype = _i32
+        R.dref_scene_render.argtypes = [_P, _P, _P, _P]
+        R._scene_ready = True
+    h = scene_desc(scene["verts"], scene["tris"],
+                   **{k: scene[k] for k in SCENE_KEYS if k in scene and scene[k] is not None})
+    out = np.zeros((params.height, params.width, 3), np.float32)
+    secs = ctypes.c_double(0.0)
+    R.dref_scene_render(ctypes.byref(h.desc), ctypes.byref(params), _ptr(out),
+                        ctypes.byref(secs))
+    return out, secs.value

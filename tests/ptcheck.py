@@ -37,3 +37,90 @@ def compare(a0, a1, b0, b1, block=8):
 def rel_rmse(x, ref):
     x, ref = np.asarray(x, np.float64), np.asarray(ref, np.float64)
     return float(np.sqrt(((x - ref) ** 2).mean()) / ref.mean())
+
+
+def compare_blocks(A0, A1, B0, B1):
+    """compare() on images already reduced to block means."""
+    A0, A1, B0, B1 = (np.asarray(x, np.float64) for x in (A0, A1, B0, B1))
+    A, B = (A0 + A1) / 2, (B0 + B1) / 2
+    num = ((A - B) ** 2).sum(axis=(0, 1))
+    den = (((A0 - A1) ** 2 + (B0 - B1) ** 2) / 4).sum(axis=(0, 1))
+    X = num / np.maximum(den, 1e-30)
+    mean_rel = (A.mean(axis=(0, 1)) - B.mean(axis=(0, 1))) / np.maximum(B.mean(axis=(0, 1)), 1e-30)
+    return {"X": X, "mean_rel": mean_rel}
+
+
+def block_means(img, block=16):
+    """Mean RGB of block x block pixel blocks; the last row / column of blocks
+    is ragged when the size does not divide the image."""
+    img = np.asarray(img, np.float64)
+    h, w = img.shape[:2]
+    by, bx = (h + block - 1) // block, (w + block - 1) // block
+    out = np.zeros((by, bx, img.shape[2]), np.float64)
+    for j in range(by):
+        for i in range(bx):
+            out[j, i] = img[j * block:(j + 1) * block, i * block:(i + 1) * block].reshape(
+                -1, img.shape[2]).mean(0)
+    return out
+
+
+def normal_cdf_inverse(p: float) -> float:
+    """Abramowitz & Stegun 26.2.23, as the reference's math.cpp:4-19 uses."""
+    def approx(t):
+        c0, c1, c2 = 2.515517, 0.802853, 0.010328
+        d0, d1, d2 = 1.432788, 0.189269, 0.001308
+        return t - ((c2 * t + c1) * t + c0) / (((d2 * t + d1) * t + d0) * t + 1.0)
+    if p < 0.5:
+        return -approx(np.sqrt(-2.0 * np.log(p)))
+    return approx(np.sqrt(-2.0 * np.log(1.0 - p)))
+
+
+def convergence_tiles(w: int, h: int, min_tile_size: int = 32) -> np.ndarray:
+    """Tiles test_convergence checks (convergence_test.cpp:31-35,69-83): the
+    image, then tiles of size min(w, h) >> depth down to min_tile_size."""
+    max_depth = 0
+    while (min(w, h) >> (max_depth + 1)) >= min_tile_size:
+        max_depth += 1
+    tiles = []
+    for depth in range(max_depth + 1):
+        size = min(w, h) >> depth
+        for ty in range((h + size - 1) // size):
+            for tx in range((w + size - 1) // size):
+                tiles.append((tx * size, ty * size, min((tx + 1) * size, w),
+                              min((ty + 1) * size, h)))
+    return np.asarray(tiles, np.int32)
+
+
+def tile_means(img, tiles):
+    img = np.asarray(img, np.float64)
+    return np.asarray([img[y0:y1, x0:x1].reshape(-1, 3).mean(0) for x0, y0, x1, y1 in tiles])
+
+
+def reference_convergence(ref_tmeans, tiles, tested, variation=8.0, bias=0.0, p_value=0.01,
+                          min_tile_size=32):
+    """The reference's own image test, test_convergence
+    (src/dort/convergence_test.cpp:10-101), from the reference image's tile
+    means.  Returns the largest |mean_diff| / threshold over all tiles (the
+    test passes when it is <= 1) and the first failing tile (or None)."""
+    h, w = tested.shape[:2]
+    max_depth = 0
+    while (min(w, h) >> (max_depth + 1)) >= min_tile_size:
+        max_depth += 1
+    test_count = float(((1 << (2 * max_depth + 2)) - 1) // 3)
+    test_p = 1.0 - (1.0 - p_value) ** (1.0 / test_count)
+    inv_phi = normal_cdf_inverse(test_p * 0.5)
+    ref_mean = np.asarray(ref_tmeans[0], np.float64)     # tile 0 is the whole image
+    ours = tile_means(tested, tiles)
+    worst, first_fail = 0.0, None
+    for k, (x0, y0, x1, y1) in enumerate(tiles):
+        tref = np.asarray(ref_tmeans[k], np.float64)
+        mean_diff = (ours[k] - tref).max()
+        stddev = max((ref_mean * variation).max(), (tref * variation).max())
+        b = min((ref_mean * bias).max(), (tref * bias).max())
+        count = float(x1 - x0) * float(y1 - y0)
+        max_diff = -stddev / np.sqrt(count) * inv_phi + b
+        r = abs(mean_diff) / max(max_diff, 1e-30)
+        worst = max(worst, r)
+        if r > 1.0 and first_fail is None:
+            first_fail = (int(x0), int(y0), int(x1), int(y1), float(mean_diff), float(max_diff))
+    return worst, first_fail

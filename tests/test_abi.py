@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_plumbing():
     lib = _abi.lib()
-    assert lib.dort_gpu_abi_version() == 1
+    assert lib.dort_gpu_abi_version() == _abi.ABI_VERSION == 2
     rc = lib.dort_gpu_scene_create(None, None)
     assert rc == -1
     assert b"null" in lib.dort_gpu_last_error()
@@ -68,3 +68,36 @@ def test_non_finite_vertex_rejected():
         assert "finite" in str(e)
     else:
         raise AssertionError("expected DortError")
+
+
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """The ctypes mirror has the C compiler's size and field offsets for every
+    structure of include/dort_gpu.h."""
+    import shutil
+    import subprocess
+    gcc = shutil.which("gcc")
+    if gcc is None:
+        import pytest
+        pytest.skip("gcc not available")
+    structs = {"dort_material": _abi.Material, "dort_shape": _abi.Shape,
+               "dort_light": _abi.Light, "dort_scene_desc": _abi.SceneDesc,
+               "dort_camera": _abi.Camera, "dort_render_params": _abi.RenderParams,
+               "dort_wavefront_tuning": _abi.WavefrontTuning, "dort_batch_job": _abi.BatchJob}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "dort_gpu.h"',
+             'int main(void) {']
+    for cname, cls in structs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ['  return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run([gcc, "-I", inc, str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run(
+        [str(exe)], check=True, capture_output=True, text=True).stdout.split("\n") if l)
+    for cname, cls in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(out[f"{cname}.{fname}"]) == getattr(cls, fname).offset, (cname, fname)
