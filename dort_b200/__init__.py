@@ -24,7 +24,7 @@ __all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
 
 # optional scene-dict keys passed through to scene_desc
 SCENE_KEYS = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
-              "sky_scale", "sky_up", "sky_fwd", "shapes", "lights")
+              "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights")
 
 
 def _ptr(a):
@@ -49,10 +49,11 @@ class _DescHolder:
 def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None,
                sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
                sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
-               bvh_width: int = 8, shapes=None, lights=None, **_ignored) -> _DescHolder:
+               bvh_width: int = 8, shapes=None, delta_lights=None, **_ignored) -> _DescHolder:
     """SceneDesc for the arrays given.  `shapes`: dicts with kind (SHAPE_*),
-    material, param (up to 4), to_world (3x4) and emission (RGB); `lights`:
-    dicts with kind (LIGHT_POINT / LIGHT_DIRECTIONAL), rgb and vec."""
+    material, param (up to 4), to_world (3x4), emission (RGB) and optionally
+    light_to_world (3x4); `delta_lights`: dicts with kind (LIGHT_POINT /
+    LIGHT_DIRECTIONAL), rgb and vec."""
     h = _DescHolder()
     d = h.desc
     verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
@@ -101,15 +102,15 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
         h.keep.append(arr)
         d.shapes = ctypes.cast(arr, ctypes.c_void_p)
         d.shape_count = len(shapes)
-    if lights:
-        arr = (_abi.Light * len(lights))()
-        for i, li in enumerate(lights):
+    if delta_lights:
+        arr = (_abi.Light * len(delta_lights))()
+        for i, li in enumerate(delta_lights):
             arr[i].kind = li["kind"]
             arr[i].rgb = (ctypes.c_float * 3)(*li["rgb"])
             arr[i].vec = (ctypes.c_float * 3)(*li["vec"])
         h.keep.append(arr)
         d.lights = ctypes.cast(arr, ctypes.c_void_p)
-        d.light_count = len(lights)
+        d.light_count = len(delta_lights)
     return h
 
 

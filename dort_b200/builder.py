@@ -27,7 +27,8 @@ records the scene the way the reference's primitive tree would hold it:
     (builder_ext.lua:38-48); the flat scene keeps both
 
 build_scene() returns the flat scene dict the Scene constructor takes
-(verts, tris, tri_material, materials, tri_emission, shapes, lights, sky_*)
+(verts, tris, tri_material, materials, tri_emission, shapes, delta_lights,
+sky_*)
 and the default camera as a camera dict.
 """
 from __future__ import annotations
@@ -477,14 +478,14 @@ class Builder:
              "tri_material": np.asarray(tri_mat, np.uint32),
              "materials": mats or [lambert_material(rgb(0.5)).as_dict()],
              "tri_emission": np.asarray(tri_em, np.float32).reshape(-1, 3),
-             "shapes": shapes, "lights": []}
+             "shapes": shapes, "delta_lights": []}
         sky = np.zeros(3)
         for light in self.lights:
             if light.kind == "point":
-                d["lights"].append({"kind": _abi.LIGHT_POINT, "rgb": light.data["intensity"],
+                d["delta_lights"].append({"kind": _abi.LIGHT_POINT, "rgb": light.data["intensity"],
                                     "vec": light.data["point"]})
             elif light.kind == "directional":
-                d["lights"].append({"kind": _abi.LIGHT_DIRECTIONAL,
+                d["delta_lights"].append({"kind": _abi.LIGHT_DIRECTIONAL,
                                     "rgb": light.data["radiance"],
                                     "vec": light.data["direction"]})
             elif light.kind == "infinite":

@@ -74,13 +74,16 @@ DG_HD float ggx_g1(V3 v, V3 m, float alpha) {
 DG_HD V3 ggx_sample_m(float u1, float u2, float alpha, float& pdf) {
   float ct = 1.f / sqrtf((sq(alpha) * u1) / (1.f - u1) + 1.f);
   float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
-  float sp = sinf(u2 * kTwoPi), cp = cosf(u2 * kTwoPi);
+  float sp, cp;
+  DG_SINCOSPI(2.f * u2, sp, cp);
   V3 m = v3(st * sp, st * cp, ct);
   pdf = ggx_d(m, alpha) * ct;
   return m;
 }
 DG_HD V3 schlick(V3 f0, float cos_i) {
-  float k = powf(1.f - fminf(fabsf(cos_i), 1.f), 5.f);
+  float x = 1.f - fminf(fabsf(cos_i), 1.f);
+  float x2 = x * x;
+  float k = x2 * x2 * x;
   return v3(f0.x + (1.f - f0.x) * k, f0.y + (1.f - f0.y) * k, f0.z + (1.f - f0.z) * k);
 }
 
@@ -363,14 +366,12 @@ DG_HD float bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo, uint32
 
 // ---- scene access ---------------------------------------------------------------
 
-// Scene::intersect / intersect_p (scene.cpp:8-18) over the flat scene: the
-// triangle BVH, then the analytic shapes (a short list, each tested in its own
-// space against the closest t so far).  A shape hit has prim = shape_base +
-// its index and b1 = the cube face.
+// The analytic shapes (a short list, each tested in its own space against the
+// closest t so far).  Out of line: only scenes with shapes call it, and the
+// path tracers query the scene from several places.
 template<bool ANY_HIT>
-DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
-  Hit h = trace_ray<ANY_HIT, false>(sc.trace, o.x, o.y, o.z, t_min, d.x, d.y, d.z, t_max);
-  if(sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
+__host__ __device__ __noinline__ Hit trace_shapes(const PtScene& sc, V3 o, float t_min, V3 d,
+                                                  float t_max, Hit h) {
   float best = h.prim == kMiss ? t_max : h.t;
   for(uint32_t k = 0; k < sc.shape_count; ++k) {
     const DevShape& s = sc.shapes[k];
@@ -387,6 +388,16 @@ DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
     }
   }
   return h;
+}
+
+// Scene::intersect / intersect_p (scene.cpp:8-18) over the flat scene: the
+// triangle BVH, then the analytic shapes.  A shape hit has prim = shape_base +
+// its index and b1 = the cube face.
+template<bool ANY_HIT>
+DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
+  Hit h = trace_ray<ANY_HIT, false>(sc.trace, o.x, o.y, o.z, t_min, d.x, d.y, d.z, t_max);
+  if(sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
+  return trace_shapes<ANY_HIT>(sc, o, t_min, d, t_max, h);
 }
 
 // Material index of a hit primitive.
@@ -407,7 +418,8 @@ struct SurfaceHit {
 // DiffGeom of an analytic shape hit (the shape's hit, transformed by
 // Transform::apply(DiffGeom), transform.cpp:15-25).  The BSDF frame is any
 // frame around the normal: every BxDF here is isotropic.
-DG_HD SurfaceHit shape_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+static __host__ __device__ __noinline__ SurfaceHit shape_surface(const PtScene& sc, const Hit& h,
+                                                                  V3 o, V3 d) {
   SurfaceHit s;
   const DevShape& sh = sc.shapes[h.prim - sc.shape_base];
   V3 ol = xf_point(sh.inv, o), dl = xf_vec(sh.inv, d);
@@ -491,9 +503,10 @@ DG_HD float distrib_pdf(const float* cdf, uint32_t n_plus_1, uint32_t i) {
 
 // EnvironmentLight helpers (environment_light.cpp:104-158)
 DG_HD V3 env_dir_from_uv(const DevEnv& e, float du, float dv, float& sin_t) {
-  float theta = dv * kPi;
-  float phi = (du - 0.5f) * kTwoPi;
-  float ct = cosf(theta), st = sinf(theta), cp = cosf(phi), sp = sinf(phi);
+  // theta = pi dv, phi = 2 pi (du - 1/2)
+  float ct, st, cp, sp;
+  DG_SINCOSPI(dv, st, ct);
+  DG_SINCOSPI(2.f * du - 1.f, sp, cp);
   sin_t = clampf(st, 0.f, 1.f);
   return v3p(e.up) * ct + v3p(e.s) * (st * cp) + v3p(e.t) * (st * sp);
 }
@@ -554,6 +567,15 @@ DG_HD V3 background_radiance(const PtScene& sc, const DevLight& l, V3 dir) {
   return env_radiance_uv(sc.env, du, dv);
 }
 
+// DiffuseLight::pivot_radiance_pdf (diffuse_light.cpp:104-110) on an analytic
+// shape, in shape space (out of line).
+static __host__ __device__ __noinline__ float shape_light_pivot_pdf(const PtScene& sc,
+                                                                    const DevLight& l, V3 wi,
+                                                                    V3 pivot) {
+  const DevShape& sh = sc.light_shapes[l.tri];
+  return shape_pivot_pdf(sh, xf_point(sh.inv, pivot), normalize(xf_vec(sh.inv, wi)));
+}
+
 DG_HD bool light_is_area(const DevLight& l) { return l.kind == LIGHT_TRI || l.kind == LIGHT_SHAPE; }
 DG_HD bool light_is_background(const DevLight& l) {
   return l.kind == LIGHT_INFINITE || l.kind == LIGHT_ENV;
@@ -565,11 +587,7 @@ DG_HD float light_pivot_pdf(const PtScene& sc, const DevLight& l, V3 wi, V3 pivo
   if(l.kind == LIGHT_ENV) { return env_dir_pdf(sc.env, wi); }
   if(l.kind == LIGHT_POINT) { return length_sq(v3p(l.p0) - pivot); }   // point_light.cpp:50-52
   if(l.kind == LIGHT_DIR) { return 1.f; }                              // directional_light.cpp:60-62
-  if(l.kind == LIGHT_SHAPE) {
-    // DiffuseLight::pivot_radiance_pdf (diffuse_light.cpp:104-110), in shape space
-    const DevShape& sh = sc.light_shapes[l.tri];
-    return shape_pivot_pdf(sh, xf_point(sh.inv, pivot), normalize(xf_vec(sh.inv, wi)));
-  }
+  if(l.kind == LIGHT_SHAPE) { return shape_light_pivot_pdf(sc, l, wi, pivot); }
   // Shape::point_pivot_pdf (shape.cpp:15-26) on the light's triangle
   V3 w = normalize(wi);
   float4 a = make_float4(l.p0[0], l.p0[1], l.p0[2], 0.f);
@@ -591,7 +609,32 @@ struct LightSample {
   float tmin, tmax;
 };
 
-// Light::sample_pivot_radiance for the three light kinds.
+// DiffuseLight::sample_pivot_radiance (diffuse_light.cpp:40-68) on an
+// analytic shape: sampled in shape space, emitting to the side of the shape's
+// normal (out of line).
+static __host__ __device__ __noinline__ LightSample shape_light_sample(const PtScene& sc,
+                                                                       const DevLight& l, V3 pivot,
+                                                                       float pivot_eps, float u,
+                                                                       float v) {
+  LightSample s;
+  const DevShape& sh = sc.light_shapes[l.tri];
+  V3 pl = xf_point(sh.inv, pivot);
+  V3 n;
+  float eps;
+  V3 ptl = shape_sample_pivot(sh, pl, u, v, n, s.pdf, eps);
+  V3 swi = normalize(ptl - pl);
+  V3 pt = xf_point(sh.m, ptl);
+  float dist = length(pt - pivot);
+  s.wi = normalize(pt - pivot);
+  s.o = pivot;
+  s.d = (pt - pivot) * (1.f / dist);
+  s.tmin = pivot_eps;
+  s.tmax = dist - eps;
+  s.L = dot(swi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+  return s;
+}
+
+// Light::sample_pivot_radiance for every light kind.
 DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, float pivot_eps,
                                float u, float v) {
   LightSample s;
@@ -615,22 +658,7 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmax = dist - 1e-3f;
     s.L = dot(wi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
   } else if(l.kind == LIGHT_SHAPE) {
-    // DiffuseLight::sample_pivot_radiance (diffuse_light.cpp:40-68): sampled
-    // in shape space, emitting to the side of the shape's normal
-    const DevShape& sh = sc.light_shapes[l.tri];
-    V3 pl = xf_point(sh.inv, pivot);
-    V3 n;
-    float eps;
-    V3 ptl = shape_sample_pivot(sh, pl, u, v, n, s.pdf, eps);
-    V3 swi = normalize(ptl - pl);
-    V3 pt = xf_point(sh.m, ptl);
-    float dist = length(pt - pivot);
-    s.wi = normalize(pt - pivot);
-    s.o = pivot;
-    s.d = (pt - pivot) * (1.f / dist);
-    s.tmin = pivot_eps;
-    s.tmax = dist - eps;
-    s.L = dot(swi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+    s = shape_light_sample(sc, l, pivot, pivot_eps, u, v);
   } else if(l.kind == LIGHT_POINT) {
     // PointLight::sample_pivot_radiance (point_light.cpp:19-31)
     V3 pt = v3p(l.p0);

@@ -7,6 +7,15 @@
 #include "trace.cuh"
 
 namespace dort_gpu {
+
+// sin(pi x) and cos(pi x).  Every angle the samplers draw is 2 pi u or pi u
+// for u in [0, 1), and sincospif needs no large-argument reduction for it.
+#ifdef __CUDA_ARCH__
+#define DG_SINCOSPI(x, s, c) sincospif((x), &(s), &(c))
+#else
+#define DG_SINCOSPI(x, s, c) \
+  do { (s) = sinf(3.14159265358979323846f * (x)); (c) = cosf(3.14159265358979323846f * (x)); } while(0)
+#endif
 constexpr float kPi = 3.14159265358979323846f;
 constexpr float kInvPi = 0.31830988618379067154f;
 constexpr float kTwoPi = 6.28318530717958647692f;
@@ -47,8 +56,9 @@ DG_HD void coordinate_system(V3 v0, V3& v1, V3& v2) {
 // monte_carlo.cpp
 DG_HD V3 cosine_hemisphere_sample(float u1, float u2) {
   float r = sqrtf(u1);
-  float th = kTwoPi * u2;
-  float x = cosf(th) * r, y = sinf(th) * r;
+  float sn, cs;
+  DG_SINCOSPI(2.f * u2, sn, cs);   // theta = 2 pi u2
+  float x = cs * r, y = sn * r;
   float z = sqrtf(fmaxf(0.f, 1.f - x * x - y * y));
   return v3(x, y, z);
 }
@@ -56,14 +66,16 @@ DG_HD float cosine_hemisphere_pdf(float cos_theta) { return fabsf(cos_theta * kI
 DG_HD V3 uniform_sphere_sample(float u1, float u2) {
   float z = 1.f - 2.f * u1;
   float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-  float phi = kTwoPi * u2;
-  return v3(cosf(phi) * r, sinf(phi) * r, z);
+  float sn, cs;
+  DG_SINCOSPI(2.f * u2, sn, cs);   // phi = 2 pi u2
+  return v3(cs * r, sn * r, z);
 }
 DG_HD V3 power_cosine_hemisphere_sample(float u1, float u2, float e) {
-  float phi = kTwoPi * u1;
   float ct = powf(u2, 1.f / (1.f + e));
   float st = sqrtf(1.f - ct * ct);
-  return v3(cosf(phi) * st, sinf(phi) * st, ct);
+  float sn, cs;
+  DG_SINCOSPI(2.f * u1, sn, cs);   // phi = 2 pi u1
+  return v3(cs * st, sn * st, ct);
 }
 DG_HD float power_cosine_hemisphere_pdf(float ct, float e) {
   return (e + 1.f) * powf(ct, e) * kInvTwoPi;
@@ -72,16 +84,18 @@ DG_HD float power_cosine_hemisphere_pdf(float ct, float e) {
 // monte_carlo.cpp:32-36
 DG_HD void uniform_disk_sample(float u1, float u2, float& x, float& y) {
   float r = sqrtf(u1);
-  float th = kTwoPi * u2;
-  x = cosf(th) * r;
-  y = sinf(th) * r;
+  float sn, cs;
+  DG_SINCOSPI(2.f * u2, sn, cs);   // theta = 2 pi u2
+  x = cs * r;
+  y = sn * r;
 }
 // monte_carlo.cpp:56-68 (lerp(u1, 1, cos_max) = (1 - u1) + u1 cos_max)
 DG_HD V3 uniform_cone_sample(float cos_max, float u1, float u2) {
   float ct = (1.f - u1) + u1 * cos_max;
   float st = sqrtf(fmaxf(0.f, 1.f - ct * ct));
-  float phi = kTwoPi * u2;
-  return v3(cosf(phi) * st, sinf(phi) * st, ct);
+  float sn, cs;
+  DG_SINCOSPI(2.f * u2, sn, cs);   // phi = 2 pi u2
+  return v3(cs * st, sn * st, ct);
 }
 DG_HD float uniform_cone_pdf(float cos_max) { return 1.f / (kTwoPi * (1.f - cos_max)); }
 

@@ -47,7 +47,19 @@ def compare_blocks(A0, A1, B0, B1):
     den = (((A0 - A1) ** 2 + (B0 - B1) ** 2) / 4).sum(axis=(0, 1))
     X = num / np.maximum(den, 1e-30)
     mean_rel = (A.mean(axis=(0, 1)) - B.mean(axis=(0, 1))) / np.maximum(B.mean(axis=(0, 1)), 1e-30)
-    return {"X": X, "mean_rel": mean_rel}
+    # per block: squared difference over its own noise estimate (channels
+    # summed); without bias its distribution is F-like with median ~1, and a
+    # few caustic or firefly blocks cannot move the median
+    nb = ((A - B) ** 2).sum(axis=-1)
+    db = (((A0 - A1) ** 2 + (B0 - B1) ** 2) / 4).sum(axis=-1)
+    noisy = db > 1e-12 * max(float(db.max()), 1e-30)
+    Xmed = float(np.median(nb[noisy] / db[noisy])) if noisy.any() else 0.0
+    # difference of the channel means over its standard error (blocks are
+    # independent; each block's variance estimated from the halves)
+    nblk = A.shape[0] * A.shape[1]
+    se = np.sqrt((((A0 - A1) ** 2 + (B0 - B1) ** 2) / 4).sum(axis=(0, 1))) / nblk
+    mean_z = (A.mean(axis=(0, 1)) - B.mean(axis=(0, 1))) / np.maximum(se, 1e-30)
+    return {"X": X, "mean_rel": mean_rel, "Xmed": Xmed, "mean_z": mean_z}
 
 
 def block_means(img, block=16):
