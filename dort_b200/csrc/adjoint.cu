@@ -80,6 +80,7 @@ struct AdjointTape {
 
 constexpr int kAdjBlock = 128;
 
+template<bool G>
 __global__ void __launch_bounds__(kAdjBlock)
 adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
                uint32_t per_slice, const float* __restrict__ dl_dimage,
@@ -110,7 +111,7 @@ adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
       fy = float(y) + j.b;
     }
     NoTape none;
-    PathResult r1 = pt_sample(sc, pp, pixel, s, fx, fy, none);
+    PathResult r1 = pt_sample<NoTape, G>(sc, pp, pixel, s, fx, fy, none);
     V3 L = r1.L;
     // samples the film drops have no gradient (renderer.cpp:36-41)
     if(!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) || L.x < 0.f || L.y < 0.f ||
@@ -125,7 +126,7 @@ adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
     tape.d_emission = d_emission;
     tape.tri_emission = sc.tri_emission;
     tape.tri_count = sc.shape_base;
-    pt_sample(sc, pp, pixel, s, fx, fy, tape);
+    pt_sample<AdjointTape, G>(sc, pp, pixel, s, fx, fy, tape);
   }
 }
 
@@ -239,8 +240,14 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   uint32_t per_slice = tiles * 32;
   uint64_t threads = uint64_t(slices) * per_slice;
   if(ok) {
-    adjoint_replay<<<uint32_t((threads + kAdjBlock - 1) / kAdjBlock), kAdjBlock, 0, st>>>(
-        scene->pt, pp, slices, per, per_slice, d_img, d_ga, d_ge);
+    uint32_t grid = uint32_t((threads + kAdjBlock - 1) / kAdjBlock);
+    if(scene_needs_general(scene->pt, pp)) {
+      adjoint_replay<true><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, slices, per, per_slice,
+                                                         d_img, d_ga, d_ge);
+    } else {
+      adjoint_replay<false><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, slices, per, per_slice,
+                                                          d_img, d_ga, d_ge);
+    }
     ok = cudaGetLastError() == cudaSuccess;
   }
   if(ok && d_albedo) {

@@ -25,6 +25,15 @@
 //     (discrete_distrib_1d.cpp, scene.cpp:20-28).
 // Random numbers come from Philox keyed by (seed, pixel, sample, block); see
 // philox.cuh for the dimension layout.
+//
+// Template flag G ("general"): the functions that depend on scene features
+// are instantiated twice.  G = false compiles only what a triangle scene with
+// triangle and sky lights, a pinhole camera and the materials Lambert,
+// mirror, dielectric (outside ior 1, not thin), Phong and conductor needs;
+// G = true adds analytic shapes, point and directional lights, orthographic
+// and thin-lens cameras, Oren-Nayar and the general dielectric.  The host
+// picks the instantiation per scene and camera (scene_needs_general), so the
+// common case does not pay in registers for code it never runs.
 #pragma once
 #include <cmath>
 
@@ -137,6 +146,7 @@ DG_HD V3 oren_nayar_f(const DevMaterial& m, V3 wi, V3 wo) {
 }
 
 // Bxdf::eval_f for the resolved BxDF of `m` (local directions).
+template<bool G>
 DG_HD V3 bxdf_eval(const DevMaterial& m, V3 wi, V3 wo, uint32_t request) {
   switch(m.kind) {
     case DORT_MAT_LAMBERT:
@@ -156,13 +166,14 @@ DG_HD V3 bxdf_eval(const DevMaterial& m, V3 wi, V3 wo, uint32_t request) {
     case DORT_MAT_CONDUCTOR:
       return conductor_f(m, wi, wo);
     case DORT_MAT_OREN_NAYAR:
-      return oren_nayar_f(m, wi, wo);
+      return G ? oren_nayar_f(m, wi, wo) : v3(0.f, 0.f, 0.f);
     default:
       return v3(0.f, 0.f, 0.f);   // mirror, dielectric: delta only
   }
 }
 
 // Bxdf light_f_pdf / symmetric_f_pdf (local directions).
+template<bool G>
 DG_HD float bxdf_pdf(const DevMaterial& m, V3 wg, V3 wf, uint32_t request) {
   switch(m.kind) {
     case DORT_MAT_LAMBERT:
@@ -185,7 +196,7 @@ DG_HD float bxdf_pdf(const DevMaterial& m, V3 wg, V3 wf, uint32_t request) {
     case DORT_MAT_CONDUCTOR:
       return conductor_pdf(m, wg, wf);
     case DORT_MAT_OREN_NAYAR:
-      return cosine_hemisphere_pdf(wg.z);
+      return G ? cosine_hemisphere_pdf(wg.z) : 0.f;
     default:
       return 0.f;
   }
@@ -210,6 +221,7 @@ DG_HD float fresnel_dielectric(float cr, float ct, float ir, float it) {
 
 // Bxdf::sample_light_f (local w_fix = wo); returns f, fills w (local), pdf,
 // flags.  Sampling as the reference's per-BxDF code.
+template<bool G>
 DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, float v,
                      float uc, V3& wg, float& pdf, uint32_t& flags) {
   V3 zero = v3(0.f, 0.f, 0.f);
@@ -230,6 +242,7 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
     }
     case DORT_MAT_OREN_NAYAR: {
       // OrenNayarBrdf::sample_symmetric_f (oren_nayar_material.cpp:40-50)
+      if(!G) { flags = 0; pdf = 0.f; return zero; }
       wg = cosine_hemisphere_sample(u, v);
       pdf = cosine_hemisphere_pdf(wg.z);
       wg.z = copysignf(wg.z, wf.z);
@@ -240,9 +253,10 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
       // dielectric_material.cpp:33-99 with fix_is_light = false; m.p0 =
       // ior_inside, m.p1 = ior_outside, m.p2 != 0: thin slab; get_iors (:101-111)
       bool s_refl = request & F_REFL, s_trans = request & F_TRANS;
-      bool thin = m.p2 != 0.f;
+      bool thin = G && m.p2 != 0.f;
+      float ior_out = G ? m.p1 : 1.f;
       float ir, it;
-      if(thin || wf.z >= 0.f) { ir = m.p1; it = m.p0; } else { ir = m.p0; it = m.p1; }
+      if(thin || wf.z >= 0.f) { ir = ior_out; it = m.p0; } else { ir = m.p0; it = ior_out; }
       float cr = fabsf(wf.z);
       V3 w_reflect = v3(-wf.x, -wf.y, wf.z);
       V3 w_trans;
@@ -301,8 +315,8 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
         flags = F_REFL | F_DIFF;
       }
       wg.z = copysignf(wg.z, wf.z);
-      pdf = bxdf_pdf(m, wg, wf, request);
-      return bxdf_eval(m, wg, wf, request);
+      pdf = bxdf_pdf<G>(m, wg, wf, request);
+      return bxdf_eval<G>(m, wg, wf, request);
     }
     case DORT_MAT_CONDUCTOR: {
       float pm;
@@ -323,6 +337,7 @@ DG_HD V3 bxdf_sample(const DevMaterial& m, V3 wf, uint32_t request, float u, flo
 }
 
 // Bsdf::sample_light_f (bsdf.cpp:95-192) for a one-BxDF Bsdf.
+template<bool G>
 DG_HD BsdfSample bsdf_sample(const DevMaterial& m, const Frame& fr, V3 wo, uint32_t request,
                              float u, float v, float uc) {
   BsdfSample s;
@@ -335,7 +350,7 @@ DG_HD BsdfSample bsdf_sample(const DevMaterial& m, const Frame& fr, V3 wo, uint3
   V3 wg;
   float pdf = 0.f;
   uint32_t flags = 0;
-  V3 f = bxdf_sample(m, wf, request, u, v, uc, wg, pdf, flags);
+  V3 f = bxdf_sample<G>(m, wf, request, u, v, uc, wg, pdf, flags);
   if(pdf == 0.f) { return s; }
   s.flags = flags;
   s.w = fr.to_world(wg);
@@ -347,30 +362,31 @@ DG_HD BsdfSample bsdf_sample(const DevMaterial& m, const Frame& fr, V3 wo, uint3
 }
 
 // Bsdf::eval_f (bsdf.cpp:72-93).
+template<bool G>
 DG_HD V3 bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo, uint32_t request) {
   V3 wi_l = fr.to_local(wi), wo_l = fr.to_local(wo);
   bool reflection = wo_l.z * wi_l.z > 0.f;
   uint32_t er = request & ((F_LOBES & ~F_DELTA) | (reflection ? F_REFL : F_TRANS));
   if(!(er & F_MODES)) { return v3(0.f, 0.f, 0.f); }
   if(!bxdf_matches(m.bxdf_flags, er)) { return v3(0.f, 0.f, 0.f); }
-  V3 f = bxdf_eval(m, wi_l, wo_l, er);
+  V3 f = bxdf_eval<G>(m, wi_l, wo_l, er);
   float dn = fabsf(dot(fr.n, wi));
   return (dn * dn == 0.f) ? v3(0.f, 0.f, 0.f) : f;
 }
 
 // Bsdf::light_f_pdf (bsdf.cpp:194-225).
+template<bool G>
 DG_HD float bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo, uint32_t request) {
   if(!bxdf_matches(m.bxdf_flags, request)) { return 0.f; }
-  return bxdf_pdf(m, fr.to_local(wi), fr.to_local(wo), request);
+  return bxdf_pdf<G>(m, fr.to_local(wi), fr.to_local(wo), request);
 }
 
 // ---- scene access ---------------------------------------------------------------
 
 // The analytic shapes (a short list, each tested in its own space against the
-// closest t so far).  Out of line: only scenes with shapes call it, and the
-// path tracers query the scene from several places.
+// closest t so far).
 template<bool ANY_HIT>
-__host__ __device__ __noinline__ Hit trace_shapes(const PtScene& sc, V3 o, float t_min, V3 d,
+DG_HD Hit trace_shapes(const PtScene& sc, V3 o, float t_min, V3 d,
                                                   float t_max, Hit h) {
   float best = h.prim == kMiss ? t_max : h.t;
   for(uint32_t k = 0; k < sc.shape_count; ++k) {
@@ -393,16 +409,17 @@ __host__ __device__ __noinline__ Hit trace_shapes(const PtScene& sc, V3 o, float
 // Scene::intersect / intersect_p (scene.cpp:8-18) over the flat scene: the
 // triangle BVH, then the analytic shapes.  A shape hit has prim = shape_base +
 // its index and b1 = the cube face.
-template<bool ANY_HIT>
+template<bool ANY_HIT, bool G>
 DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
   Hit h = trace_ray<ANY_HIT, false>(sc.trace, o.x, o.y, o.z, t_min, d.x, d.y, d.z, t_max);
-  if(sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
+  if(!G || sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
   return trace_shapes<ANY_HIT>(sc, o, t_min, d, t_max, h);
 }
 
 // Material index of a hit primitive.
+template<bool G>
 DG_HD uint32_t prim_material(const PtScene& sc, uint32_t prim) {
-  if(prim >= sc.shape_base) { return sc.shapes[prim - sc.shape_base].mat; }
+  if(G && prim >= sc.shape_base) { return sc.shapes[prim - sc.shape_base].mat; }
   return DG_AS_UINT(DG_LDG(&sc.shade[3 * size_t(prim)].w));
 }
 
@@ -418,12 +435,11 @@ struct SurfaceHit {
 // DiffGeom of an analytic shape hit (the shape's hit, transformed by
 // Transform::apply(DiffGeom), transform.cpp:15-25).  The BSDF frame is any
 // frame around the normal: every BxDF here is isotropic.
-static __host__ __device__ __noinline__ SurfaceHit shape_surface(const PtScene& sc, const Hit& h,
-                                                                  V3 o, V3 d) {
+DG_HD SurfaceHit shape_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
   SurfaceHit s;
   const DevShape& sh = sc.shapes[h.prim - sc.shape_base];
   V3 ol = xf_point(sh.inv, o), dl = xf_vec(sh.inv, d);
-  V3 pl = ol + dl * h.t;
+  V3 pl = madd_rn(ol, dl, h.t);
   V3 nl = shape_local_normal(sh, pl, uint32_t(h.b1));
   s.p = xf_point(sh.m, pl);
   s.n = normalize(xf_normal(sh.inv, nl));
@@ -437,8 +453,9 @@ static __host__ __device__ __noinline__ SurfaceHit shape_surface(const PtScene& 
 }
 
 // Surface at the closest hit h of the ray (o, d).
+template<bool G>
 DG_HD SurfaceHit surface_at(const PtScene& sc, const Hit& h, V3 o, V3 d) {
-  if(h.prim >= sc.shape_base) { return shape_surface(sc, h, o, d); }
+  if(G && h.prim >= sc.shape_base) { return shape_surface(sc, h, o, d); }
   SurfaceHit s;
   const float4* sh = sc.shade + 3 * size_t(h.prim);
   float4 a = DG_LDG(sh), b = DG_LDG(sh + 1), c = DG_LDG(sh + 2);
@@ -568,10 +585,8 @@ DG_HD V3 background_radiance(const PtScene& sc, const DevLight& l, V3 dir) {
 }
 
 // DiffuseLight::pivot_radiance_pdf (diffuse_light.cpp:104-110) on an analytic
-// shape, in shape space (out of line).
-static __host__ __device__ __noinline__ float shape_light_pivot_pdf(const PtScene& sc,
-                                                                    const DevLight& l, V3 wi,
-                                                                    V3 pivot) {
+// shape, in shape space.
+DG_HD float shape_light_pivot_pdf(const PtScene& sc, const DevLight& l, V3 wi, V3 pivot) {
   const DevShape& sh = sc.light_shapes[l.tri];
   return shape_pivot_pdf(sh, xf_point(sh.inv, pivot), normalize(xf_vec(sh.inv, wi)));
 }
@@ -582,12 +597,15 @@ DG_HD bool light_is_background(const DevLight& l) {
 }
 
 // Light::pivot_radiance_pdf
+template<bool G>
 DG_HD float light_pivot_pdf(const PtScene& sc, const DevLight& l, V3 wi, V3 pivot) {
   if(l.kind == LIGHT_INFINITE) { return kInvFourPi; }
   if(l.kind == LIGHT_ENV) { return env_dir_pdf(sc.env, wi); }
-  if(l.kind == LIGHT_POINT) { return length_sq(v3p(l.p0) - pivot); }   // point_light.cpp:50-52
-  if(l.kind == LIGHT_DIR) { return 1.f; }                              // directional_light.cpp:60-62
-  if(l.kind == LIGHT_SHAPE) { return shape_light_pivot_pdf(sc, l, wi, pivot); }
+  if(G) {
+    if(l.kind == LIGHT_POINT) { return length_sq(v3p(l.p0) - pivot); }  // point_light.cpp:50-52
+    if(l.kind == LIGHT_DIR) { return 1.f; }                             // directional_light.cpp:60-62
+    if(l.kind == LIGHT_SHAPE) { return shape_light_pivot_pdf(sc, l, wi, pivot); }
+  }
   // Shape::point_pivot_pdf (shape.cpp:15-26) on the light's triangle
   V3 w = normalize(wi);
   float4 a = make_float4(l.p0[0], l.p0[1], l.p0[2], 0.f);
@@ -611,11 +629,9 @@ struct LightSample {
 
 // DiffuseLight::sample_pivot_radiance (diffuse_light.cpp:40-68) on an
 // analytic shape: sampled in shape space, emitting to the side of the shape's
-// normal (out of line).
-static __host__ __device__ __noinline__ LightSample shape_light_sample(const PtScene& sc,
-                                                                       const DevLight& l, V3 pivot,
-                                                                       float pivot_eps, float u,
-                                                                       float v) {
+// normal.
+DG_HD LightSample shape_light_sample(const PtScene& sc, const DevLight& l, V3 pivot,
+                                     float pivot_eps, float u, float v) {
   LightSample s;
   const DevShape& sh = sc.light_shapes[l.tri];
   V3 pl = xf_point(sh.inv, pivot);
@@ -635,6 +651,7 @@ static __host__ __device__ __noinline__ LightSample shape_light_sample(const PtS
 }
 
 // Light::sample_pivot_radiance for every light kind.
+template<bool G>
 DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, float pivot_eps,
                                float u, float v) {
   LightSample s;
@@ -657,9 +674,9 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmin = pivot_eps;
     s.tmax = dist - 1e-3f;
     s.L = dot(wi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
-  } else if(l.kind == LIGHT_SHAPE) {
+  } else if(G && l.kind == LIGHT_SHAPE) {
     s = shape_light_sample(sc, l, pivot, pivot_eps, u, v);
-  } else if(l.kind == LIGHT_POINT) {
+  } else if(G && l.kind == LIGHT_POINT) {
     // PointLight::sample_pivot_radiance (point_light.cpp:19-31)
     V3 pt = v3p(l.p0);
     float dist = length(pt - pivot);
@@ -670,7 +687,7 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmin = pivot_eps;
     s.tmax = dist;
     s.L = v3p(l.L);
-  } else if(l.kind == LIGHT_DIR) {
+  } else if(G && l.kind == LIGHT_DIR) {
     // DirectionalLight::sample_pivot_radiance (directional_light.cpp:28-42)
     s.wi = -v3p(l.nn);
     s.pdf = 1.f;
@@ -724,19 +741,21 @@ struct PathResult {
 // Radiance that area light `li` sends along a BSDF-strategy ray from p whose
 // closest hit is h: only a hit on the light's own primitive counts
 // (estimate_direct_from_bsdf, path_renderer.cpp:158-166).
+template<bool G>
 DG_HD V3 area_light_hit_radiance(const PtScene& sc, uint32_t li, const Hit& h, V3 p, V3 wi) {
   if(h.prim == kMiss) { return v3(0.f, 0.f, 0.f); }
-  SurfaceHit g = surface_at(sc, h, p, wi);
+  SurfaceHit g = surface_at<G>(sc, h, p, wi);
   if(g.light != li + 1) { return v3(0.f, 0.f, 0.f); }
   return area_eval_radiance(sc, sc.lights[li], g.p, g.n, p);
 }
 
 // Camera ray of film position (fx, fy) for sample `sample` of `pixel`; the
 // thin lens draws its lens point from the camera block of the sample.
+template<bool G>
 DG_HD void camera_ray(const PtParams& pp, uint32_t pixel, uint32_t sample, float fx, float fy,
                       V3& o, V3& d) {
   float w = float(pp.width), h = float(pp.height);
-  if(pp.camera == CAMERA_ORTHO) {
+  if(G && pp.camera == CAMERA_ORTHO) {
     // OrthoCamera::sample_ray_importance / get_plane_pos (ortho_camera.cpp:13-26,84-88)
     float k = pp.ortho_dim / fmaxf(w, h);
     float px = (fx - 0.5f * w) * k, py = (fy - 0.5f * h) * k;
@@ -744,7 +763,7 @@ DG_HD void camera_ray(const PtParams& pp, uint32_t pixel, uint32_t sample, float
     d = normalize(v3p(pp.forward));
     return;
   }
-  if(pp.camera == CAMERA_THIN_LENS) {
+  if(G && pp.camera == CAMERA_THIN_LENS) {
     // ThinLensCamera::sample_ray_importance, get_focus_point, sample_lens_point
     // (thin_lens_camera.cpp:15-33,100-114)
     float k = pp.proj_dim / fmaxf(w, h);
@@ -771,6 +790,7 @@ DG_HD void camera_ray(const PtParams& pp, uint32_t pixel, uint32_t sample, float
 }
 
 // Direct lighting from one light (estimate_direct, path_renderer.cpp:135-206).
+template<bool G>
 DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, uint32_t li,
                          const SurfaceHit& g, const DevMaterial& m, V3 wo,
                          float u_bsdf, float v_bsdf, float c_bsdf, float u_l, float v_l,
@@ -782,24 +802,24 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, uint32_t li,
   bool use_light = pp.strategy != 1;
   V3 sum = v3(0.f, 0.f, 0.f);
   if(use_bsdf) {
-    BsdfSample bs = bsdf_sample(m, g.frame, wo, req, u_bsdf, v_bsdf, c_bsdf);
+    BsdfSample bs = bsdf_sample<G>(m, g.frame, wo, req, u_bsdf, v_bsdf, c_bsdf);
     if(!(bs.pdf == 0.f || is_black(bs.f))) {
       // A background light counts only if the ray escapes, so whether anything
       // is hit is all that matters: an any-hit query gives the same answer.
       bool area = light_is_area(l);
-      Hit h = area ? scene_trace<false>(sc, g.p, g.eps, bs.w, INFINITY)
-                   : scene_trace<true>(sc, g.p, g.eps, bs.w, INFINITY);
+      Hit h = area ? scene_trace<false, G>(sc, g.p, g.eps, bs.w, INFINITY)
+                   : scene_trace<true, G>(sc, g.p, g.eps, bs.w, INFINITY);
       rays += 1;
       V3 L = v3(0.f, 0.f, 0.f);
       if(area) {
-        L = area_light_hit_radiance(sc, li, h, g.p, bs.w);
+        L = area_light_hit_radiance<G>(sc, li, h, g.p, bs.w);
       } else if(h.prim == kMiss) {
         L = background_radiance(sc, l, bs.w);
       }
       if(!is_black(L)) {
         float w = 1.f;
         if(use_light) {
-          float lp = light_pivot_pdf(sc, l, bs.w, g.p);
+          float lp = light_pivot_pdf<G>(sc, l, bs.w, g.p);
           w = bs.pdf / (bs.pdf + lp);
         }
         sum = sum + bs.f * L * (w * fabsf(dot(g.n, bs.w)) / bs.pdf);
@@ -807,16 +827,16 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, uint32_t li,
     }
   }
   if(use_light) {
-    LightSample ls = light_sample(sc, l, g.p, g.eps, u_l, v_l);
+    LightSample ls = light_sample<G>(sc, l, g.p, g.eps, u_l, v_l);
     if(!(ls.pdf == 0.f || is_black(ls.L))) {
-      V3 f = bsdf_eval(m, g.frame, ls.wi, wo, req);
+      V3 f = bsdf_eval<G>(m, g.frame, ls.wi, wo, req);
       if(!is_black(f)) {
-        Hit h = scene_trace<true>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
+        Hit h = scene_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
         rays += 1;
         if(h.prim == kMiss) {
           float w = 1.f;
           if(use_bsdf) {
-            float bp = bsdf_pdf(m, g.frame, ls.wi, wo, req);
+            float bp = bsdf_pdf<G>(m, g.frame, ls.wi, wo, req);
             w = ls.pdf / (ls.pdf + bp);
           }
           sum = sum + f * ls.L * (w * fabsf(dot(g.n, ls.wi)) / ls.pdf);
@@ -828,13 +848,13 @@ DG_HD V3 estimate_direct(const PtScene& sc, const PtParams& pp, uint32_t li,
 }
 
 // PathRenderer::sample (path_renderer.cpp:23-111) for one film position.
-template<class Tape>
+template<class Tape, bool G>
 DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel,
                            uint32_t sample, float fx, float fy, Tape& tape) {
   PathResult res;
   res.rays = 0;
   V3 o, d;
-  camera_ray(pp, pixel, sample, fx, fy, o, d);
+  camera_ray<G>(pp, pixel, sample, fx, fy, o, d);
   float tmin = 0.f;
   V3 sum = v3(0.f, 0.f, 0.f);
   V3 thr = v3(1.f, 1.f, 1.f);
@@ -842,11 +862,11 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
   bool last_delta = false;
   const uint32_t req_nd = F_ALL & ~F_DELTA;
   for(;;) {
-    Hit h = scene_trace<false>(sc, o, tmin, d, INFINITY);
+    Hit h = scene_trace<false, G>(sc, o, tmin, d, INFINITY);
     res.rays += 1;
     bool hit = h.prim != kMiss;
     SurfaceHit g;
-    if(hit) { g = surface_at(sc, h, o, d); }
+    if(hit) { g = surface_at<G>(sc, h, o, d); }
     if((bounces == 0 || last_delta) && bounces >= pp.min_depth && bounces <= pp.max_depth) {
       if(hit) {
         if(g.light) {
@@ -882,7 +902,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
           Rand4 a = rand4(pp.seed, pixel, sample, b2);
           Rand4 b = rand4(pp.seed, pixel, sample, b2 + 1);
           const DevLight& l = sc.lights[li];
-          V3 c = estimate_direct(sc, pp, li, g, m, wo, a.a, a.b, a.c, b.a, b.b, res.rays) * thr;
+          V3 c = estimate_direct<G>(sc, pp, li, g, m, wo, a.a, a.b, a.c, b.a, b.b, res.rays) * thr;
           tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
           sum = sum + c;
         }
@@ -891,7 +911,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
         float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
         if(lpdf != 0.f) {
           const DevLight& l = sc.lights[li];
-          V3 e = estimate_direct(sc, pp, li, g, m, wo, r0.b, r0.c, r0.d, r1.a, r1.b, res.rays);
+          V3 e = estimate_direct<G>(sc, pp, li, g, m, wo, r0.b, r0.c, r0.d, r1.a, r1.b, res.rays);
           V3 c = e * (1.f / lpdf) * thr;
           tape.direct(l.kind == LIGHT_TRI ? l.tri : kMiss, c);
           sum = sum + c;
@@ -900,7 +920,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
     }
 
     uint32_t req = (pp.only_direct || bounces == pp.max_depth) ? (F_MODES | F_DELTA) : F_ALL;
-    BsdfSample bs = bsdf_sample(m, g.frame, wo, req, r1.c, r1.d, r2.a);
+    BsdfSample bs = bsdf_sample<G>(m, g.frame, wo, req, r1.c, r1.d, r2.a);
     if(is_black(bs.f) || bs.pdf == 0.f) { break; }
     V3 contrib = bs.f * (fabsf(dot(bs.w, g.n)) / bs.pdf);
     last_delta = (bs.flags & F_DELTA) != 0;

@@ -40,6 +40,7 @@ DG_HD bool keep_sample(V3 L) {
          L.z >= 0.f;
 }
 
+template<bool G>
 __global__ void __launch_bounds__(kPtBlock)
 pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
               uint32_t per_slice, float4* __restrict__ partial,
@@ -65,7 +66,7 @@ pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
       for(uint32_t s = s0; s < s1; ++s) {
         float fx, fy;
         film_pos(pp, pixel, x, y, s, fx, fy);
-        PathResult r = pt_sample(sc, pp, pixel, s, fx, fy, tape);
+        PathResult r = pt_sample<NoTape, G>(sc, pp, pixel, s, fx, fy, tape);
         rays += r.rays;
         if(keep_sample(r.L)) {
           acc.x += r.L.x;
@@ -81,6 +82,11 @@ pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
   for(int o = 16; o > 0; o >>= 1) { rays += __shfl_down_sync(0xffffffffu, rays, o); }
   if((threadIdx.x & 31) == 0 && rays) { atomicAdd(ray_count, (unsigned long long)rays); }
 }
+
+template __global__ void pt_megakernel<false>(PtScene, PtParams, uint32_t, uint32_t, uint32_t,
+                                               float4*, unsigned long long*);
+template __global__ void pt_megakernel<true>(PtScene, PtParams, uint32_t, uint32_t, uint32_t,
+                                              float4*, unsigned long long*);
 
 __global__ void pt_resolve(const float4* __restrict__ partial, uint32_t slices, uint32_t npix,
                            float* __restrict__ out_rgb, unsigned long long* __restrict__ kept) {
@@ -199,8 +205,13 @@ int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t 
   float4* partial = static_cast<float4*>(scratch);
   uint64_t threads = uint64_t(slices) * per_slice;
   uint32_t blocks = uint32_t((threads + kPtBlock - 1) / kPtBlock);
-  pt_megakernel<<<blocks, kPtBlock, 0, st>>>(s->pt, pp, slices, per, per_slice, partial,
-                                             d_counters);
+  if(scene_needs_general(s->pt, pp)) {
+    pt_megakernel<true><<<blocks, kPtBlock, 0, st>>>(s->pt, pp, slices, per, per_slice, partial,
+                                                     d_counters);
+  } else {
+    pt_megakernel<false><<<blocks, kPtBlock, 0, st>>>(s->pt, pp, slices, per, per_slice, partial,
+                                                      d_counters);
+  }
   DG_CUDA(cudaGetLastError());
   pt_resolve<<<(npix + 255) / 256, 256, 0, st>>>(partial, slices, npix, d_out, d_counters + 1);
   DG_CUDA(cudaGetLastError());
@@ -296,7 +307,7 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
       for(uint32_t s = 0; s < pp.spp; ++s) {
         float fx, fy;
         film_pos(pp, pixel, x, y, s, fx, fy);
-        PathResult r = pt_sample(sc, pp, pixel, s, fx, fy, tape);
+        PathResult r = pt_sample<NoTape, true>(sc, pp, pixel, s, fx, fy, tape);
         if(keep_sample(r.L)) {
           acc[0] += r.L.x; acc[1] += r.L.y; acc[2] += r.L.z;
           w += 1;

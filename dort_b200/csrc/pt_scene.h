@@ -95,6 +95,8 @@ struct PtScene {
   uint32_t shape_base;       // number of triangles
   const DevShape* light_shapes;  // the shapes of LIGHT_SHAPE lights, under the
                                  // lights' own transforms
+  uint32_t general;          // 1 if the scene has analytic shapes, delta lights,
+                             // Oren-Nayar or a general dielectric (host use)
 };
 
 enum : uint32_t { CAMERA_PINHOLE = 0, CAMERA_ORTHO = 1, CAMERA_THIN_LENS = 2 };
@@ -112,5 +114,11 @@ struct PtParams {
   uint32_t strategy;         // 0 mis, 1 bsdf, 2 light
   uint64_t seed;
 };
+
+// Whether rendering `sc` with `pp` needs the general instantiation of the
+// path code (pt.cuh, template flag G).
+inline bool scene_needs_general(const PtScene& sc, const PtParams& pp) {
+  return sc.general != 0 || pp.camera != CAMERA_PINHOLE;
+}
 
 }  // namespace dort_gpu

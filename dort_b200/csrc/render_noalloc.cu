@@ -33,7 +33,8 @@
 
 namespace dort_gpu {
 
-// The megakernel and its resolve step (pt_render.cu).
+// The megakernel (both instantiations) and its resolve step (pt_render.cu).
+template<bool G>
 __global__ void pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
                               uint32_t per_slice, float4* __restrict__ partial,
                               unsigned long long* __restrict__ ray_count);
@@ -113,8 +114,13 @@ extern "C" int dort_gpu_render_device_noalloc(dort_scene* scene,
   uint32_t per_slice = tiles * 32;
   uint64_t threads = uint64_t(slices) * per_slice;
   const int block = 128;   // the megakernel's launch bound
-  pt_megakernel<<<uint32_t((threads + block - 1) / block), block, 0, st>>>(
-      scene->pt, pp, slices, per, per_slice, partial, counters);
+  if(scene_needs_general(scene->pt, pp)) {
+    pt_megakernel<true><<<uint32_t((threads + block - 1) / block), block, 0, st>>>(
+        scene->pt, pp, slices, per, per_slice, partial, counters);
+  } else {
+    pt_megakernel<false><<<uint32_t((threads + block - 1) / block), block, 0, st>>>(
+        scene->pt, pp, slices, per, per_slice, partial, counters);
+  }
   DG_CUDA(cudaGetLastError());
   pt_resolve<<<uint32_t((npix + 255) / 256), 256, 0, st>>>(partial, slices, uint32_t(npix),
                                                             d_out_rgb, counters + 1);

@@ -87,6 +87,7 @@ static int scene_upload(dort_scene* s, const HostScene& hs) {
   pt.shape_count = uint32_t(hs.shapes.size());
   pt.shape_base = hs.shape_base;
   if((rc = upload(s, hs.light_shapes, &pt.light_shapes)) != DORT_OK) { return rc; }
+  pt.general = hs.general;
 
   void* w = nullptr;
   if(cudaMalloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {

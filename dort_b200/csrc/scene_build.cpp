@@ -490,6 +490,12 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
     hs.bg_light[hs.bg_count++] = uint32_t(hs.lights.size() - 1);
   }
   hs.light_cdf = make_cdf(powers);
+  // features only the general instantiation of the path code handles
+  hs.general = (!hs.shapes.empty() || desc->light_count > 0) ? 1u : 0u;
+  for(const DevMaterial& m : hs.mats) {
+    if(m.kind == DORT_MAT_OREN_NAYAR && m.bxdf_flags) { hs.general = 1u; }
+    if(m.kind == DORT_MAT_DIELECTRIC && (m.p1 != 1.f || m.p2 != 0.f)) { hs.general = 1u; }
+  }
   return true;
 }
 
@@ -518,6 +524,7 @@ PtScene host_view(const HostScene& hs) {
   sc.shape_count = uint32_t(hs.shapes.size());
   sc.shape_base = hs.shape_base;
   sc.light_shapes = hs.light_shapes.empty() ? nullptr : hs.light_shapes.data();
+  sc.general = hs.general;
   return sc;
 }
 

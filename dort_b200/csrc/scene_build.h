@@ -21,6 +21,7 @@ struct HostScene {
   std::vector<float> env_rgb, env_marginal, env_cond, env_pdfs;
   std::vector<DevShape> shapes;
   std::vector<DevShape> light_shapes;
+  uint32_t general = 0;   // needs the general path instantiation (pt.cuh)
   uint32_t shape_base = 0;
   DevEnv env{};
   uint32_t emissive_count = 0;

@@ -13,30 +13,39 @@
 
 namespace dort_gpu {
 
-// 3x4 row-major affine transforms
-DG_HD V3 xf_point(const float* m, V3 p) {
-  return v3(m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3],
-            m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7],
-            m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11]);
+// The shape code rounds every product and sum on its own (DG_MUL / DG_ADD /
+// DG_SUB: no fused multiply-add), as the reference's float arithmetic does.
+// Where a shape's face and a triangle coincide (a box standing on a floor)
+// the hit found depends on that rounding.
+
+DG_HD float dot3_rn(V3 a, V3 b) { return dot_rn(a.x, a.y, a.z, b.x, b.y, b.z); }
+DG_HD V3 madd_rn(V3 o, V3 d, float t) {   // o + d t
+  return v3(DG_ADD(o.x, DG_MUL(d.x, t)), DG_ADD(o.y, DG_MUL(d.y, t)),
+            DG_ADD(o.z, DG_MUL(d.z, t)));
 }
+
+// 3x4 row-major affine transforms
 DG_HD V3 xf_vec(const float* m, V3 v) {
-  return v3(m[0] * v.x + m[1] * v.y + m[2] * v.z,
-            m[4] * v.x + m[5] * v.y + m[6] * v.z,
-            m[8] * v.x + m[9] * v.y + m[10] * v.z);
+  return v3(dot_rn(m[0], m[1], m[2], v.x, v.y, v.z), dot_rn(m[4], m[5], m[6], v.x, v.y, v.z),
+            dot_rn(m[8], m[9], m[10], v.x, v.y, v.z));
+}
+DG_HD V3 xf_point(const float* m, V3 p) {
+  V3 r = xf_vec(m, p);
+  return v3(DG_ADD(r.x, m[3]), DG_ADD(r.y, m[7]), DG_ADD(r.z, m[11]));
 }
 // A shape-space normal taken to world space: the transpose of the inverse.
 DG_HD V3 xf_normal(const float* inv, V3 n) {
-  return v3(inv[0] * n.x + inv[4] * n.y + inv[8] * n.z,
-            inv[1] * n.x + inv[5] * n.y + inv[9] * n.z,
-            inv[2] * n.x + inv[6] * n.y + inv[10] * n.z);
+  return v3(dot_rn(inv[0], inv[4], inv[8], n.x, n.y, n.z),
+            dot_rn(inv[1], inv[5], inv[9], n.x, n.y, n.z),
+            dot_rn(inv[2], inv[6], inv[10], n.x, n.y, n.z));
 }
 
 // math.cpp:21-38: the two roots of A x^2 + B x + C (false if none or one)
 DG_HD bool solve_quadratic(float A, float B, float C, float& x1, float& x2) {
-  float disc = B * B - 4.f * A * C;
+  float disc = DG_SUB(DG_MUL(B, B), DG_MUL(DG_MUL(4.f, A), C));
   if(disc <= 0.f) { return false; }
   float sd = sqrtf(disc);
-  float q = B < 0.f ? -0.5f * (B - sd) : -0.5f * (B + sd);
+  float q = B < 0.f ? DG_MUL(-0.5f, DG_SUB(B, sd)) : DG_MUL(-0.5f, DG_ADD(B, sd));
   x1 = q / A;
   x2 = C / q;
   return true;
@@ -54,7 +63,8 @@ DG_HD bool shape_hit(const DevShape& s, V3 o, V3 d, float t_min, float t_max, fl
   switch(s.kind) {
     case SHAPE_SPHERE: {
       // SphereShape::solve_hit_t (sphere_shape.cpp:123-146)
-      float a = dot(d, d), b = 2.f * dot(o, d), c = dot(o, o) - s.r * s.r;
+      float a = dot3_rn(d, d), b = DG_MUL(2.f, dot3_rn(o, d));
+      float c = DG_SUB(dot3_rn(o, o), DG_MUL(s.r, s.r));
       float t0, t1;
       if(!solve_quadratic(a, b, c, t0, t1)) { return false; }
       if(t1 < t0) { float x = t0; t0 = t1; t1 = x; }
@@ -65,10 +75,10 @@ DG_HD bool shape_hit(const DevShape& s, V3 o, V3 d, float t_min, float t_max, fl
     case SHAPE_DISK: {
       // DiskShape::hit / hit_p (disk_shape.cpp:5-56)
       if(d.z == 0.f) { return false; }
-      float t = (s.z0 - o.z) / d.z;
+      float t = DG_SUB(s.z0, o.z) / d.z;
       if(!(t_min <= t && t <= t_max)) { return false; }
-      float px = o.x + d.x * t, py = o.y + d.y * t;
-      if(px * px + py * py > s.r * s.r) { return false; }
+      float px = DG_ADD(o.x, DG_MUL(d.x, t)), py = DG_ADD(o.y, DG_MUL(d.y, t));
+      if(DG_ADD(DG_MUL(px, px), DG_MUL(py, py)) > DG_MUL(s.r, s.r)) { return false; }
       t_out = t;
       return true;
     }
@@ -80,7 +90,7 @@ DG_HD bool shape_hit(const DevShape& s, V3 o, V3 d, float t_min, float t_max, fl
       for(uint32_t axis = 0; axis < 3; ++axis) {
         float inv = 1.f / v3_get(d, axis);
         float oa = v3_get(o, axis);
-        float tn = (-1.f - oa) * inv, tf = (1.f - oa) * inv;
+        float tn = DG_MUL(DG_SUB(-1.f, oa), inv), tf = DG_MUL(DG_SUB(1.f, oa), inv);
         bool negative = false;
         if(tn > tf) { float x = tn; tn = tf; tf = x; negative = true; }
         if(tn > t0) { t0 = tn; ax0 = axis; neg0 = negative; }
@@ -101,18 +111,18 @@ DG_HD bool shape_hit(const DevShape& s, V3 o, V3 d, float t_min, float t_max, fl
     }
     case SHAPE_CYLINDER: {
       // CylinderShape::solve_hit_t (cylinder_shape.cpp:75-110)
-      float a = d.x * d.x + d.y * d.y;
-      float b = 2.f * (o.x * d.x + o.y * d.y);
-      float c = o.x * o.x + o.y * o.y - s.r * s.r;
+      float a = DG_ADD(DG_MUL(d.x, d.x), DG_MUL(d.y, d.y));
+      float b = DG_MUL(2.f, DG_ADD(DG_MUL(o.x, d.x), DG_MUL(o.y, d.y)));
+      float c = DG_SUB(DG_ADD(DG_MUL(o.x, o.x), DG_MUL(o.y, o.y)), DG_MUL(s.r, s.r));
       float t0, t1;
       if(!solve_quadratic(a, b, c, t0, t1)) { return false; }
       if(t1 < t0) { float x = t0; t0 = t1; t1 = x; }
       if(t_min <= t0 && t0 <= t_max) {
-        float z = o.z + d.z * t0;
+        float z = DG_ADD(o.z, DG_MUL(d.z, t0));
         if(s.z0 <= z && z <= s.z1) { t_out = t0; return true; }
       }
       if(t_min <= t1 && t1 <= t_max) {
-        float z = o.z + d.z * t1;
+        float z = DG_ADD(o.z, DG_MUL(d.z, t1));
         if(s.z0 <= z && z <= s.z1) { t_out = t1; return true; }
       }
       return false;
@@ -160,7 +170,7 @@ DG_HD float shape_generic_pivot_pdf(const DevShape& s, V3 pivot, V3 w) {
   float t;
   uint32_t face;
   if(!shape_hit<false>(s, pivot, w, 0.f, INFINITY, t, face)) { return 0.f; }
-  V3 pt = pivot + w * t;
+  V3 pt = madd_rn(pivot, w, t);
   V3 n = shape_local_normal(s, pt, face);
   return (1.f / shape_area(s)) * length_sq(pt - pivot) / fabsf(dot(w, n));
 }
@@ -207,7 +217,7 @@ DG_HD V3 shape_sample_pivot(const DevShape& s, V3 pivot, float u, float v, V3& n
     float t;
     uint32_t face;
     if(!shape_hit<false>(s, pivot, dir, 0.f, INFINITY, t, face)) { t = dist; }
-    V3 pt = pivot + dir * t;
+    V3 pt = madd_rn(pivot, dir, t);
     n = pt * (1.f / s.r);
     dir_pdf = uniform_cone_pdf(cos_max);
     return pt;

@@ -126,8 +126,11 @@ struct WfDev {
 // passes them as kernel arguments; a batch of frames (many scenes, each with
 // its own resolution, spp and depth) reads a device table of jobs, and every
 // path carries its job index in the high bits of meta.w.
+// G selects the instantiation of the path code (pt.cuh).
+template<bool G>
 struct SingleJob {
   static constexpr bool kBatched = false;
+  static constexpr bool kGeneral = G;
   PtScene sc;
   PtParams pp;
   __device__ __forceinline__ uint32_t job_of_sample(uint64_t) const { return 0; }
@@ -145,8 +148,10 @@ struct WfJob {
   uint32_t pad;
 };
 
+template<bool G>
 struct JobTable {
   static constexpr bool kBatched = true;
+  static constexpr bool kGeneral = G;
   const WfJob* jobs;
   uint32_t count;
   __device__ __forceinline__ uint32_t job_of_sample(uint64_t sid) const {
@@ -182,6 +187,7 @@ __global__ void wf_init(WfDev w, uint32_t npix) {
 }
 
 // Starts sample s of `pixel` in `slot`: camera ray, unit throughput.
+template<bool G>
 __device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_t slot,
                                            uint32_t pixel, uint32_t s) {
   uint32_t x = pixel % pp.width, y = pixel / pp.width;
@@ -195,7 +201,7 @@ __device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_
     fy = float(y) + j.b;
   }
   V3 o, d;
-  camera_ray(pp, pixel, s, fx, fy, o, d);
+  camera_ray<G>(pp, pixel, s, fx, fy, o, d);
   w.ray_o[slot] = make_float4(o.x, o.y, o.z, 0.f);
   w.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.f);
   w.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
@@ -232,7 +238,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
     uint32_t unit_end = min(pp.spp, (m.y / kChunk + 1u) * kChunk);
     if(next_s < unit_end) {
       w.acc[slot] = a;
-      start_path(w, pp, slot, m.x, next_s);
+      start_path<J::kGeneral>(w, pp, slot, m.x, next_s);
       m = make_uint4(m.x, next_s, 0u, SLOT_ACTIVE | (job << 8));
       started = true;
     } else {
@@ -263,7 +269,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
     unit_to_pixel(pp, uid - jobs.sample_begin(job), pixel, x, y, s0);
     if(x < pp.width && y < pp.height) {
       w.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-      start_path(w, pp, slot, pixel, s0);
+      start_path<J::kGeneral>(w, pp, slot, pixel, s0);
       m = make_uint4(pixel, s0, 0u, SLOT_ACTIVE | (job << 8));
       started = true;
       atomicAdd(w.ctr + C_LIVE, 1u);
@@ -316,11 +322,12 @@ __global__ void wf_extend(J jobs, WfDev w) {
       uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
       const PtScene& sc = jobs.scene(job);
       float4 o = w.ray_o[slot], d = w.ray_d[slot];
-      Hit h = scene_trace<false>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), INFINITY);
+      Hit h = scene_trace<false, J::kGeneral>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z),
+                                              INFINITY);
       w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
       kind = kMissQueue;
       if(h.prim != kMiss) {
-        uint32_t mat = prim_material(sc, h.prim);
+        uint32_t mat = prim_material<J::kGeneral>(sc, h.prim);
         kind = __ldg(&sc.mats[mat].kind);
         // Oren-Nayar shares the Lambert queue (the queues only group work)
         if(kind >= kMissQueue) { kind = DORT_MAT_LAMBERT; }
@@ -377,7 +384,7 @@ __global__ void wf_shade(J jobs, WfDev w) {
       bool last_delta = (m.z >> 31) != 0;
       bool hit = h.prim != kMiss;
       SurfaceHit g;
-      if(hit) { g = surface_at(sc, h, o, d); }
+      if(hit) { g = surface_at<J::kGeneral>(sc, h, o, d); }
       if((bounces == 0 || last_delta) && bounces >= pp.min_depth && bounces <= pp.max_depth) {
         if(hit) {
           if(g.light) {
@@ -409,7 +416,8 @@ __global__ void wf_shade(J jobs, WfDev w) {
             bool use_bsdf = pp.strategy != 2 && (light_is_area(l) || light_is_background(l));
             bool use_light = pp.strategy != 1;
             if(use_bsdf) {
-              BsdfSample bs = bsdf_sample(mt, g.frame, wo, req_nd, r0.b, r0.c, r0.d);
+              BsdfSample bs = bsdf_sample<J::kGeneral>(mt, g.frame, wo, req_nd, r0.b, r0.c,
+                                                       r0.d);
               if(!(bs.pdf == 0.f || is_black(bs.f))) {
                 // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf
                 V3 fac = thr * (bs.f * (fabsf(dot(g.n, bs.w)) / bs.pdf)) * (1.f / lpdf);
@@ -428,7 +436,7 @@ __global__ void wf_shade(J jobs, WfDev w) {
                   if(!is_black(L)) {
                     float wgt = 1.f;
                     if(use_light) {
-                      float lp = light_pivot_pdf(sc, l, bs.w, g.p);
+                      float lp = light_pivot_pdf<J::kGeneral>(sc, l, bs.w, g.p);
                       wgt = bs.pdf / (bs.pdf + lp);
                     }
                     V3 c = fac * L * wgt;
@@ -441,13 +449,13 @@ __global__ void wf_shade(J jobs, WfDev w) {
               }
             }
             if(use_light) {
-              LightSample ls = light_sample(sc, l, g.p, g.eps, r1.a, r1.b);
+              LightSample ls = light_sample<J::kGeneral>(sc, l, g.p, g.eps, r1.a, r1.b);
               if(!(ls.pdf == 0.f || is_black(ls.L))) {
-                V3 f = bsdf_eval(mt, g.frame, ls.wi, wo, req_nd);
+                V3 f = bsdf_eval<J::kGeneral>(mt, g.frame, ls.wi, wo, req_nd);
                 if(!is_black(f)) {
                   float wgt = 1.f;
                   if(use_bsdf) {
-                    float bp = bsdf_pdf(mt, g.frame, ls.wi, wo, req_nd);
+                    float bp = bsdf_pdf<J::kGeneral>(mt, g.frame, ls.wi, wo, req_nd);
                     wgt = ls.pdf / (ls.pdf + bp);
                   }
                   V3 c = (f * ls.L * (wgt * fabsf(dot(g.n, ls.wi)) / ls.pdf)) * (1.f / lpdf) * thr;
@@ -461,7 +469,7 @@ __global__ void wf_shade(J jobs, WfDev w) {
           }
         }
         uint32_t req = (pp.only_direct || bounces == pp.max_depth) ? (F_MODES | F_DELTA) : F_ALL;
-        BsdfSample bs = bsdf_sample(mt, g.frame, wo, req, r1.c, r1.d, r2.a);
+        BsdfSample bs = bsdf_sample<J::kGeneral>(mt, g.frame, wo, req, r1.c, r1.d, r2.a);
         if(is_black(bs.f) || bs.pdf == 0.f) {
           finished = true;
         } else {
@@ -530,7 +538,7 @@ __global__ void wf_shadow(J jobs, WfDev w) {
       uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
       const PtScene& sc = jobs.scene(job);
       float4 o = w.sh_o[i], d = w.sh_d[i];
-      Hit h = scene_trace<true>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), d.w);
+      Hit h = scene_trace<true, J::kGeneral>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), d.w);
       if(h.prim == kMiss) {
         // a path can own two entries (light and BSDF strategy for a
         // background light), so the additions are atomic
@@ -544,6 +552,7 @@ __global__ void wf_shadow(J jobs, WfDev w) {
   }
 }
 
+template<bool G>
 __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i);
 
 template<class J>
@@ -555,11 +564,12 @@ __global__ void wf_neeb(J jobs, WfDev w) {
     uint32_t i = base + (threadIdx.x & 31u);
     if(i < n) {
       uint32_t job = J::kBatched ? (w.meta[w.nb_slot[i]].w >> 8) : 0u;
-      neeb_one_impl(jobs.scene(job), w, i);
+      neeb_one_impl<J::kGeneral>(jobs.scene(job), w, i);
     }
   }
 }
 
+template<bool G>
 __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i) {
     float4 o = w.nb_o[i], d = w.nb_d[i], f = w.nb_f[i];
     uint32_t lw = f2u(f.w);
@@ -569,17 +579,17 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
     V3 L = v3(0.f, 0.f, 0.f);
     V3 p = v3(o.x, o.y, o.z), wi = v3(d.x, d.y, d.z);
     if(light_is_area(l)) {
-      Hit h = scene_trace<false>(sc, p, o.w, wi, INFINITY);
-      L = area_light_hit_radiance(sc, li, h, p, wi);
+      Hit h = scene_trace<false, G>(sc, p, o.w, wi, INFINITY);
+      L = area_light_hit_radiance<G>(sc, li, h, p, wi);
     } else {
       // background light: only escaping rays count, an any-hit query decides
-      Hit h = scene_trace<true>(sc, p, o.w, wi, INFINITY);
+      Hit h = scene_trace<true, G>(sc, p, o.w, wi, INFINITY);
       if(h.prim == kMiss) { L = background_radiance(sc, l, wi); }
     }
     if(!is_black(L)) {
       float wgt = 1.f;
       if(use_mis) {
-        float lp = light_pivot_pdf(sc, l, wi, p);
+        float lp = light_pivot_pdf<G>(sc, l, wi, p);
         wgt = d.w / (d.w + lp);
       }
       V3 c = v3(f.x, f.y, f.z) * L * wgt;
@@ -809,8 +819,8 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   if(!wf->valid || wf->jobs_cached != nullptr ||
      std::memcmp(&wf->pp_cached, &pp, sizeof(PtParams)) != 0 ||
      std::memcmp(&wf->tune_cached, &tn, sizeof(WfTuning)) != 0) {
-    SingleJob jobs{s->pt, pp};
-    rc = wf_build_graph(wf, jobs, tn);
+    rc = scene_needs_general(s->pt, pp) ? wf_build_graph(wf, SingleJob<true>{s->pt, pp}, tn)
+                                        : wf_build_graph(wf, SingleJob<false>{s->pt, pp}, tn);
     if(rc != DORT_OK) { return rc; }
     wf->pp_cached = pp;
     wf->jobs_cached = nullptr;
@@ -830,8 +840,9 @@ __global__ void wf_control_host(WfDev w, uint32_t* more_flag) {
   *more_flag = wf_end_wave(w) ? 1u : 0u;
 }
 
-int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
-                          float* d_out, cudaStream_t st, double ms[6]) {
+template<bool G>
+static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
+                         cudaStream_t st, double ms[6]) {
   if(!s->wavefront) { s->wavefront = new Wavefront(); }
   Wavefront* wf = s->wavefront;
   uint32_t npix = pp.width * pp.height;
@@ -839,8 +850,8 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   if(rc != DORT_OK) { return rc; }
   wf->dev.total_samples = padded_samples(pp);
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth);
-  SingleJob jobs{s->pt, pp};
-  WfGrids g = wf_grids<SingleJob>(tn);
+  SingleJob<G> jobs{s->pt, pp};
+  WfGrids g = wf_grids<SingleJob<G>>(tn);
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
   uint32_t* more = nullptr;
   DG_CUDA(cudaMallocHost(&more, sizeof(uint32_t)));
@@ -851,15 +862,15 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
   bool ok = cudaGetLastError() == cudaSuccess;
   for(uint32_t wave = 0; ok && wave < wf->dev.max_waves + 1; ++wave) {
     cudaEventRecord(ev[0], st);
-    wf_regen<SingleJob><<<g.regen, 256, 0, st>>>(jobs, wf->dev);
+    wf_regen<SingleJob<G>><<<g.regen, 256, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[1], st);
-    wf_extend<SingleJob><<<g.ext, bt, 0, st>>>(jobs, wf->dev);
+    wf_extend<SingleJob<G>><<<g.ext, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[2], st);
-    wf_shade<SingleJob><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
+    wf_shade<SingleJob<G>><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[3], st);
-    wf_shadow<SingleJob><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
+    wf_shadow<SingleJob<G>><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[4], st);
-    wf_neeb<SingleJob><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
+    wf_neeb<SingleJob<G>><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);
     wf_control_host<<<1, 1, 0, st>>>(wf->dev, more);
     ok = cudaStreamSynchronize(st) == cudaSuccess;
@@ -884,6 +895,12 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
                                cudaGetErrorString(cudaGetLastError()));
   }
   return DORT_OK;
+}
+
+int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
+                          float* d_out, cudaStream_t st, double ms[6]) {
+  return scene_needs_general(s->pt, pp) ? stage_times_g<true>(s, pp, tn, d_out, st, ms)
+                                        : stage_times_g<false>(s, pp, tn, d_out, st, ms);
 }
 
 int wavefront_counters_of(Wavefront* wf, uint64_t* rays, uint32_t* waves, uint32_t* error,
@@ -979,8 +996,10 @@ int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32
   if(rc == DORT_OK) {
     b->wf.dev.total_samples = b->total_samples;
     b->wf.dev.max_waves = wave_bound(b->total_samples, tn.capacity, b->max_depth);
-    JobTable table{b->d_jobs, n};
-    rc = wf_build_graph(&b->wf, table, tn);
+    bool general = false;
+    for(uint32_t j = 0; j < n; ++j) { general = general || scene_needs_general(scenes[j], params[j]); }
+    rc = general ? wf_build_graph(&b->wf, JobTable<true>{b->d_jobs, n}, tn)
+                 : wf_build_graph(&b->wf, JobTable<false>{b->d_jobs, n}, tn);
     b->wf.jobs_cached = b->d_jobs;
   }
   if(rc != DORT_OK) {
