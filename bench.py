@@ -540,15 +540,16 @@ def run_dort_pt(args):
                    "sample": f"{procs} single-threaded reference PathRenderer processes, each "
                              f"one {REF_SAMPLE_W}x{REF_SAMPLE_H} frame at 1 spp of the same "
                              f"scene and camera ({secs:.1f}s); GGX conductor timed as Phong"}
-            # dominant stage: the extend (closest-hit) stage
-            ext_rays = rays_per_frame * stages["extend"] / max(1e-9, sum(
-                stages[k] for k in ("extend", "shadow", "neeb")))
+            # dominant stage: the extend (closest-hit) stage, over the frame's
+            # extension rays (counted by the staged run)
+            ext_rays = stages["extend_rays"]
             bytes_per_ray = 32 + 16 + n_node * 32 + n_tri * 36
             achieved = ext_rays * bytes_per_ray / (stages["extend"] / 1e3) / 1e9
             rl = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                   "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
                   "kernel": "wf_extend (closest hit)", "bytes_per_ray": bytes_per_ray,
                   "n_node": n_node, "n_tri": n_tri, "work_sample_rays": nwork,
+                  "extend_rays_per_frame": ext_rays,
                   "stage_ms_per_frame": {k: stages[k] for k in
                                          ("regen", "extend", "shade", "shadow", "neeb")}}
         line = {
@@ -565,6 +566,7 @@ def run_dort_pt(args):
                        "rays_per_frame": rays_per_frame,
                        "mrays_per_s": rays_per_frame * args.steps * world / (ms_max / 1e3) / 1e6,
                        "queue_capacity": tuning["queue_capacity"],
+                       "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
                        "l2": "frame state (queues 1 GB, image 25 MB) larger than L2"},

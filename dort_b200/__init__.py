@@ -183,15 +183,15 @@ class Scene:
     def wavefront_stage_times(self, params: _abi.RenderParams, tuning: dict | None = None):
         """Per-stage milliseconds of one frame run wave by wave (measurement)."""
         ms = (ctypes.c_double * 6)()
-        rays = ctypes.c_double(0.0)
+        rays = (ctypes.c_double * 4)()
         t = wavefront_tuning(**tuning) if tuning else None
         _abi.check(_abi.lib().dort_gpu_wavefront_stage_times(
-            self.handle, ctypes.byref(params), ctypes.byref(t) if t else None, ms,
-            ctypes.byref(rays)))
+            self.handle, ctypes.byref(params), ctypes.byref(t) if t else None, ms, rays))
         names = ["regen", "extend", "shade", "shadow", "neeb"]
         out = {n: ms[i] for i, n in enumerate(names)}
         out["waves"] = ms[5]
-        out["rays"] = rays.value
+        out["rays"] = rays[0]
+        out["extend_rays"], out["shadow_rays"], out["neeb_rays"] = rays[1], rays[2], rays[3]
         return out
 
     def adjoint_forward(self, params: _abi.RenderParams, tri_albedo=None, tri_emission=None):

@@ -424,7 +424,7 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
 
 extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* params,
                                               const dort_wavefront_tuning* tuning,
-                                              double out_ms[6], double* out_rays) {
+                                              double out_ms[6], double out_rays[4]) {
   clear_error();
   if(!scene || !params || !out_ms) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -439,14 +439,18 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
   }
-  int rc = wavefront_stage_times(scene, pp, tn, d_out, 0, out_ms);
+  double stage_rays[3];
+  int rc = wavefront_stage_times(scene, pp, tn, d_out, 0, out_ms, stage_rays);
   cudaFree(d_out);
-  if(rc == DORT_OK && out_rays) {
+  if(rc == DORT_OK) {
     uint64_t rays = 0;
     uint32_t waves = 0, error = 0;
     rc = wavefront_counters(scene, &rays, &waves, &error, 0);
-    *out_rays = double(rays);
     out_ms[5] = double(waves);
+    if(out_rays) {
+      out_rays[0] = double(rays);
+      for(int k = 0; k < 3; ++k) { out_rays[k + 1] = stage_rays[k]; }
+    }
   }
   return rc;
 }

@@ -842,7 +842,7 @@ __global__ void wf_control_host(WfDev w, uint32_t* more_flag) {
 
 template<bool G>
 static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
-                         cudaStream_t st, double ms[6]) {
+                         cudaStream_t st, double ms[6], double stage_rays[3]) {
   if(!s->wavefront) { s->wavefront = new Wavefront(); }
   Wavefront* wf = s->wavefront;
   uint32_t npix = pp.width * pp.height;
@@ -853,11 +853,13 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   SingleJob<G> jobs{s->pt, pp};
   WfGrids g = wf_grids<SingleJob<G>>(tn);
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
+  // more[0]: loop flag; more[1..6]: the counters C_ACT0 .. C_NEEB of the wave
   uint32_t* more = nullptr;
-  DG_CUDA(cudaMallocHost(&more, sizeof(uint32_t)));
+  DG_CUDA(cudaMallocHost(&more, 8 * sizeof(uint32_t)));
   cudaEvent_t ev[6];
   for(auto& e : ev) { cudaEventCreate(&e); }
   for(int k = 0; k < 6; ++k) { ms[k] = 0.0; }
+  for(int k = 0; k < 3; ++k) { stage_rays[k] = 0.0; }
   wf_init<<<(std::max(tn.capacity, npix) + 255) / 256, 256, 0, st>>>(wf->dev, npix);
   bool ok = cudaGetLastError() == cudaSuccess;
   for(uint32_t wave = 0; ok && wave < wf->dev.max_waves + 1; ++wave) {
@@ -872,12 +874,19 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
     cudaEventRecord(ev[4], st);
     wf_neeb<SingleJob<G>><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);
+    cudaMemcpyAsync(more + 1, wf->dev.ctr, (C_NEEB + 1) * sizeof(uint32_t),
+                    cudaMemcpyDeviceToHost, st);
     wf_control_host<<<1, 1, 0, st>>>(wf->dev, more);
     ok = cudaStreamSynchronize(st) == cudaSuccess;
     for(int k = 0; ok && k < 5; ++k) {
       float t = 0.f;
       cudaEventElapsedTime(&t, ev[k], ev[k + 1]);
       ms[k] += t;
+    }
+    if(ok) {
+      stage_rays[0] += double(more[1 + C_ACT0 + (wave & 1u)]);
+      stage_rays[1] += double(more[1 + C_SHADOW]);
+      stage_rays[2] += double(more[1 + C_NEEB]);
     }
     if(!*more) { break; }
   }
@@ -898,9 +907,10 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
 }
 
 int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
-                          float* d_out, cudaStream_t st, double ms[6]) {
-  return scene_needs_general(s->pt, pp) ? stage_times_g<true>(s, pp, tn, d_out, st, ms)
-                                        : stage_times_g<false>(s, pp, tn, d_out, st, ms);
+                          float* d_out, cudaStream_t st, double ms[6], double stage_rays[3]) {
+  return scene_needs_general(s->pt, pp)
+      ? stage_times_g<true>(s, pp, tn, d_out, st, ms, stage_rays)
+      : stage_times_g<false>(s, pp, tn, d_out, st, ms, stage_rays);
 }
 
 int wavefront_counters_of(Wavefront* wf, uint64_t* rays, uint32_t* waves, uint32_t* error,

@@ -20,8 +20,10 @@ struct Wavefront;
 void wavefront_destroy(Wavefront* wf);
 int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, float* d_out,
                      cudaStream_t st);
+// ms: per-stage milliseconds (5) and waves; stage_rays: extend, shadow and
+// BSDF-strategy rays of the frame.
 int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
-                          float* d_out, cudaStream_t st, double ms[6]);
+                          float* d_out, cudaStream_t st, double ms[6], double stage_rays[3]);
 struct WavefrontBatch;
 int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32_t n,
                            const WfTuning& tn, WavefrontBatch** out);

@@ -365,10 +365,12 @@ int dort_gpu_batch_destroy(dort_batch* batch);
 /* Measurement entry: renders the same frame wave by wave from the host
  * (without the graph) with CUDA events around each stage; out_ms[0..4] =
  * total milliseconds of regen, extend, shade, shadow, neeb; out_ms[5] = waves;
- * out_rays = rays traced. */
+ * out_rays (optional, 4 doubles) = rays traced in total, by the extend stage
+ * (closest hit), by the shadow stage (any hit) and by the BSDF-strategy stage
+ * (closest hit). */
 int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* params,
                                    const dort_wavefront_tuning* tuning, double out_ms[6],
-                                   double* out_rays);
+                                   double out_rays[4]);
 
 /* ---- adjoint --------------------------------------------------------------
  * No reference counterpart.  Differentiable rendering of the "pt" estimator
