@@ -410,6 +410,31 @@ struct Collapser {
 
 }  // namespace
 
+void expand_node_planes(const std::vector<WideNode>& in, std::vector<WideNodeF>& out) {
+  out.resize(in.size());
+  for(size_t i = 0; i < in.size(); ++i) {
+    const WideNode& n = in[i];
+    WideNodeF& f = out[i];
+    std::memset(&f, 0, sizeof(f));
+    f.child_base = n.child_base;
+    f.tri_base = n.tri_base;
+    std::memcpy(f.meta, n.meta, 8);
+    f.imask = n.imask;
+    for(int a = 0; a < 3; ++a) {
+      double s = std::ldexp(1.0, int(n.e[a]) - 127);
+      for(int k = 0; k < 8; ++k) {
+        double lo = double(n.p[a]) + double(n.qlo[a][k]) * s;
+        double hi = double(n.p[a]) + double(n.qhi[a][k]) * s;
+        float lf = float(lo), hf = float(hi);
+        if(double(lf) > lo) { lf = std::nextafter(lf, -INFINITY); }
+        if(double(hf) < hi) { hf = std::nextafter(hf, INFINITY); }
+        f.pl[a][0][k] = lf;
+        f.pl[a][1][k] = hf;
+      }
+    }
+  }
+}
+
 bool build_wide_bvh(const float* verts, uint32_t vert_count,
                     const uint32_t* tris, uint32_t tri_count,
                     const BuildOptions& opts, WideBvh& out, std::string& err) {
@@ -448,7 +473,11 @@ bool build_wide_bvh(const float* verts, uint32_t vert_count,
   BinaryBuilder bb(prims, opts);
   if(tri_count > 0) { bb.build(); }
   Collapser col{bb.nodes, bb.order_, verts, tris, opts, out, err};
-  return col.run();
+  if(!col.run()) { return false; }
+#ifndef DORT_NODE_QUANTIZED
+  expand_node_planes(out.nodes, out.nodes_f);
+#endif
+  return true;
 }
 
 }  // namespace dort_gpu

@@ -20,7 +20,8 @@
 //
 // Child boxes are quantized outward with one full grid step of margin on
 // every side, so that the device slab test (rounded float arithmetic) never
-// culls a child that contains a hit.
+// culls a child that contains a hit.  The device traverses WideNodeF (below):
+// the same nodes with those quantized planes expanded to floats.
 //
 //   Triangle (48 bytes = 3 x float4, leaf order):
 //     (p0.xyz, original triangle index as bits), (e1.xyz, 0), (e2.xyz, 0)
@@ -45,6 +46,22 @@ struct alignas(16) WideNode {
 };
 static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
 
+// The same node with float child planes: the quantized planes p + s q of
+// every child (margin included) rounded outward to float, so the device box
+// test needs no byte-to-float conversion.  224 bytes = 14 x uint4.
+struct alignas(16) WideNodeF {
+  uint32_t child_base;
+  uint32_t tri_base;
+  uint8_t meta[8];
+  uint32_t imask;
+  uint32_t pad[3];
+  float pl[3][2][8];   // [axis][0: lo, 1: hi][slot]
+};
+static_assert(sizeof(WideNodeF) == 224, "WideNodeF must be 224 bytes");
+
+// Expands quantized nodes into WideNodeF.
+void expand_node_planes(const std::vector<WideNode>& in, std::vector<WideNodeF>& out);
+
 struct alignas(16) LeafTri {
   float p0[3];
   uint32_t id;
@@ -64,11 +81,28 @@ struct BuildOptions {
 
 struct WideBvh {
   std::vector<WideNode> nodes;
+  std::vector<WideNodeF> nodes_f;   // float-plane nodes (traversed unless DORT_NODE_QUANTIZED)
   std::vector<LeafTri> tris;
   uint32_t depth = 0;          // levels of wide nodes
   double root_lo[3] = {0, 0, 0};
   double root_hi[3] = {0, 0, 0};
 };
+
+// The node array the device traversal reads, and its size in bytes.
+inline const void* traversal_nodes(const WideBvh& b) {
+#ifndef DORT_NODE_QUANTIZED
+  return b.nodes_f.data();
+#else
+  return b.nodes.data();
+#endif
+}
+inline size_t traversal_node_bytes(const WideBvh& b) {
+#ifndef DORT_NODE_QUANTIZED
+  return b.nodes_f.size() * sizeof(WideNodeF);
+#else
+  return b.nodes.size() * sizeof(WideNode);
+#endif
+}
 
 // Maximum stack depth the device traversal supports; the builder guarantees
 // that no root-to-leaf path of the wide tree is deeper.

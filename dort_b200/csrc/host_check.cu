@@ -32,7 +32,7 @@ extern "C" int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const fl
     return fail(DORT_ERR_INVALID, err);
   }
   TraceScene sc;
-  sc.nodes = reinterpret_cast<const uint4*>(bvh.nodes.data());
+  sc.nodes = reinterpret_cast<const uint4*>(traversal_nodes(bvh));
   sc.tris = reinterpret_cast<const float4*>(bvh.tris.data());
   sc.node_count = uint32_t(bvh.nodes.size());
   sc.tri_count = uint32_t(bvh.tris.size());

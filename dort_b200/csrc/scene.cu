@@ -57,9 +57,13 @@ static int upload(dort_scene* s, const std::vector<T>& v, const T** out) {
 
 static int scene_upload(dort_scene* s, const HostScene& hs) {
   int rc;
-  const WideNode* nodes;
+  const unsigned char* nodes;
   const LeafTri* tris;
-  if((rc = upload(s, hs.bvh.nodes, &nodes)) != DORT_OK) { return rc; }
+  {
+    const unsigned char* src = static_cast<const unsigned char*>(traversal_nodes(hs.bvh));
+    std::vector<unsigned char> bytes(src, src + traversal_node_bytes(hs.bvh));
+    if((rc = upload(s, bytes, &nodes)) != DORT_OK) { return rc; }
+  }
   if((rc = upload(s, hs.bvh.tris, &tris)) != DORT_OK) { return rc; }
   s->trace.nodes = reinterpret_cast<const uint4*>(nodes);
   s->trace.tris = reinterpret_cast<const float4*>(tris);

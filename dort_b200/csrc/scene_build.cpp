@@ -502,7 +502,7 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
 PtScene host_view(const HostScene& hs) {
   PtScene sc;
   std::memset(&sc, 0, sizeof(sc));
-  sc.trace.nodes = reinterpret_cast<const uint4*>(hs.bvh.nodes.data());
+  sc.trace.nodes = reinterpret_cast<const uint4*>(traversal_nodes(hs.bvh));
   sc.trace.tris = reinterpret_cast<const float4*>(hs.bvh.tris.data());
   sc.trace.node_count = uint32_t(hs.bvh.nodes.size());
   sc.trace.tri_count = uint32_t(hs.bvh.tris.size());

