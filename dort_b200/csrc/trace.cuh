@@ -248,95 +248,122 @@ DG_HD uint32_t node_hitmask_f(const uint4* np, uint4 h0, float ix, float iy, flo
   return hitmask;
 }
 
-// Closest hit (ANY_HIT = false) or any hit (ANY_HIT = true) of one ray.
-// Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
-// triangle found to intersect.  `steps` (optional) counts node visits and
-// triangle tests.
-template<bool ANY_HIT, bool EXACT_MT = true>
-DG_HD Hit trace_ray(const TraceScene& sc,
-                                         float ox, float oy, float oz, float t_min,
-                                         float dx, float dy, float dz, float t_max) {
-  Hit best;
-  best.t = t_max;
-  best.b1 = 0.f;
-  best.b2 = 0.f;
-  best.prim = kMiss;
-  if(sc.node_count == 0) { return best; }
+// Traversal state of one ray.  trav_step advances it by one node (the
+// node's child boxes, then the triangles of its leaf children), so a kernel
+// can hand a lane whose ray has finished a new ray between steps (see
+// raycast_kernel) instead of letting it idle until the warp's slowest ray is
+// done.  trace_ray runs the steps of one ray to the end.
+struct TravState {
+  float ox, oy, oz, dx, dy, dz, t_min;
+  float ix, iy, iz;
+#ifndef DORT_NODE_QUANTIZED
+  float nox, noy, noz;   // -o * inv: one FMA per plane
+#endif
+  uint32_t oct_inv, oct_inv4;
+  uint2 group;           // current node group: (base, child-hit bits << 24 | internal mask)
+  int sp;                // entries on the caller's stack
+  Hit best;              // closest hit so far (best.t = t_max while none)
+};
 
+DG_HD void trav_init(TravState& s, const TraceScene& sc, float ox, float oy, float oz,
+                     float t_min, float dx, float dy, float dz, float t_max) {
+  s.ox = ox; s.oy = oy; s.oz = oz; s.dx = dx; s.dy = dy; s.dz = dz; s.t_min = t_min;
+  s.best.t = t_max;
+  s.best.b1 = 0.f;
+  s.best.b2 = 0.f;
+  s.best.prim = kMiss;
   // Box-test reciprocals; zero components become tiny so no NaN appears.
   const float tiny = 1e-20f;
-  float ix = 1.f / (fabsf(dx) < tiny ? copysignf(tiny, dx) : dx);
-  float iy = 1.f / (fabsf(dy) < tiny ? copysignf(tiny, dy) : dy);
-  float iz = 1.f / (fabsf(dz) < tiny ? copysignf(tiny, dz) : dz);
-  const uint32_t oct_inv = (ix < 0.f ? 0u : 1u) | (iy < 0.f ? 0u : 2u) | (iz < 0.f ? 0u : 4u);
-  const uint32_t oct_inv4 = oct_inv * 0x01010101u;
+  s.ix = 1.f / (fabsf(dx) < tiny ? copysignf(tiny, dx) : dx);
+  s.iy = 1.f / (fabsf(dy) < tiny ? copysignf(tiny, dy) : dy);
+  s.iz = 1.f / (fabsf(dz) < tiny ? copysignf(tiny, dz) : dz);
+  s.oct_inv = (s.ix < 0.f ? 0u : 1u) | (s.iy < 0.f ? 0u : 2u) | (s.iz < 0.f ? 0u : 4u);
+  s.oct_inv4 = s.oct_inv * 0x01010101u;
 #ifndef DORT_NODE_QUANTIZED
-  const float nox = -ox * ix, noy = -oy * iy, noz = -oz * iz;
+  s.nox = -ox * s.ix;
+  s.noy = -oy * s.iy;
+  s.noz = -oz * s.iz;
 #endif
+  s.sp = 0;
+  // root group: internal bit 31 with an empty internal-slot mask -> node 0;
+  // an empty tree starts finished
+  s.group = make_uint2(0u, sc.node_count ? 0x80000000u : 0u);
+}
 
-  uint2 stack[kTraceStack];
-  int sp = 0;
-  // root group: internal bit 31 with an empty internal-slot mask -> node 0
-  uint2 group = make_uint2(0u, 0x80000000u);
+// One traversal step; returns true when the ray is finished (s.best holds
+// the closest hit, or for ANY_HIT the first hit found, or prim = kMiss).
+// `stack` has kTraceStack entries.
+template<bool ANY_HIT, bool EXACT_MT>
+DG_HD bool trav_step(TravState& s, const TraceScene& sc, uint2* stack) {
+  if((s.group.y & 0xff000000u) == 0u) {
+    if(s.sp == 0) { return true; }
+    s.group = stack[--s.sp];
+  }
+  uint32_t bit = 31u - DG_CLZ(s.group.y & 0xff000000u);
+  s.group.y &= ~(1u << bit);
+  uint32_t slot = (bit - 24u) ^ s.oct_inv;
+  uint32_t node_idx = s.group.x + DG_POPC(s.group.y & 0xffu & ((1u << slot) - 1u));
 
-  for(;;) {
-    if((group.y & 0xff000000u) == 0u) {
-      if(sp == 0) { break; }
-      group = stack[--sp];
-    }
-    uint32_t bit = 31u - DG_CLZ(group.y & 0xff000000u);
-    group.y &= ~(1u << bit);
-    uint32_t slot = (bit - 24u) ^ oct_inv;
-    uint32_t node_idx = group.x + DG_POPC(group.y & 0xffu & ((1u << slot) - 1u));
-
-    const uint4* np = sc.nodes + kNodeWords * size_t(node_idx);
+  const uint4* np = sc.nodes + kNodeWords * size_t(node_idx);
 #ifndef DORT_NODE_QUANTIZED
-    uint4 h0 = DG_LDG(np);
-    uint32_t imask = DG_LDG(&np[1].x);
-    uint32_t hitmask = node_hitmask_f(np, h0, ix, iy, iz, nox, noy, noz, t_min, best.t,
-                                      oct_inv4);
-    const uint32_t child_base = h0.x, tri_base = h0.y;
+  uint4 h0 = DG_LDG(np);
+  uint32_t imask = DG_LDG(&np[1].x);
+  uint32_t hitmask = node_hitmask_f(np, h0, s.ix, s.iy, s.iz, s.nox, s.noy, s.noz, s.t_min,
+                                    s.best.t, s.oct_inv4);
+  const uint32_t child_base = h0.x, tri_base = h0.y;
 #else
-    uint4 n0 = DG_LDG(np), n1 = DG_LDG(np + 1), n2 = DG_LDG(np + 2);
-    uint4 n3 = DG_LDG(np + 3), n4 = DG_LDG(np + 4);
-    uint32_t hitmask = node_hitmask(n0, n1, n2, n3, n4, ox, oy, oz, ix, iy, iz,
-                                    t_min, best.t, oct_inv4);
-    const uint32_t child_base = n1.x, tri_base = n1.y, imask = n0.w >> 24;
+  uint4 n0 = DG_LDG(np), n1 = DG_LDG(np + 1), n2 = DG_LDG(np + 2);
+  uint4 n3 = DG_LDG(np + 3), n4 = DG_LDG(np + 4);
+  uint32_t hitmask = node_hitmask(n0, n1, n2, n3, n4, s.ox, s.oy, s.oz, s.ix, s.iy, s.iz,
+                                  s.t_min, s.best.t, s.oct_inv4);
+  const uint32_t child_base = n1.x, tri_base = n1.y, imask = n0.w >> 24;
 #endif
 
-    uint32_t child_hits = hitmask & 0xff000000u;
-    if(child_hits) {
-      if(group.y & 0xff000000u) {
-        // sp < kTraceStack: each push descends one level and the builder
-        // bounds the depth by kMaxWideDepth.
-        stack[sp++] = group;
-      }
-      group = make_uint2(child_base, child_hits | imask);
+  uint32_t child_hits = hitmask & 0xff000000u;
+  if(child_hits) {
+    if(s.group.y & 0xff000000u) {
+      // sp < kTraceStack: each push descends one level and the builder
+      // bounds the depth by kMaxWideDepth.
+      stack[s.sp++] = s.group;
     }
+    s.group = make_uint2(child_base, child_hits | imask);
+  }
 
-    uint32_t tri_hits = hitmask & 0x00ffffffu;
-    while(tri_hits) {
-      uint32_t b = DG_FFS(tri_hits) - 1u;
-      tri_hits &= tri_hits - 1u;
-      const float4* tp = sc.tris + 3 * size_t(tri_base + b);
-      float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
-      float t, b1, b2;
-      bool h = EXACT_MT
-          ? mt_exact(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2)
-          : mt_fast(a, e1, e2, ox, oy, oz, dx, dy, dz, t_min, best.t, t, b1, b2);
-      if(h) {
-        uint32_t id = DG_AS_UINT(a.w);
-        if(ANY_HIT) {
-          best.t = t; best.b1 = b1; best.b2 = b2; best.prim = id;
-          return best;
-        }
-        if(best.prim == kMiss || t < best.t || id > best.prim) {
-          best.t = t; best.b1 = b1; best.b2 = b2; best.prim = id;
-        }
+  uint32_t tri_hits = hitmask & 0x00ffffffu;
+  while(tri_hits) {
+    uint32_t b = DG_FFS(tri_hits) - 1u;
+    tri_hits &= tri_hits - 1u;
+    const float4* tp = sc.tris + 3 * size_t(tri_base + b);
+    float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
+    float t, b1, b2;
+    bool h = EXACT_MT
+        ? mt_exact(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2)
+        : mt_fast(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2);
+    if(h) {
+      uint32_t id = DG_AS_UINT(a.w);
+      if(ANY_HIT) {
+        s.best.t = t; s.best.b1 = b1; s.best.b2 = b2; s.best.prim = id;
+        return true;
+      }
+      if(s.best.prim == kMiss || t < s.best.t || id > s.best.prim) {
+        s.best.t = t; s.best.b1 = b1; s.best.b2 = b2; s.best.prim = id;
       }
     }
   }
-  return best;
+  return (s.group.y & 0xff000000u) == 0u && s.sp == 0;
+}
+
+// Closest hit (ANY_HIT = false) or any hit (ANY_HIT = true) of one ray.
+// Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
+// triangle found to intersect.
+template<bool ANY_HIT, bool EXACT_MT = true>
+DG_HD Hit trace_ray(const TraceScene& sc, float ox, float oy, float oz, float t_min,
+                    float dx, float dy, float dz, float t_max) {
+  TravState s;
+  trav_init(s, sc, ox, oy, oz, t_min, dx, dy, dz, t_max);
+  uint2 stack[kTraceStack];
+  while(!trav_step<ANY_HIT, EXACT_MT>(s, sc, stack)) {}
+  return s.best;
 }
 
 }  // namespace dort_gpu
