@@ -24,7 +24,7 @@ __all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
 
 # optional scene-dict keys passed through to scene_desc
 SCENE_KEYS = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
-              "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights")
+              "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights", "tri_light_verts")
 
 
 def _ptr(a):
@@ -49,7 +49,8 @@ class _DescHolder:
 def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None,
                sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
                sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
-               bvh_width: int = 8, shapes=None, delta_lights=None, **_ignored) -> _DescHolder:
+               bvh_width: int = 8, shapes=None, delta_lights=None, tri_light_verts=None,
+               **_ignored) -> _DescHolder:
     """SceneDesc for the arrays given.  `shapes`: dicts with kind (SHAPE_*),
     material, param (up to 4), to_world (3x4), emission (RGB) and optionally
     light_to_world (3x4); `delta_lights`: dicts with kind (LIGHT_POINT /
@@ -76,6 +77,7 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
         d.materials = ctypes.cast(mats, ctypes.c_void_p)
         d.material_count = len(materials)
     d.tri_emission = h.arr(tri_emission, np.float32)
+    d.tri_light_verts = h.arr(tri_light_verts, np.float32)
     if sky_rgb is not None:
         sky = np.ascontiguousarray(sky_rgb, np.float32)
         d.sky_rgb = h.arr(sky, np.float32)

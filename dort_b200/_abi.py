@@ -67,7 +67,9 @@ class SceneDesc(ctypes.Structure):
         ("shapes", c_p),
         ("lights", c_p),
         ("light_count", c_u32),
-        ("reserved", c_u32 * 5),
+        ("pad0", c_u32),
+        ("tri_light_verts", c_p),
+        ("reserved", c_u32 * 2),
     ]
 
 

@@ -426,7 +426,7 @@ class Builder:
             raise ValueError("Frame stack is not empty")
         if self.state_stack:
             raise ValueError("State stack is not empty")
-        verts, tris, tri_mat, tri_em = [], [], [], []
+        verts, tris, tri_mat, tri_em, light_verts = [], [], [], [], []
         shapes = []
         mats, mat_index = [], {}
 
@@ -438,6 +438,7 @@ class Builder:
             return mat_index[k]
 
         lit_prims = set()
+        any_light_verts = [False]
 
         def emit(prims, outer: Transform):
             for p in prims:
@@ -453,14 +454,17 @@ class Builder:
                     if not np.allclose(p.light.data["transform"].m, prim_t.m, rtol=0, atol=0):
                         light_t = p.light.data["transform"]
                 if p.kind == "triangle" or p.shape.kind == "tri":
-                    if light_t is not None:
-                        raise ValueError("a triangle light whose transform differs from its "
-                                         "primitive's is not supported")
                     mesh, i = p.shape.mesh, p.shape.index
                     t = outer if p.kind == "triangle" else outer * p.transform
                     base = len(verts)
                     for k in range(3):
-                        verts.append(t.apply_point(mesh.points[mesh.vertices[i + k]]))
+                        src = mesh.points[mesh.vertices[i + k]]
+                        verts.append(t.apply_point(src))
+                        # the triangle the light samples (its own transform)
+                        light_verts.append(verts[-1] if light_t is None
+                                           else light_t.apply_point(src))
+                    if light_t is not None:
+                        any_light_verts[0] = True
                     tris.append((base, base + 1, base + 2))
                     tri_mat.append(mat_id(p.material))
                     tri_em.append(em)
@@ -479,6 +483,8 @@ class Builder:
              "materials": mats or [lambert_material(rgb(0.5)).as_dict()],
              "tri_emission": np.asarray(tri_em, np.float32).reshape(-1, 3),
              "shapes": shapes, "delta_lights": []}
+        if any_light_verts[0]:
+            d["tri_light_verts"] = np.asarray(light_verts, np.float32).reshape(-1, 9)
         sky = np.zeros(3)
         for light in self.lights:
             if light.kind == "point":

@@ -245,7 +245,13 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
         l.kind = LIGHT_TRI;
         l.tri = t;
         for(int a = 0; a < 3; ++a) { l.L[a] = le[a]; }
-        F3 p0 = f3(p[0]), e1 = sub(f3(p[1]), p0), e2 = sub(f3(p[2]), p0);
+        // the light's own triangle when it differs from the primitive
+        const float* lv = desc->tri_light_verts ? desc->tri_light_verts + 9 * size_t(t) : nullptr;
+        for(int a = 0; lv && a < 9; ++a) {
+          if(!std::isfinite(lv[a])) { err = "tri_light_verts must be finite"; return false; }
+        }
+        F3 p0 = lv ? f3(lv) : f3(p[0]);
+        F3 e1 = sub(lv ? f3(lv + 3) : f3(p[1]), p0), e2 = sub(lv ? f3(lv + 6) : f3(p[2]), p0);
         l.area = 0.5f * len(crs(e1, e2));      // Triangle::area (triangle.cpp:56-60)
         F3 nn = nrm(crs(e2, e1));
         l.p0[0] = p0.x; l.p0[1] = p0.y; l.p0[2] = p0.z;

@@ -164,6 +164,13 @@ typedef struct dort_light {
  *                 sky_scale (0,0,0 = 1,1,1), up and forward vectors sky_up /
  *                 sky_fwd (0 = +y / +x)
  *   bvh_width     children per BVH node, 2..8 (0: 8)
+ *   tri_light_verts  for each emissive triangle, the triangle (3 points) its
+ *                 light samples and weights, when that differs from the
+ *                 primitive: a light and its primitive placed by different
+ *                 transforms, as dort.builder.add_diffuse_light makes them
+ *                 under a non-identity builder transform (builder_ext.lua:
+ *                 38-48, lua_builder.cpp:227-232); the primitive is still
+ *                 what rays hit.  Entries of other triangles are ignored.
  */
 typedef struct dort_scene_desc {
   uint32_t struct_size;            /* sizeof(dort_scene_desc) */
@@ -187,7 +194,9 @@ typedef struct dort_scene_desc {
   const dort_shape* shapes;        /* shape_count, or NULL */
   const dort_light* lights;        /* light_count delta lights, or NULL */
   uint32_t light_count;
-  uint32_t reserved[5];
+  uint32_t pad0;
+  const float* tri_light_verts;    /* tri_count * 9, or NULL: see below */
+  uint32_t reserved[2];
 } dort_scene_desc;
 
 typedef struct dort_scene dort_scene;

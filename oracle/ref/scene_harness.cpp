@@ -151,6 +151,8 @@ extern "C" int dref_scene_render(const dort_scene_desc* d, const dort_render_par
     materials.push_back(std::make_shared<LambertMaterial>(const_texture<Spectrum>(Spectrum(0.5f))));
   }
 
+  // the triangles lights sample when they differ from their primitives
+  auto light_mesh = std::make_shared<Mesh>();
   std::vector<std::unique_ptr<Primitive>> prims;
   std::vector<std::shared_ptr<Light>> lights;
   for(uint32_t t = 0; t < d->tri_count; ++t) {
@@ -158,7 +160,18 @@ extern "C" int dref_scene_render(const dort_scene_desc* d, const dort_render_par
     const float* le = d->tri_emission ? d->tri_emission + 3 * size_t(t) : nullptr;
     if(le && !black(le)) {
       auto shape = std::make_shared<TriangleShape>(mesh.get(), 3 * t);
-      auto light = std::make_shared<DiffuseLight>(shape, identity(), Spectrum(le[0], le[1], le[2]));
+      std::shared_ptr<Shape> light_shape = shape;
+      if(d->tri_light_verts) {
+        const float* lv = d->tri_light_verts + 9 * size_t(t);
+        uint32_t base = uint32_t(light_mesh->points.size());
+        for(int k = 0; k < 3; ++k) {
+          light_mesh->points.push_back(Point(lv[3 * k], lv[3 * k + 1], lv[3 * k + 2]));
+          light_mesh->vertices.push_back(base + uint32_t(k));
+        }
+        light_shape = std::make_shared<TriangleShape>(light_mesh.get(), base);
+      }
+      auto light = std::make_shared<DiffuseLight>(light_shape, identity(),
+          Spectrum(le[0], le[1], le[2]));
       prims.push_back(std::make_unique<ShapePrimitive>(shape, mat, light, identity()));
       lights.push_back(light);
     } else {
@@ -225,6 +238,7 @@ extern "C" int dref_scene_render(const dort_scene_desc* d, const dort_render_par
     if(light->flags & LIGHT_BACKGROUND) { scene->background_lights.push_back(light); }
   }
   scene->meshes.push_back(mesh);
+  scene->meshes.push_back(light_mesh);
 
   const dort_camera& c = rp->camera;
   Mat4x4 m(1.f);
