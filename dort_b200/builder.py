@@ -37,7 +37,7 @@ import math
 
 import numpy as np
 
-from . import _abi
+from . import _abi, ply
 
 # ---- geometry (transform.cpp:49-165; 4x4 matrices, column vectors) ---------
 
@@ -54,6 +54,10 @@ class Transform:
     def apply_point(self, p):
         p = np.asarray(p, np.float64)
         return self.m[:3, :3] @ p + self.m[:3, 3]
+
+    def apply_points(self, p):
+        """apply_point over the rows of an (n, 3) array."""
+        return np.asarray(p, np.float64).reshape(-1, 3) @ self.m[:3, :3].T + self.m[:3, 3]
 
     def apply_vector(self, v):
         return self.m[:3, :3] @ np.asarray(v, np.float64)
@@ -204,6 +208,13 @@ class Shape:
 
     def __init__(self, kind, param=(), mesh=None, index=0):
         self.kind, self.param, self.mesh, self.index = kind, tuple(param), mesh, index
+
+
+def read_ply_mesh(file_name) -> Mesh:
+    """dort.shape.read_ply_mesh (lua_shape.cpp:225-241): the file's points
+    (untransformed) and its faces fanned into triangles."""
+    pts, verts = ply.read_ply(file_name)
+    return Mesh(pts, verts)
 
 
 def sphere(radius):
@@ -371,6 +382,30 @@ class Builder:
         self.frame.append(_Prim("triangle", shape=Shape("tri", mesh=mesh, index=index),
                                 material=self.material))
 
+    def add_read_ply_mesh(self, file_name):
+        """lua_builder.cpp:418-448: every triangle of the file as a separate
+        primitive with the current material, its points taken through the
+        builder's transform."""
+        mesh = read_ply_mesh(file_name)
+        self._need_material()
+        self._add_mesh(mesh)
+
+    def add_ply_mesh(self, mesh: Mesh):
+        """lua_builder.cpp:501-525: the triangles of a mesh read by
+        read_ply_mesh, its points taken through the builder's transform."""
+        self._need_material()
+        self._add_mesh(mesh)
+
+    # one BVH per mesh in the reference (MeshBvhPrimitive); the same
+    # triangles in the scene's one BVH here
+    add_read_ply_mesh_as_bvh = add_read_ply_mesh
+    add_ply_mesh_as_bvh = add_ply_mesh
+
+    def _add_mesh(self, mesh: Mesh):
+        pts = self.transform.apply_points(mesh.points)
+        self.frame.append(_Prim("mesh", shape=Shape("tri", mesh=Mesh(pts, mesh.vertices)),
+                                material=self.material))
+
     def add_primitive(self, prim: _Prim):
         self.frame.append(_Prim("instance", frame=prim.frame, transform=self.transform))
 
@@ -444,6 +479,18 @@ class Builder:
             for p in prims:
                 if p.kind == "instance":
                     emit(p.frame, outer * p.transform)
+                    continue
+                if p.kind == "mesh":
+                    # all triangles of a mesh at once, in index order
+                    tri_vertices = p.shape.mesh.vertices[:len(p.shape.mesh.vertices) // 3 * 3]
+                    n = len(tri_vertices) // 3
+                    base = len(verts)
+                    world = outer.apply_points(p.shape.mesh.points)[tri_vertices].tolist()
+                    verts.extend(world)
+                    light_verts.extend(world)
+                    tris.extend((base + np.arange(3 * n)).reshape(-1, 3).tolist())
+                    tri_mat.extend([mat_id(p.material)] * n)
+                    tri_em.extend([(0.0, 0.0, 0.0)] * n)
                     continue
                 em = (0.0, 0.0, 0.0)
                 light_t = None

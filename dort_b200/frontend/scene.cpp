@@ -125,15 +125,22 @@ static int shape_mesh(lua_State* l) {
   return 1;
 }
 
-// PLY reading (ascii and binary little / big endian; "vertex" x y z and
-// "face" vertex_indices, polygons fanned into triangles as the reference's
-// ply_mesh.cpp:45-63 does).
+// PLY reading as the reference's read_ply_callbacks (ply_mesh.cpp:9-78, over
+// rply): ascii and binary little / big endian; x / y / z of "vertex" update
+// one persistent point, emitted (rounded to float) when z is read; the
+// "vertex_indices" list of "face" fanned into triangles (i0, i_{j-1}, i_j).
+// An index past the points is an error here (the reference reads out of
+// bounds later).
 static bool read_ply(const char* path, const Transform& t, Mesh& out, std::string& err) {
   std::ifstream f(path, std::ios::binary);
   if(!f) { err = std::string("Could not open ply mesh file for reading: ") + path; return false; }
+  auto fail = [&](const std::string& why) {
+    err = std::string("Could not read ply file: ") + path + " (" + why + ")";
+    return false;
+  };
   std::string line;
   std::getline(f, line);
-  if(line.rfind("ply", 0) != 0) { err = "not a PLY file"; return false; }
+  if(line.rfind("ply", 0) != 0) { return fail("not a PLY file"); }
   enum Fmt { ASCII, BLE, BBE } fmt = ASCII;
   struct Prop { std::string name, type, count_type; bool list = false; };
   struct Elem { std::string name; uint64_t count = 0; std::vector<Prop> props; };
@@ -146,13 +153,16 @@ static bool read_ply(const char* path, const Transform& t, Mesh& out, std::strin
     if(w == "format") {
       std::string fm;
       ss >> fm;
-      fmt = fm == "ascii" ? ASCII : (fm == "binary_little_endian" ? BLE : BBE);
+      if(fm == "ascii") { fmt = ASCII; }
+      else if(fm == "binary_little_endian") { fmt = BLE; }
+      else if(fm == "binary_big_endian") { fmt = BBE; }
+      else { return fail("unknown PLY format " + fm); }
     } else if(w == "element") {
       Elem e;
       ss >> e.name >> e.count;
       elems.push_back(e);
     } else if(w == "property") {
-      if(elems.empty()) { err = "PLY property before element"; return false; }
+      if(elems.empty()) { return fail("PLY property before element"); }
       Prop pr;
       ss >> pr.type;
       if(pr.type == "list") { pr.list = true; ss >> pr.count_type >> pr.type; }
@@ -190,34 +200,32 @@ static bool read_ply(const char* path, const Transform& t, Mesh& out, std::strin
     return read_bin(ty, v);
   };
   size_t base = out.points.size();
+  float xyz[3] = {0, 0, 0};
   for(const Elem& e : elems) {
     for(uint64_t k = 0; k < e.count; ++k) {
-      double xyz[3] = {0, 0, 0};
       std::vector<uint32_t> face;
       for(const Prop& pr : e.props) {
         if(pr.list) {
           double cnt;
-          if(!read_val(pr.count_type, cnt)) { err = "truncated PLY file"; return false; }
+          if(!read_val(pr.count_type, cnt)) { return fail("truncated PLY file"); }
           for(int64_t j = 0; j < int64_t(cnt); ++j) {
             double v;
-            if(!read_val(pr.type, v)) { err = "truncated PLY file"; return false; }
-            if(e.name == "face" && (pr.name == "vertex_indices" || pr.name == "vertex_index")) {
-              face.push_back(uint32_t(v));
-            }
+            if(!read_val(pr.type, v)) { return fail("truncated PLY file"); }
+            if(e.name == "face" && pr.name == "vertex_indices") { face.push_back(uint32_t(v)); }
           }
         } else {
           double v;
-          if(!read_val(pr.type, v)) { err = "truncated PLY file"; return false; }
+          if(!read_val(pr.type, v)) { return fail("truncated PLY file"); }
           if(e.name == "vertex") {
-            if(pr.name == "x") { xyz[0] = v; } else if(pr.name == "y") { xyz[1] = v; }
-            else if(pr.name == "z") { xyz[2] = v; }
+            if(pr.name == "x") { xyz[0] = float(v); } else if(pr.name == "y") { xyz[1] = float(v); }
+            else if(pr.name == "z") {
+              xyz[2] = float(v);
+              out.points.push_back(t.mat.point(V3{xyz[0], xyz[1], xyz[2]}));
+            }
           }
         }
       }
-      if(e.name == "vertex") {
-        V3 pt{float(xyz[0]), float(xyz[1]), float(xyz[2])};
-        out.points.push_back(t.mat.point(pt));
-      } else if(e.name == "face") {
+      if(e.name == "face") {
         for(size_t j = 2; j < face.size(); ++j) {
           out.vertices.push_back(uint32_t(base + face[0]));
           out.vertices.push_back(uint32_t(base + face[j - 1]));
@@ -227,7 +235,7 @@ static bool read_ply(const char* path, const Transform& t, Mesh& out, std::strin
     }
   }
   for(uint32_t v : out.vertices) {
-    if(v >= out.points.size()) { err = "PLY face index out of range"; return false; }
+    if(v >= out.points.size()) { return fail("PLY face index out of range"); }
   }
   return true;
 }

@@ -324,3 +324,25 @@ def ref_scene_render(scene: dict, params) -> tuple[np.ndarray, float]:
     R.dref_scene_render(ctypes.byref(h.desc), ctypes.byref(params), _ptr(out),
                         ctypes.byref(secs))
     return out, secs.value
+
+
+def ref_read_ply(path: str) -> tuple[np.ndarray, np.ndarray]:
+    """Reads a PLY file with the reference's read_ply_to_mesh (over the rply
+    library it vendors).  Returns (points float32 (n, 3), vertex indices
+    uint32 (3m,)); raises OSError / ValueError as the reference's callers
+    fail."""
+    R = ref()
+    if not hasattr(R, "_ply_ready"):
+        R.dref_read_ply.restype = _i32
+        R.dref_read_ply.argtypes = [ctypes.c_char_p, _P, _u32, _P, _u32, _P]
+        R._ply_ready = True
+    counts = np.zeros(2, np.uint32)
+    rc = R.dref_read_ply(path.encode(), None, 0, None, 0, _ptr(counts))
+    if rc == -1:
+        raise OSError(f"Could not open ply mesh file for reading: {path}")
+    if rc != 0:
+        raise ValueError(f"Could not read ply file: {path}")
+    pts = np.zeros((int(counts[0]), 3), np.float32)
+    verts = np.zeros(int(counts[1]), np.uint32)
+    R.dref_read_ply(path.encode(), _ptr(pts), len(pts), _ptr(verts), len(verts), _ptr(counts))
+    return pts, verts
