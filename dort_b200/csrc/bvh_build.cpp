@@ -9,6 +9,7 @@
 // property of the triangle set), so the device tree is free to be a better
 // one.
 #include "bvh_build.h"
+#include "bvh_wide.h"
 
 #include <algorithm>
 #include <cmath>
@@ -187,43 +188,6 @@ class BinaryBuilder {
   }
 };
 
-// Picks the quantization grid of one axis: step 2^e, origin p one step below
-// the node's lower bound, 253 steps covering the extent; returns false if the
-// exponent cannot be represented.
-bool quantize_axis(float node_lo, float node_hi, const float* clo, const float* chi,
-                   int n, float& p_out, uint8_t& e_out, uint8_t* qlo, uint8_t* qhi) {
-  double lo = node_lo, hi = node_hi;
-  double ext = hi - lo;
-  double mag = std::max(std::fabs(lo), std::fabs(hi));
-  double min_step = std::max(mag * std::ldexp(1.0, -20), std::ldexp(1.0, -100));
-  double step = std::max(ext / 253.0, min_step);
-  int e = int(std::ceil(std::log2(step)));
-  for(int attempt = 0; attempt < 8; ++attempt, ++e) {
-    if(e + 127 < 1 || e + 127 > 254) { return false; }
-    double s = std::ldexp(1.0, e);
-    double pd = lo - s;
-    float pf = float(pd);
-    if(double(pf) > pd) { pf = std::nextafter(pf, -INFINITY); }
-    bool ok = true;
-    for(int i = 0; i < n && ok; ++i) {
-      double ql = std::floor((double(clo[i]) - pf) / s) - 1.0;
-      double qh = std::ceil((double(chi[i]) - pf) / s) + 1.0;
-      if(ql < 0.0 || qh > 255.0) { ok = false; break; }
-      // the dequantized planes must enclose the child with at least one step
-      if(double(pf) + ql * s > double(clo[i]) - s * 0.999 ||
-         double(pf) + qh * s < double(chi[i]) + s * 0.999) { ok = false; break; }
-      qlo[i] = uint8_t(ql);
-      qhi[i] = uint8_t(qh);
-    }
-    if(ok) {
-      p_out = pf;
-      e_out = uint8_t(e + 127);
-      return true;
-    }
-  }
-  return false;
-}
-
 struct Collapser {
   const std::vector<BinNode>& bn;
   const std::vector<uint32_t>& order;
@@ -250,6 +214,15 @@ struct Collapser {
 
   bool is_leaf(uint32_t b) const { return bn[b].left == 0 && bn[b].right == 0; }
 
+  struct Acc {
+    const std::vector<BinNode>& bn;
+    bool leaf(uint32_t b) const { return bn[b].left == 0 && bn[b].right == 0; }
+    uint32_t left(uint32_t b) const { return bn[b].left; }
+    uint32_t right(uint32_t b) const { return bn[b].right; }
+    const float* lo(uint32_t b) const { return bn[b].box.lo; }
+    const float* hi(uint32_t b) const { return bn[b].box.hi; }
+  };
+
   bool run() {
     out.nodes.clear();
     out.tris.clear();
@@ -260,83 +233,20 @@ struct Collapser {
     uint32_t max_depth = 1;
     size_t head = 0;
     uint32_t width = std::min(8u, std::max(2u, opts.width));
+    Acc acc{bn};
     while(head < queue.size()) {
       Pending cur = queue[head++];
       max_depth = std::max(max_depth, cur.depth);
-      // Candidate children: open the largest internal candidate until full.
-      std::vector<uint32_t> cands;
-      if(is_leaf(cur.bin)) {
-        cands.push_back(cur.bin);
-      } else {
-        cands.push_back(bn[cur.bin].left);
-        cands.push_back(bn[cur.bin].right);
-      }
-      while(cands.size() < width) {
-        int best = -1;
-        double best_area = -1.0;
-        for(size_t i = 0; i < cands.size(); ++i) {
-          if(is_leaf(cands[i])) { continue; }
-          double a = bn[cands[i]].box.area();
-          if(a > best_area) { best_area = a; best = int(i); }
-        }
-        if(best < 0) { break; }
-        uint32_t b = cands[best];
-        cands[best] = bn[b].left;
-        cands.push_back(bn[b].right);
-      }
-      size_t n = cands.size();
-
-      // Node box and octant slot assignment.
-      Aabb nbox;
-      for(uint32_t c : cands) { nbox.grow(bn[c].box); }
-      double pc[3];
-      for(int a = 0; a < 3; ++a) { pc[a] = 0.5 * (double(nbox.lo[a]) + nbox.hi[a]); }
-      int slot_of[8];
-      bool slot_used[8] = {false};
-      bool cand_done[8] = {false};
-      for(size_t k = 0; k < n; ++k) {
-        double best = std::numeric_limits<double>::infinity();
-        int bc = -1, bs = -1;
-        for(size_t c = 0; c < n; ++c) {
-          if(cand_done[c]) { continue; }
-          const Aabb& cb = bn[cands[c]].box;
-          double d[3];
-          for(int a = 0; a < 3; ++a) { d[a] = 0.5 * (double(cb.lo[a]) + cb.hi[a]) - pc[a]; }
-          for(int s = 0; s < 8; ++s) {
-            if(slot_used[s]) { continue; }
-            double cost = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) +
-                          ((s & 4) ? -d[2] : d[2]);
-            if(cost < best) { best = cost; bc = int(c); bs = s; }
-          }
-        }
-        cand_done[bc] = true;
-        slot_used[bs] = true;
-        slot_of[bc] = bs;
-      }
-
+      uint32_t cands[8];
+      uint32_t n = open_candidates(acc, cur.bin, width, cands);
+      float nlo[3], nhi[3];
       int cand_in_slot[8];
-      for(int s = 0; s < 8; ++s) { cand_in_slot[s] = -1; }
-      for(size_t c = 0; c < n; ++c) { cand_in_slot[slot_of[c]] = int(c); }
-
+      assign_slots(acc, cands, n, nlo, nhi, cand_in_slot);
       WideNode node;
       std::memset(&node, 0, sizeof(node));
-      float clo[3][8], chi[3][8];
-      int nslots = 0;
-      for(int s = 0; s < 8; ++s) {
-        int c = cand_in_slot[s];
-        const Aabb& cb = c >= 0 ? bn[cands[c]].box : nbox;
-        for(int a = 0; a < 3; ++a) {
-          clo[a][s] = c >= 0 ? cb.lo[a] : nbox.lo[a];
-          chi[a][s] = c >= 0 ? cb.hi[a] : nbox.lo[a];
-        }
-        nslots = 8;
-      }
-      for(int a = 0; a < 3; ++a) {
-        if(!quantize_axis(nbox.lo[a], nbox.hi[a], clo[a], chi[a], nslots,
-                          node.p[a], node.e[a], node.qlo[a], node.qhi[a])) {
-          err = "BVH quantization failed (scene coordinates out of range)";
-          return false;
-        }
+      if(!quantize_node(acc, cands, cand_in_slot, nlo, nhi, node)) {
+        err = "BVH quantization failed (scene coordinates out of range)";
+        return false;
       }
 
       // Internal children first (contiguous, slot order), then leaf triangles.
@@ -349,9 +259,7 @@ struct Collapser {
       for(int s = 0; s < 8; ++s) {
         int c = cand_in_slot[s];
         if(c < 0) {
-          node.meta[s] = 0;
-          // empty slots get an inverted box so they never report a hit
-          for(int a = 0; a < 3; ++a) { node.qlo[a][s] = 255; node.qhi[a][s] = 0; }
+          node.meta[s] = 0;   // an empty slot (inverted box)
           continue;
         }
         uint32_t b = cands[c];
@@ -412,27 +320,7 @@ struct Collapser {
 
 void expand_node_planes(const std::vector<WideNode>& in, std::vector<WideNodeF>& out) {
   out.resize(in.size());
-  for(size_t i = 0; i < in.size(); ++i) {
-    const WideNode& n = in[i];
-    WideNodeF& f = out[i];
-    std::memset(&f, 0, sizeof(f));
-    f.child_base = n.child_base;
-    f.tri_base = n.tri_base;
-    std::memcpy(f.meta, n.meta, 8);
-    f.imask = n.imask;
-    for(int a = 0; a < 3; ++a) {
-      double s = std::ldexp(1.0, int(n.e[a]) - 127);
-      for(int k = 0; k < 8; ++k) {
-        double lo = double(n.p[a]) + double(n.qlo[a][k]) * s;
-        double hi = double(n.p[a]) + double(n.qhi[a][k]) * s;
-        float lf = float(lo), hf = float(hi);
-        if(double(lf) > lo) { lf = std::nextafter(lf, -INFINITY); }
-        if(double(hf) < hi) { hf = std::nextafter(hf, INFINITY); }
-        f.pl[a][0][k] = lf;
-        f.pl[a][1][k] = hf;
-      }
-    }
-  }
+  for(size_t i = 0; i < in.size(); ++i) { expand_planes(in[i], out[i]); }
 }
 
 bool build_wide_bvh(const float* verts, uint32_t vert_count,
