@@ -285,10 +285,11 @@ def run_dort(args):
 
     t0 = time.time()
     verts, tris, rays = raycast_workload(rank, caster)
-    scene = db.Scene(verts, tris)
+    scene = db.Scene(verts, tris, bvh_build=args.bvh_build)
     st = scene.stats()
     log(f"[rank {rank}] workload ready in {time.time() - t0:.1f}s; bvh nodes={st['nodes']} "
-        f"depth={st['depth']} build={st['build_ms']:.0f}ms")
+        f"depth={st['depth']} build={st['build_ms']:.0f}ms ({st['bvh_build']} BVH "
+        f"{st['bvh_ms']:.0f}ms)")
 
     n = len(rays)
     d_rays = torch.from_numpy(rays).to(dev)
@@ -375,7 +376,8 @@ def run_dort(args):
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "tris": N_TRIS, "rays_per_step": n,
                        "l2": "inputs larger than L2 (512 MB of rays per step)",
-                       "bvh": f"wide BVH width 8, {st['nodes']} nodes, depth {st['depth']}"},
+                       "bvh": f"wide BVH width 8, {st['nodes']} nodes, depth {st['depth']}",
+                       "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2)},
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 16},
@@ -457,10 +459,12 @@ def run_dort_pt(args):
     torch.cuda.set_device(dev)
     t0 = time.time()
     sd = scenes.wavefront_scene()
+    sd["bvh_build"] = args.bvh_build
     sc = db.scene_from_dict(sd)
     st = sc.stats()
     log(f"[rank {rank}] scene ready in {time.time() - t0:.1f}s; nodes={st['nodes']} "
-        f"depth={st['depth']} build={st['build_ms']:.0f}ms")
+        f"depth={st['depth']} build={st['build_ms']:.0f}ms ({st['bvh_build']} BVH "
+        f"{st['bvh_ms']:.0f}ms)")
     spp = args.spp or PT_SPP
     p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH, seed=42 + rank)
     tuning = {"queue_capacity": 1 << 22}
@@ -569,6 +573,7 @@ def run_dort_pt(args):
                        "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
+                       "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2),
                        "l2": "frame state (queues 1 GB, image 25 MB) larger than L2"},
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 0,
@@ -756,6 +761,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--bvh-build", default=None, choices=["host", "device", "ploc"],
+                    help="where scenes build their BVH (default: the library's, the device)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -16,7 +16,7 @@ from ._abi import (CAMERA_ORTHO, CAMERA_PINHOLE, CAMERA_THIN_LENS, DortError, LI
                    MAT_OREN_NAYAR, MAT_PHONG, SHAPE_CUBE, SHAPE_CYLINDER, SHAPE_DISK,
                    SHAPE_SPHERE)
 
-__all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
+__all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc", "check_device_bvh",
            "MAT_LAMBERT", "MAT_MIRROR", "MAT_DIELECTRIC", "MAT_PHONG", "MAT_CONDUCTOR",
            "MAT_OREN_NAYAR", "SHAPE_SPHERE", "SHAPE_DISK", "SHAPE_CUBE", "SHAPE_CYLINDER",
            "LIGHT_POINT", "LIGHT_DIRECTIONAL", "CAMERA_PINHOLE", "CAMERA_ORTHO",
@@ -24,7 +24,12 @@ __all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc",
 
 # optional scene-dict keys passed through to scene_desc
 SCENE_KEYS = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
-              "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights", "tri_light_verts")
+              "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights", "tri_light_verts",
+              "bvh_build")
+
+_BVH_BUILD = {None: _abi.BVH_BUILD_DEFAULT, "default": _abi.BVH_BUILD_DEFAULT,
+              "host": _abi.BVH_BUILD_HOST, "device": _abi.BVH_BUILD_DEVICE,
+              "ploc": _abi.BVH_BUILD_PLOC}
 
 
 def _ptr(a):
@@ -50,11 +55,14 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
                sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
                sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
                bvh_width: int = 8, shapes=None, delta_lights=None, tri_light_verts=None,
-               **_ignored) -> _DescHolder:
+               bvh_build: str | None = None, **_ignored) -> _DescHolder:
     """SceneDesc for the arrays given.  `shapes`: dicts with kind (SHAPE_*),
     material, param (up to 4), to_world (3x4), emission (RGB) and optionally
     light_to_world (3x4); `delta_lights`: dicts with kind (LIGHT_POINT /
-    LIGHT_DIRECTIONAL), rgb and vec."""
+    LIGHT_DIRECTIONAL), rgb and vec; `bvh_build`: "host" (binned SAH on the
+    host), "device" (the same on the device), "ploc" (Morton order + PLOC on
+    the device: fastest build, slower traversal) or None (the library's
+    default, "device")."""
     h = _DescHolder()
     d = h.desc
     verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
@@ -87,6 +95,9 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
     d.sky_up = (ctypes.c_float * 3)(*sky_up)
     d.sky_fwd = (ctypes.c_float * 3)(*sky_fwd)
     d.bvh_width = bvh_width
+    if bvh_build not in _BVH_BUILD:
+        raise ValueError(f"bvh_build must be one of {sorted(k for k in _BVH_BUILD if k)}")
+    d.bvh_build = _BVH_BUILD[bvh_build]
     if shapes:
         arr = (_abi.Shape * len(shapes))()
         for i, sh in enumerate(shapes):
@@ -140,7 +151,17 @@ class Scene:
         _abi.check(_abi.lib().dort_gpu_scene_stats(self.handle, out))
         return {"nodes": int(out[0]), "depth": int(out[1]), "tris": int(out[2]),
                 "emissive": int(out[3]), "device_bytes": int(out[4]),
-                "build_ms": out[5]}
+                "build_ms": out[5],
+                "bvh_build": {_abi.BVH_BUILD_HOST: "host", _abi.BVH_BUILD_DEVICE: "device",
+                              _abi.BVH_BUILD_PLOC: "ploc"}.get(int(out[6]), "none"),
+                "bvh_ms": out[7]}
+
+    def bvh_cost(self) -> dict:
+        """Surface-area cost of the scene's BVH (dort_gpu_scene_bvh_cost)."""
+        out = (ctypes.c_double * 4)()
+        _abi.check(_abi.lib().dort_gpu_scene_bvh_cost(self.handle, out))
+        return {"sah": out[0], "nodes": int(out[1]), "leaf_slots": int(out[2]),
+                "depth": int(out[3])}
 
     def raycast(self, rays, any_hit: bool = False):
         """Host arrays in and out (dort_gpu_raycast)."""
@@ -337,6 +358,18 @@ def loss_l2(image, target):
     loss = ctypes.c_double(0.0)
     _abi.check(_abi.lib().dort_gpu_loss_l2(_ptr(a), _ptr(b), a.size, ctypes.byref(loss), _ptr(g)))
     return loss.value, g
+
+
+def check_device_bvh(verts, tris, bvh_width: int = 8, bvh_build: str | None = None) -> dict:
+    """Builds the BVH on the device ("device" = binned SAH, or "ploc") and
+    compares it with the host collapse of the same binary tree
+    (dort_gpu_check_device_bvh)."""
+    h = scene_desc(verts, tris, bvh_width=bvh_width, bvh_build=bvh_build)
+    out = (ctypes.c_double * 8)()
+    _abi.check(_abi.lib().dort_gpu_check_device_bvh(ctypes.byref(h.desc), out))
+    return {"node_bytes_differ": int(out[0]), "tri_bytes_differ": int(out[1]),
+            "nodes": int(out[2]), "each_tri_once": bool(out[3]), "build_ms": out[4],
+            "iterations": int(out[5]), "depth": int(out[6]), "sah": out[7]}
 
 
 def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8):

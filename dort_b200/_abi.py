@@ -31,6 +31,7 @@ SHAPE_SPHERE, SHAPE_DISK, SHAPE_CUBE, SHAPE_CYLINDER = 1, 2, 3, 4
 SHAPE_LIGHT_TRANSFORM = 1
 LIGHT_POINT, LIGHT_DIRECTIONAL = 1, 2
 CAMERA_PINHOLE, CAMERA_ORTHO, CAMERA_THIN_LENS = 0, 1, 2
+BVH_BUILD_DEFAULT, BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_PLOC = 0, 1, 2, 3
 ABI_VERSION = 2
 
 
@@ -67,7 +68,7 @@ class SceneDesc(ctypes.Structure):
         ("shapes", c_p),
         ("lights", c_p),
         ("light_count", c_u32),
-        ("pad0", c_u32),
+        ("bvh_build", c_u32),
         ("tri_light_verts", c_p),
         ("reserved", c_u32 * 2),
     ]
@@ -183,6 +184,11 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_batch_stats.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
         L.dort_gpu_batch_destroy.restype = c_i32
         L.dort_gpu_batch_destroy.argtypes = [c_p]
+        L.dort_gpu_scene_bvh_cost.restype = c_i32
+        L.dort_gpu_scene_bvh_cost.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_check_device_bvh.restype = c_i32
+        L.dort_gpu_check_device_bvh.argtypes = [ctypes.POINTER(SceneDesc),
+                                                ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 

@@ -323,6 +323,102 @@ void expand_node_planes(const std::vector<WideNode>& in, std::vector<WideNodeF>&
   for(size_t i = 0; i < in.size(); ++i) { expand_planes(in[i], out[i]); }
 }
 
+bool collapse_binary_dump(const BinaryDump& tree, const float* verts, const uint32_t* tris,
+                          uint32_t tri_count, const BuildOptions& opts, WideBvh& out,
+                          std::string& err) {
+  const uint32_t kLeaf = 0x80000000u;
+  size_t count = tree.left.size();
+  // the host collapse starts at node 0: swap the root into place
+  auto map = [&](uint32_t i) -> uint32_t {
+    return i == tree.root ? 0u : (i == 0 ? tree.root : i);
+  };
+  std::vector<BinNode> bn(count);
+  const std::vector<uint32_t>& order = tree.leaf_idx;
+  for(size_t i = 0; i < count; ++i) {
+    BinNode& b = bn[map(uint32_t(i))];
+    for(int a = 0; a < 3; ++a) {
+      b.box.lo[a] = tree.lo[3 * i + a];
+      b.box.hi[a] = tree.hi[3 * i + a];
+    }
+    b.tri_total = tree.count[i];
+    if(tree.left[i] & kLeaf) {
+      b.left = b.right = 0;
+      b.first = tree.left[i] & ~kLeaf;
+      b.count = tree.right[i];
+      if(size_t(b.first) + b.count > order.size()) {
+        err = "binary tree leaf out of range";
+        return false;
+      }
+    } else {
+      b.left = map(tree.left[i]);
+      b.right = map(tree.right[i]);
+      b.count = 0;
+    }
+  }
+  Collapser col{bn, order, verts, tris, opts, out, err};
+  if(tri_count > 0 && !col.run()) { return false; }
+#ifndef DORT_NODE_QUANTIZED
+  expand_node_planes(out.nodes, out.nodes_f);
+#endif
+  return true;
+}
+
+double wide_sah_cost(const WideNodeF* nodes, size_t node_count) {
+  if(node_count == 0) { return 0.0; }
+  auto slot_area = [](const WideNodeF& n, int s) {
+    float lo[3], hi[3];
+    for(int a = 0; a < 3; ++a) { lo[a] = n.pl[a][0][s]; hi[a] = n.pl[a][1][s]; }
+    return bw_area(lo, hi);
+  };
+  float rlo[3] = {INFINITY, INFINITY, INFINITY}, rhi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for(int s = 0; s < 8; ++s) {
+    if(nodes[0].meta[s] == 0) { continue; }
+    for(int a = 0; a < 3; ++a) {
+      rlo[a] = std::min(rlo[a], nodes[0].pl[a][0][s]);
+      rhi[a] = std::max(rhi[a], nodes[0].pl[a][1][s]);
+    }
+  }
+  double root = std::max(bw_area(rlo, rhi), 1e-300);
+  double cost = 1.0;   // the root itself
+  for(size_t i = 0; i < node_count; ++i) {
+    const WideNodeF& n = nodes[i];
+    for(int s = 0; s < 8; ++s) {
+      if(n.meta[s] == 0) { continue; }
+      double a = slot_area(n, s) / root;
+      if(n.imask & (1u << s)) {
+        cost += a;
+      } else {
+        cost += a * double(__builtin_popcount(n.meta[s] >> 5));
+      }
+    }
+  }
+  return cost;
+}
+
+bool validate_mesh(const float* verts, uint32_t vert_count, const uint32_t* tris,
+                   uint32_t tri_count, std::string& err) {
+  for(uint32_t t = 0; t < tri_count; ++t) {
+    for(int k = 0; k < 3; ++k) {
+      uint32_t vi = tris[3 * size_t(t) + k];
+      if(vi >= vert_count) {
+        err = "triangle " + std::to_string(t) + " references vertex " + std::to_string(vi) +
+              " >= vert_count";
+        return false;
+      }
+      const float* v = verts + 3 * size_t(vi);
+      if(!std::isfinite(v[0]) || !std::isfinite(v[1]) || !std::isfinite(v[2])) {
+        err = "vertex " + std::to_string(vi) + " is not finite";
+        return false;
+      }
+      if(std::fabs(v[0]) > 1e15f || std::fabs(v[1]) > 1e15f || std::fabs(v[2]) > 1e15f) {
+        err = "vertex " + std::to_string(vi) + " is out of range (|coord| > 1e15)";
+        return false;
+      }
+    }
+  }
+  return true;
+}
+
 bool build_wide_bvh(const float* verts, uint32_t vert_count,
                     const uint32_t* tris, uint32_t tri_count,
                     const BuildOptions& opts, WideBvh& out, std::string& err) {

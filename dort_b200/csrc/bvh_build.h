@@ -108,6 +108,33 @@ inline size_t traversal_node_bytes(const WideBvh& b) {
 // that no root-to-leaf path of the wide tree is deeper.
 constexpr uint32_t kMaxWideDepth = 64;
 
+// The binary tree the device made, for checks.  A leaf has bit 31 set in
+// `left`, the rest of `left` is its first position in leaf_idx and `right`
+// its triangle count; an internal node has its children in left / right.
+// count = triangles below each node.
+struct BinaryDump {
+  std::vector<float> lo, hi;      // 3 per node
+  std::vector<uint32_t> left, right, count;
+  std::vector<uint32_t> leaf_idx;    // triangle indices in leaf order
+  uint32_t root = 0;
+};
+
+// Collapses a binary tree made elsewhere (the device builder's) with the
+// host's collapse, for checking the device collapse byte for byte.
+bool collapse_binary_dump(const BinaryDump& tree, const float* verts, const uint32_t* tris,
+                          uint32_t tri_count, const BuildOptions& opts, WideBvh& out,
+                          std::string& err);
+
+// Surface-area cost of a wide BVH from its float planes, relative to the
+// root box: sum over visited child nodes of area, plus sum over leaf slots of
+// area x triangle count (traversal and intersection cost 1 each).
+double wide_sah_cost(const WideNodeF* nodes, size_t node_count);
+
+// The input checks of build_wide_bvh, with the same messages (indices in
+// range, finite coordinates of magnitude at most 1e15).
+bool validate_mesh(const float* verts, uint32_t vert_count, const uint32_t* tris,
+                   uint32_t tri_count, std::string& err);
+
 // Builds the wide BVH; returns false (with a message) on invalid input.
 bool build_wide_bvh(const float* verts, uint32_t vert_count,
                     const uint32_t* tris, uint32_t tri_count,

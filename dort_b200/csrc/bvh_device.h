@@ -28,6 +28,8 @@
 
 namespace dort_gpu {
 
+enum class DeviceBuilder { kSah, kPloc };
+
 struct DeviceBvh {
   void* nodes = nullptr;          // traversal nodes (WideNodeF, or WideNode when quantized)
   size_t node_bytes = 0;          // allocated bytes of `nodes`
@@ -35,17 +37,8 @@ struct DeviceBvh {
   LeafTri* tris = nullptr;        // tri_count leaf triangles
   uint32_t tri_count = 0;
   uint32_t depth = 0;             // levels of wide nodes
-  uint32_t ploc_iterations = 0;
+  uint32_t iterations = 0;        // SAH levels, or PLOC iterations
   double ms = 0.0;                // wall time of the build (uploads included)
-};
-
-// The binary tree the device made, for checks: nodes in creation order
-// (leaves 0..n-1 in Morton order, then the merged clusters; root last).
-struct BinaryDump {
-  std::vector<float> lo, hi;      // 3 per node
-  std::vector<uint32_t> left, right, count;
-  std::vector<uint32_t> leaf_prim;   // per leaf node
-  uint32_t root = 0;
 };
 
 // Builds the wide BVH of a host triangle mesh on the current device.  The
@@ -53,11 +46,8 @@ struct BinaryDump {
 // most 1e15: validate_mesh).  On success the caller owns out.nodes and
 // out.tris (cudaFree).
 bool build_wide_bvh_device(const float* verts, uint32_t vert_count, const uint32_t* tris,
-                           uint32_t tri_count, const BuildOptions& opts, cudaStream_t stream,
-                           DeviceBvh& out, std::string& err, BinaryDump* dump = nullptr);
-
-// The input checks of build_wide_bvh, with the same messages.
-bool validate_mesh(const float* verts, uint32_t vert_count, const uint32_t* tris,
-                   uint32_t tri_count, std::string& err);
+                           uint32_t tri_count, const BuildOptions& opts, DeviceBuilder method,
+                           cudaStream_t stream, DeviceBvh& out, std::string& err,
+                           BinaryDump* dump = nullptr);
 
 }  // namespace dort_gpu

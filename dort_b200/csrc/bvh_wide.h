@@ -13,8 +13,10 @@
 //   quantize_axis     8-bit conservative child planes on a power-of-two grid
 //   expand_planes     the quantized planes as floats rounded outward
 //
-// Only exact double operations are used (frexp / ldexp / floor / ceil, one
-// division), so host and device agree bit for bit.
+// Every double product and sum is rounded on its own (BW_MUL / BW_ADD /
+// BW_SUB: no fused multiply-add on the device), the divisions are IEEE and
+// the rest (frexp, ldexp, floor, ceil, nextafterf) is exact, so host and
+// device agree bit for bit.
 #pragma once
 #include <math.h>
 #include <stdint.h>
@@ -27,12 +29,26 @@
 #define BW_HD inline
 #endif
 
+// Double products and sums rounded one at a time on the device too (no
+// fused multiply-add), as the host evaluates them.
+#ifdef __CUDA_ARCH__
+#define BW_MUL(a, b) __dmul_rn(a, b)
+#define BW_ADD(a, b) __dadd_rn(a, b)
+#define BW_SUB(a, b) __dsub_rn(a, b)
+#else
+#define BW_MUL(a, b) ((a) * (b))
+#define BW_ADD(a, b) ((a) + (b))
+#define BW_SUB(a, b) ((a) - (b))
+#endif
+
 namespace dort_gpu {
 
 BW_HD double bw_area(const float lo[3], const float hi[3]) {
   if(!(lo[0] <= hi[0])) { return 0.0; }
-  double x = double(hi[0]) - lo[0], y = double(hi[1]) - lo[1], z = double(hi[2]) - lo[2];
-  return 2.0 * (x * y + y * z + z * x);
+  double x = BW_SUB(double(hi[0]), double(lo[0]));
+  double y = BW_SUB(double(hi[1]), double(lo[1]));
+  double z = BW_SUB(double(hi[2]), double(lo[2]));
+  return BW_MUL(2.0, BW_ADD(BW_ADD(BW_MUL(x, y), BW_MUL(y, z)), BW_MUL(z, x)));
 }
 
 // Accessor A: bool leaf(b), uint32_t left(b), uint32_t right(b),
@@ -76,7 +92,7 @@ BW_HD void assign_slots(const A& acc, const uint32_t* cands, uint32_t n, float n
     }
   }
   double pc[3];
-  for(int a = 0; a < 3; ++a) { pc[a] = 0.5 * (double(nlo[a]) + nhi[a]); }
+  for(int a = 0; a < 3; ++a) { pc[a] = BW_MUL(0.5, BW_ADD(double(nlo[a]), double(nhi[a]))); }
   bool slot_used[8] = {false, false, false, false, false, false, false, false};
   bool cand_done[8] = {false, false, false, false, false, false, false, false};
   for(int s = 0; s < 8; ++s) { cand_in_slot[s] = -1; }
@@ -88,11 +104,13 @@ BW_HD void assign_slots(const A& acc, const uint32_t* cands, uint32_t n, float n
       const float* lo = acc.lo(cands[c]);
       const float* hi = acc.hi(cands[c]);
       double d[3];
-      for(int a = 0; a < 3; ++a) { d[a] = 0.5 * (double(lo[a]) + hi[a]) - pc[a]; }
+      for(int a = 0; a < 3; ++a) {
+        d[a] = BW_SUB(BW_MUL(0.5, BW_ADD(double(lo[a]), double(hi[a]))), pc[a]);
+      }
       for(int s = 0; s < 8; ++s) {
         if(slot_used[s]) { continue; }
-        double cost = ((s & 1) ? -d[0] : d[0]) + ((s & 2) ? -d[1] : d[1]) +
-                      ((s & 4) ? -d[2] : d[2]);
+        double cost = BW_ADD(BW_ADD((s & 1) ? -d[0] : d[0], (s & 2) ? -d[1] : d[1]),
+                             (s & 4) ? -d[2] : d[2]);
         if(cost < best) { best = cost; bc = int(c); bs = s; }
       }
     }
@@ -109,9 +127,9 @@ BW_HD void assign_slots(const A& acc, const uint32_t* cands, uint32_t n, float n
 BW_HD bool quantize_axis(float node_lo, float node_hi, const float* clo, const float* chi,
                          int n, float& p_out, uint8_t& e_out, uint8_t* qlo, uint8_t* qhi) {
   double lo = node_lo, hi = node_hi;
-  double ext = hi - lo;
+  double ext = BW_SUB(hi, lo);
   double mag = fmax(fabs(lo), fabs(hi));
-  double min_step = fmax(mag * ldexp(1.0, -20), ldexp(1.0, -100));
+  double min_step = fmax(BW_MUL(mag, ldexp(1.0, -20)), ldexp(1.0, -100));
   double step = fmax(ext / 253.0, min_step);
   int ex;
   double m = frexp(step, &ex);       // step = m 2^ex, m in [0.5, 1)
@@ -119,16 +137,20 @@ BW_HD bool quantize_axis(float node_lo, float node_hi, const float* clo, const f
   for(int attempt = 0; attempt < 8; ++attempt, ++e) {
     if(e + 127 < 1 || e + 127 > 254) { return false; }
     double s = ldexp(1.0, e);
-    double pd = lo - s;
+    double pd = BW_SUB(lo, s);
     float pf = float(pd);
     if(double(pf) > pd) { pf = nextafterf(pf, -INFINITY); }
     bool ok = true;
     for(int i = 0; i < n && ok; ++i) {
-      double ql = floor((double(clo[i]) - pf) / s) - 1.0;
-      double qh = ceil((double(chi[i]) - pf) / s) + 1.0;
+      double ql = BW_SUB(floor(BW_SUB(double(clo[i]), double(pf)) / s), 1.0);
+      double qh = BW_ADD(ceil(BW_SUB(double(chi[i]), double(pf)) / s), 1.0);
       if(ql < 0.0 || qh > 255.0) { ok = false; break; }
-      if(double(pf) + ql * s > double(clo[i]) - s * 0.999 ||
-         double(pf) + qh * s < double(chi[i]) + s * 0.999) { ok = false; break; }
+      double margin = BW_MUL(s, 0.999);
+      if(BW_ADD(double(pf), BW_MUL(ql, s)) > BW_SUB(double(clo[i]), margin) ||
+         BW_ADD(double(pf), BW_MUL(qh, s)) < BW_ADD(double(chi[i]), margin)) {
+        ok = false;
+        break;
+      }
       qlo[i] = uint8_t(ql);
       qhi[i] = uint8_t(qh);
     }
@@ -178,8 +200,8 @@ BW_HD void expand_planes(const WideNode& n, WideNodeF& f) {
   for(int a = 0; a < 3; ++a) {
     double s = ldexp(1.0, int(n.e[a]) - 127);
     for(int k = 0; k < 8; ++k) {
-      double lo = double(n.p[a]) + double(n.qlo[a][k]) * s;
-      double hi = double(n.p[a]) + double(n.qhi[a][k]) * s;
+      double lo = BW_ADD(double(n.p[a]), BW_MUL(double(n.qlo[a][k]), s));
+      double hi = BW_ADD(double(n.p[a]), BW_MUL(double(n.qhi[a][k]), s));
       float lf = float(lo), hf = float(hi);
       if(double(lf) > lo) { lf = nextafterf(lf, -INFINITY); }
       if(double(hf) < hi) { hf = nextafterf(hf, INFINITY); }

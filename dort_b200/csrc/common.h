@@ -40,6 +40,9 @@ struct dort_scene {
   uint32_t emissive_count = 0;
   size_t device_bytes = 0;
   double build_ms = 0.0;
+  double bvh_ms = 0.0;                  // BVH build alone
+  uint32_t bvh_builder = 0;             // DORT_BVH_BUILD_HOST / _DEVICE
+  uint32_t bvh_iterations = 0;          // SAH levels / PLOC iterations of a device build
   std::vector<void*> allocations;       // every device buffer owned by the scene
   dort_gpu::Wavefront* wavefront = nullptr;  // wavefront queues + frame graph (lazy)
   float* d_tri_albedo = nullptr;        // per-triangle overrides (adjoint), lazy

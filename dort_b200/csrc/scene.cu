@@ -4,6 +4,7 @@
 #include <string>
 
 #include "bvh_build.h"
+#include "bvh_device.h"
 #include "common.h"
 #include "scene_build.h"
 #include "wavefront.h"
@@ -55,20 +56,61 @@ static int upload(dort_scene* s, const std::vector<T>& v, const T** out) {
   return DORT_OK;
 }
 
-static int scene_upload(dort_scene* s, const HostScene& hs) {
+// Builds the BVH on the device (the scene owns the result).
+static int device_bvh(dort_scene* s, const dort_scene_desc* desc) {
+  BuildOptions opts;
+  opts.width = desc->bvh_width ? desc->bvh_width : 8;
+  DeviceBvh db;
+  std::string err;
+  DeviceBuilder method =
+      desc->bvh_build == DORT_BVH_BUILD_PLOC ? DeviceBuilder::kPloc : DeviceBuilder::kSah;
+  if(!build_wide_bvh_device(desc->verts, desc->vert_count, desc->tris, desc->tri_count, opts,
+                            method, nullptr, db, err)) {
+    int code = DORT_ERR_CUDA;
+    if(err.rfind("cudaMalloc", 0) == 0) { code = DORT_ERR_OOM; }
+    if(err.find("quantization") != std::string::npos || err.find("too ") != std::string::npos) {
+      code = DORT_ERR_INVALID;
+    }
+    return fail(code, err);
+  }
+  if(db.nodes) {
+    s->allocations.push_back(db.nodes);
+    s->device_bytes += db.node_bytes;
+  }
+  if(db.tris) {
+    s->allocations.push_back(db.tris);
+    s->device_bytes += size_t(db.tri_count) * sizeof(LeafTri);
+  }
+  s->trace.nodes = static_cast<const uint4*>(db.nodes);
+  s->trace.tris = reinterpret_cast<const float4*>(db.tris);
+  s->trace.node_count = db.node_count;
+  s->trace.tri_count = db.tri_count;
+  s->depth = db.depth;
+  s->bvh_ms = db.ms;
+  s->bvh_builder = method == DeviceBuilder::kPloc ? DORT_BVH_BUILD_PLOC : DORT_BVH_BUILD_DEVICE;
+  s->bvh_iterations = db.iterations;
+  return DORT_OK;
+}
+
+static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostScene& hs) {
   int rc;
-  const unsigned char* nodes;
-  const LeafTri* tris;
-  {
+  if(hs.device_bvh) {
+    if((rc = device_bvh(s, desc)) != DORT_OK) { return rc; }
+  } else {
+    const unsigned char* nodes;
+    const LeafTri* tris;
     const unsigned char* src = static_cast<const unsigned char*>(traversal_nodes(hs.bvh));
     std::vector<unsigned char> bytes(src, src + traversal_node_bytes(hs.bvh));
     if((rc = upload(s, bytes, &nodes)) != DORT_OK) { return rc; }
+    if((rc = upload(s, hs.bvh.tris, &tris)) != DORT_OK) { return rc; }
+    s->trace.nodes = reinterpret_cast<const uint4*>(nodes);
+    s->trace.tris = reinterpret_cast<const float4*>(tris);
+    s->trace.node_count = uint32_t(hs.bvh.nodes.size());
+    s->trace.tri_count = uint32_t(hs.bvh.tris.size());
+    s->depth = hs.bvh.depth;
+    s->bvh_ms = hs.bvh_ms;
+    s->bvh_builder = DORT_BVH_BUILD_HOST;
   }
-  if((rc = upload(s, hs.bvh.tris, &tris)) != DORT_OK) { return rc; }
-  s->trace.nodes = reinterpret_cast<const uint4*>(nodes);
-  s->trace.tris = reinterpret_cast<const float4*>(tris);
-  s->trace.node_count = uint32_t(hs.bvh.nodes.size());
-  s->trace.tri_count = uint32_t(hs.bvh.tris.size());
 
   PtScene& pt = s->pt;
   std::memset(&pt, 0, sizeof(pt));
@@ -112,16 +154,15 @@ extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** o
   auto t0 = std::chrono::steady_clock::now();
   HostScene hs;
   std::string err;
-  if(!build_host_scene(desc, hs, err)) { return fail(DORT_ERR_INVALID, err); }
-  auto t1 = std::chrono::steady_clock::now();
+  if(!build_host_scene(desc, hs, err, true)) { return fail(DORT_ERR_INVALID, err); }
 
   dort_scene* s = new dort_scene();
   cudaGetDevice(&s->device);
   s->tri_count = desc->tri_count;
-  s->depth = hs.bvh.depth;
   s->emissive_count = hs.emissive_count;
-  s->build_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
-  int rc = scene_upload(s, hs);
+  int rc = scene_upload(s, desc, hs);
+  s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                    .count();
   if(rc != DORT_OK) {
     std::string msg = g_last_error;
     scene_free_device(s);
@@ -149,7 +190,7 @@ extern "C" int dort_gpu_scene_stats(const dort_scene* s, double out[8]) {
   out[3] = s->emissive_count;
   out[4] = double(s->device_bytes);
   out[5] = s->build_ms;
-  out[6] = 0.0;
-  out[7] = 0.0;
+  out[6] = s->bvh_builder;
+  out[7] = s->bvh_ms;
   return DORT_OK;
 }

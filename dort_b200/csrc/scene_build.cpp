@@ -20,6 +20,7 @@
 #include "scene_build.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 
@@ -169,7 +170,8 @@ void shape_local_bounds(const DevShape& s, float lo[3], float hi[3]) {
 
 }  // namespace
 
-bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& err) {
+bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& err,
+                      bool allow_device_bvh) {
   if(desc->struct_size != sizeof(dort_scene_desc)) {
     err = "dort_scene_desc.struct_size mismatch (ABI version)";
     return false;
@@ -203,10 +205,26 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
     hs.mats.push_back(m);
   }
 
+  if(desc->bvh_build > DORT_BVH_BUILD_PLOC) {
+    err = "bvh_build must be DORT_BVH_BUILD_DEFAULT, _HOST, _DEVICE or _PLOC";
+    return false;
+  }
+  hs.device_bvh = allow_device_bvh && desc->bvh_build != DORT_BVH_BUILD_HOST;
   BuildOptions opts;
   opts.width = desc->bvh_width ? desc->bvh_width : 8;
-  if(!build_wide_bvh(desc->verts, desc->vert_count, desc->tris, n, opts, hs.bvh, err)) {
-    return false;
+  if(hs.device_bvh) {
+    if(opts.width < 2 || opts.width > 8) {
+      err = "bvh_width must be 2..8";
+      return false;
+    }
+    if(!validate_mesh(desc->verts, desc->vert_count, desc->tris, n, err)) { return false; }
+  } else {
+    auto b0 = std::chrono::steady_clock::now();
+    if(!build_wide_bvh(desc->verts, desc->vert_count, desc->tris, n, opts, hs.bvh, err)) {
+      return false;
+    }
+    hs.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - b0)
+                    .count();
   }
 
   // per-triangle shading records and area lights

@@ -11,7 +11,9 @@
 namespace dort_gpu {
 
 struct HostScene {
-  WideBvh bvh;
+  WideBvh bvh;                       // empty when device_bvh (built on the device)
+  bool device_bvh = false;
+  double bvh_ms = 0.0;               // host BVH build time
   std::vector<float4> shade;         // 3 per triangle
   std::vector<DevMaterial> mats;
   std::vector<DevLight> lights;
@@ -32,7 +34,11 @@ struct HostScene {
 constexpr uint32_t kMaxShapes = 4096;
 
 // Validates the description and builds everything; false + message on error.
-bool build_host_scene(const dort_scene_desc* desc, HostScene& out, std::string& err);
+// With allow_device_bvh and a description that asks for the device build
+// (bvh_build DEFAULT or DEVICE) the mesh is only validated and hs.bvh stays
+// empty: the caller builds the BVH on the device.
+bool build_host_scene(const dort_scene_desc* desc, HostScene& out, std::string& err,
+                      bool allow_device_bvh = false);
 
 // Device-view structures pointing at the host arrays (host checks only).
 PtScene host_view(const HostScene& hs);

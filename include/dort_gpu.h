@@ -125,6 +125,14 @@ enum dort_shape_kind {
 
 #define DORT_SHAPE_LIGHT_TRANSFORM 1u
 
+/* Where the BVH is built (dort_scene_desc.bvh_build). */
+enum {
+  DORT_BVH_BUILD_DEFAULT = 0,   /* the device, binned SAH */
+  DORT_BVH_BUILD_HOST = 1,      /* binned SAH on the host (32 bins, 3 axes) */
+  DORT_BVH_BUILD_DEVICE = 2,    /* binned SAH on the device (same bins and costs) */
+  DORT_BVH_BUILD_PLOC = 3       /* Morton order + PLOC on the device: fastest build */
+};
+
 typedef struct dort_shape {
   uint32_t kind;
   uint32_t material;
@@ -164,6 +172,13 @@ typedef struct dort_light {
  *                 sky_scale (0,0,0 = 1,1,1), up and forward vectors sky_up /
  *                 sky_fwd (0 = +y / +x)
  *   bvh_width     children per BVH node, 2..8 (0: 8)
+ *   bvh_build     DORT_BVH_BUILD_HOST: binned-SAH binary tree built on the
+ *                 host; DORT_BVH_BUILD_DEVICE (and DEFAULT): the same binned
+ *                 SAH on the device; DORT_BVH_BUILD_PLOC: Morton order and
+ *                 Parallel Locally-Ordered Clustering on the device (fastest
+ *                 build, slower traversal).  All collapse to the same wide
+ *                 format; hits do not depend on the choice (closest hit is a
+ *                 property of the triangles).
  *   tri_light_verts  for each emissive triangle, the triangle (3 points) its
  *                 light samples and weights, when that differs from the
  *                 primitive: a light and its primitive placed by different
@@ -194,15 +209,15 @@ typedef struct dort_scene_desc {
   const dort_shape* shapes;        /* shape_count, or NULL */
   const dort_light* lights;        /* light_count delta lights, or NULL */
   uint32_t light_count;
-  uint32_t pad0;
+  uint32_t bvh_build;              /* DORT_BVH_BUILD_* */
   const float* tri_light_verts;    /* tri_count * 9, or NULL: see below */
   uint32_t reserved[2];
 } dort_scene_desc;
 
 typedef struct dort_scene dort_scene;
 
-/* Builds the acceleration structure on the host and uploads the scene to the
- * current CUDA device.  Replaces the scene build of build_scene
+/* Builds the acceleration structure (on the device or the host, bvh_build)
+ * and uploads the scene to the current CUDA device.  Replaces the scene build of build_scene
  * (lua_builder.cpp:113-146) and the Bvh constructor (bvh.cpp:9-55). */
 int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** out_scene);
 
@@ -211,7 +226,9 @@ int dort_gpu_scene_destroy(dort_scene* scene);
 
 /* Scene statistics: out[0] = BVH node count, out[1] = BVH depth,
  * out[2] = triangle count, out[3] = emissive triangle count,
- * out[4] = device bytes held, out[5] = host build milliseconds. */
+ * out[4] = device bytes held, out[5] = build milliseconds (scene create:
+ * host preparation and BVH build), out[6] = how the BVH was built
+ * (DORT_BVH_BUILD_HOST / _DEVICE / _PLOC), out[7] = BVH build milliseconds. */
 int dort_gpu_scene_stats(const dort_scene* scene, double out[8]);
 
 /* ---- ray casting ----------------------------------------------------------
@@ -423,6 +440,21 @@ int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const float* rays,
  * only); writes those rows of out_rgb.  For checking without a GPU. */
 int dort_gpu_host_check_render(const dort_scene_desc* desc, const dort_render_params* params,
                                uint32_t row_begin, uint32_t row_end, float* out_rgb);
+
+/* No reference counterpart.  Quality of the scene's BVH: out[0] = surface
+ * area cost relative to the root box (each visited child node and each
+ * triangle test costs its box's area), out[1] = node count, out[2] = leaf
+ * slots, out[3] = depth.  Reads the nodes back from the device. */
+int dort_gpu_scene_bvh_cost(const dort_scene* scene, double out[4]);
+
+/* No reference counterpart.  Builds the mesh's BVH on the device (the binned
+ * SAH builder, or PLOC when desc->bvh_build is DORT_BVH_BUILD_PLOC), collapses
+ * the device's binary tree again with the host code, and compares:
+ * out[0] = node bytes that differ, out[1] = leaf-triangle bytes that differ,
+ * out[2] = node count, out[3] = 1 if every triangle is in exactly one leaf,
+ * out[4] = device build milliseconds, out[5] = SAH levels or PLOC iterations,
+ * out[6] = depth, out[7] = surface area cost.  Needs a GPU. */
+int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out[8]);
 
 #ifdef __cplusplus
 }

@@ -24,14 +24,16 @@ def _rays_for(verts, tris, n, seed):
     return ob, np.ascontiguousarray(np.concatenate([coh, dif]))
 
 
+@pytest.mark.parametrize("build", ["device", "host"])
 @pytest.mark.parametrize("n_tris,n_rays,width", [
     (1, 500, 8), (16, 4000, 8), (2000, 20000, 8), (2000, 20000, 4),
     (2000, 20000, 2), (100000, 200000, 8)])
-def test_random_soup_matches_oracle(cuda, n_tris, n_rays, width):
+def test_random_soup_matches_oracle(cuda, n_tris, n_rays, width, build):
     verts, tris = scenes.random_triangles(n_tris, seed=100 + n_tris)
     ob, rays = _rays_for(verts, tris, n_rays, seed=7)
     ref_prim, ref_tb = ob.raycast(rays)
-    sc = db.Scene(verts, tris, bvh_width=width)
+    sc = db.Scene(verts, tris, bvh_width=width, bvh_build=build)
+    assert sc.stats()["bvh_build"] == build
     prim, tb = sc.raycast(rays)
     same, ties, box_miss, bugs = classify(verts, tris, rays, prim, tb, ref_prim, ref_tb)
     assert bugs == [], f"{len(bugs)} unexplained differences, e.g. rays {bugs[:5]}"
