@@ -635,11 +635,17 @@ def run_dort_batch(args):
     t0 = time.time()
     specs = scenes.batch_jobs(count=64, seed=4 + 1000 * rank)
     jobs = []
+    t_create = time.time()
     for k, (sd, w, h, spp, depth) in enumerate(specs):
+        sd["bvh_build"] = args.bvh_build
         sc = db.scene_from_dict(sd)
         jobs.append((sc, db.render_params(sd["camera"], w, h, spp, max_depth=depth, seed=k)))
+    create_s = time.time() - t_create
+    bvh_ms = sum(sc.stats()["bvh_ms"] for sc, _ in jobs)
+    built = jobs[0][0].stats()["bvh_build"]
     samples = sum(w * h * spp for (_, w, h, spp, _) in specs)
-    log(f"[rank {rank}] 64 scenes ready in {time.time() - t0:.1f}s, {samples / 1e9:.2f}G samples")
+    log(f"[rank {rank}] 64 scenes ready in {time.time() - t0:.1f}s ({create_s:.2f}s to create, "
+        f"{built} BVH builds {bvh_ms:.0f} ms), {samples / 1e9:.2f}G samples")
     b = db.Batch(jobs, {"queue_capacity": 1 << 22})
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
@@ -681,7 +687,9 @@ def run_dort_batch(args):
             "config": {"workload": BATCH_WORKLOAD, "jobs": len(jobs), "samples": samples,
                        "megakernel_samples_per_s": world * samples / (mega_ms / 1e3),
                        "batch_over_megakernel": (mega_ms / (ms / args.steps)),
-                       "rays_per_batch": st["rays"], "waves": st["waves"]},
+                       "rays_per_batch": st["rays"], "waves": st["waves"],
+                       "bvh_build": built, "bvh_build_ms_total": round(bvh_ms, 1),
+                       "scene_create_s_total": round(create_s, 3)},
             "roofline": None, "cpu_baseline": None,
             "e2e": None, "gpu_launches": args.steps * int(st["waves"] * 6 + 2), "clocks": clk,
         }
