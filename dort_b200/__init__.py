@@ -262,8 +262,9 @@ class Scene:
 def render_params(camera: dict, width: int, height: int, iterations: int = 1,
                   min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
                   sample_all_lights: bool = False, direct_strategy: str = "mis",
-                  seed: int = 42) -> _abi.RenderParams:
-    """dort.render.make parameters (lua_render.cpp:102-145) with its defaults."""
+                  seed: int = 42, renderer: str = "pt") -> _abi.RenderParams:
+    """dort.render.make parameters (lua_render.cpp:102-150) with its defaults;
+    `renderer` "pt" (the path tracer) or "lt" / "light" (the light tracer)."""
     p = _abi.RenderParams()
     p.struct_size = ctypes.sizeof(_abi.RenderParams)
     p.width, p.height, p.iterations = width, height, iterations
@@ -271,6 +272,8 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     p.only_direct, p.sample_all_lights = int(only_direct), int(sample_all_lights)
     p.direct_strategy = {"mis": 0, "bsdf": 1, "light": 2}[direct_strategy]
     p.seed = seed
+    p.renderer = {"pt": _abi.RENDERER_PT, "path": _abi.RENDERER_PT, "lt": _abi.RENDERER_LT,
+                  "light": _abi.RENDERER_LT}[renderer]
     c = p.camera
     c.origin = (ctypes.c_float * 3)(*camera["origin"])
     c.right = (ctypes.c_float * 3)(*camera["right"])

@@ -204,6 +204,9 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   PtParams pp;
   std::string err;
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.renderer != RENDERER_PT) {
+    return fail(DORT_ERR_UNSUPPORTED, "the adjoint renders only the pt renderer");
+  }
   int rc = set_tri_params(scene, tri_albedo, tri_emission);
   if(rc != DORT_OK) { return rc; }
   if(d_emission && !scene->pt.tri_emission) {

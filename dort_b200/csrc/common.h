@@ -30,6 +30,20 @@ int fail(int code, const std::string& msg);
 
 }  // namespace dort_gpu
 
+struct dort_scene;
+
+namespace dort_gpu {
+
+// Render scratch kept with the scene (grown on demand; pt_render.cu).
+int render_scratch(dort_scene* s, size_t bytes, void** out);
+
+// The "lt" renderer into d_out (width * height * 3 floats) on stream st;
+// d_counters[0] += rays traced, d_counters[1] += paths (lt.cu).
+int launch_light_trace(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
+                       unsigned long long* d_counters);
+
+}  // namespace dort_gpu
+
 // Host-side scene handle behind the opaque dort_scene.
 struct dort_scene {
   int device = 0;

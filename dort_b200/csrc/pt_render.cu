@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "common.h"
+#include "lt.cuh"
 #include "pt.cuh"
 #include "scene_build.h"
 
@@ -123,6 +124,7 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   }
   if(rp->max_depth > 1000) { err = "max_depth must be <= 1000"; return false; }
   if(rp->direct_strategy > 2) { err = "direct_strategy must be 0 (mis), 1 (bsdf) or 2 (light)"; return false; }
+  if(rp->renderer > DORT_RENDERER_LT) { err = "renderer must be 0 (pt) or 1 (lt)"; return false; }
   std::memset(&pp, 0, sizeof(pp));
   const dort_camera& c = rp->camera;
   for(int a = 0; a < 3; ++a) {
@@ -166,12 +168,42 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   pp.sample_all_lights = rp->sample_all_lights;
   pp.strategy = rp->direct_strategy;
   pp.seed = rp->seed;
+  pp.renderer = rp->renderer;
+  // world -> camera: the inverse of the camera's linear part [right up forward]
+  double m[3][3];
+  for(int a = 0; a < 3; ++a) {
+    m[a][0] = c.right[a];
+    m[a][1] = c.up[a];
+    m[a][2] = c.forward[a];
+  }
+  double det = m[0][0] * (m[1][1] * m[2][2] - m[1][2] * m[2][1]) -
+               m[0][1] * (m[1][0] * m[2][2] - m[1][2] * m[2][0]) +
+               m[0][2] * (m[1][0] * m[2][1] - m[1][1] * m[2][0]);
+  if(std::fabs(det) > 1e-30) {
+    double inv[3][3] = {
+        {m[1][1] * m[2][2] - m[1][2] * m[2][1], m[0][2] * m[2][1] - m[0][1] * m[2][2],
+         m[0][1] * m[1][2] - m[0][2] * m[1][1]},
+        {m[1][2] * m[2][0] - m[1][0] * m[2][2], m[0][0] * m[2][2] - m[0][2] * m[2][0],
+         m[0][2] * m[1][0] - m[0][0] * m[1][2]},
+        {m[1][0] * m[2][1] - m[1][1] * m[2][0], m[0][1] * m[2][0] - m[0][0] * m[2][1],
+         m[0][0] * m[1][1] - m[0][1] * m[1][0]}};
+    for(int r = 0; r < 3; ++r) {
+      for(int k = 0; k < 3; ++k) { pp.cam_inv[3 * r + k] = float(inv[r][k] / det); }
+    }
+  } else if(pp.renderer == RENDERER_LT) {
+    err = "the light tracer needs an invertible camera transform";
+    return false;
+  }
+  if(pp.renderer == RENDERER_LT && pp.camera == CAMERA_THIN_LENS && !(pp.lens_radius > 0.f)) {
+    err = "the light tracer needs a thin lens with lens_radius > 0";
+    return false;
+  }
   return true;
 }
 
-// Scratch for the megakernel: per-(slice, pixel) partial sums plus counters,
-// grown on demand and kept with the scene.
-static int ensure_scratch(dort_scene* s, size_t bytes, void** out) {
+// Scratch for the megakernel (per-(slice, pixel) partial sums) and the light
+// tracer (its film), grown on demand and kept with the scene.
+int render_scratch(dort_scene* s, size_t bytes, void** out) {
   if(s->stage_bytes < bytes) {
     if(s->d_stage) { cudaFree(s->d_stage); s->d_stage = nullptr; s->stage_bytes = 0; }
     if(cudaMalloc(&s->d_stage, bytes) != cudaSuccess) {
@@ -186,6 +218,7 @@ static int ensure_scratch(dort_scene* s, size_t bytes, void** out) {
 
 int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
                   unsigned long long* d_counters) {
+  if(pp.renderer == RENDERER_LT) { return launch_light_trace(s, pp, d_out, st, d_counters); }
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -200,7 +233,7 @@ int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t 
   uint32_t per_slice = tiles * 32;
   size_t partial_bytes = size_t(slices) * npix * sizeof(float4);
   void* scratch = nullptr;
-  int rc = ensure_scratch(s, partial_bytes, &scratch);
+  int rc = render_scratch(s, partial_bytes, &scratch);
   if(rc != DORT_OK) { return rc; }
   float4* partial = static_cast<float4*>(scratch);
   uint64_t threads = uint64_t(slices) * per_slice;
@@ -298,6 +331,19 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
   if(row_end > pp.height) { row_end = pp.height; }
   PtScene sc = host_view(hs);
+  if(pp.renderer == RENDERER_LT) {
+    // light paths splat anywhere: the whole frame at once
+    if(row_begin != 0 || row_end != pp.height) {
+      return fail(DORT_ERR_INVALID, "the light tracer's host check renders whole frames only");
+    }
+    size_t npix = size_t(pp.width) * pp.height;
+    std::vector<float> film(npix * 3, 0.f);
+    for(uint64_t i = 0; i < uint64_t(npix) * pp.spp; ++i) {
+      lt_path<true>(sc, pp, uint32_t(i % npix), uint32_t(i / npix), film.data());
+    }
+    for(size_t k = 0; k < film.size(); ++k) { out_rgb[k] = film[k] / float(pp.spp); }
+    return DORT_OK;
+  }
   NoTape tape;
   for(uint32_t y = row_begin; y < row_end; ++y) {
     for(uint32_t x = 0; x < pp.width; ++x) {
@@ -364,6 +410,9 @@ extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
   PtParams pp;
   std::string err;
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.renderer != RENDERER_PT) {
+    return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_render_wavefront_device renders only the pt renderer");
+  }
   if(pp.sample_all_lights) {
     return fail(DORT_ERR_UNSUPPORTED, "the wavefront renderer does not do sample_all_lights; "
                                       "use dort_gpu_render");
@@ -381,6 +430,9 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
   PtParams pp;
   std::string err;
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.renderer != RENDERER_PT) {
+    return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_render_wavefront renders only the pt renderer");
+  }
   size_t npix = size_t(pp.width) * pp.height;
   float* d_out = nullptr;
   if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
@@ -430,6 +482,9 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
   PtParams pp;
   std::string err;
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.renderer != RENDERER_PT) {
+    return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_wavefront_stage_times renders only the pt renderer");
+  }
   if(pp.sample_all_lights) { return fail(DORT_ERR_UNSUPPORTED, "sample_all_lights"); }
   WfTuning tn;
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
@@ -485,6 +540,9 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
     }
     if(params[j].sample_all_lights) {
       return fail(DORT_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": sample_all_lights");
+    }
+    if(params[j].renderer != RENDERER_PT) {
+      return fail(DORT_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": batches render only pt");
     }
     scenes[j] = jobs[j].scene->pt;
     total += uint64_t(params[j].width) * params[j].height * params[j].spp;

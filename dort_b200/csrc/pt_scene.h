@@ -97,6 +97,8 @@ struct PtScene {
                                  // lights' own transforms
   uint32_t general;          // 1 if the scene has analytic shapes, delta lights,
                              // Oren-Nayar or a general dielectric (host use)
+  float centroid[3];         // Scene::centroid / radius: the bounds' centre and
+  float radius;              // half diagonal (distant lights start on its disk)
 };
 
 enum : uint32_t { CAMERA_PINHOLE = 0, CAMERA_ORTHO = 1, CAMERA_THIN_LENS = 2 };
@@ -113,7 +115,11 @@ struct PtParams {
   uint32_t only_direct, sample_all_lights;
   uint32_t strategy;         // 0 mis, 1 bsdf, 2 light
   uint64_t seed;
+  uint32_t renderer;         // RENDERER_PT, RENDERER_LT
+  float cam_inv[9];          // rows of [right up forward]^-1 (world to camera)
 };
+
+enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1 };
 
 // Whether rendering `sc` with `pp` needs the general instantiation of the
 // path code (pt.cuh, template flag G).

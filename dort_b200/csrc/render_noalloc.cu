@@ -85,6 +85,9 @@ extern "C" int dort_gpu_render_device_noalloc(dort_scene* scene,
   PtParams pp;
   std::string err;
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
+  if(pp.renderer != RENDERER_PT) {
+    return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_render_device_noalloc renders only the pt renderer");
+  }
   size_t npix = size_t(pp.width) * pp.height;
   if(npix > kNoAllocMaxPixels) {
     return fail(DORT_ERR_INVALID, "image of " + std::to_string(npix) + " pixels exceeds the " +

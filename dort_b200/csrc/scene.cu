@@ -134,6 +134,8 @@ static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostSc
   pt.shape_base = hs.shape_base;
   if((rc = upload(s, hs.light_shapes, &pt.light_shapes)) != DORT_OK) { return rc; }
   pt.general = hs.general;
+  for(int a = 0; a < 3; ++a) { pt.centroid[a] = hs.centroid[a]; }
+  pt.radius = hs.radius;
 
   void* w = nullptr;
   if(cudaMalloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {

@@ -397,6 +397,7 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
   bool any = n > 0 || desc->shape_count > 0;
   F3 ext = any ? F3{hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]} : F3{0.f, 0.f, 0.f};
   hs.radius = len(ext) * 0.5f;
+  for(int a = 0; a < 3; ++a) { hs.centroid[a] = any ? 0.5f * (lo[a] + hi[a]) : 0.f; }
   float r2pi = 3.14159265358979323846f * hs.radius * hs.radius;
 
   // delta lights
@@ -546,6 +547,8 @@ PtScene host_view(const HostScene& hs) {
   sc.env.pdfs = hs.env_pdfs.empty() ? nullptr : hs.env_pdfs.data();
   sc.shapes = hs.shapes.empty() ? nullptr : hs.shapes.data();
   sc.shape_count = uint32_t(hs.shapes.size());
+  for(int a = 0; a < 3; ++a) { sc.centroid[a] = hs.centroid[a]; }
+  sc.radius = hs.radius;
   sc.shape_base = hs.shape_base;
   sc.light_shapes = hs.light_shapes.empty() ? nullptr : hs.light_shapes.data();
   sc.general = hs.general;

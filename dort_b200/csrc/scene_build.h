@@ -28,6 +28,7 @@ struct HostScene {
   DevEnv env{};
   uint32_t emissive_count = 0;
   float radius = 0.f;
+  float centroid[3] = {0.f, 0.f, 0.f};
 };
 
 // Analytic shapes are intersected as a list after the BVH.

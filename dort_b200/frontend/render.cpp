@@ -494,9 +494,13 @@ static int render_make(lua_State* l) {
     else if(st == "bsdf") { rp.direct_strategy = DORT_DIRECT_BSDF; }
     else if(st == "light") { rp.direct_strategy = DORT_DIRECT_LIGHT; }
     else { return luaL_error(l, "Unknown direct strategy '%s'", st.c_str()); }
-  } else if(method == "dot" || method == "lt" || method == "light" || method == "bdpt" ||
-            method == "vcm") {
-    return luaL_error(l, "renderer '%s' is not available in this build (only \"pt\")",
+  } else if(method == "lt" || method == "light") {
+    // lua_render.cpp:146-150: path lengths min_depth + 2 .. max_depth + 2
+    rp.renderer = DORT_RENDERER_LT;
+    rp.min_depth = param_uint_opt(l, p, "min_depth", 0);
+    rp.max_depth = param_uint_opt(l, p, "max_depth", 5);
+  } else if(method == "dot" || method == "bdpt" || method == "vcm" || method == "sppm") {
+    return luaL_error(l, "renderer '%s' is not available in this build (\"pt\" and \"lt\")",
                       method.c_str());
   } else {
     return luaL_error(l, "Unrecognized rendering method: %s", method.c_str());
@@ -521,7 +525,8 @@ static int render_sync(lua_State* l) {
   img->px.assign(size_t(img->w) * img->h * 3, 0.f);
   if(job->scene->handle) {
     // the wavefront unless the per-pixel renderer is needed (sample_all_lights)
-    int rc = job->params.sample_all_lights
+    // or the light tracer is asked for
+    int rc = job->params.sample_all_lights || job->params.renderer == DORT_RENDERER_LT
         ? dort_gpu_render(job->scene->handle, &job->params, img->px.data(), nullptr)
         : dort_gpu_render_wavefront(job->scene->handle, &job->params, nullptr, img->px.data(),
                                     nullptr);

@@ -1,4 +1,4 @@
-// Whole-scene harness around the reference renderer's "pt" renderer.
+// Whole-scene harness around the reference renderer's "pt" and "lt" renderers.
 //
 // TEST INFRASTRUCTURE ONLY: compiled with the reference's sources by
 // oracle/Makefile into oracle/_ref/.  Renders a scene given in the product's
@@ -19,7 +19,8 @@
 //   - the frame as lua_make_aggregate would (BvhPrimitive, middle split),
 //     bounds / centroid / radius / background lights as build_scene;
 //   - PinholeCamera / OrthoCamera / ThinLensCamera from the camera columns;
-//   - PathRenderer with the render parameters, RandomSampler(1, seed)
+//   - PathRenderer (or LightRenderer for renderer = lt, path lengths = depths
+//     + 2) with the render parameters, RandomSampler(1, seed)
 //     split(seed), box filter of radius 0.5 (lua_render.cpp:102-145).
 #include <chrono>
 #include <cmath>
@@ -45,6 +46,7 @@
 #include "dort/mirror_material.hpp"
 #include "dort/oren_nayar_material.hpp"
 #include "dort/ortho_camera.hpp"
+#include "dort/light_renderer.hpp"
 #include "dort/path_renderer.hpp"
 #include "dort/phong_material.hpp"
 #include "dort/pinhole_camera.hpp"
@@ -272,13 +274,20 @@ extern "C" int dref_scene_render(const dort_scene_desc* d, const dort_render_par
     ? PathRenderer::DirectStrategy::SAMPLE_BSDF
     : rp->direct_strategy == 2 ? PathRenderer::DirectStrategy::SAMPLE_LIGHT
     : PathRenderer::DirectStrategy::MIS;
-  PathRenderer renderer(scene, film, sampler, camera, rp->iterations, rp->min_depth,
-      rp->max_depth, rp->only_direct != 0, rp->sample_all_lights != 0, ds);
+  std::unique_ptr<Renderer> renderer;
+  if(rp->renderer == DORT_RENDERER_LT) {
+    // dort.render.make for "lt": path lengths = depths + 2 (lua_render.cpp:146-150)
+    renderer.reset(new LightRenderer(scene, film, sampler, camera, rp->iterations,
+        rp->min_depth + 2, rp->max_depth + 2));
+  } else {
+    renderer.reset(new PathRenderer(scene, film, sampler, camera, rp->iterations,
+        rp->min_depth, rp->max_depth, rp->only_direct != 0, rp->sample_all_lights != 0, ds));
+  }
   CtxG ctx;
   ctx.pool = pool;
   NoProgress progress;
   auto t0 = std::chrono::steady_clock::now();
-  renderer.render(ctx, progress);
+  renderer->render(ctx, progress);
   auto t1 = std::chrono::steady_clock::now();
   if(out_seconds) { *out_seconds = std::chrono::duration<double>(t1 - t0).count(); }
   Image<PixelRgbFloat> img = film->to_image<PixelRgbFloat>();

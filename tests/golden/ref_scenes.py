@@ -319,6 +319,16 @@ def _bsdf_cases():
 CASES = _cornell_cases() + _simple_cases() + _bsdf_cases()
 
 
+def case_by_name(name: str) -> dict:
+    """A case of CASES by name; "<name>@square" is the same case rendered
+    square (width x width), for renderers that need a square film."""
+    base, _, variant = name.partition("@")
+    case = next(c for c in CASES if c["name"] == base)
+    if variant == "square":
+        return dict(case, name=name, height=case["width"])
+    return case
+
+
 def build(case: dict) -> dict:
     if case["kind"] == "cornell":
         return cornell_scene(*case["args"])

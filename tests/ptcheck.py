@@ -62,6 +62,28 @@ def compare_blocks(A0, A1, B0, B1):
     return {"X": X, "mean_rel": mean_rel, "Xmed": Xmed, "mean_z": mean_z}
 
 
+def compare_single(A0, A1, B, b_var_ratio):
+    """compare_blocks() against one image B instead of two halves, for a
+    reference whose renders cannot be made independent: B's noise is taken as
+    b_var_ratio times the noise of the mean of A0 and A1 (the ratio of their
+    sample counts when both come from the same estimator)."""
+    A0, A1, B = (np.asarray(x, np.float64) for x in (A0, A1, B))
+    A = (A0 + A1) / 2
+    va = (A0 - A1) ** 2 / 4                      # noise of A, per block and channel
+    v = va * (1.0 + b_var_ratio)                 # noise of A - B
+    num = ((A - B) ** 2).sum(axis=(0, 1))
+    X = num / np.maximum(v.sum(axis=(0, 1)), 1e-30)
+    mean_rel = (A.mean(axis=(0, 1)) - B.mean(axis=(0, 1))) / np.maximum(B.mean(axis=(0, 1)), 1e-30)
+    nb = ((A - B) ** 2).sum(axis=-1)
+    db = v.sum(axis=-1)
+    noisy = db > 1e-12 * max(float(db.max()), 1e-30)
+    Xmed = float(np.median(nb[noisy] / db[noisy])) if noisy.any() else 0.0
+    nblk = A.shape[0] * A.shape[1]
+    se = np.sqrt(v.sum(axis=(0, 1))) / nblk
+    mean_z = (A.mean(axis=(0, 1)) - B.mean(axis=(0, 1))) / np.maximum(se, 1e-30)
+    return {"X": X, "mean_rel": mean_rel, "Xmed": Xmed, "mean_z": mean_z}
+
+
 def block_means(img, block=16):
     """Mean RGB of block x block pixel blocks; the last row / column of blocks
     is ragged when the size does not divide the image."""
