@@ -467,7 +467,7 @@ def run_dort_pt(args):
         f"{st['bvh_ms']:.0f}ms)")
     spp = args.spp or PT_SPP
     p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH, seed=42 + rank)
-    tuning = {"queue_capacity": 1 << 22}
+    tuning = {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"}
     d_out = torch.empty(PT_H * PT_W * 3, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
@@ -570,6 +570,7 @@ def run_dort_pt(args):
                        "rays_per_frame": rays_per_frame,
                        "mrays_per_s": rays_per_frame * args.steps * world / (ms_max / 1e3) / 1e6,
                        "queue_capacity": tuning["queue_capacity"],
+                       "sort_rays": tuning["sort_rays"],
                        "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
@@ -646,7 +647,7 @@ def run_dort_batch(args):
     samples = sum(w * h * spp for (_, w, h, spp, _) in specs)
     log(f"[rank {rank}] 64 scenes ready in {time.time() - t0:.1f}s ({create_s:.2f}s to create, "
         f"{built} BVH builds {bvh_ms:.0f} ms), {samples / 1e9:.2f}G samples")
-    b = db.Batch(jobs, {"queue_capacity": 1 << 22})
+    b = db.Batch(jobs, {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"})
     stream = torch.cuda.current_stream()
     for _ in range(args.warmup):
         b.render(stream.cuda_stream)
@@ -769,6 +770,8 @@ def main():
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--sort-rays", default="off", choices=["on", "off"],
+                    help="sort each wave's extension rays (wavefront)")
     ap.add_argument("--bvh-build", default=None, choices=["host", "device", "ploc"],
                     help="where scenes build their BVH (default: the library's, the device)")
     args = ap.parse_args()

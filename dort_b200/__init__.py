@@ -139,7 +139,7 @@ class Scene:
         self.tri_count = self._holder.desc.tri_count
 
     def close(self):
-        if getattr(self, "handle", None):
+        if getattr(self, "handle", None) and _abi is not None:
             _abi.lib().dort_gpu_scene_destroy(self.handle)
             self.handle = None
 
@@ -288,10 +288,11 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
 
 
 def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
-                     shade_block: int = 0) -> _abi.WavefrontTuning:
+                     shade_block: int = 0, sort_rays: bool | None = None) -> _abi.WavefrontTuning:
     t = _abi.WavefrontTuning()
     t.struct_size = ctypes.sizeof(_abi.WavefrontTuning)
     t.queue_capacity, t.trace_block, t.shade_block = queue_capacity, trace_block, shade_block
+    t.sort_rays = 0 if sort_rays is None else (1 if sort_rays else 2)
     return t
 
 

@@ -93,7 +93,7 @@ class RenderParams(ctypes.Structure):
 
 class WavefrontTuning(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
-                ("shade_block", c_u32), ("reserved", c_u32 * 4)]
+                ("shade_block", c_u32), ("sort_rays", c_u32), ("reserved", c_u32 * 3)]
 
 
 class BatchJob(ctypes.Structure):

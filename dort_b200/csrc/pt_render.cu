@@ -377,7 +377,7 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
   tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 21));
   tn.trace_block = 128;
   tn.shade_block = 128;
-  tn.pad = 0;
+  tn.sort = 0;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
@@ -386,6 +386,11 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
     if(t->queue_capacity) { tn.capacity = t->queue_capacity; }
     if(t->trace_block) { tn.trace_block = t->trace_block; }
     if(t->shade_block) { tn.shade_block = t->shade_block; }
+    if(t->sort_rays > 2) {
+      err = "sort_rays must be 0 (auto), 1 (on) or 2 (off)";
+      return false;
+    }
+    if(t->sort_rays == 1) { tn.sort = 1; }
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
   if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
@@ -551,7 +556,7 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
   tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 22));
   tn.trace_block = 128;
   tn.shade_block = 128;
-  tn.pad = 0;
+  tn.sort = 0;
   if(tuning) {
     if(tuning->struct_size != sizeof(dort_wavefront_tuning)) {
       return fail(DORT_ERR_INVALID, "dort_wavefront_tuning.struct_size mismatch (ABI version)");
@@ -559,6 +564,10 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
     if(tuning->queue_capacity) { tn.capacity = tuning->queue_capacity; }
     if(tuning->trace_block) { tn.trace_block = tuning->trace_block; }
     if(tuning->shade_block) { tn.shade_block = tuning->shade_block; }
+    if(tuning->sort_rays > 2) {
+      return fail(DORT_ERR_INVALID, "sort_rays must be 0 (auto), 1 (on) or 2 (off)");
+    }
+    if(tuning->sort_rays == 1) { tn.sort = 1; }
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
   if(tn.capacity < 32 || tn.capacity > (1u << 26)) {

@@ -22,6 +22,8 @@
 // Random numbers are the megakernel's (philox.cuh, keyed by pixel, sample and
 // bounce), so both renderers trace the same paths; only the order of film
 // additions (float atomics here) differs.
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cstring>
 #include <string>
@@ -116,6 +118,12 @@ struct WfDev {
   float4* nb_d;    // d.xyz, pdf
   float4* nb_f;    // factor.xyz, light index (bits) | use_mis << 31
   float4* film;    // sum rgb, kept count
+  uint32_t* sort_key[2];   // ray sort: keys in / out (capacity each)
+  uint32_t* sort_val[2];   // slots in (the active queue's order) / out (sorted)
+  uint32_t* hit_kind;      // per slot: shade queue of the hit (sorted extension)
+  void* sort_temp;         // CUB temporary storage
+  size_t sort_temp_bytes;
+  uint32_t sorted;         // 1: the extension stage traces in sorted order
   uint32_t* ctr;
   uint32_t capacity;
   uint64_t total_samples;   // work units (see kChunk) of all jobs
@@ -307,11 +315,81 @@ __global__ void wf_regen(J jobs, WfDev w) {
   }
 }
 
+// Ray sort before the extension stage: key = direction octant (3 bits) and
+// the Morton code of the origin's cell on a 32^3 grid over the scene's
+// bounding cube (15 bits).  The sort is stable, so primary rays (one origin
+// for a pinhole) keep their pixel order within an octant.  Every wave sorts
+// the whole queue capacity (the graph is built once; the length lives on the
+// device): positions past the active length get the largest key and stay
+// behind the rays.
+constexpr int kSortBits = 18;
+
+__device__ __forceinline__ uint32_t spread5(uint32_t v) {
+  uint32_t r = 0;
+#pragma unroll
+  for(int b = 0; b < 5; ++b) { r |= ((v >> b) & 1u) << (3 * b); }
+  return r;
+}
+
+__device__ __forceinline__ uint32_t cell_of(float x, float lo, float inv) {
+  float f = (x - lo) * inv;
+  return f <= 0.f ? 0u : (f >= 31.f ? 31u : uint32_t(f));
+}
+
+template<class J>
+__global__ void wf_sort_keys(J jobs, WfDev w) {
+  const uint32_t cur = wave_of(w) & 1u;
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t* act = w.active[cur];
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.capacity;
+      i += gridDim.x * blockDim.x) {
+    uint32_t key = (1u << kSortBits) - 1u, val = 0u;
+    if(i < n) {
+      val = act[i];
+      uint32_t job = J::kBatched ? (w.meta[val].w >> 8) : 0u;
+      const PtScene& sc = jobs.scene(job);
+      float4 o = w.ray_o[val], d = w.ray_d[val];
+      float r = sc.radius;
+      float inv = r > 0.f ? 16.f / r : 0.f;   // 32 cells over 2r
+      uint32_t m = spread5(cell_of(o.x, sc.centroid[0] - r, inv)) |
+                   (spread5(cell_of(o.y, sc.centroid[1] - r, inv)) << 1) |
+                   (spread5(cell_of(o.z, sc.centroid[2] - r, inv)) << 2);
+      uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+      key = (oct << 15) | m;
+    }
+    w.sort_key[0][i] = key;
+    w.sort_val[0][i] = val;
+  }
+}
+
+// After a sorted extension: the shade queues in the active queue's own order,
+// so that the shade stage and the next regeneration walk the path slots as
+// they did unsorted (mostly ascending, coalesced) rather than in ray order.
+__global__ void wf_classify(WfDev w) {
+  const uint32_t cur = wave_of(w) & 1u;
+  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t* act = w.active[cur];
+  uint32_t np = (n + 31u) & ~31u;
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
+    uint32_t slot = 0, kind = kShadeQueues;
+    if(i < n) {
+      slot = act[i];
+      kind = w.hit_kind[slot];
+    }
+#pragma unroll
+    for(uint32_t k = 0; k < kShadeQueues; ++k) {
+      bool mine = kind == k;
+      uint32_t at = warp_append(w.ctr + C_KQ0 + k, mine);
+      if(mine) { w.kq[k][at] = slot; }
+    }
+  }
+}
+
 template<class J>
 __global__ void wf_extend(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
   const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
-  const uint32_t* act = w.active[cur];
+  const uint32_t* act = w.sorted ? w.sort_val[1] : w.active[cur];
   for(;;) {
     uint32_t base = warp_fetch(w.ctr + C_F_EXT);
     if(base >= n) { break; }
@@ -332,6 +410,10 @@ __global__ void wf_extend(J jobs, WfDev w) {
         // Oren-Nayar shares the Lambert queue (the queues only group work)
         if(kind >= kMissQueue) { kind = DORT_MAT_LAMBERT; }
       }
+    }
+    if(w.sorted) {
+      if(i < n) { w.hit_kind[slot] = kind; }
+      continue;
     }
 #pragma unroll
     for(uint32_t k = 0; k < kShadeQueues; ++k) {
@@ -682,9 +764,15 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   size_t Q = capacity;
   size_t f4 = al(Q * sizeof(float4)), u4 = al(Q * sizeof(uint4)), u1 = al(Q * sizeof(uint32_t));
   size_t f4x2 = al(2 * Q * sizeof(float4)), u1x2 = al(2 * Q * sizeof(uint32_t));
+  size_t sort_temp = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, sort_temp, static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), int(capacity), 0, kSortBits);
+  sort_temp = al(sort_temp);
   size_t bytes = 5 * f4 + u4 + f4 /*hit*/ + (4 + kShadeQueues) * u1 /*queues*/ + u1x2 +
                  3 * f4x2 /*shadow, two per path*/ + u1 + 3 * f4 /*neeb*/ +
-                 al(size_t(npix) * sizeof(float4)) + al(C_COUNT * 4);
+                 al(size_t(npix) * sizeof(float4)) + 5 * u1 /*sort*/ + sort_temp +
+                 al(C_COUNT * 4);
   if(cudaMalloc(&wf->mem, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of wavefront queues failed (" +
@@ -714,6 +802,13 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.nb_d = reinterpret_cast<float4*>(take(f4));
   d.nb_f = reinterpret_cast<float4*>(take(f4));
   d.film = reinterpret_cast<float4*>(take(al(size_t(npix) * sizeof(float4))));
+  for(int k = 0; k < 2; ++k) {
+    d.sort_key[k] = reinterpret_cast<uint32_t*>(take(u1));
+    d.sort_val[k] = reinterpret_cast<uint32_t*>(take(u1));
+  }
+  d.hit_kind = reinterpret_cast<uint32_t*>(take(u1));
+  d.sort_temp = take(sort_temp);
+  d.sort_temp_bytes = sort_temp;
   d.ctr = reinterpret_cast<uint32_t*>(take(al(C_COUNT * 4)));
   d.capacity = capacity;
   wf->capacity = capacity;
@@ -745,12 +840,24 @@ static WfGrids wf_grids(const WfTuning& tn) {
   return g;
 }
 
+// The ray sort between regeneration and extension (tn.sort).
+template<class J>
+static void wf_sort(const J& jobs, WfDev& dev, const WfGrids& g, cudaStream_t st) {
+  wf_sort_keys<J><<<g.regen, 256, 0, st>>>(jobs, dev);
+  size_t tb = dev.sort_temp_bytes;
+  cub::DeviceRadixSort::SortPairs(dev.sort_temp, tb, dev.sort_key[0], dev.sort_key[1],
+                                  dev.sort_val[0], dev.sort_val[1], int(dev.capacity), 0,
+                                  kSortBits, st);
+}
+
 template<class J>
 static void wf_launch_wave(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
                            cudaStream_t st) {
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
   wf_regen<J><<<g.regen, 256, 0, st>>>(jobs, dev);
+  if(tn.sort) { wf_sort<J>(jobs, dev, g, st); }
   wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
+  if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(dev); }
   wf_shade<J><<<g.sha, bs, 0, st>>>(jobs, dev);
   wf_shadow<J><<<g.shw, bt, 0, st>>>(jobs, dev);
   wf_neeb<J><<<g.nb, bt, 0, st>>>(jobs, dev);
@@ -777,6 +884,7 @@ static int wf_build_graph(Wavefront* wf, const J& jobs, const WfTuning& tn) {
   DG_CUDA(cudaGraphAddNode(&cnode, wf->graph, nullptr, 0, &cp));
   cudaGraph_t body = cp.conditional.phGraph_out[0];
   WfGrids g = wf_grids<J>(tn);
+  wf->dev.sorted = tn.sort;
   DG_CUDA(cudaStreamBeginCaptureToGraph(st, body, nullptr, nullptr, 0,
                                         cudaStreamCaptureModeThreadLocal));
   wf_launch_wave<J>(jobs, wf->dev, tn, g, st);
@@ -853,6 +961,7 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   SingleJob<G> jobs{s->pt, pp};
   WfGrids g = wf_grids<SingleJob<G>>(tn);
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
+  wf->dev.sorted = tn.sort;
   // more[0]: loop flag; more[1..6]: the counters C_ACT0 .. C_NEEB of the wave
   uint32_t* more = nullptr;
   DG_CUDA(cudaMallocHost(&more, 8 * sizeof(uint32_t)));
@@ -866,7 +975,10 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
     cudaEventRecord(ev[0], st);
     wf_regen<SingleJob<G>><<<g.regen, 256, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[1], st);
+    // the sort counts as part of the extension stage
+    if(tn.sort) { wf_sort<SingleJob<G>>(jobs, wf->dev, g, st); }
     wf_extend<SingleJob<G>><<<g.ext, bt, 0, st>>>(jobs, wf->dev);
+    if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(wf->dev); }
     cudaEventRecord(ev[2], st);
     wf_shade<SingleJob<G>><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[3], st);

@@ -13,7 +13,7 @@ struct WfTuning {
   uint32_t capacity;      // paths in flight
   uint32_t trace_block;   // threads per block of extend / shadow / neeb
   uint32_t shade_block;   // threads per block of shade
-  uint32_t pad;
+  uint32_t sort;          // 1: sort each wave's rays by direction octant and origin cell
 };
 
 struct Wavefront;

@@ -357,7 +357,10 @@ typedef struct dort_wavefront_tuning {
   uint32_t queue_capacity;     /* paths in flight (0: auto) */
   uint32_t trace_block;        /* threads per block, trace stages (0: auto) */
   uint32_t shade_block;        /* threads per block, shade stage (0: auto) */
-  uint32_t reserved[4];
+  uint32_t sort_rays;          /* 0: auto (off), 1: on, 2: off -- sort each
+                                  wave's extension rays by direction octant
+                                  and origin cell before tracing them */
+  uint32_t reserved[3];
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel
