@@ -37,6 +37,10 @@ namespace dort_gpu {
 // Render scratch kept with the scene (grown on demand; pt_render.cu).
 int render_scratch(dort_scene* s, size_t bytes, void** out);
 
+// The device image of the host-pointer render entry points, kept with the
+// scene (grown on demand; pt_render.cu).
+int render_image_buffer(dort_scene* s, size_t bytes, float** out);
+
 // The "lt" renderer into d_out (width * height * 3 floats) on stream st;
 // d_counters[0] += rays traced, d_counters[1] += paths (lt.cu).
 int launch_light_trace(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
@@ -62,7 +66,10 @@ struct dort_scene {
   float* d_tri_albedo = nullptr;        // per-triangle overrides (adjoint), lazy
   float* d_tri_emission = nullptr;
   uint32_t* d_work = nullptr;           // work counters of persistent kernels (scratch)
-  // staging for the host-pointer entry points (grow-only)
+  // render scratch (grow-only)
   void* d_stage = nullptr;
   size_t stage_bytes = 0;
+  // device image of the host-pointer render entry points (grow-only)
+  void* d_image = nullptr;
+  size_t image_bytes = 0;
 };

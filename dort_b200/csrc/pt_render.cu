@@ -216,6 +216,19 @@ int render_scratch(dort_scene* s, size_t bytes, void** out) {
   return DORT_OK;
 }
 
+int render_image_buffer(dort_scene* s, size_t bytes, float** out) {
+  if(s->image_bytes < bytes) {
+    if(s->d_image) { cudaFree(s->d_image); s->d_image = nullptr; s->image_bytes = 0; }
+    if(cudaMalloc(&s->d_image, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
+    }
+    s->image_bytes = bytes;
+  }
+  *out = static_cast<float*>(s->d_image);
+  return DORT_OK;
+}
+
 int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
                   unsigned long long* d_counters) {
   if(pp.renderer == RENDERER_LT) { return launch_light_trace(s, pp, d_out, st, d_counters); }
@@ -277,10 +290,8 @@ extern "C" int dort_gpu_render(dort_scene* scene, const dort_render_params* para
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
   size_t npix = size_t(pp.width) * pp.height;
   float* d_out = nullptr;
-  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
-  }
+  int brc = render_image_buffer(scene, npix * 3 * sizeof(float), &d_out);
+  if(brc != DORT_OK) { return brc; }
   cudaStream_t st = 0;
   unsigned long long* ctr = reinterpret_cast<unsigned long long*>(scene->d_work);
   cudaEvent_t e0, e1;
@@ -308,7 +319,6 @@ extern "C" int dort_gpu_render(dort_scene* scene, const dort_render_params* para
   if(rc == DORT_OK) { cudaEventElapsedTime(&ms, e0, e1); }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(d_out);
   if(rc == DORT_OK && out_stats) {
     out_stats[0] = double(counters[0]);
     out_stats[1] = double(counters[1]);
@@ -440,10 +450,8 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
   }
   size_t npix = size_t(pp.width) * pp.height;
   float* d_out = nullptr;
-  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
-  }
+  int brc = render_image_buffer(scene, npix * 3 * sizeof(float), &d_out);
+  if(brc != DORT_OK) { return brc; }
   cudaStream_t st = 0;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -469,7 +477,6 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
   if(rc == DORT_OK) { cudaEventElapsedTime(&ms, e0, e1); }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  cudaFree(d_out);
   if(rc == DORT_OK && out_stats) {
     out_stats[0] = double(rays);
     out_stats[1] = 0.0;
@@ -495,13 +502,10 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
   size_t npix = size_t(pp.width) * pp.height;
   float* d_out = nullptr;
-  if(cudaMalloc(&d_out, npix * 3 * sizeof(float)) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
-  }
+  int brc = render_image_buffer(scene, npix * 3 * sizeof(float), &d_out);
+  if(brc != DORT_OK) { return brc; }
   double stage_rays[3];
   int rc = wavefront_stage_times(scene, pp, tn, d_out, 0, out_ms, stage_rays);
-  cudaFree(d_out);
   if(rc == DORT_OK) {
     uint64_t rays = 0;
     uint32_t waves = 0, error = 0;

@@ -35,6 +35,9 @@ static void scene_free_device(dort_scene* s) {
   if(s->d_stage) { cudaFree(s->d_stage); }
   s->d_stage = nullptr;
   s->stage_bytes = 0;
+  if(s->d_image) { cudaFree(s->d_image); }
+  s->d_image = nullptr;
+  s->image_bytes = 0;
   s->d_work = nullptr;
 }
 
