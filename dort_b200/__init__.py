@@ -262,9 +262,11 @@ class Scene:
 def render_params(camera: dict, width: int, height: int, iterations: int = 1,
                   min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
                   sample_all_lights: bool = False, direct_strategy: str = "mis",
-                  seed: int = 42, renderer: str = "pt") -> _abi.RenderParams:
-    """dort.render.make parameters (lua_render.cpp:102-150) with its defaults;
-    `renderer` "pt" (the path tracer) or "lt" / "light" (the light tracer)."""
+                  seed: int = 42, renderer: str = "pt",
+                  use_t1_paths: bool = True) -> _abi.RenderParams:
+    """dort.render.make parameters (lua_render.cpp:102-160) with its defaults;
+    `renderer` "pt" (the path tracer), "lt" / "light" (the light tracer) or
+    "bdpt" (the bidirectional path tracer, with use_t1_paths)."""
     p = _abi.RenderParams()
     p.struct_size = ctypes.sizeof(_abi.RenderParams)
     p.width, p.height, p.iterations = width, height, iterations
@@ -273,7 +275,8 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     p.direct_strategy = {"mis": 0, "bsdf": 1, "light": 2}[direct_strategy]
     p.seed = seed
     p.renderer = {"pt": _abi.RENDERER_PT, "path": _abi.RENDERER_PT, "lt": _abi.RENDERER_LT,
-                  "light": _abi.RENDERER_LT}[renderer]
+                  "light": _abi.RENDERER_LT, "bdpt": _abi.RENDERER_BDPT}[renderer]
+    p.renderer_flags = 0 if use_t1_paths else _abi.BDPT_NO_T1_PATHS
     c = p.camera
     c.origin = (ctypes.c_float * 3)(*camera["origin"])
     c.right = (ctypes.c_float * 3)(*camera["right"])

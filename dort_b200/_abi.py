@@ -32,7 +32,8 @@ SHAPE_LIGHT_TRANSFORM = 1
 LIGHT_POINT, LIGHT_DIRECTIONAL = 1, 2
 CAMERA_PINHOLE, CAMERA_ORTHO, CAMERA_THIN_LENS = 0, 1, 2
 BVH_BUILD_DEFAULT, BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_PLOC = 0, 1, 2, 3
-RENDERER_PT, RENDERER_LT = 0, 1
+RENDERER_PT, RENDERER_LT, RENDERER_BDPT = 0, 1, 2
+BDPT_NO_T1_PATHS = 1
 ABI_VERSION = 2
 
 
@@ -87,7 +88,7 @@ class RenderParams(ctypes.Structure):
         ("iterations", c_u32), ("min_depth", c_u32), ("max_depth", c_u32),
         ("only_direct", c_u32), ("sample_all_lights", c_u32),
         ("direct_strategy", c_u32), ("renderer", c_u32), ("seed", ctypes.c_uint64),
-        ("camera", Camera), ("reserved", c_u32 * 8),
+        ("camera", Camera), ("renderer_flags", c_u32), ("reserved", c_u32 * 7),
     ]
 
 

@@ -46,6 +46,10 @@ int render_image_buffer(dort_scene* s, size_t bytes, float** out);
 int launch_light_trace(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
                        unsigned long long* d_counters);
 
+// The "bdpt" renderer into d_out; counters as launch_light_trace (bdpt.cu).
+int launch_bdpt(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
+                unsigned long long* d_counters);
+
 }  // namespace dort_gpu
 
 // Host-side scene handle behind the opaque dort_scene.

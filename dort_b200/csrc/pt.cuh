@@ -625,6 +625,10 @@ struct LightSample {
   // shadow segment
   V3 o, d;
   float tmin, tmax;
+  // the sampled light point, its normal and ray epsilon (area and point
+  // lights; bidirectional connections)
+  V3 p, nn;
+  float p_eps;
 };
 
 // DiffuseLight::sample_pivot_radiance (diffuse_light.cpp:40-68) on an
@@ -647,6 +651,9 @@ DG_HD LightSample shape_light_sample(const PtScene& sc, const DevLight& l, V3 pi
   s.tmin = pivot_eps;
   s.tmax = dist - eps;
   s.L = dot(swi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+  s.p = pt;
+  s.nn = normalize(xf_normal(sh.inv, n));
+  s.p_eps = eps;
   return s;
 }
 
@@ -674,6 +681,9 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmin = pivot_eps;
     s.tmax = dist - 1e-3f;
     s.L = dot(wi, n) < 0.f ? light_radiance(sc, l) : v3(0.f, 0.f, 0.f);
+    s.p = pt;
+    s.nn = n;
+    s.p_eps = 1e-3f;
   } else if(G && l.kind == LIGHT_SHAPE) {
     s = shape_light_sample(sc, l, pivot, pivot_eps, u, v);
   } else if(G && l.kind == LIGHT_POINT) {
@@ -687,6 +697,9 @@ DG_HD LightSample light_sample(const PtScene& sc, const DevLight& l, V3 pivot, f
     s.tmin = pivot_eps;
     s.tmax = dist;
     s.L = v3p(l.L);
+    s.p = pt;
+    s.nn = -s.wi;     // point_light.cpp:27
+    s.p_eps = 0.f;
   } else if(G && l.kind == LIGHT_DIR) {
     // DirectionalLight::sample_pivot_radiance (directional_light.cpp:28-42)
     s.wi = -v3p(l.nn);

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "bdpt.cuh"
 #include "common.h"
 #include "lt.cuh"
 #include "pt.cuh"
@@ -124,7 +125,14 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   }
   if(rp->max_depth > 1000) { err = "max_depth must be <= 1000"; return false; }
   if(rp->direct_strategy > 2) { err = "direct_strategy must be 0 (mis), 1 (bsdf) or 2 (light)"; return false; }
-  if(rp->renderer > DORT_RENDERER_LT) { err = "renderer must be 0 (pt) or 1 (lt)"; return false; }
+  if(rp->renderer > DORT_RENDERER_BDPT) {
+    err = "renderer must be 0 (pt), 1 (lt) or 2 (bdpt)";
+    return false;
+  }
+  if(rp->renderer == DORT_RENDERER_BDPT && rp->max_depth > 13) {
+    err = "the bdpt renderer supports max_depth <= 13";
+    return false;
+  }
   std::memset(&pp, 0, sizeof(pp));
   const dort_camera& c = rp->camera;
   for(int a = 0; a < 3; ++a) {
@@ -169,6 +177,7 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   pp.strategy = rp->direct_strategy;
   pp.seed = rp->seed;
   pp.renderer = rp->renderer;
+  pp.use_t1 = (rp->renderer_flags & DORT_BDPT_NO_T1_PATHS) ? 0u : 1u;
   // world -> camera: the inverse of the camera's linear part [right up forward]
   double m[3][3];
   for(int a = 0; a < 3; ++a) {
@@ -190,12 +199,12 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
     for(int r = 0; r < 3; ++r) {
       for(int k = 0; k < 3; ++k) { pp.cam_inv[3 * r + k] = float(inv[r][k] / det); }
     }
-  } else if(pp.renderer == RENDERER_LT) {
-    err = "the light tracer needs an invertible camera transform";
+  } else if(pp.renderer != RENDERER_PT) {
+    err = "the light and bidirectional tracers need an invertible camera transform";
     return false;
   }
-  if(pp.renderer == RENDERER_LT && pp.camera == CAMERA_THIN_LENS && !(pp.lens_radius > 0.f)) {
-    err = "the light tracer needs a thin lens with lens_radius > 0";
+  if(pp.renderer != RENDERER_PT && pp.camera == CAMERA_THIN_LENS && !(pp.lens_radius > 0.f)) {
+    err = "the light and bidirectional tracers need a thin lens with lens_radius > 0";
     return false;
   }
   return true;
@@ -232,6 +241,7 @@ int render_image_buffer(dort_scene* s, size_t bytes, float** out) {
 int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
                   unsigned long long* d_counters) {
   if(pp.renderer == RENDERER_LT) { return launch_light_trace(s, pp, d_out, st, d_counters); }
+  if(pp.renderer == RENDERER_BDPT) { return launch_bdpt(s, pp, d_out, st, d_counters); }
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -341,11 +351,38 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
   if(!make_params(params, pp, err)) { return fail(DORT_ERR_INVALID, err); }
   if(row_end > pp.height) { row_end = pp.height; }
   PtScene sc = host_view(hs);
-  if(pp.renderer == RENDERER_LT) {
-    // light paths splat anywhere: the whole frame at once
-    if(row_begin != 0 || row_end != pp.height) {
-      return fail(DORT_ERR_INVALID, "the light tracer's host check renders whole frames only");
+  if(pp.renderer != RENDERER_PT && (row_begin != 0 || row_end != pp.height)) {
+    // light paths and t = 1 connections splat anywhere: whole frames only
+    return fail(DORT_ERR_INVALID, "the light and bidirectional tracers' host check renders "
+                                  "whole frames only");
+  }
+  if(pp.renderer == RENDERER_BDPT) {
+    size_t npix = size_t(pp.width) * pp.height;
+    std::vector<float> splat(npix * 3, 0.f);
+    std::vector<double> acc(npix * 4, 0.0);
+    uint32_t rays = 0;
+    for(uint32_t s = 0; s < pp.spp; ++s) {
+      for(uint32_t pixel = 0; pixel < npix; ++pixel) {
+        Rand4 r0 = rand4(pp.seed, pixel, s, 0);
+        V3 L = bdpt_sample<true>(sc, pp, pixel, s, float(pixel % pp.width) + r0.a,
+                                 float(pixel / pp.width) + r0.b, pp.use_t1 != 0, splat.data(),
+                                 rays);
+        if(keep_sample(L)) {
+          acc[4 * pixel] += L.x; acc[4 * pixel + 1] += L.y; acc[4 * pixel + 2] += L.z;
+          acc[4 * pixel + 3] += 1;
+        }
+      }
     }
+    for(size_t p = 0; p < npix; ++p) {
+      double w = acc[4 * p + 3];
+      for(int a = 0; a < 3; ++a) {
+        out_rgb[3 * p + a] = float((w != 0 ? acc[4 * p + a] / w : 0.0) +
+                                   double(splat[3 * p + a]) / pp.spp);
+      }
+    }
+    return DORT_OK;
+  }
+  if(pp.renderer == RENDERER_LT) {
     size_t npix = size_t(pp.width) * pp.height;
     std::vector<float> film(npix * 3, 0.f);
     for(uint64_t i = 0; i < uint64_t(npix) * pp.spp; ++i) {

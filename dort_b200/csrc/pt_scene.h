@@ -115,11 +115,12 @@ struct PtParams {
   uint32_t only_direct, sample_all_lights;
   uint32_t strategy;         // 0 mis, 1 bsdf, 2 light
   uint64_t seed;
-  uint32_t renderer;         // RENDERER_PT, RENDERER_LT
+  uint32_t renderer;         // RENDERER_PT, RENDERER_LT, RENDERER_BDPT
   float cam_inv[9];          // rows of [right up forward]^-1 (world to camera)
+  uint32_t use_t1;           // bdpt: connect light subpaths to the camera (t = 1)
 };
 
-enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1 };
+enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1, RENDERER_BDPT = 2 };
 
 // Whether rendering `sc` with `pp` needs the general instantiation of the
 // path code (pt.cuh, template flag G).

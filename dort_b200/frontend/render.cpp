@@ -499,9 +499,20 @@ static int render_make(lua_State* l) {
     rp.renderer = DORT_RENDERER_LT;
     rp.min_depth = param_uint_opt(l, p, "min_depth", 0);
     rp.max_depth = param_uint_opt(l, p, "max_depth", 5);
-  } else if(method == "dot" || method == "bdpt" || method == "vcm" || method == "sppm") {
-    return luaL_error(l, "renderer '%s' is not available in this build (\"pt\" and \"lt\")",
-                      method.c_str());
+  } else if(method == "bdpt") {
+    // lua_render.cpp:151-159; the per-(s, t) debug films are not kept
+    rp.renderer = DORT_RENDERER_BDPT;
+    rp.min_depth = param_uint_opt(l, p, "min_depth", 0);
+    rp.max_depth = param_uint_opt(l, p, "max_depth", 5);
+    if(!param_bool_opt(l, p, "use_t1_paths", true)) {
+      rp.renderer_flags |= DORT_BDPT_NO_T1_PATHS;
+    }
+    if(!param_string_opt(l, p, "debug_image_dir", "").empty()) {
+      return luaL_error(l, "debug_image_dir is not supported by this build's bdpt renderer");
+    }
+  } else if(method == "dot" || method == "vcm" || method == "sppm") {
+    return luaL_error(l, "renderer '%s' is not available in this build "
+                      "(\"pt\", \"lt\" and \"bdpt\")", method.c_str());
   } else {
     return luaL_error(l, "Unrecognized rendering method: %s", method.c_str());
   }
@@ -525,8 +536,8 @@ static int render_sync(lua_State* l) {
   img->px.assign(size_t(img->w) * img->h * 3, 0.f);
   if(job->scene->handle) {
     // the wavefront unless the per-pixel renderer is needed (sample_all_lights)
-    // or the light tracer is asked for
-    int rc = job->params.sample_all_lights || job->params.renderer == DORT_RENDERER_LT
+    // or the light or bidirectional tracer is asked for
+    int rc = job->params.sample_all_lights || job->params.renderer != DORT_RENDERER_PT
         ? dort_gpu_render(job->scene->handle, &job->params, img->px.data(), nullptr)
         : dort_gpu_render_wavefront(job->scene->handle, &job->params, nullptr, img->px.data(),
                                     nullptr);

@@ -300,13 +300,20 @@ typedef struct dort_camera {
 enum dort_direct_strategy { DORT_DIRECT_MIS = 0, DORT_DIRECT_BSDF = 1, DORT_DIRECT_LIGHT = 2 };
 
 /* dort_render_params.renderer: the "pt" renderer (PathRenderer,
- * path_renderer.cpp) or the "lt" light tracer (LightRenderer,
+ * path_renderer.cpp), the "lt" light tracer (LightRenderer,
  * light_renderer.cpp:13-181: width x height x iterations light paths, each
  * connected to the camera at its first vertex and every non-delta vertex,
  * min / max path length = min_depth / max_depth + 2 as dort.render.make sets
- * them, lua_render.cpp:146-150).  only_direct, sample_all_lights and
- * direct_strategy are "pt" parameters. */
-enum dort_renderer { DORT_RENDERER_PT = 0, DORT_RENDERER_LT = 1 };
+ * them, lua_render.cpp:146-150) or the "bdpt" bidirectional path tracer
+ * (BdptRenderer, bdpt_renderer.cpp: a light and a camera walk per pixel
+ * sample, every connection weighted by the balance heuristic, t = 1
+ * connections splatted unless renderer_flags has DORT_BDPT_NO_T1_PATHS;
+ * max_depth <= 13).  only_direct, sample_all_lights and direct_strategy are
+ * "pt" parameters. */
+enum dort_renderer { DORT_RENDERER_PT = 0, DORT_RENDERER_LT = 1, DORT_RENDERER_BDPT = 2 };
+
+/* dort_render_params.renderer_flags */
+#define DORT_BDPT_NO_T1_PATHS 1u   /* bdpt: use_t1_paths = false */
 
 typedef struct dort_render_params {
   uint32_t struct_size;        /* sizeof(dort_render_params) */
@@ -319,7 +326,8 @@ typedef struct dort_render_params {
   uint32_t renderer;           /* dort_renderer */
   uint64_t seed;
   dort_camera camera;
-  uint32_t reserved[8];
+  uint32_t renderer_flags;     /* DORT_BDPT_NO_T1_PATHS */
+  uint32_t reserved[7];
 } dort_render_params;
 
 /* Renders into out_rgb (host, width * height * 3 floats, row-major, row 0 at
@@ -449,9 +457,9 @@ int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const float* rays,
 
 /* No reference counterpart.  Runs the device path-sampling code compiled for
  * the CPU over the pixels [row_begin, row_end) of the image (small images
- * only); writes those rows of out_rgb.  The light tracer (params->renderer
- * = DORT_RENDERER_LT) renders whole frames only (rows 0 .. height).  For
- * checking without a GPU. */
+ * only); writes those rows of out_rgb.  The light tracer and the
+ * bidirectional tracer (params->renderer = DORT_RENDERER_LT / _BDPT) render
+ * whole frames only (rows 0 .. height).  For checking without a GPU. */
 int dort_gpu_host_check_render(const dort_scene_desc* desc, const dort_render_params* params,
                                uint32_t row_begin, uint32_t row_end, float* out_rgb);
 

@@ -20,13 +20,15 @@
 //     bounds / centroid / radius / background lights as build_scene;
 //   - PinholeCamera / OrthoCamera / ThinLensCamera from the camera columns;
 //   - PathRenderer (or LightRenderer for renderer = lt, path lengths = depths
-//     + 2) with the render parameters, RandomSampler(1, seed)
+//     + 2; BdptRenderer for renderer = bdpt, no debug images) with the render
+//     parameters, RandomSampler(1, seed)
 //     split(seed), box filter of radius 0.5 (lua_render.cpp:102-145).
 #include <chrono>
 #include <cmath>
 #include <memory>
 #include <vector>
 
+#include "dort/bdpt_renderer.hpp"
 #include "dort/bvh_primitive.hpp"
 #include "dort/ctx.hpp"
 #include "dort/cube_shape.hpp"
@@ -279,6 +281,10 @@ extern "C" int dref_scene_render(const dort_scene_desc* d, const dort_render_par
     // dort.render.make for "lt": path lengths = depths + 2 (lua_render.cpp:146-150)
     renderer.reset(new LightRenderer(scene, film, sampler, camera, rp->iterations,
         rp->min_depth + 2, rp->max_depth + 2));
+  } else if(rp->renderer == DORT_RENDERER_BDPT) {
+    // dort.render.make for "bdpt" (lua_render.cpp:151-159)
+    renderer.reset(new BdptRenderer(scene, film, sampler, camera, rp->iterations,
+        rp->min_depth, rp->max_depth, (rp->renderer_flags & DORT_BDPT_NO_T1_PATHS) == 0, ""));
   } else {
     renderer.reset(new PathRenderer(scene, film, sampler, camera, rp->iterations,
         rp->min_depth, rp->max_depth, rp->only_direct != 0, rp->sample_all_lights != 0, ds));

@@ -1,0 +1,162 @@
+"""The bidirectional path tracer ("bdpt" renderer) on the GPU.
+
+1. Against the reference's own BdptRenderer (bdpt_renderer.cpp:9-468) on the
+   scenes its image tests render with "bdpt" (tests/golden/bdpt_images.npz,
+   two independent halves by the compiled reference): channel means within
+   4.5 standard errors, median per-block chi-square ratio below 1.5 -- the
+   bounds of the path tracer's parity test (tests/test_ref_scenes_gpu.py).
+   With t = 1 connections off on a subset, against the reference's renders
+   with use_t1_paths = false (<name>/nt0, nt1): the reference keeps those
+   connections in its MIS weights, so the image without them is darker, a
+   debugging switch that the GPU reproduces.
+2. Against the path tracer: on the scenes where the reference's own "bdpt"
+   and "pt" renders agree (its two fixtures pass these statistics against
+   each other), the GPU's bidirectional image and the reference's "pt" image
+   (tests/golden/ref_images.npz) agree too -- the check the reference's
+   tests make (each renderer's image against a converged "pt" image).  On
+   the other scenes the reference's bidirectional tracer converges elsewhere
+   (Phong surfaces 0.3-2 % darker, delta surfaces ~10 % and infinite lights
+   ~3 % brighter, the thin lens through its pivot importance) and test 1
+   holds the GPU to that.
+3. The contract of the entry points: the bidirectional tracer renders through
+   dort_gpu_render / _device only, with max_depth <= 13.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+sys.path.insert(0, HERE)
+
+import ptcheck  # noqa: E402
+import ref_scenes  # noqa: E402
+
+BD_PATH = os.path.join(HERE, "golden", "bdpt_images.npz")
+PT_PATH = os.path.join(HERE, "golden", "ref_images.npz")
+BD = np.load(BD_PATH) if os.path.exists(BD_PATH) else None
+PT = np.load(PT_PATH) if os.path.exists(PT_PATH) else None
+NAMES = [str(n) for n in BD["names"]] if BD is not None else []
+PT_NAMES = set(str(n) for n in PT["names"]) if PT is not None else set()
+
+Z_MAX = 4.5
+XMED_MAX = 1.5
+# the subset rendered without t = 1 connections (use_t1_paths = false)
+NO_T1 = [n for n in NAMES if n + "/nt0" in BD] if BD is not None else []
+
+
+def _agrees_with_pt(name):
+    """The reference's bidirectional and path-traced fixtures agree."""
+    r = ptcheck.compare_blocks(BD[name + "/rb0"], BD[name + "/rb1"], PT[name + "/rb0"],
+                               PT[name + "/rb1"])
+    return bool(np.all(np.abs(r["mean_z"]) < Z_MAX) and r["Xmed"] < XMED_MAX)
+
+
+AGREE = ([n for n in NAMES if n in PT_NAMES and _agrees_with_pt(n)]
+         if BD is not None and PT is not None else [])
+
+
+def _render(name, spp, seeds=(101, 102), use_t1=True):
+    import dort_b200 as db
+    case = ref_scenes.case_by_name(name)
+    d = ref_scenes.build(case)
+    sc = db.scene_from_dict(d)
+    out = []
+    for seed in seeds:
+        p = db.render_params(d["camera"], case["width"], case["height"], spp,
+                             min_depth=case["min_depth"], max_depth=case["max_depth"],
+                             seed=seed, renderer="bdpt", use_t1_paths=use_t1)
+        img, st = sc.render(p)
+        assert st["samples"] + st["dropped"] == case["width"] * case["height"] * spp
+        assert st["dropped"] <= 1e-4 * st["samples"]
+        out.append(ptcheck.block_means(img.astype(np.float64)))
+    sc.close()
+    return out
+
+
+def _assert_close(name, ours, ref0, ref1):
+    r = ptcheck.compare_blocks(ours[0], ours[1], ref0, ref1)
+    ref_mean = (np.asarray(ref0, np.float64) + np.asarray(ref1, np.float64)).mean(axis=(0, 1)) / 2
+    lit = ref_mean > 1e-4
+    ours_mean = (np.asarray(ours[0]) + np.asarray(ours[1])).mean(axis=(0, 1)) / 2
+    assert np.all(ours_mean[~lit] < 1e-4), (name, ours_mean, ref_mean)
+    if lit.any():
+        assert np.all(np.abs(r["mean_z"][lit]) < Z_MAX), (name, r)
+        assert r["Xmed"] < XMED_MAX, (name, r)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(BD is None, reason="tests/golden/bdpt_images.npz missing")
+@pytest.mark.parametrize("name", NAMES)
+def test_bdpt_matches_reference_bdpt(name, cuda):
+    ours = _render(name, int(BD["spp"]))
+    _assert_close(name, ours, BD[name + "/rb0"], BD[name + "/rb1"])
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(BD is None, reason="tests/golden/bdpt_images.npz missing")
+@pytest.mark.parametrize("name", NO_T1)
+def test_bdpt_without_t1_paths_matches_reference_bdpt(name, cuda):
+    ours = _render(name, int(BD["spp"]), seeds=(301, 302), use_t1=False)
+    _assert_close(name, ours, BD[name + "/nt0"], BD[name + "/nt1"])
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(BD is None or PT is None, reason="fixtures missing")
+@pytest.mark.parametrize("name", AGREE)
+def test_bdpt_converges_to_the_path_tracer(name, cuda):
+    ours = _render(name, 2 * int(BD["spp"]), seeds=(201, 202))
+    _assert_close(name, ours, PT[name + "/rb0"], PT[name + "/rb1"])
+
+
+@pytest.mark.gpu
+def test_bdpt_entry_points(cuda):
+    import dort_b200 as db
+    case = ref_scenes.case_by_name("box_diff_area_pin")
+    d = ref_scenes.build(case)
+    sc = db.scene_from_dict(d)
+    p = db.render_params(d["camera"], 64, 64, 2, max_depth=3, renderer="bdpt")
+    img, st = sc.render(p)
+    assert img.shape == (64, 64, 3) and np.isfinite(img).all() and img.mean() > 0
+    assert st["rays"] > 0 and st["samples"] == 64 * 64 * 2
+    with pytest.raises(db.DortError, match="DORT_ERR_UNSUPPORTED"):
+        sc.render_wavefront(p)
+    with pytest.raises(db.DortError, match="max_depth"):
+        sc.render(db.render_params(d["camera"], 64, 64, 1, max_depth=14, renderer="bdpt"))
+    sc.close()
+
+
+def test_bdpt_fixture_is_consistent():
+    """CPU: the fixture covers the reference's "bdpt" test scenes with the
+    expected shapes."""
+    if BD is None:
+        pytest.skip("fixture missing")
+    assert len(NAMES) >= 70 and len(NO_T1) >= 5 and len(AGREE) >= 40
+    for name in NAMES:
+        case = ref_scenes.case_by_name(name)
+        by, bx = (case["height"] + 15) // 16, (case["width"] + 15) // 16
+        assert BD[name + "/rb0"].shape == (by, bx, 3)
+        assert BD[name + "/rb1"].shape == (by, bx, 3)
+
+
+def test_bdpt_statistics_flag_a_planted_bias():
+    """CPU: the reference's halves against the same halves scaled by 5 % (a
+    mistake planted on the reference side) fail the checks on at least 90 %
+    of the lit fixture scenes."""
+    if BD is None:
+        pytest.skip("fixture missing")
+    flagged = lit_scenes = 0
+    for name in NAMES:
+        b0 = np.asarray(BD[name + "/rb0"], np.float64)
+        b1 = np.asarray(BD[name + "/rb1"], np.float64)
+        lit = (b0 + b1).mean(axis=(0, 1)) > 1e-4
+        if not lit.any():
+            continue
+        lit_scenes += 1
+        bad = ptcheck.compare_blocks(b0 * 1.05, b1 * 1.05, b0, b1)
+        flagged += bool(np.any(np.abs(bad["mean_z"][lit]) >= Z_MAX) or bad["Xmed"] >= XMED_MAX)
+    assert lit_scenes >= 60 and flagged >= 0.9 * lit_scenes

@@ -216,3 +216,37 @@ def test_script_renders_like_the_python_api(tmp_path, cuda):
     # rounding of the two flattenings' vertex transforms
     diff = np.abs(lua_img.astype(np.float64) - py_img)
     assert float(diff.mean()) < 1e-3 * max(float(py_img.mean()), 1e-6), float(diff.mean())
+
+
+@needs_frontend
+@pytest.mark.gpu
+@pytest.mark.parametrize("renderer", ["lt", "bdpt"])
+def test_script_renders_other_renderers_like_the_python_api(tmp_path, cuda, renderer):
+    import dort_b200 as db
+    from dort_b200.image import read_rgbe, rgbe_quantize
+    script = tmp_path / "scene.lua"
+    script.write_text(SCENE_LUA.replace("max_depth = 4,", f'max_depth = 4, renderer = "{renderer}",'))
+    out = subprocess.run([DORT, str(script), str(tmp_path / "img.hdr")], capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lua_img = read_rgbe(str(tmp_path / "img.hdr"))
+    d = _python_scene()
+    sc = db.scene_from_dict(d)
+    p = db.render_params(d["camera"], 96, 64, 16, max_depth=4, seed=7, renderer=renderer)
+    py_img = rgbe_quantize(sc.render(p)[0])
+    sc.close()
+    # same sample streams; splats are summed by float atomics in any order
+    diff = np.abs(lua_img.astype(np.float64) - py_img)
+    assert float(diff.mean()) < 1e-3 * max(float(py_img.mean()), 1e-6), float(diff.mean())
+
+
+@needs_frontend
+def test_frontend_bdpt_debug_images_are_refused(tmp_path):
+    script = tmp_path / "scene.lua"
+    script.write_text(SCENE_LUA.replace(
+        "max_depth = 4,", 'max_depth = 4, renderer = "bdpt", debug_image_dir = "x",'))
+    env = dict(os.environ, DORT_LUA_RECORD=str(tmp_path / "rec.json"))
+    out = subprocess.run([DORT, str(script), str(tmp_path / "img.hdr")], env=env,
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 1
+    assert "debug_image_dir" in out.stderr
