@@ -51,6 +51,14 @@ enum : uint32_t {
   C_COUNT = 32
 };
 
+// Each counter sits alone at the start of a 128-byte line (a 64-bit counter
+// takes the line's first two words): the stages' warp-aggregated atomics on
+// different counters then go to different L2 lines instead of queueing on
+// one.
+constexpr uint32_t kCtrStride = 32;
+
+DG_HD uint32_t* ctr_at(uint32_t* ctr, uint32_t i) { return ctr + i * kCtrStride; }
+
 // Shade queues: paths are sorted by what they hit (material kind 0..4, or a
 // miss) so that the warps of the shade stage run one BSDF's code.
 constexpr uint32_t kShadeQueues = 6;
@@ -177,7 +185,7 @@ struct JobTable {
 };
 
 __device__ __forceinline__ uint32_t wave_of(const WfDev& w) {
-  return *(volatile uint32_t*)(w.ctr + C_WAVES);
+  return *(volatile uint32_t*)ctr_at(w.ctr, C_WAVES);
 }
 
 __global__ void wf_init(WfDev w, uint32_t npix) {
@@ -189,8 +197,10 @@ __global__ void wf_init(WfDev w, uint32_t npix) {
   for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npix; i += stride) {
     w.film[i] = make_float4(0.f, 0.f, 0.f, 0.f);
   }
-  if(blockIdx.x == 0 && threadIdx.x < C_COUNT) {
-    w.ctr[threadIdx.x] = threadIdx.x == C_FIN0 ? w.capacity : 0u;
+  if(blockIdx.x == 0) {
+    for(uint32_t i = threadIdx.x; i < C_COUNT * kCtrStride; i += blockDim.x) {
+      w.ctr[i] = i == C_FIN0 * kCtrStride ? w.capacity : 0u;
+    }
   }
 }
 
@@ -224,14 +234,42 @@ __device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_
 // outside the image later).  Keeping the queue order keeps neighbouring
 // pixels' primary rays next to each other whatever order the shade stage ran
 // the paths in.
+// Block-wide counts of the regen stage: per warp, then one atomic per block
+// and counter (the stage's appends would otherwise queue one atomic per warp
+// on the same counters).  kRegenBlock threads, every thread of a block takes
+// part in every round.
+constexpr uint32_t kRegenBlock = 256;
+constexpr uint32_t kRegenWarps = kRegenBlock / 32;
+
+struct RegenShared {
+  uint32_t cnt[3][kRegenWarps];   // per warp: new units, active appends, free appends
+  int live[kRegenWarps];          // per warp: change of the live-unit count
+  unsigned long long next_base;
+  uint32_t base[2];
+};
+
+// Exclusive scan of cnt[k] over the warps (thread 0); returns the total.
+__device__ __forceinline__ uint32_t regen_scan(uint32_t* cnt) {
+  uint32_t t = 0;
+  for(uint32_t w = 0; w < kRegenWarps; ++w) {
+    uint32_t c = cnt[w];
+    cnt[w] = t;
+    t += c;
+  }
+  return t;
+}
+
 template<class J>
 __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32_t slot,
-                                           uint32_t cur, bool from_free) {
-  uint64_t* next = reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
+                                           uint32_t cur, bool from_free, RegenShared& sh) {
+  uint64_t* next = reinterpret_cast<uint64_t*>(ctr_at(w.ctr, C_NEXT_LO));
   uint32_t* act = w.active[cur];
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
   uint4 m = valid ? w.meta[slot] : make_uint4(0u, 0u, 0u, SLOT_FREE + 7u);
   bool keep = valid && (m.w & 0xffu) == SLOT_ACTIVE && !from_free;
   bool started = false;
+  int live = 0;
   if(valid && (m.w & 0xffu) == SLOT_FINISHED) {
     const uint32_t job = m.w >> 8;
     const PtParams& pp = jobs.params(job);
@@ -253,23 +291,22 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
       if(a.w > 0.f || a.x != 0.f || a.y != 0.f || a.z != 0.f) {
         atomicAdd(w.film + jobs.film_offset(job) + m.x, a);
       }
-      atomicSub(w.ctr + C_LIVE, 1u);
+      live -= 1;
       m.w = SLOT_FREE;
     }
   }
+  // new units: one 64-bit atomic per block on the next-unit counter
   bool want_new = valid && (m.w & 0xffu) == SLOT_FREE;
   uint32_t nmask = __ballot_sync(0xffffffffu, want_new);
-  uint64_t uid = ~0ull;
-  if(want_new) {
-    uint32_t lane = threadIdx.x & 31u, leader = __ffs(nmask) - 1u;
-    unsigned long long base = 0;
-    if(lane == leader) {
-      base = atomicAdd(reinterpret_cast<unsigned long long*>(next),
-                       (unsigned long long)__popc(nmask));
-    }
-    base = __shfl_sync(nmask, base, leader);
-    uid = base + __popc(nmask & ((1u << lane) - 1u));
+  if(lane == 0) { sh.cnt[0][warp] = __popc(nmask); }
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    uint32_t t = regen_scan(sh.cnt[0]);
+    sh.next_base = t ? atomicAdd(reinterpret_cast<unsigned long long*>(next),
+                                 (unsigned long long)t) : 0ull;
   }
+  __syncthreads();
+  uint64_t uid = want_new ? sh.next_base + sh.cnt[0][warp] + __popc(nmask & lt) : ~0ull;
   if(want_new && uid < w.total_samples) {
     uint32_t job = jobs.job_of_sample(uid);
     const PtParams& pp = jobs.params(job);
@@ -280,7 +317,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
       start_path<J::kGeneral>(w, pp, slot, pixel, s0);
       m = make_uint4(pixel, s0, 0u, SLOT_ACTIVE | (job << 8));
       started = true;
-      atomicAdd(w.ctr + C_LIVE, 1u);
+      live += 1;
     }
   }
   if(valid && (started || want_new)) { w.meta[slot] = m; }
@@ -288,30 +325,49 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
   // that it keeps taking units
   bool retry = want_new && !started && uid < w.total_samples;
   bool put = keep || started;
-  uint32_t at = warp_append(w.ctr + C_ACT0 + cur, put);
-  if(put) { act[at] = slot; }
-  uint32_t rt = warp_append(w.ctr + C_FIN0 + (cur ^ 1u), retry);
-  if(retry) { w.finished[cur ^ 1u][rt] = slot; }
+  uint32_t pmask = __ballot_sync(0xffffffffu, put);
+  uint32_t rmask = __ballot_sync(0xffffffffu, retry);
+  int wlive = __reduce_add_sync(0xffffffffu, live);
+  if(lane == 0) {
+    sh.cnt[1][warp] = __popc(pmask);
+    sh.cnt[2][warp] = __popc(rmask);
+    sh.live[warp] = wlive;
+  }
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    uint32_t ta = regen_scan(sh.cnt[1]), tr = regen_scan(sh.cnt[2]);
+    int tl = 0;
+    for(uint32_t k = 0; k < kRegenWarps; ++k) { tl += sh.live[k]; }
+    sh.base[0] = ta ? atomicAdd(ctr_at(w.ctr, C_ACT0 + cur), ta) : 0u;
+    sh.base[1] = tr ? atomicAdd(ctr_at(w.ctr, C_FIN0 + (cur ^ 1u)), tr) : 0u;
+    if(tl != 0) { atomicAdd(ctr_at(w.ctr, C_LIVE), uint32_t(tl)); }
+  }
+  __syncthreads();
+  if(put) { act[sh.base[0] + sh.cnt[1][warp] + __popc(pmask & lt)] = slot; }
+  if(retry) { w.finished[cur ^ 1u][sh.base[1] + sh.cnt[2][warp] + __popc(rmask & lt)] = slot; }
 }
 
 template<class J>
-__global__ void wf_regen(J jobs, WfDev w) {
+__global__ void __launch_bounds__(kRegenBlock) wf_regen(J jobs, WfDev w) {
+  __shared__ RegenShared sh;
   const uint32_t wave = wave_of(w);
   const uint32_t cur = wave & 1u, prev = cur ^ 1u;
-  const uint32_t n_prev = *(volatile uint32_t*)(w.ctr + C_ACT0 + prev);
-  const uint32_t n_free = *(volatile uint32_t*)(w.ctr + C_FIN0 + cur);
+  const uint32_t n_prev = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + prev);
+  const uint32_t n_free = *(volatile uint32_t*)ctr_at(w.ctr, C_FIN0 + cur);
   const uint32_t* old = w.active[prev];
   const uint32_t* fre = w.finished[cur];
-  uint32_t stride = gridDim.x * blockDim.x;
-  uint32_t np = (n_prev + 31u) & ~31u;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += stride) {
+  // every thread of a block runs the same number of iterations (the rounds
+  // of regen_slot synchronise the block)
+  const uint32_t stride = gridDim.x * kRegenBlock;
+  const uint32_t np = (n_prev + kRegenBlock - 1u) / kRegenBlock * kRegenBlock;
+  for(uint32_t i = blockIdx.x * kRegenBlock + threadIdx.x; i < np; i += stride) {
     bool valid = i < n_prev;
-    regen_slot(jobs, w, valid, valid ? old[i] : 0u, cur, false);
+    regen_slot(jobs, w, valid, valid ? old[i] : 0u, cur, false, sh);
   }
-  uint32_t nf = (n_free + 31u) & ~31u;
-  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nf; i += stride) {
+  const uint32_t nf = (n_free + kRegenBlock - 1u) / kRegenBlock * kRegenBlock;
+  for(uint32_t i = blockIdx.x * kRegenBlock + threadIdx.x; i < nf; i += stride) {
     bool valid = i < n_free;
-    regen_slot(jobs, w, valid, valid ? fre[i] : 0u, cur, true);
+    regen_slot(jobs, w, valid, valid ? fre[i] : 0u, cur, true, sh);
   }
 }
 
@@ -339,7 +395,7 @@ __device__ __forceinline__ uint32_t cell_of(float x, float lo, float inv) {
 template<class J>
 __global__ void wf_sort_keys(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + cur);
   const uint32_t* act = w.active[cur];
   for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < w.capacity;
       i += gridDim.x * blockDim.x) {
@@ -367,7 +423,7 @@ __global__ void wf_sort_keys(J jobs, WfDev w) {
 // they did unsorted (mostly ascending, coalesced) rather than in ray order.
 __global__ void wf_classify(WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + cur);
   const uint32_t* act = w.active[cur];
   uint32_t np = (n + 31u) & ~31u;
   for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < np; i += gridDim.x * blockDim.x) {
@@ -379,7 +435,7 @@ __global__ void wf_classify(WfDev w) {
 #pragma unroll
     for(uint32_t k = 0; k < kShadeQueues; ++k) {
       bool mine = kind == k;
-      uint32_t at = warp_append(w.ctr + C_KQ0 + k, mine);
+      uint32_t at = warp_append(ctr_at(w.ctr, C_KQ0 + k), mine);
       if(mine) { w.kq[k][at] = slot; }
     }
   }
@@ -388,10 +444,10 @@ __global__ void wf_classify(WfDev w) {
 template<class J>
 __global__ void wf_extend(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_ACT0 + cur);
+  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + cur);
   const uint32_t* act = w.sorted ? w.sort_val[1] : w.active[cur];
   for(;;) {
-    uint32_t base = warp_fetch(w.ctr + C_F_EXT);
+    uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_EXT));
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     uint32_t slot = 0, kind = kShadeQueues;
@@ -418,7 +474,7 @@ __global__ void wf_extend(J jobs, WfDev w) {
 #pragma unroll
     for(uint32_t k = 0; k < kShadeQueues; ++k) {
       bool mine = kind == k;
-      uint32_t at = warp_append(w.ctr + C_KQ0 + k, mine);
+      uint32_t at = warp_append(ctr_at(w.ctr, C_KQ0 + k), mine);
       if(mine) { w.kq[k][at] = slot; }
     }
   }
@@ -431,12 +487,12 @@ __global__ void wf_shade(J jobs, WfDev w) {
   uint32_t n = 0;
 #pragma unroll
   for(uint32_t k = 0; k < kShadeQueues; ++k) {
-    qn[k] = *(volatile uint32_t*)(w.ctr + C_KQ0 + k);
+    qn[k] = *(volatile uint32_t*)ctr_at(w.ctr, C_KQ0 + k);
     n += qn[k];
   }
   const uint32_t req_nd = F_ALL & ~F_DELTA;
   for(;;) {
-    uint32_t base = warp_fetch(w.ctr + C_F_SHADE);
+    uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_SHADE));
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     bool valid = i < n;
@@ -584,21 +640,21 @@ __global__ void wf_shade(J jobs, WfDev w) {
     }
     (void)cont;
     (void)done;
-    uint32_t si = warp_append(w.ctr + C_SHADOW, push_sh);
+    uint32_t si = warp_append(ctr_at(w.ctr, C_SHADOW), push_sh);
     if(push_sh) {
       w.sh_slot[si] = slot;
       w.sh_o[si] = sh_o;
       w.sh_d[si] = sh_d;
       w.sh_c[si] = sh_c;
     }
-    uint32_t si2 = warp_append(w.ctr + C_SHADOW, push_sh2);
+    uint32_t si2 = warp_append(ctr_at(w.ctr, C_SHADOW), push_sh2);
     if(push_sh2) {
       w.sh_slot[si2] = slot;
       w.sh_o[si2] = sh2_o;
       w.sh_d[si2] = sh2_d;
       w.sh_c[si2] = sh2_c;
     }
-    uint32_t ni = warp_append(w.ctr + C_NEEB, push_nb);
+    uint32_t ni = warp_append(ctr_at(w.ctr, C_NEEB), push_nb);
     if(push_nb) {
       w.nb_slot[ni] = slot;
       w.nb_o[ni] = nb_o;
@@ -610,9 +666,9 @@ __global__ void wf_shade(J jobs, WfDev w) {
 
 template<class J>
 __global__ void wf_shadow(J jobs, WfDev w) {
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_SHADOW);
+  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_SHADOW);
   for(;;) {
-    uint32_t base = warp_fetch(w.ctr + C_F_SH);
+    uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_SH));
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     if(i < n) {
@@ -639,9 +695,9 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
 
 template<class J>
 __global__ void wf_neeb(J jobs, WfDev w) {
-  const uint32_t n = *(volatile uint32_t*)(w.ctr + C_NEEB);
+  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_NEEB);
   for(;;) {
-    uint32_t base = warp_fetch(w.ctr + C_F_NB);
+    uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_NB));
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     if(i < n) {
@@ -683,28 +739,28 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
 
 // Single thread: account the wave, retire its queues, decide whether to loop.
 __device__ __forceinline__ bool wf_end_wave(WfDev& w) {
-  uint32_t wave = w.ctr[C_WAVES];
+  uint32_t wave = *ctr_at(w.ctr, C_WAVES);
   uint32_t cur = wave & 1u;
-  uint32_t a = w.ctr[C_ACT0 + cur], s = w.ctr[C_SHADOW], b = w.ctr[C_NEEB];
-  unsigned long long* rays = reinterpret_cast<unsigned long long*>(w.ctr + C_RAYS_LO);
+  uint32_t a = *ctr_at(w.ctr, C_ACT0 + cur), s = *ctr_at(w.ctr, C_SHADOW), b = *ctr_at(w.ctr, C_NEEB);
+  unsigned long long* rays = reinterpret_cast<unsigned long long*>(ctr_at(w.ctr, C_RAYS_LO));
   *rays += (unsigned long long)a + s + b;
   // this wave's active queue stays for the next regen; the lists this wave's
   // regen read are consumed
-  w.ctr[C_ACT0 + (cur ^ 1u)] = 0u;
-  w.ctr[C_FIN0 + cur] = 0u;
-  w.ctr[C_SHADOW] = 0u;
-  w.ctr[C_NEEB] = 0u;
-  w.ctr[C_F_EXT] = 0u;
-  w.ctr[C_F_SHADE] = 0u;
-  w.ctr[C_F_SH] = 0u;
-  w.ctr[C_F_NB] = 0u;
-  for(uint32_t k = 0; k < kShadeQueues; ++k) { w.ctr[C_KQ0 + k] = 0u; }
-  w.ctr[C_WAVES] = wave + 1u;
-  uint64_t next = *reinterpret_cast<uint64_t*>(w.ctr + C_NEXT_LO);
-  bool more = w.ctr[C_LIVE] > 0u || next < w.total_samples;
+  *ctr_at(w.ctr, C_ACT0 + (cur ^ 1u)) = 0u;
+  *ctr_at(w.ctr, C_FIN0 + cur) = 0u;
+  *ctr_at(w.ctr, C_SHADOW) = 0u;
+  *ctr_at(w.ctr, C_NEEB) = 0u;
+  *ctr_at(w.ctr, C_F_EXT) = 0u;
+  *ctr_at(w.ctr, C_F_SHADE) = 0u;
+  *ctr_at(w.ctr, C_F_SH) = 0u;
+  *ctr_at(w.ctr, C_F_NB) = 0u;
+  for(uint32_t k = 0; k < kShadeQueues; ++k) { *ctr_at(w.ctr, C_KQ0 + k) = 0u; }
+  *ctr_at(w.ctr, C_WAVES) = wave + 1u;
+  uint64_t next = *reinterpret_cast<uint64_t*>(ctr_at(w.ctr, C_NEXT_LO));
+  bool more = *ctr_at(w.ctr, C_LIVE) > 0u || next < w.total_samples;
   if(more && wave + 1u >= w.max_waves) {
     // bounded: a frame never loops forever; the host reports the error
-    w.ctr[C_ERROR] = 1u;
+    *ctr_at(w.ctr, C_ERROR) = 1u;
     more = false;
   }
   return more;
@@ -772,7 +828,7 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   size_t bytes = 5 * f4 + u4 + f4 /*hit*/ + (4 + kShadeQueues) * u1 /*queues*/ + u1x2 +
                  3 * f4x2 /*shadow, two per path*/ + u1 + 3 * f4 /*neeb*/ +
                  al(size_t(npix) * sizeof(float4)) + 5 * u1 /*sort*/ + sort_temp +
-                 al(C_COUNT * 4);
+                 al(C_COUNT * kCtrStride * 4);
   if(cudaMalloc(&wf->mem, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of wavefront queues failed (" +
@@ -809,7 +865,7 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.hit_kind = reinterpret_cast<uint32_t*>(take(u1));
   d.sort_temp = take(sort_temp);
   d.sort_temp_bytes = sort_temp;
-  d.ctr = reinterpret_cast<uint32_t*>(take(al(C_COUNT * 4)));
+  d.ctr = reinterpret_cast<uint32_t*>(take(al(C_COUNT * kCtrStride * 4)));
   d.capacity = capacity;
   wf->capacity = capacity;
   wf->npix_cap = npix;
@@ -832,7 +888,7 @@ struct WfGrids {
 template<class J>
 static WfGrids wf_grids(const WfTuning& tn) {
   WfGrids g;
-  g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), 256);
+  g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), int(kRegenBlock));
   g.ext = grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
   g.sha = grid_for(reinterpret_cast<const void*>(&wf_shade<J>), int(tn.shade_block));
   g.shw = grid_for(reinterpret_cast<const void*>(&wf_shadow<J>), int(tn.trace_block));
@@ -854,7 +910,7 @@ template<class J>
 static void wf_launch_wave(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
                            cudaStream_t st) {
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
-  wf_regen<J><<<g.regen, 256, 0, st>>>(jobs, dev);
+  wf_regen<J><<<g.regen, kRegenBlock, 0, st>>>(jobs, dev);
   if(tn.sort) { wf_sort<J>(jobs, dev, g, st); }
   wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
   if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(dev); }
@@ -973,7 +1029,7 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   bool ok = cudaGetLastError() == cudaSuccess;
   for(uint32_t wave = 0; ok && wave < wf->dev.max_waves + 1; ++wave) {
     cudaEventRecord(ev[0], st);
-    wf_regen<SingleJob<G>><<<g.regen, 256, 0, st>>>(jobs, wf->dev);
+    wf_regen<SingleJob<G>><<<g.regen, kRegenBlock, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[1], st);
     // the sort counts as part of the extension stage
     if(tn.sort) { wf_sort<SingleJob<G>>(jobs, wf->dev, g, st); }
@@ -986,8 +1042,8 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
     cudaEventRecord(ev[4], st);
     wf_neeb<SingleJob<G>><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);
-    cudaMemcpyAsync(more + 1, wf->dev.ctr, (C_NEEB + 1) * sizeof(uint32_t),
-                    cudaMemcpyDeviceToHost, st);
+    cudaMemcpy2DAsync(more + 1, sizeof(uint32_t), wf->dev.ctr, kCtrStride * sizeof(uint32_t),
+                      sizeof(uint32_t), C_NEEB + 1, cudaMemcpyDeviceToHost, st);
     wf_control_host<<<1, 1, 0, st>>>(wf->dev, more);
     ok = cudaStreamSynchronize(st) == cudaSuccess;
     for(int k = 0; ok && k < 5; ++k) {
@@ -1028,12 +1084,14 @@ int wavefront_stage_times(dort_scene* s, const PtParams& pp, const WfTuning& tn,
 int wavefront_counters_of(Wavefront* wf, uint64_t* rays, uint32_t* waves, uint32_t* error,
                           cudaStream_t st) {
   if(!wf || !wf->mem) { return fail(DORT_ERR_INVALID, "no wavefront state"); }
-  uint32_t c[C_COUNT];
-  DG_CUDA(cudaMemcpyAsync(c, wf->dev.ctr, sizeof(c), cudaMemcpyDeviceToHost, st));
+  // the first two words of every counter's line
+  uint32_t c[2 * C_COUNT];
+  DG_CUDA(cudaMemcpy2DAsync(c, 2 * sizeof(uint32_t), wf->dev.ctr, kCtrStride * sizeof(uint32_t),
+                            2 * sizeof(uint32_t), C_COUNT, cudaMemcpyDeviceToHost, st));
   DG_CUDA(cudaStreamSynchronize(st));
-  *rays = uint64_t(c[C_RAYS_LO]) | (uint64_t(c[C_RAYS_LO + 1]) << 32);
-  *waves = c[C_WAVES];
-  *error = c[C_ERROR];
+  *rays = uint64_t(c[2 * C_RAYS_LO]) | (uint64_t(c[2 * C_RAYS_LO + 1]) << 32);
+  *waves = c[2 * C_WAVES];
+  *error = c[2 * C_ERROR];
   return DORT_OK;
 }
 
