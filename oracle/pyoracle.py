@@ -304,7 +304,8 @@ class RefPtScene:
 
 def ref_scene_render(scene: dict, params) -> tuple[np.ndarray, float]:
     """Renders a scene dict (the form dort_b200.scene_desc takes: triangles,
-    analytic shapes, delta lights, sky) with the reference's own PathRenderer,
+    analytic shapes, delta lights, sky) with the reference's own PathRenderer
+    (LightRenderer / BdptRenderer for params.renderer = lt / bdpt),
     single-threaded; `params` is a dort_b200 RenderParams (camera kind
     included).  Returns (image [h, w, 3] f32, seconds).  The ctypes structures
     of the product's C ABI only describe the input here; nothing of the

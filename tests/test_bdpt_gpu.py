@@ -11,11 +11,11 @@
    debugging switch that the GPU reproduces.
 2. Against the path tracer: on the scenes where the reference's own "bdpt"
    and "pt" renders agree (its two fixtures pass these statistics against
-   each other), the GPU's bidirectional image and the reference's "pt" image
+   each other with a margin; no Phong surfaces), the GPU's bidirectional image and the reference's "pt" image
    (tests/golden/ref_images.npz) agree too -- the check the reference's
    tests make (each renderer's image against a converged "pt" image).  On
    the other scenes the reference's bidirectional tracer converges elsewhere
-   (Phong surfaces 0.3-2 % darker, delta surfaces ~10 % and infinite lights
+   (Phong surfaces 0.1-2 % darker, delta surfaces ~10 % and infinite lights
    ~3 % brighter, the thin lens through its pivot importance) and test 1
    holds the GPU to that.
 3. The contract of the entry points: the bidirectional tracer renders through
@@ -50,10 +50,16 @@ NO_T1 = [n for n in NAMES if n + "/nt0" in BD] if BD is not None else []
 
 
 def _agrees_with_pt(name):
-    """The reference's bidirectional and path-traced fixtures agree."""
+    """The reference's bidirectional and path-traced fixtures agree, with a
+    margin (channel means within 2.5 standard errors: the GPU's halves have
+    twice the samples, so a bias the fixtures' noise hides shows there), and
+    the scene has no Phong surface (on those the reference's bidirectional
+    tracer is darker by 0.1-2 %, a bias the GPU reproduces)."""
+    if "_glos_" in name or "phong" in name:
+        return False
     r = ptcheck.compare_blocks(BD[name + "/rb0"], BD[name + "/rb1"], PT[name + "/rb0"],
                                PT[name + "/rb1"])
-    return bool(np.all(np.abs(r["mean_z"]) < Z_MAX) and r["Xmed"] < XMED_MAX)
+    return bool(np.all(np.abs(r["mean_z"]) < 2.5) and r["Xmed"] < XMED_MAX)
 
 
 AGREE = ([n for n in NAMES if n in PT_NAMES and _agrees_with_pt(n)]
@@ -135,7 +141,7 @@ def test_bdpt_fixture_is_consistent():
     expected shapes."""
     if BD is None:
         pytest.skip("fixture missing")
-    assert len(NAMES) >= 70 and len(NO_T1) >= 5 and len(AGREE) >= 40
+    assert len(NAMES) >= 70 and len(NO_T1) >= 5 and len(AGREE) >= 30
     for name in NAMES:
         case = ref_scenes.case_by_name(name)
         by, bx = (case["height"] + 15) // 16, (case["width"] + 15) // 16
