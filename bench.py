@@ -62,6 +62,11 @@ sys.path.insert(0, ROOT)
 
 N_TRIS = 1_000_000
 N_RAYS = 16 * 1024 * 1024
+# DRAM bytes (read + write) of one raycast_kernel launch over the 16M-ray
+# workload, from the ncu capture summarised in
+# profiles/raycast_kernel_1Mtri_16Mrays.md (dram__bytes_read.sum +
+# dram__bytes_write.sum); reported as the roofline's traffic.
+RAYCAST_TRAFFIC_BYTES = 791.8e6
 WORKLOAD = "raycast: 1M random tris (SAH BVH), 16M rays (8M coherent pinhole 4096x2048 + 8M diffuse bounce), closest hit"
 
 
@@ -365,7 +370,9 @@ def run_dort(args):
             bytes_per_ray = 32 + 16 + c["n_node"] * 32 + c["n_tri"] * 36
             achieved = n * bytes_per_ray / (per_launch / 1e3) / 1e9
             rl = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                  "frac": achieved / hbm, "traffic": None,
+                  "frac": achieved / hbm, "traffic": RAYCAST_TRAFFIC_BYTES,
+                  "traffic_source": "ncu capture of one launch "
+                                    "(profiles/raycast_kernel_1Mtri_16Mrays.md)",
                   "peak_source": peak_kind,
                   "bytes_per_ray": bytes_per_ray, "n_node": c["n_node"], "n_tri": c["n_tri"],
                   "kernel_ms_per_launch": per_launch}
