@@ -404,6 +404,12 @@ PT_WORKLOAD = ("pt1080p: wavefront path tracing 1920x1080, 256 spp, max depth 16
                "1,997,122-tri fBm-displaced icosphere + ground plane, Lambert / GGX conductor / "
                "dielectric mix, procedural 1024x512 HDR sky")
 REF_SAMPLE_W, REF_SAMPLE_H = 480, 270
+# DRAM bytes (read + write) of one wf_extend launch over a full queue
+# (4,194,304 rays, waves 6-8 of the 16-spp frame), mean of three launches of
+# the ncu capture summarised in profiles/wf_extend_pt1080p.md: 742 MB, 177 B
+# per ray; reported as the roofline's traffic.
+EXTEND_TRAFFIC_BYTES = 742.2e6
+EXTEND_TRAFFIC_RAYS = 4194304
 
 _ref_worker_scene = None
 
@@ -557,7 +563,12 @@ def run_dort_pt(args):
             bytes_per_ray = 32 + 16 + n_node * 32 + n_tri * 36
             achieved = ext_rays * bytes_per_ray / (stages["extend"] / 1e3) / 1e9
             rl = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                  "frac": achieved / hbm, "traffic": None, "peak_source": peak_kind,
+                  "frac": achieved / hbm, "traffic": EXTEND_TRAFFIC_BYTES,
+                  "traffic_source": f"ncu capture of full-queue launches "
+                                    f"({EXTEND_TRAFFIC_RAYS} rays; "
+                                    f"profiles/wf_extend_pt1080p.md)",
+                  "algorithmic_bytes_per_full_launch": EXTEND_TRAFFIC_RAYS * bytes_per_ray,
+                  "peak_source": peak_kind,
                   "kernel": "wf_extend (closest hit)", "bytes_per_ray": bytes_per_ray,
                   "n_node": n_node, "n_tri": n_tri, "work_sample_rays": nwork,
                   "extend_rays_per_frame": ext_rays,
