@@ -468,14 +468,28 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
   uint32_t nt = bdpt_camera_walk<G>(c, fx, fy, cw, rays);
   if(ns == 0) { lw[0] = bvert_empty(); }
   if(nt == 0) { return total; }
-  for(uint32_t s = 0; s <= ns; ++s) {
-    for(uint32_t t = 1; t <= nt; ++t) {
+  // On the device the lanes of a warp run the (s, t) loop in lock step, to
+  // the warp's largest walk lengths, so that they take the same connection
+  // case together instead of drifting apart by their own walk lengths.
+#ifdef __CUDA_ARCH__
+  const uint32_t lanes = __activemask();
+  const uint32_t s_end = __reduce_max_sync(lanes, ns), t_end = __reduce_max_sync(lanes, nt);
+#else
+  const uint32_t s_end = ns, t_end = nt;
+#endif
+  for(uint32_t s = 0; s <= s_end; ++s) {
+    for(uint32_t t = 1; t <= t_end; ++t) {
+      if(s > ns || t > nt) { continue; }
       if(t == 1 && !use_t1) { continue; }
       if(s + t < pp.min_depth + 2 || s + t > pp.max_depth + 2) { continue; }
       Rand4 rc = rand4(pp.seed, pixel, sample, kBdConnect + 32 * s + t);
       const BVert& last_camera = cw[t - 1];
       uint32_t new_light = light_i;
-      BVert first_light = lw[0], first_camera = cw[0];
+      // the connection's own end vertices where it makes new ones (s = 1
+      // light sample, t = 1 camera point), else the walks' first vertices
+      BVert first_light, first_camera;
+      const BVert* fl = &lw[0];
+      const BVert* fc = &cw[0];
       float sfx = fx, sfy = fy;
       V3 contrib = v3(0.f, 0.f, 0.f);
       if(s > 0 && last_camera.bg != 0) {
@@ -536,6 +550,7 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         }
         first_light.delta = (light_flags(l2) & LF_DELTA_DIR) ? 1u : 0u;
         first_light.bwd_pdf = bsdf_pdf<G>(m, fr, ls.wi, bwo, F_ALL);
+        fl = &first_light;
         contrib = last_camera.alpha * f * ls.L *
                   (fabsf(dot(last_camera.nn, ls.wi)) / (lp * ls.pdf));
       } else if(s >= 2 && t == 1) {
@@ -558,6 +573,7 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         first_camera.p = cam.p;
         first_camera.fwd_pdf = cam.pdf;
         first_camera.alpha = v3(cam.We, cam.We, cam.We);
+        fc = &first_camera;
         contrib = last_light.alpha * f *
                   (cam.We * fabsf(dot(last_light.nn, wo)) / (length_sq(cam.p - last_light.p) * cam.pdf));
       } else {
@@ -581,7 +597,7 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         contrib = last_light.alpha * last_camera.alpha * fl * fc * geom;
       }
       if(is_black(contrib)) { continue; }
-      BdptPath path{lw, cw, s == 1 ? &first_light : &lw[0], t == 1 ? &first_camera : &cw[0], s, t};
+      BdptPath path{lw, cw, fl, fc, s, t};
       float w = bdpt_weight<G>(c, sc.lights[new_light], path);
       V3 wc = contrib * w;
       if(t == 1) {
