@@ -204,10 +204,22 @@ __global__ void wf_init(WfDev w, uint32_t npix) {
   }
 }
 
+// Direction octant of a ray (sign bits of x, y, z).  The path state keeps
+// the octant of its next extension ray in bits 28..30 of meta.z (bounces
+// take the bits below: max_depth <= 1000), so that regen can group the
+// active queue by octant without reading the rays.
+constexpr uint32_t kOctShift = 28;
+constexpr uint32_t kBounceMask = (1u << kOctShift) - 1u;
+
+DG_HD uint32_t dir_octant(V3 d) {
+  return (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+}
+
 // Starts sample s of `pixel` in `slot`: camera ray, unit throughput.
+// Returns the camera ray's direction octant.
 template<bool G>
-__device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_t slot,
-                                           uint32_t pixel, uint32_t s) {
+__device__ __forceinline__ uint32_t start_path(WfDev& w, const PtParams& pp, uint32_t slot,
+                                               uint32_t pixel, uint32_t s) {
   uint32_t x = pixel % pp.width, y = pixel / pp.width;
   float fx, fy;
   if(s == 0) {
@@ -224,6 +236,7 @@ __device__ __forceinline__ void start_path(WfDev& w, const PtParams& pp, uint32_
   w.ray_d[slot] = make_float4(d.x, d.y, d.z, 0.f);
   w.thr[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
   w.sum[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
+  return dir_octant(d);
 }
 
 // Builds this wave's active queue.  It walks the previous wave's active queue
@@ -242,10 +255,11 @@ constexpr uint32_t kRegenBlock = 256;
 constexpr uint32_t kRegenWarps = kRegenBlock / 32;
 
 struct RegenShared {
-  uint32_t cnt[3][kRegenWarps];   // per warp: new units, active appends, free appends
+  uint32_t cnt[3][kRegenWarps];   // per warp: new units, (unused), free appends
   int live[kRegenWarps];          // per warp: change of the live-unit count
   unsigned long long next_base;
   uint32_t base[2];
+  uint32_t oc[8][kRegenWarps];    // per direction octant and warp: active appends
 };
 
 // Exclusive scan of cnt[k] over the warps (thread 0); returns the total.
@@ -270,6 +284,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
   bool keep = valid && (m.w & 0xffu) == SLOT_ACTIVE && !from_free;
   bool started = false;
   int live = 0;
+  uint32_t oct = (m.z >> kOctShift) & 7u;
   if(valid && (m.w & 0xffu) == SLOT_FINISHED) {
     const uint32_t job = m.w >> 8;
     const PtParams& pp = jobs.params(job);
@@ -284,8 +299,8 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
     uint32_t unit_end = min(pp.spp, (m.y / kChunk + 1u) * kChunk);
     if(next_s < unit_end) {
       w.acc[slot] = a;
-      start_path<J::kGeneral>(w, pp, slot, m.x, next_s);
-      m = make_uint4(m.x, next_s, 0u, SLOT_ACTIVE | (job << 8));
+      oct = start_path<J::kGeneral>(w, pp, slot, m.x, next_s);
+      m = make_uint4(m.x, next_s, oct << kOctShift, SLOT_ACTIVE | (job << 8));
       started = true;
     } else {
       if(a.w > 0.f || a.x != 0.f || a.y != 0.f || a.z != 0.f) {
@@ -314,8 +329,8 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
     unit_to_pixel(pp, uid - jobs.sample_begin(job), pixel, x, y, s0);
     if(x < pp.width && y < pp.height) {
       w.acc[slot] = make_float4(0.f, 0.f, 0.f, 0.f);
-      start_path<J::kGeneral>(w, pp, slot, pixel, s0);
-      m = make_uint4(pixel, s0, 0u, SLOT_ACTIVE | (job << 8));
+      oct = start_path<J::kGeneral>(w, pp, slot, pixel, s0);
+      m = make_uint4(pixel, s0, oct << kOctShift, SLOT_ACTIVE | (job << 8));
       started = true;
       live += 1;
     }
@@ -325,17 +340,34 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
   // that it keeps taking units
   bool retry = want_new && !started && uid < w.total_samples;
   bool put = keep || started;
-  uint32_t pmask = __ballot_sync(0xffffffffu, put);
+  // the active queue is grouped by direction octant within each block's
+  // share (slot order kept within an octant): the extension stage's warps
+  // then take rays that visit a node's children in the same order
+  uint32_t omask = 0u;
+#pragma unroll
+  for(uint32_t k = 0; k < 8u; ++k) {
+    uint32_t mk = __ballot_sync(0xffffffffu, put && oct == k);
+    if(lane == 0) { sh.oc[k][warp] = __popc(mk); }
+    if(oct == k) { omask = mk; }
+  }
   uint32_t rmask = __ballot_sync(0xffffffffu, retry);
   int wlive = __reduce_add_sync(0xffffffffu, live);
   if(lane == 0) {
-    sh.cnt[1][warp] = __popc(pmask);
     sh.cnt[2][warp] = __popc(rmask);
     sh.live[warp] = wlive;
   }
   __syncthreads();
   if(threadIdx.x == 0) {
-    uint32_t ta = regen_scan(sh.cnt[1]), tr = regen_scan(sh.cnt[2]);
+    // exclusive scan in (octant, warp) order
+    uint32_t ta = 0;
+    for(uint32_t k = 0; k < 8u; ++k) {
+      for(uint32_t q = 0; q < kRegenWarps; ++q) {
+        uint32_t c = sh.oc[k][q];
+        sh.oc[k][q] = ta;
+        ta += c;
+      }
+    }
+    uint32_t tr = regen_scan(sh.cnt[2]);
     int tl = 0;
     for(uint32_t k = 0; k < kRegenWarps; ++k) { tl += sh.live[k]; }
     sh.base[0] = ta ? atomicAdd(ctr_at(w.ctr, C_ACT0 + cur), ta) : 0u;
@@ -343,7 +375,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
     if(tl != 0) { atomicAdd(ctr_at(w.ctr, C_LIVE), uint32_t(tl)); }
   }
   __syncthreads();
-  if(put) { act[sh.base[0] + sh.cnt[1][warp] + __popc(pmask & lt)] = slot; }
+  if(put) { act[sh.base[0] + sh.oc[oct][warp] + __popc(omask & lt)] = slot; }
   if(retry) { w.finished[cur ^ 1u][sh.base[1] + sh.cnt[2][warp] + __popc(rmask & lt)] = slot; }
 }
 
@@ -518,8 +550,9 @@ __global__ void wf_shade(J jobs, WfDev w) {
       h.t = h4.x; h.b1 = h4.y; h.b2 = h4.z; h.prim = f2u(h4.w);
       V3 o = v3(ro.x, ro.y, ro.z), d = v3(rd.x, rd.y, rd.z);
       V3 thr = v3(t4.x, t4.y, t4.z), sum = v3(s4.x, s4.y, s4.z);
-      uint32_t bounces = m.z & 0x7fffffffu;
+      uint32_t bounces = m.z & kBounceMask;
       bool last_delta = (m.z >> 31) != 0;
+      uint32_t next_oct = 0;
       bool hit = h.prim != kMiss;
       SurfaceHit g;
       if(hit) { g = surface_at<J::kGeneral>(sc, h, o, d); }
@@ -628,11 +661,12 @@ __global__ void wf_shade(J jobs, WfDev w) {
             w.ray_o[slot] = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
             w.ray_d[slot] = make_float4(bs.w.x, bs.w.y, bs.w.z, 0.f);
             w.thr[slot] = make_float4(thr.x, thr.y, thr.z, 0.f);
+            next_oct = dir_octant(bs.w);
           }
         }
       }
       w.sum[slot] = make_float4(sum.x, sum.y, sum.z, 0.f);
-      m.z = bounces | (last_delta ? 0x80000000u : 0u);
+      m.z = bounces | (next_oct << kOctShift) | (last_delta ? 0x80000000u : 0u);
       m.w = (finished ? SLOT_FINISHED : SLOT_ACTIVE) | (job << 8);
       w.meta[slot] = m;
       cont = !finished;
