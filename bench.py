@@ -77,6 +77,9 @@ def log(*a):
 # ---- distributed plumbing ------------------------------------------------------
 
 def dist_setup(n_gpus: int):
+    """One process per GPU (torchrun's RANK / LOCAL_RANK / WORLD_SIZE).  The
+    process group runs over NCCL; DORT_DIST_BACKEND=gloo runs the same
+    plumbing on CPU processes (the multi-rank tests)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -85,9 +88,13 @@ def dist_setup(n_gpus: int):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        backend = os.environ.get("DORT_DIST_BACKEND", "nccl")
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=60))
         pg = dist
     return rank, world, local, pg
 
@@ -101,9 +108,22 @@ def max_over_ranks(pg, x: float) -> float:
     if pg is None:
         return x
     import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if pg.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     pg.all_reduce(t, op=pg.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Seed of a rank's shard: every rank renders or casts its own
+    independent work (weak scaling, no data-path exchange)."""
+    return base + 1000 * rank
+
+
+def job_rate(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the slowest
+    rank's time."""
+    return world * units_per_rank / seconds_max
 
 
 # ---- clocks ----------------------------------------------------------------------
@@ -169,7 +189,7 @@ def raycast_workload(rank: int, caster):
     verts, tris = scenes.random_triangles(N_TRIS, seed=1)
     coh = scenes.pinhole_rays(4096, 2048)
     dif = scenes.diffuse_rays(verts, tris, N_RAYS - len(coh), caster(verts, tris),
-                              seed=2 + 1000 * rank)
+                              seed=rank_seed(2, rank))
     return verts, tris, np.ascontiguousarray(np.concatenate([coh, dif]))
 
 
@@ -327,7 +347,7 @@ def run_dort(args):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     ms_max = max_over_ranks(pg, ms)
-    value = world * n * args.steps / (ms_max / 1e3) / 1e6
+    value = job_rate(n * args.steps, world, ms_max / 1e3) / 1e6
 
     # kernel-only duration per launch (events around each launch on its stream)
     per_launch = scene.raycast_timed(d_rays.data_ptr(), n, d_prim.data_ptr(),
@@ -479,7 +499,8 @@ def run_dort_pt(args):
         f"depth={st['depth']} build={st['build_ms']:.0f}ms ({st['bvh_build']} BVH "
         f"{st['bvh_ms']:.0f}ms)")
     spp = args.spp or PT_SPP
-    p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH, seed=42 + rank)
+    p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH,
+                         seed=rank_seed(42, rank))
     tuning = {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"}
     d_out = torch.empty(PT_H * PT_W * 3, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
@@ -508,7 +529,7 @@ def run_dort_pt(args):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     ms_max = max_over_ranks(pg, ms)
-    value = world * samples * args.steps / (ms_max / 1e3)
+    value = job_rate(samples * args.steps, world, ms_max / 1e3)
     wf_img = d_out.view(PT_H, PT_W, 3).cpu().numpy()
 
     # the plain per-pixel megakernel on the same frame
@@ -652,7 +673,7 @@ def run_dort_batch(args):
     rank, world, local, pg = dist_setup(args.gpus)
     torch.cuda.set_device(local)
     t0 = time.time()
-    specs = scenes.batch_jobs(count=64, seed=4 + 1000 * rank)
+    specs = scenes.batch_jobs(count=64, seed=rank_seed(4, rank))
     jobs = []
     t_create = time.time()
     for k, (sd, w, h, spp, depth) in enumerate(specs):
@@ -734,7 +755,7 @@ def run_dort_adjoint(args):
     torch.cuda.set_device(local)
     sd = scenes.adjoint_scene()
     sc = db.scene_from_dict(sd)
-    p = db.render_params(sd["camera"], 512, 512, 64, max_depth=6, seed=1 + rank)
+    p = db.render_params(sd["camera"], 512, 512, 64, max_depth=6, seed=rank_seed(1, rank))
     alb, em = sd["tri_albedo"], sd["tri_emission"]
     rng = np.random.default_rng(9)
     target = sc.adjoint_forward(p, np.clip(alb * rng.uniform(0.8, 1.2, alb.shape), 0, 1)
