@@ -90,7 +90,11 @@ class BinaryBuilder {
     nodes[node_idx].box = box;
     nodes[node_idx].tri_total = n;
 
-    const double c_trav = 1.0, c_isect = 1.0;
+    // Binary SAH costs (relative): a traversal step at half a triangle test.
+    // The wide collapse then packs more single-triangle leaves; measured +3 %
+    // on the ray cast and the 1080p frame against equal costs (and -5 % at
+    // 2 or 4).  The device builder uses the same constant (kSahTraversal).
+    const double c_trav = kSahTraversal, c_isect = 1.0;
     if(n <= 1) { make_leaf(node_idx, begin, n); return; }
 
     int best_axis = -1;

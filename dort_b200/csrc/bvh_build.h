@@ -72,6 +72,10 @@ struct alignas(16) LeafTri {
 };
 static_assert(sizeof(LeafTri) == 48, "LeafTri must be 48 bytes");
 
+// Cost of a traversal step relative to a triangle test in the binary SAH of
+// both builders (host and device build the same tree).
+constexpr double kSahTraversal = 0.5;
+
 struct BuildOptions {
   uint32_t width = 8;          // children per node, 2..8
   uint32_t max_leaf_tris = 3;  // triangles per leaf slot, 1..3

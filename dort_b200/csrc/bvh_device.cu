@@ -423,7 +423,7 @@ __device__ void evaluate_split(const uint32_t* __restrict__ bins, const Task& ta
   s.leaf = 0;
   double parent = fmax(box_area_d(task.lo[0], task.lo[1], task.lo[2], task.hi[0], task.hi[1],
                                   task.hi[2]), 1e-300);
-  double split_cost = 1.0 + best / parent;
+  double split_cost = kSahTraversal + best / parent;
   double leaf_cost = double(task.count);
   if(task.count <= max_leaf && (best_axis < 0 || leaf_cost <= split_cost)) {
     s.leaf = 1;
