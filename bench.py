@@ -66,7 +66,7 @@ N_RAYS = 16 * 1024 * 1024
 # workload, from the ncu capture summarised in
 # profiles/raycast_kernel_1Mtri_16Mrays.md (dram__bytes_read.sum +
 # dram__bytes_write.sum); reported as the roofline's traffic.
-RAYCAST_TRAFFIC_BYTES = 791.8e6
+RAYCAST_TRAFFIC_BYTES = 800.7e6
 WORKLOAD = "raycast: 1M random tris (SAH BVH), 16M rays (8M coherent pinhole 4096x2048 + 8M diffuse bounce), closest hit"
 
 
@@ -426,9 +426,9 @@ PT_WORKLOAD = ("pt1080p: wavefront path tracing 1920x1080, 256 spp, max depth 16
 REF_SAMPLE_W, REF_SAMPLE_H = 480, 270
 # DRAM bytes (read + write) of one wf_extend launch over a full queue
 # (4,194,304 rays, waves 6-8 of the 16-spp frame), mean of three launches of
-# the ncu capture summarised in profiles/wf_extend_pt1080p.md: 742 MB, 177 B
+# the ncu capture summarised in profiles/wf_extend_pt1080p.md: 777 MB, 185 B
 # per ray; reported as the roofline's traffic.
-EXTEND_TRAFFIC_BYTES = 742.2e6
+EXTEND_TRAFFIC_BYTES = 777.0e6
 EXTEND_TRAFFIC_RAYS = 4194304
 
 _ref_worker_scene = None
