@@ -501,7 +501,10 @@ def run_dort_pt(args):
     spp = args.spp or PT_SPP
     p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH,
                          seed=rank_seed(42, rank))
-    tuning = {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"}
+    # 2^25 path slots (about 11 GB of path state): fewer, fuller waves; at
+    # 256 spp 2^22 / 2^23 / 2^24 / 2^25 slots measured 567 / 592 / 606 / 616
+    # M samples/s
+    tuning = {"queue_capacity": 1 << 25, "sort_rays": args.sort_rays == "on"}
     d_out = torch.empty(PT_H * PT_W * 3, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
@@ -614,7 +617,7 @@ def run_dort_pt(args):
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
                        "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2),
-                       "l2": "frame state (queues 1 GB, image 25 MB) larger than L2"},
+                       "l2": "frame state (path queues ~11 GB, image 25 MB) larger than L2"},
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": PT_W * PT_H * 12},

@@ -421,7 +421,10 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
                         std::string& err) {
   uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
   uint64_t total = tiles * 32 * pp.spp;
-  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 21));
+  // default: up to 2^24 path slots (about 5.5 GB of path state); more slots
+  // make fewer, fuller waves (1080p at 256 spp: 567 M samples/s at 2^22,
+  // 606 M at 2^24)
+  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 24));
   tn.trace_block = 128;
   tn.shade_block = 128;
   tn.sort = 0;
@@ -594,6 +597,8 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
     total += uint64_t(params[j].width) * params[j].height * params[j].spp;
   }
   WfTuning tn;
+  // batches keep 2^22 slots: the batch workload measured 192 M samples/s at
+  // 2^22 and 187 M at 2^24
   tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 22));
   tn.trace_block = 128;
   tn.shade_block = 128;

@@ -362,7 +362,10 @@ int dort_gpu_render_device_noalloc(dort_scene* scene, const dort_render_params* 
  * (DORT_ERR_UNSUPPORTED); use dort_gpu_render for it. */
 typedef struct dort_wavefront_tuning {
   uint32_t struct_size;        /* sizeof(dort_wavefront_tuning) */
-  uint32_t queue_capacity;     /* paths in flight (0: auto) */
+  uint32_t queue_capacity;     /* paths in flight (0: auto, up to 2^24 for a
+                                  frame, 2^22 for a batch; each path slot
+                                  holds about 330 bytes of device memory;
+                                  more slots, fewer and fuller waves) */
   uint32_t trace_block;        /* threads per block, trace stages (0: auto) */
   uint32_t shade_block;        /* threads per block, shade stage (0: auto) */
   uint32_t sort_rays;          /* 0: auto (off), 1: on, 2: off -- sort each
