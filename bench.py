@@ -586,12 +586,19 @@ def run_dort_pt(args):
             ext_rays = stages["extend_rays"]
             bytes_per_ray = 32 + 16 + n_node * 32 + n_tri * 36
             achieved = ext_rays * bytes_per_ray / (stages["extend"] / 1e3) / 1e9
+            cap = tuning["queue_capacity"]
             rl = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                  "frac": achieved / hbm, "traffic": EXTEND_TRAFFIC_BYTES,
-                  "traffic_source": f"ncu capture of full-queue launches "
-                                    f"({EXTEND_TRAFFIC_RAYS} rays; "
-                                    f"profiles/wf_extend_pt1080p.md)",
-                  "algorithmic_bytes_per_full_launch": EXTEND_TRAFFIC_RAYS * bytes_per_ray,
+                  "frac": achieved / hbm,
+                  # per full-queue launch of this run's capacity: the captured
+                  # bytes per ray times the rays of such a launch (the
+                  # traffic grows with the rays a launch traces)
+                  "traffic": EXTEND_TRAFFIC_BYTES / EXTEND_TRAFFIC_RAYS * cap,
+                  "traffic_source": f"ncu capture of full-queue launches of "
+                                    f"{EXTEND_TRAFFIC_RAYS} rays "
+                                    f"(profiles/wf_extend_pt1080p.md), scaled to "
+                                    f"{cap} rays",
+                  "traffic_bytes_per_ray": EXTEND_TRAFFIC_BYTES / EXTEND_TRAFFIC_RAYS,
+                  "algorithmic_bytes_per_full_launch": cap * bytes_per_ray,
                   "peak_source": peak_kind,
                   "kernel": "wf_extend (closest hit)", "bytes_per_ray": bytes_per_ray,
                   "n_node": n_node, "n_tri": n_tri, "work_sample_rays": nwork,
