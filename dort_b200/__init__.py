@@ -291,12 +291,24 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
 
 
 def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
-                     shade_block: int = 0, sort_rays: bool | None = None) -> _abi.WavefrontTuning:
+                     shade_block: int = 0, sort_rays: bool | None = None,
+                     max_waves: int = 0) -> _abi.WavefrontTuning:
+    """dort_wavefront_tuning; zeros select the library's automatic choices.
+    max_waves caps the waves of a frame (a frame that reaches it stops with
+    DORT_ERR_TIMEOUT)."""
     t = _abi.WavefrontTuning()
     t.struct_size = ctypes.sizeof(_abi.WavefrontTuning)
     t.queue_capacity, t.trace_block, t.shade_block = queue_capacity, trace_block, shade_block
     t.sort_rays = 0 if sort_rays is None else (1 if sort_rays else 2)
+    t.max_waves = max_waves
     return t
+
+
+def debug_fail_alloc(after: int) -> None:
+    """Failure injection (dort_gpu_debug_fail_alloc): the library's next
+    `after` allocations succeed and the one after fails as if memory were
+    exhausted; a negative value switches injection off."""
+    _abi.check(_abi.lib().dort_gpu_debug_fail_alloc(int(after)))
 
 
 def scene_from_dict(d: dict, **kw) -> "Scene":

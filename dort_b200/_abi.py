@@ -94,7 +94,8 @@ class RenderParams(ctypes.Structure):
 
 class WavefrontTuning(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
-                ("shade_block", c_u32), ("sort_rays", c_u32), ("reserved", c_u32 * 3)]
+                ("shade_block", c_u32), ("sort_rays", c_u32), ("max_waves", c_u32),
+                ("reserved", c_u32 * 2)]
 
 
 class BatchJob(ctypes.Structure):
@@ -188,6 +189,8 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_batch_destroy.argtypes = [c_p]
         L.dort_gpu_scene_bvh_cost.restype = c_i32
         L.dort_gpu_scene_bvh_cost.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_debug_fail_alloc.restype = c_i32
+        L.dort_gpu_debug_fail_alloc.argtypes = [ctypes.c_longlong]
         L.dort_gpu_check_device_bvh.restype = c_i32
         L.dort_gpu_check_device_bvh.argtypes = [ctypes.POINTER(SceneDesc),
                                                 ctypes.POINTER(ctypes.c_double)]

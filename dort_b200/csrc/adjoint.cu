@@ -22,6 +22,7 @@
 #include <string>
 
 #include "common.h"
+#include "launch_plan.h"
 #include "pt.cuh"
 #include "scene_build.h"
 
@@ -162,7 +163,7 @@ static int set_tri_params(dort_scene* s, const float* albedo, const float* emiss
     if(!src) { *view = nullptr; return DORT_OK; }
     if(!*buf) {
       void* d = nullptr;
-      if(cudaMalloc(&d, bytes ? bytes : 4) != cudaSuccess) {
+      if(dev_alloc(&d, bytes ? bytes : 4) != cudaSuccess) {
         cudaGetLastError();
         return fail(DORT_ERR_OOM, "cudaMalloc of triangle parameters failed");
       }
@@ -185,18 +186,20 @@ using namespace dort_gpu;
 
 extern "C" int dort_gpu_adjoint_forward(dort_scene* scene, const dort_render_params* params,
                                         const float* tri_albedo, const float* tri_emission,
-                                        float* out_image) {
+                                        float* out_image) try {
   clear_error();
   if(!scene || !params || !out_image) { return fail(DORT_ERR_INVALID, "null argument"); }
-  int rc = set_tri_params(scene, tri_albedo, tri_emission);
+  int rc = require_scene_device(scene);
+  if(rc != DORT_OK) { return rc; }
+  rc = set_tri_params(scene, tri_albedo, tri_emission);
   if(rc != DORT_OK) { return rc; }
   return dort_gpu_render(scene, params, out_image, nullptr);
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_params* params,
                                          const float* tri_albedo, const float* tri_emission,
                                          const float* dl_dimage, float* d_albedo,
-                                         float* d_emission) {
+                                         float* d_emission) try {
   clear_error();
   if(!scene || !params || !dl_dimage || (!d_albedo && !d_emission)) {
     return fail(DORT_ERR_INVALID, "null argument");
@@ -207,7 +210,9 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   if(pp.renderer != RENDERER_PT) {
     return fail(DORT_ERR_UNSUPPORTED, "the adjoint renders only the pt renderer");
   }
-  int rc = set_tri_params(scene, tri_albedo, tri_emission);
+  int rc = require_scene_device(scene);
+  if(rc != DORT_OK) { return rc; }
+  rc = set_tri_params(scene, tri_albedo, tri_emission);
   if(rc != DORT_OK) { return rc; }
   if(d_emission && !scene->pt.tri_emission) {
     return fail(DORT_ERR_INVALID, "emission gradients need tri_emission");
@@ -220,9 +225,9 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
     if(d_ga) { cudaFree(d_ga); }
     if(d_ge) { cudaFree(d_ge); }
   };
-  if(cudaMalloc(&d_img, npix * 3 * sizeof(float)) != cudaSuccess ||
-     (d_albedo && cudaMalloc(&d_ga, tbytes ? tbytes : 4) != cudaSuccess) ||
-     (d_emission && cudaMalloc(&d_ge, tbytes ? tbytes : 4) != cudaSuccess)) {
+  if(dev_alloc(&d_img, npix * 3 * sizeof(float)) != cudaSuccess ||
+     (d_albedo && dev_alloc(&d_ga, tbytes ? tbytes : 4) != cudaSuccess) ||
+     (d_emission && dev_alloc(&d_ge, tbytes ? tbytes : 4) != cudaSuccess)) {
     cudaGetLastError();
     cleanup();
     return fail(DORT_ERR_OOM, "cudaMalloc for the adjoint failed");
@@ -235,12 +240,12 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  uint64_t target = uint64_t(sms) * 1024 * 4;
-  uint32_t slices = uint32_t(std::min<uint64_t>(pp.spp, std::max<uint64_t>(1, target / npix)));
-  uint32_t per = (pp.spp + slices - 1) / slices;
-  slices = (pp.spp + per - 1) / per;
-  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  uint32_t per_slice = tiles * 32;
+  MegaPlan plan;
+  if(megakernel_plan(scene->device, dev, sms, pp.width, pp.height, pp.spp, 0, &plan) != 0) {
+    cleanup();
+    return fail(DORT_ERR_INVALID, plan.why);
+  }
+  const uint32_t slices = plan.slices, per = plan.per, per_slice = plan.per_slice;
   uint64_t threads = uint64_t(slices) * per_slice;
   if(ok) {
     uint32_t grid = uint32_t((threads + kAdjBlock - 1) / kAdjBlock);
@@ -266,10 +271,10 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
                                cudaGetErrorString(cudaGetLastError()));
   }
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t count,
-                                double* out_loss, float* out_grad) {
+                                double* out_loss, float* out_grad) try {
   clear_error();
   if(!image || !target || !out_loss || !out_grad) {
     return fail(DORT_ERR_INVALID, "null argument");
@@ -278,10 +283,10 @@ extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t 
   float *d_a = nullptr, *d_b = nullptr, *d_g = nullptr;
   double* d_l = nullptr;
   size_t bytes = count * sizeof(float);
-  bool ok = cudaMalloc(&d_a, bytes ? bytes : 4) == cudaSuccess &&
-            cudaMalloc(&d_b, bytes ? bytes : 4) == cudaSuccess &&
-            cudaMalloc(&d_g, bytes ? bytes : 4) == cudaSuccess &&
-            cudaMalloc(&d_l, sizeof(double)) == cudaSuccess;
+  bool ok = dev_alloc(&d_a, bytes ? bytes : 4) == cudaSuccess &&
+            dev_alloc(&d_b, bytes ? bytes : 4) == cudaSuccess &&
+            dev_alloc(&d_g, bytes ? bytes : 4) == cudaSuccess &&
+            dev_alloc(&d_l, sizeof(double)) == cudaSuccess;
   cudaStream_t st = 0;
   ok = ok && cudaMemcpyAsync(d_a, image, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync(d_b, target, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -304,4 +309,4 @@ extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t 
     return fail(DORT_ERR_CUDA, "l2 loss failed");
   }
   return DORT_OK;
-}
+} DORT_ABI_CATCH

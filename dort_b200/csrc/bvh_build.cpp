@@ -434,6 +434,7 @@ bool build_wide_bvh(const float* verts, uint32_t vert_count,
     err = "bvh_width must be 2..8";
     return false;
   }
+  alloc_checkpoint();
   std::vector<Prim> prims(tri_count);
   for(uint32_t t = 0; t < tri_count; ++t) {
     Prim& p = prims[t];
@@ -458,8 +459,10 @@ bool build_wide_bvh(const float* verts, uint32_t vert_count,
     }
     for(int a = 0; a < 3; ++a) { p.c[a] = 0.5f * (p.box.lo[a] + p.box.hi[a]); }
   }
+  alloc_checkpoint();
   BinaryBuilder bb(prims, opts);
   if(tri_count > 0) { bb.build(); }
+  alloc_checkpoint();
   Collapser col{bb.nodes, bb.order_, verts, tris, opts, out, err};
   if(!col.run()) { return false; }
 #ifndef DORT_NODE_QUANTIZED

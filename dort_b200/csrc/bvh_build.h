@@ -34,6 +34,11 @@
 
 namespace dort_gpu {
 
+// Throws std::bad_alloc when a test's injected allocation failure is due
+// (dort_gpu_debug_fail_alloc); called before the builders' large allocations.
+void alloc_checkpoint();
+
+
 struct alignas(16) WideNode {
   float p[3];
   uint8_t e[3];

@@ -794,7 +794,7 @@ struct Scratch {
   template<class T>
   T* alloc(size_t count, std::string& err) {
     void* p = nullptr;
-    if(cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
+    if(dev_alloc(&p, std::max<size_t>(count, 1) * sizeof(T)) != cudaSuccess) {
       cudaGetLastError();
       err = "cudaMalloc of " + std::to_string(count * sizeof(T)) + " bytes failed (BVH build)";
       return nullptr;
@@ -1092,7 +1092,7 @@ bool build_wide_bvh_device(const float* h_verts, uint32_t vert_count, const uint
   void* temp = sc.alloc<unsigned char>(temp_bytes, err);
   PinnedWords pin;
   if(!temp ||
-     !cuda_ok(cudaMallocHost(&pin.p, 2 * sizeof(uint64_t)), "pinned counter", err)) {
+     !cuda_ok(host_pinned_alloc(&pin.p, 2 * sizeof(uint64_t)), "pinned counter", err)) {
     return false;
   }
   BinTree bt;
@@ -1157,13 +1157,13 @@ bool build_wide_bvh_device(const float* h_verts, uint32_t vert_count, const uint
 #endif
   size_t wide_cap = std::max<size_t>(16, n / 4 + 16);
   void* wide = nullptr;
-  if(cudaMalloc(&wide, wide_cap * node_size) != cudaSuccess) {
+  if(dev_alloc(&wide, wide_cap * node_size) != cudaSuccess) {
     cudaGetLastError();
     err = "cudaMalloc of the BVH nodes failed";
     return false;
   }
   LeafTri* leaf = nullptr;
-  if(cudaMalloc(&leaf, size_t(n) * sizeof(LeafTri)) != cudaSuccess) {
+  if(dev_alloc(&leaf, size_t(n) * sizeof(LeafTri)) != cudaSuccess) {
     cudaGetLastError();
     cudaFree(wide);
     err = "cudaMalloc of the BVH triangles failed";
@@ -1197,7 +1197,7 @@ bool build_wide_bvh_device(const float* h_verts, uint32_t vert_count, const uint
     if(wide_count + children > wide_cap) {
       size_t cap2 = std::max<size_t>(wide_cap * 2, wide_count + children);
       void* w2 = nullptr;
-      if(cudaMalloc(&w2, cap2 * node_size) != cudaSuccess) {
+      if(dev_alloc(&w2, cap2 * node_size) != cudaSuccess) {
         cudaGetLastError();
         err = "cudaMalloc of the BVH nodes failed";
         return false;
@@ -1252,7 +1252,7 @@ bool build_wide_bvh_device(const float* h_verts, uint32_t vert_count, const uint
 
 using namespace dort_gpu;
 
-extern "C" int dort_gpu_scene_bvh_cost(const dort_scene* s, double out[4]) {
+extern "C" int dort_gpu_scene_bvh_cost(const dort_scene* s, double out[4]) try {
   clear_error();
   if(!s || !out) { return fail(DORT_ERR_INVALID, "null argument"); }
   size_t count = s->trace.node_count;
@@ -1281,9 +1281,9 @@ extern "C" int dort_gpu_scene_bvh_cost(const dort_scene* s, double out[4]) {
   out[2] = double(leaf_slots);
   out[3] = s->depth;
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out[8]) {
+extern "C" int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out[8]) try {
   clear_error();
   if(!desc || !out) { return fail(DORT_ERR_INVALID, "null argument"); }
   if(desc->struct_size != sizeof(dort_scene_desc)) {
@@ -1357,4 +1357,4 @@ extern "C" int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out
   out[6] = db.depth;
   out[7] = wide_sah_cost(f.data(), f.size());
   return DORT_OK;
-}
+} DORT_ABI_CATCH

@@ -10,6 +10,8 @@
 #include "../../include/dort_gpu.h"
 #include "pt_scene.h"
 
+struct dort_scene;
+
 namespace dort_gpu {
 
 struct Wavefront;
@@ -18,6 +20,38 @@ struct Wavefront;
 void set_error(const std::string& msg);
 void clear_error();
 int fail(int code, const std::string& msg);
+
+// Every entry point of the C ABI ends in a function-try-block whose handler
+// is DORT_ABI_CATCH: an exception (a host allocation that failed, ...)
+// becomes a status code (DORT_ERR_OOM for std::bad_alloc) and never crosses
+// the C ABI.
+int abi_exception();
+#define DORT_ABI_CATCH \
+  catch(...) { return ::dort_gpu::abi_exception(); }
+
+// DORT_OK when the scene lives on the current device, else DORT_ERR_INVALID:
+// a kernel given another GPU's BVH and triangle pointers would read a peer's
+// memory (or fault), so entry points check before launching.
+int require_scene_device(const dort_scene* s);
+
+// Allocation hooks.  Every device and pinned host allocation of the library
+// goes through dev_alloc / host_pinned_alloc, and the host-side builders call
+// alloc_checkpoint() before their large allocations; a test can make the
+// n-th of these fail (dort_gpu_debug_fail_alloc) to drive the error paths
+// without exhausting memory.  alloc_checkpoint throws std::bad_alloc when
+// the injected failure is due.
+bool alloc_injected_failure();
+cudaError_t dev_alloc_bytes(void** p, size_t bytes);
+cudaError_t host_pinned_alloc_bytes(void** p, size_t bytes);
+void alloc_checkpoint();
+template<class T>
+cudaError_t dev_alloc(T** p, size_t bytes) {
+  return dev_alloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
+template<class T>
+cudaError_t host_pinned_alloc(T** p, size_t bytes) {
+  return host_pinned_alloc_bytes(reinterpret_cast<void**>(p), bytes);
+}
 
 #define DG_CUDA(call)                                                        \
   do {                                                                       \

@@ -15,7 +15,7 @@ using namespace dort_gpu;
 extern "C" int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const float* rays,
                                            size_t ray_count, int any_hit,
                                            uint32_t* out_prim, float* out_tb,
-                                           uint32_t* out_depth) {
+                                           uint32_t* out_depth) try {
   clear_error();
   if(!desc || (ray_count && (!rays || !out_prim || (!any_hit && !out_tb)))) {
     return fail(DORT_ERR_INVALID, "null argument");
@@ -53,4 +53,4 @@ extern "C" int dort_gpu_host_check_raycast(const dort_scene_desc* desc, const fl
     }
   }
   return DORT_OK;
-}
+} DORT_ABI_CATCH

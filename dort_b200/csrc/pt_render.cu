@@ -14,6 +14,7 @@
 
 #include "bdpt.cuh"
 #include "common.h"
+#include "launch_plan.h"
 #include "lt.cuh"
 #include "pt.cuh"
 #include "scene_build.h"
@@ -215,7 +216,7 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
 int render_scratch(dort_scene* s, size_t bytes, void** out) {
   if(s->stage_bytes < bytes) {
     if(s->d_stage) { cudaFree(s->d_stage); s->d_stage = nullptr; s->stage_bytes = 0; }
-    if(cudaMalloc(&s->d_stage, bytes) != cudaSuccess) {
+    if(dev_alloc(&s->d_stage, bytes) != cudaSuccess) {
       cudaGetLastError();
       return fail(DORT_ERR_OOM, "cudaMalloc of render scratch failed");
     }
@@ -228,7 +229,7 @@ int render_scratch(dort_scene* s, size_t bytes, void** out) {
 int render_image_buffer(dort_scene* s, size_t bytes, float** out) {
   if(s->image_bytes < bytes) {
     if(s->d_image) { cudaFree(s->d_image); s->d_image = nullptr; s->image_bytes = 0; }
-    if(cudaMalloc(&s->d_image, bytes) != cudaSuccess) {
+    if(dev_alloc(&s->d_image, bytes) != cudaSuccess) {
       cudaGetLastError();
       return fail(DORT_ERR_OOM, "cudaMalloc of the image failed");
     }
@@ -240,20 +241,21 @@ int render_image_buffer(dort_scene* s, size_t bytes, float** out) {
 
 int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st,
                   unsigned long long* d_counters) {
+  int drc = require_scene_device(s);
+  if(drc != DORT_OK) { return drc; }
   if(pp.renderer == RENDERER_LT) { return launch_light_trace(s, pp, d_out, st, d_counters); }
   if(pp.renderer == RENDERER_BDPT) { return launch_bdpt(s, pp, d_out, st, d_counters); }
   int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  DG_CUDA(cudaGetDevice(&dev));
+  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   uint32_t npix = pp.width * pp.height;
-  // enough (pixel, slice) threads for ~4 waves of 1024 threads per SM
-  uint64_t target = uint64_t(sms) * 1024 * 4;
-  uint32_t slices = uint32_t(std::min<uint64_t>(pp.spp, std::max<uint64_t>(1, target / npix)));
-  uint32_t per = (pp.spp + slices - 1) / slices;
-  slices = (pp.spp + per - 1) / per;
-  // tiles of 8x4 pixels: the thread grid covers the padded tile area
-  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  uint32_t per_slice = tiles * 32;
+  // enough (pixel, slice) threads for ~4 waves of 1024 threads per SM; the
+  // thread grid covers whole 8x4 pixel tiles
+  MegaPlan plan;
+  if(megakernel_plan(s->device, dev, sms, pp.width, pp.height, pp.spp, 0, &plan) != 0) {
+    return fail(DORT_ERR_INVALID, plan.why);
+  }
+  const uint32_t slices = plan.slices, per = plan.per, per_slice = plan.per_slice;
   size_t partial_bytes = size_t(slices) * npix * sizeof(float4);
   void* scratch = nullptr;
   int rc = render_scratch(s, partial_bytes, &scratch);
@@ -279,7 +281,7 @@ int launch_render(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t 
 using namespace dort_gpu;
 
 extern "C" int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
-                                      float* d_out_rgb, void* stream) {
+                                      float* d_out_rgb, void* stream) try {
   clear_error();
   if(!scene || !params || !d_out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -289,10 +291,10 @@ extern "C" int dort_gpu_render_device(dort_scene* scene, const dort_render_param
   DG_CUDA(cudaMemsetAsync(scene->d_work, 0, 2 * sizeof(unsigned long long), st));
   return launch_render(scene, pp, d_out_rgb, st,
                        reinterpret_cast<unsigned long long*>(scene->d_work));
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_render(dort_scene* scene, const dort_render_params* params,
-                               float* out_rgb, double* out_stats) {
+                               float* out_rgb, double* out_stats) try {
   clear_error();
   if(!scene || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -336,12 +338,12 @@ extern "C" int dort_gpu_render(dort_scene* scene, const dort_render_params* para
     out_stats[3] = double(uint64_t(npix) * pp.spp - counters[1]);
   }
   return rc;
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
                                           const dort_render_params* params,
                                           uint32_t row_begin, uint32_t row_end,
-                                          float* out_rgb) {
+                                          float* out_rgb) try {
   clear_error();
   if(!desc || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   HostScene hs;
@@ -411,7 +413,7 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
     }
   }
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
 // ---- wavefront entry points -------------------------------------------------
 
@@ -428,11 +430,13 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
   tn.trace_block = 128;
   tn.shade_block = 128;
   tn.sort = 0;
+  tn.max_waves = 0;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
       return false;
     }
+    tn.max_waves = t->max_waves;
     if(t->queue_capacity) { tn.capacity = t->queue_capacity; }
     if(t->trace_block) { tn.trace_block = t->trace_block; }
     if(t->shade_block) { tn.shade_block = t->shade_block; }
@@ -459,7 +463,7 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
 extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
                                                 const dort_render_params* params,
                                                 const dort_wavefront_tuning* tuning,
-                                                float* d_out_rgb, void* stream) {
+                                                float* d_out_rgb, void* stream) try {
   clear_error();
   if(!scene || !params || !d_out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -474,12 +478,14 @@ extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
   }
   WfTuning tn;
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
+  int drc = require_scene_device(scene);
+  if(drc != DORT_OK) { return drc; }
   return wavefront_render(scene, pp, tn, d_out_rgb, static_cast<cudaStream_t>(stream));
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_params* params,
                                          const dort_wavefront_tuning* tuning, float* out_rgb,
-                                         double* out_stats) {
+                                         double* out_stats) try {
   clear_error();
   if(!scene || !params || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -524,11 +530,11 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
     out_stats[3] = double(waves);
   }
   return rc;
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* params,
                                               const dort_wavefront_tuning* tuning,
-                                              double out_ms[6], double out_rays[4]) {
+                                              double out_ms[6], double out_rays[4]) try {
   clear_error();
   if(!scene || !params || !out_ms) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -540,6 +546,8 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
   if(pp.sample_all_lights) { return fail(DORT_ERR_UNSUPPORTED, "sample_all_lights"); }
   WfTuning tn;
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
+  int drc = require_scene_device(scene);
+  if(drc != DORT_OK) { return drc; }
   size_t npix = size_t(pp.width) * pp.height;
   float* d_out = nullptr;
   int brc = render_image_buffer(scene, npix * 3 * sizeof(float), &d_out);
@@ -557,7 +565,7 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
     }
   }
   return rc;
-}
+} DORT_ABI_CATCH
 
 // ---- batches ------------------------------------------------------------------
 
@@ -568,7 +576,7 @@ struct dort_batch {
 
 extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_count,
                                      const dort_wavefront_tuning* tuning,
-                                     dort_batch** out_batch) {
+                                     dort_batch** out_batch) try {
   clear_error();
   if(!jobs || !out_batch || job_count == 0) { return fail(DORT_ERR_INVALID, "null argument"); }
   if(job_count > 65536) { return fail(DORT_ERR_INVALID, "job_count exceeds 65536"); }
@@ -603,10 +611,12 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
   tn.trace_block = 128;
   tn.shade_block = 128;
   tn.sort = 0;
+  tn.max_waves = 0;
   if(tuning) {
     if(tuning->struct_size != sizeof(dort_wavefront_tuning)) {
       return fail(DORT_ERR_INVALID, "dort_wavefront_tuning.struct_size mismatch (ABI version)");
     }
+    tn.max_waves = tuning->max_waves;
     if(tuning->queue_capacity) { tn.capacity = tuning->queue_capacity; }
     if(tuning->trace_block) { tn.trace_block = tuning->trace_block; }
     if(tuning->shade_block) { tn.shade_block = tuning->shade_block; }
@@ -633,23 +643,23 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
   batch->total_samples = total;
   *out_batch = batch;
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_batch_render(dort_batch* batch, void* stream) {
+extern "C" int dort_gpu_batch_render(dort_batch* batch, void* stream) try {
   clear_error();
   if(!batch) { return fail(DORT_ERR_INVALID, "null argument"); }
   return wavefront_batch_render(batch->impl, static_cast<cudaStream_t>(stream));
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_batch_image_device(dort_batch* batch, uint32_t job,
-                                           const float** out_d_rgb) {
+                                           const float** out_d_rgb) try {
   clear_error();
   if(!batch || !out_d_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   uint32_t npix = 0;
   return wavefront_batch_image(batch->impl, job, out_d_rgb, &npix);
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_batch_image(dort_batch* batch, uint32_t job, float* out_rgb) {
+extern "C" int dort_gpu_batch_image(dort_batch* batch, uint32_t job, float* out_rgb) try {
   clear_error();
   if(!batch || !out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   const float* d = nullptr;
@@ -658,9 +668,9 @@ extern "C" int dort_gpu_batch_image(dort_batch* batch, uint32_t job, float* out_
   if(rc != DORT_OK) { return rc; }
   DG_CUDA(cudaMemcpy(out_rgb, d, size_t(npix) * 3 * sizeof(float), cudaMemcpyDeviceToHost));
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_batch_stats(dort_batch* batch, double out[4]) {
+extern "C" int dort_gpu_batch_stats(dort_batch* batch, double out[4]) try {
   clear_error();
   if(!batch || !out) { return fail(DORT_ERR_INVALID, "null argument"); }
   DG_CUDA(cudaDeviceSynchronize());
@@ -673,12 +683,12 @@ extern "C" int dort_gpu_batch_stats(dort_batch* batch, double out[4]) {
   out[2] = double(error);
   out[3] = double(batch->total_samples);
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_batch_destroy(dort_batch* batch) {
+extern "C" int dort_gpu_batch_destroy(dort_batch* batch) try {
   clear_error();
   if(!batch) { return DORT_OK; }
   wavefront_batch_destroy(batch->impl);
   delete batch;
   return DORT_OK;
-}
+} DORT_ABI_CATCH

@@ -62,6 +62,8 @@ int launch_raycast(dort_scene* s, const float* d_rays, size_t n, int any_hit,
     return fail(DORT_ERR_INVALID, "rays must be 16-byte aligned");
   }
   if(!any_hit && !d_tb) { return fail(DORT_ERR_INVALID, "out_tb is required for closest hit"); }
+  int drc = require_scene_device(s);
+  if(drc != DORT_OK) { return drc; }
   DG_CUDA(cudaMemsetAsync(s->d_work, 0, sizeof(uint32_t), stream));
   const void* kfn = any_hit ? reinterpret_cast<const void*>(&raycast_kernel<true>)
                             : reinterpret_cast<const void*>(&raycast_kernel<false>);
@@ -86,17 +88,17 @@ using namespace dort_gpu;
 
 extern "C" int dort_gpu_raycast_device(dort_scene* scene, const float* d_rays,
                                        size_t ray_count, int any_hit, uint32_t* d_prim,
-                                       float* d_tb, void* stream) {
+                                       float* d_tb, void* stream) try {
   clear_error();
   if(!scene || (ray_count && (!d_rays || !d_prim))) {
     return fail(DORT_ERR_INVALID, "null argument");
   }
   return launch_raycast(scene, d_rays, ray_count, any_hit, d_prim, d_tb,
                         static_cast<cudaStream_t>(stream));
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_raycast(dort_scene* scene, const float* rays, size_t ray_count,
-                                int any_hit, uint32_t* out_prim, float* out_tb) {
+                                int any_hit, uint32_t* out_prim, float* out_tb) try {
   clear_error();
   if(!scene || (ray_count && (!rays || !out_prim || (!any_hit && !out_tb)))) {
     return fail(DORT_ERR_INVALID, "null argument");
@@ -109,7 +111,7 @@ extern "C" int dort_gpu_raycast(dort_scene* scene, const float* rays, size_t ray
   size_t need = align(ray_bytes) + align(prim_bytes) + align(tb_bytes);
   if(scene->stage_bytes < need) {
     if(scene->d_stage) { cudaFree(scene->d_stage); scene->d_stage = nullptr; }
-    if(cudaMalloc(&scene->d_stage, need) != cudaSuccess) {
+    if(dev_alloc(&scene->d_stage, need) != cudaSuccess) {
       cudaGetLastError();
       scene->stage_bytes = 0;
       return fail(DORT_ERR_OOM, "cudaMalloc of ray staging buffer failed");
@@ -134,12 +136,12 @@ extern "C" int dort_gpu_raycast(dort_scene* scene, const float* rays, size_t ray
   }
   DG_CUDA(cudaStreamSynchronize(st));
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
 extern "C" int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
                                       size_t ray_count, int any_hit, uint32_t* d_prim,
                                       float* d_tb, void* stream, int repeat,
-                                      float* out_ms_per_launch) {
+                                      float* out_ms_per_launch) try {
   clear_error();
   if(!scene || !out_ms_per_launch || repeat < 1) {
     return fail(DORT_ERR_INVALID, "bad argument");
@@ -165,4 +167,4 @@ extern "C" int dort_gpu_raycast_timed(dort_scene* scene, const float* d_rays,
   cudaEventDestroy(e1);
   *out_ms_per_launch = ms / float(repeat);
   return DORT_OK;
-}
+} DORT_ABI_CATCH

@@ -2,14 +2,14 @@
 // must not allocate GPU memory during a render.
 //
 // Some callers of a renderer cannot let it call cudaMalloc / cudaFree while
-// they run: an application that records its frame into a CUDA graph (memory
-// cannot be allocated inside the captured region), a host application that
-// owns every device allocation under a fixed budget (e.g. a plugin inside
-// another program's render loop), or a real-time loop that cannot afford the
-// device-wide synchronisation cudaFree implies.  dort_gpu_render_device grows
-// a per-scene scratch buffer on demand; this variant keeps its scratch in a
-// fixed array that the library holds on every GPU it is loaded on, so a call
-// only launches kernels and clears that array.
+// they run: a host application that owns every device allocation under a
+// fixed budget (a plugin inside another program's render loop, whose memory
+// manager accounts for all device memory), or a real-time loop that cannot
+// afford the device-wide synchronisation cudaFree implies.
+// dort_gpu_render_device grows a per-scene scratch buffer on demand; this
+// variant keeps its scratch in a fixed array that the library holds on every
+// GPU it is loaded on, so a call only launches kernels and clears part of
+// that array.
 //
 // The scratch holds the per-(slice, pixel) partial sums of the megakernel and
 // two counters, kNoAllocScratchBytes in total, which caps the image at
@@ -22,13 +22,16 @@
 // callers serialise them.
 //
 // The first call on a device looks up the array's device address with
-// cudaGetSymbolAddress (once per device, with that device current); make that
-// first call before any stream capture begins.
+// cudaGetSymbolAddress (once per device, with that device current) and keeps
+// it; make that first call before any stream capture begins.  A process that
+// calls cudaDeviceReset must not call this entry point on that device
+// afterwards: the kept address belonged to the destroyed context.
 #include <algorithm>
 #include <mutex>
 #include <string>
 
 #include "common.h"
+#include "launch_plan.h"
 #include "pt_scene.h"
 
 namespace dort_gpu {
@@ -79,7 +82,7 @@ using namespace dort_gpu;
 
 extern "C" int dort_gpu_render_device_noalloc(dort_scene* scene,
                                               const dort_render_params* params,
-                                              float* d_out_rgb, void* stream) {
+                                              float* d_out_rgb, void* stream) try {
   clear_error();
   if(!scene || !params || !d_out_rgb) { return fail(DORT_ERR_INVALID, "null argument"); }
   PtParams pp;
@@ -94,27 +97,29 @@ extern "C" int dort_gpu_render_device_noalloc(dort_scene* scene,
                                   std::to_string(kNoAllocMaxPixels) +
                                   "-pixel limit of dort_gpu_render_device_noalloc");
   }
+  // the launch shape of dort_gpu_render_device, with the slices capped so
+  // that slices * pixels partial sums fit in the scratch; a scene on another
+  // device is refused before anything is launched
+  int dev = 0, sms = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  MegaPlan plan;
+  if(megakernel_plan(scene->device, dev, sms, pp.width, pp.height, pp.spp, kNoAllocMaxPixels,
+                     &plan) != 0) {
+    return fail(DORT_ERR_INVALID, std::string("dort_gpu_render_device_noalloc: ") + plan.why);
+  }
+  const uint32_t slices = plan.slices, per = plan.per, per_slice = plan.per_slice;
+  if(size_t(slices) * npix > kNoAllocMaxPixels) {
+    return fail(DORT_ERR_INVALID, "partial sums exceed the no-alloc scratch");
+  }
   void* scratch = nullptr;
   int rc = noalloc_scratch(&scratch);
   if(rc != DORT_OK) { return rc; }
   cudaStream_t st = static_cast<cudaStream_t>(stream);
 
-  // the slice count of dort_gpu_render_device, capped by the scratch size
-  int dev = 0, sms = 0;
-  DG_CUDA(cudaGetDevice(&dev));
-  DG_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  uint64_t target = uint64_t(sms) * 1024 * 4;
-  uint32_t slices = uint32_t(std::min<uint64_t>(pp.spp, std::max<uint64_t>(1, target / npix)));
-  uint32_t max_slices = uint32_t(std::max<size_t>(1, kNoAllocMaxPixels / npix));
-  slices = std::min(slices, max_slices);
-  uint32_t per = (pp.spp + slices - 1) / slices;
-  slices = (pp.spp + per - 1) / per;
-
   unsigned long long* counters = static_cast<unsigned long long*>(scratch);
   float4* partial = reinterpret_cast<float4*>(static_cast<char*>(scratch) + kNoAllocHeader);
   DG_CUDA(cudaMemsetAsync(counters, 0, 2 * sizeof(unsigned long long), st));
-  uint32_t tiles = ((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  uint32_t per_slice = tiles * 32;
   uint64_t threads = uint64_t(slices) * per_slice;
   const int block = 128;   // the megakernel's launch bound
   if(scene_needs_general(scene->pt, pp)) {
@@ -129,4 +134,4 @@ extern "C" int dort_gpu_render_device_noalloc(dort_scene* scene,
                                                             d_out_rgb, counters + 1);
   DG_CUDA(cudaGetLastError());
   return DORT_OK;
-}
+} DORT_ABI_CATCH

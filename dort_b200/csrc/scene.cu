@@ -1,5 +1,8 @@
 // Scene creation / destruction and the error plumbing of the C ABI.
+#include <atomic>
 #include <chrono>
+#include <new>
+#include <stdexcept>
 #include <cstring>
 #include <string>
 
@@ -20,13 +23,73 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+int abi_exception() {
+  try {
+    throw;
+  } catch(const std::bad_alloc&) {
+    return fail(DORT_ERR_OOM, "host allocation failed");
+  } catch(const std::exception& e) {
+    return fail(DORT_ERR_INVALID, std::string("exception: ") + e.what());
+  } catch(...) {
+    return fail(DORT_ERR_INVALID, "unknown exception");
+  }
+}
+
+int require_scene_device(const dort_scene* s) {
+  int dev = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  if(s->device != dev) {
+    return fail(DORT_ERR_INVALID, "scene on device " + std::to_string(s->device) +
+                                  ", current device is " + std::to_string(dev));
+  }
+  return DORT_OK;
+}
+
+// Failure injection: the number of allocations (device, pinned host, host
+// checkpoints) still allowed to succeed before one fails; negative = off.
+static std::atomic<long long> g_alloc_budget{-1};
+
+bool alloc_injected_failure() {
+  long long b = g_alloc_budget.load();
+  while(b >= 0) {
+    if(g_alloc_budget.compare_exchange_weak(b, b - 1)) { return b == 0; }
+  }
+  return false;
+}
+
+cudaError_t dev_alloc_bytes(void** p, size_t bytes) {
+  if(alloc_injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
+cudaError_t host_pinned_alloc_bytes(void** p, size_t bytes) {
+  if(alloc_injected_failure()) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMallocHost(p, bytes);
+}
+
+void alloc_checkpoint() {
+  if(alloc_injected_failure()) { throw std::bad_alloc(); }
+}
+
 }  // namespace dort_gpu
 
 using namespace dort_gpu;
 
 extern "C" const char* dort_gpu_last_error(void) { return g_last_error.c_str(); }
 
-extern "C" int dort_gpu_abi_version(void) { return DORT_GPU_ABI_VERSION; }
+extern "C" int dort_gpu_abi_version(void) try { return DORT_GPU_ABI_VERSION; } DORT_ABI_CATCH
+
+extern "C" int dort_gpu_debug_fail_alloc(long long after) try {
+  clear_error();
+  g_alloc_budget.store(after < 0 ? -1 : after);
+  return DORT_OK;
+} DORT_ABI_CATCH
 
 static void scene_free_device(dort_scene* s) {
   if(s->wavefront) { wavefront_destroy(s->wavefront); s->wavefront = nullptr; }
@@ -48,7 +111,7 @@ static int upload(dort_scene* s, const std::vector<T>& v, const T** out) {
   if(v.empty()) { return DORT_OK; }
   void* d = nullptr;
   size_t bytes = v.size() * sizeof(T);
-  if(cudaMalloc(&d, bytes) != cudaSuccess) {
+  if(dev_alloc(&d, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
   }
@@ -70,7 +133,9 @@ static int device_bvh(dort_scene* s, const dort_scene_desc* desc) {
   if(!build_wide_bvh_device(desc->verts, desc->vert_count, desc->tris, desc->tri_count, opts,
                             method, nullptr, db, err)) {
     int code = DORT_ERR_CUDA;
-    if(err.rfind("cudaMalloc", 0) == 0) { code = DORT_ERR_OOM; }
+    if(err.rfind("cudaMalloc", 0) == 0 || err.find("out of memory") != std::string::npos) {
+      code = DORT_ERR_OOM;
+    }
     if(err.find("quantization") != std::string::npos || err.find("too ") != std::string::npos) {
       code = DORT_ERR_INVALID;
     }
@@ -141,7 +206,7 @@ static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostSc
   pt.radius = hs.radius;
 
   void* w = nullptr;
-  if(cudaMalloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {
+  if(dev_alloc(&w, 64 * sizeof(uint32_t)) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of work counters failed");
   }
@@ -151,7 +216,7 @@ static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostSc
   return DORT_OK;
 }
 
-extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** out_scene) {
+extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** out_scene) try {
   clear_error();
   if(!desc || !out_scene) { return fail(DORT_ERR_INVALID, "null argument"); }
   *out_scene = nullptr;
@@ -165,7 +230,14 @@ extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** o
   cudaGetDevice(&s->device);
   s->tri_count = desc->tri_count;
   s->emissive_count = hs.emissive_count;
-  int rc = scene_upload(s, desc, hs);
+  int rc;
+  try {
+    rc = scene_upload(s, desc, hs);
+  } catch(...) {
+    scene_free_device(s);
+    delete s;
+    throw;
+  }
   s->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
                     .count();
   if(rc != DORT_OK) {
@@ -176,17 +248,17 @@ extern "C" int dort_gpu_scene_create(const dort_scene_desc* desc, dort_scene** o
   }
   *out_scene = s;
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_scene_destroy(dort_scene* scene) {
+extern "C" int dort_gpu_scene_destroy(dort_scene* scene) try {
   clear_error();
   if(!scene) { return DORT_OK; }
   scene_free_device(scene);
   delete scene;
   return DORT_OK;
-}
+} DORT_ABI_CATCH
 
-extern "C" int dort_gpu_scene_stats(const dort_scene* s, double out[8]) {
+extern "C" int dort_gpu_scene_stats(const dort_scene* s, double out[8]) try {
   clear_error();
   if(!s || !out) { return fail(DORT_ERR_INVALID, "null argument"); }
   out[0] = s->trace.node_count;
@@ -198,4 +270,4 @@ extern "C" int dort_gpu_scene_stats(const dort_scene* s, double out[8]) {
   out[6] = s->bvh_builder;
   out[7] = s->bvh_ms;
   return DORT_OK;
-}
+} DORT_ABI_CATCH

@@ -187,6 +187,7 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
     return false;
   }
 
+  alloc_checkpoint();
   // materials (material 0 is a white Lambert when none are given)
   hs.mats.clear();
   if(desc->materials && desc->material_count > 0) {

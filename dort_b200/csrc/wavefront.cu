@@ -863,7 +863,7 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
                  3 * f4x2 /*shadow, two per path*/ + u1 + 3 * f4 /*neeb*/ +
                  al(size_t(npix) * sizeof(float4)) + 5 * u1 /*sort*/ + sort_temp +
                  al(C_COUNT * kCtrStride * 4);
-  if(cudaMalloc(&wf->mem, bytes) != cudaSuccess) {
+  if(dev_alloc(&wf->mem, bytes) != cudaSuccess) {
     cudaGetLastError();
     return fail(DORT_ERR_OOM, "cudaMalloc of wavefront queues failed (" +
                 std::to_string(bytes) + " bytes)");
@@ -990,12 +990,16 @@ static int wf_build_graph(Wavefront* wf, const J& jobs, const WfTuning& tn) {
   return DORT_OK;
 }
 
-static uint32_t wave_bound(uint64_t total_units, uint32_t capacity, uint32_t max_depth) {
+static uint32_t wave_bound(uint64_t total_units, uint32_t capacity, uint32_t max_depth,
+                           uint32_t cap = 0) {
   // each slot runs at most ceil(units / capacity) + 1 units of kChunk samples
-  // of at most max_depth + 2 waves each
-  return uint32_t(std::min<uint64_t>(
+  // of at most max_depth + 2 waves each; a caller's cap (tuning.max_waves)
+  // may lower the bound
+  uint64_t b = std::min<uint64_t>(
       0x7fffffffull, (total_units / std::max(1u, capacity) + 2) * kChunk *
-                     (uint64_t(max_depth) + 3) + 64));
+                     (uint64_t(max_depth) + 3) + 64);
+  if(cap) { b = std::min<uint64_t>(b, cap); }
+  return uint32_t(b);
 }
 
 // Work units of a frame (kChunk samples of one pixel each, padded to whole
@@ -1013,7 +1017,7 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   int rc = wf_alloc(wf, tn.capacity, npix);
   if(rc != DORT_OK) { return rc; }
   wf->dev.total_samples = padded_samples(pp);
-  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth);
+  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
   if(!wf->valid || wf->jobs_cached != nullptr ||
      std::memcmp(&wf->pp_cached, &pp, sizeof(PtParams)) != 0 ||
      std::memcmp(&wf->tune_cached, &tn, sizeof(WfTuning)) != 0) {
@@ -1047,14 +1051,14 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   int rc = wf_alloc(wf, tn.capacity, npix);
   if(rc != DORT_OK) { return rc; }
   wf->dev.total_samples = padded_samples(pp);
-  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth);
+  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
   SingleJob<G> jobs{s->pt, pp};
   WfGrids g = wf_grids<SingleJob<G>>(tn);
   int bt = int(tn.trace_block), bs = int(tn.shade_block);
   wf->dev.sorted = tn.sort;
   // more[0]: loop flag; more[1..6]: the counters C_ACT0 .. C_NEEB of the wave
   uint32_t* more = nullptr;
-  DG_CUDA(cudaMallocHost(&more, 8 * sizeof(uint32_t)));
+  DG_CUDA(host_pinned_alloc(&more, 8 * sizeof(uint32_t)));
   cudaEvent_t ev[6];
   for(auto& e : ev) { cudaEventCreate(&e); }
   for(int k = 0; k < 6; ++k) { ms[k] = 0.0; }
@@ -1198,8 +1202,8 @@ int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32
   b->total_samples = sample;
   b->tn = tn;
   int rc = wf_alloc(&b->wf, tn.capacity, pix);
-  if(rc == DORT_OK && (cudaMalloc(&b->d_jobs, n * sizeof(WfJob)) != cudaSuccess ||
-                       cudaMalloc(&b->d_images, size_t(pix) * 3 * sizeof(float)) != cudaSuccess)) {
+  if(rc == DORT_OK && (dev_alloc(&b->d_jobs, n * sizeof(WfJob)) != cudaSuccess ||
+                       dev_alloc(&b->d_images, size_t(pix) * 3 * sizeof(float)) != cudaSuccess)) {
     cudaGetLastError();
     rc = fail(DORT_ERR_OOM, "cudaMalloc for the batch failed");
   }
@@ -1209,7 +1213,7 @@ int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32
   }
   if(rc == DORT_OK) {
     b->wf.dev.total_samples = b->total_samples;
-    b->wf.dev.max_waves = wave_bound(b->total_samples, tn.capacity, b->max_depth);
+    b->wf.dev.max_waves = wave_bound(b->total_samples, tn.capacity, b->max_depth, tn.max_waves);
     bool general = false;
     for(uint32_t j = 0; j < n; ++j) { general = general || scene_needs_general(scenes[j], params[j]); }
     rc = general ? wf_build_graph(&b->wf, JobTable<true>{b->d_jobs, n}, tn)

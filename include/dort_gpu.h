@@ -341,15 +341,17 @@ int dort_gpu_render_device(dort_scene* scene, const dort_render_params* params,
                            float* d_out_rgb, void* stream);
 
 /* No reference counterpart.  dort_gpu_render_device for callers that must not
- * allocate GPU memory during a render (a frame recorded into a CUDA graph, a
- * host application that owns every device allocation under a fixed budget, a
- * real-time loop that cannot absorb cudaFree's device synchronisation).  Same
- * kernels and result; the scratch is a fixed 16 MiB array that the library
- * holds on every GPU it is loaded on, so this call allocates nothing.  Images
- * above 1,048,560 pixels are rejected (DORT_ERR_INVALID).  All calls on a
- * device share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  The first call on a device looks up the array's
- * address (cudaGetSymbolAddress); make it before any stream capture. */
+ * allocate GPU memory during a render (a host application that owns every
+ * device allocation under a fixed budget, a real-time loop that cannot absorb
+ * cudaFree's device synchronisation).  Same kernels and result; the scratch
+ * is a fixed 16 MiB array that the library holds on every GPU it is loaded
+ * on, so this call allocates nothing.  Images above 1,048,560 pixels are
+ * rejected (DORT_ERR_INVALID), and so is a scene that lives on another device
+ * than the current one.  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller.  The first
+ * call on a device looks up the array's address (cudaGetSymbolAddress) and
+ * keeps it; make it before any stream capture, and do not call this entry
+ * point on a device after cudaDeviceReset. */
 int dort_gpu_render_device_noalloc(dort_scene* scene, const dort_render_params* params,
                                    float* d_out_rgb, void* stream);
 
@@ -371,7 +373,15 @@ typedef struct dort_wavefront_tuning {
   uint32_t sort_rays;          /* 0: auto (off), 1: on, 2: off -- sort each
                                   wave's extension rays by direction octant
                                   and origin cell before tracing them */
-  uint32_t reserved[3];
+  uint32_t max_waves;          /* waves one frame may take (0: automatic, a
+                                  bound a correct frame never reaches: every
+                                  path slot's share of the samples times
+                                  max_depth + 3 waves each).  A frame that
+                                  reaches the bound stops; the host-pointer
+                                  entry points return DORT_ERR_TIMEOUT and
+                                  the device-pointer ones leave the flag for
+                                  dort_gpu_batch_stats / out_stats. */
+  uint32_t reserved[2];
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel
@@ -480,6 +490,15 @@ int dort_gpu_scene_bvh_cost(const dort_scene* scene, double out[4]);
  * out[4] = device build milliseconds, out[5] = SAH levels or PLOC iterations,
  * out[6] = depth, out[7] = surface area cost.  Needs a GPU. */
 int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out[8]);
+
+/* No reference counterpart.  Failure injection for tests of the error paths:
+ * after this call the library's next `after` allocations succeed and the one
+ * after that fails as if memory were exhausted (device and pinned host
+ * allocations, and the host-side scene and BVH builders' large allocations);
+ * the entry point that made it returns DORT_ERR_OOM, frees what it had
+ * allocated, and later calls work normally.  A negative `after` switches
+ * injection off.  Process-wide; not for production use. */
+int dort_gpu_debug_fail_alloc(long long after);
 
 #ifdef __cplusplus
 }

@@ -102,4 +102,5 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else
+         os.environ.get("DORT_REFERENCE_TREE") or os.path.join(os.path.dirname(ROOT), "reference"))

@@ -27,7 +27,11 @@ sys.path.insert(0, HERE)
 import ref_scenes  # noqa: E402
 
 DORT = os.path.join(ROOT, "dort_b200", "bin", "dort")
-REFERENCE_TESTS = os.environ.get("DORT_REFERENCE_TESTS", "/root/reference/test")
+# the reference's test scripts: DORT_REFERENCE_TESTS, else the test/ folder of
+# DORT_REFERENCE_TREE or of a "reference" checkout beside this repository
+REFERENCE_TESTS = os.environ.get("DORT_REFERENCE_TESTS") or os.path.join(
+    os.environ.get("DORT_REFERENCE_TREE") or os.path.join(os.path.dirname(ROOT), "reference"),
+    "test")
 
 needs_frontend = pytest.mark.skipif(not os.path.exists(DORT),
                                     reason="front-end not built (needs Lua 5.3 sources)")
