@@ -2,7 +2,8 @@
 """Benchmark of the dort B200 hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dort|reference]
-                    [--workload pt1080p|raycast] [--spp S]
+                    [--workload pt1080p|raycast|batch|adjoint] [--spp S]
+                    [--converged-spp C] [--no-sub] [--no-cpu] [--no-e2e]
 
 Workload "pt1080p" (default; the wavefront configuration): 1920x1080, 256
 samples per pixel, max depth 16, a 1,997,122-triangle scene (geodesic
@@ -12,15 +13,25 @@ materials) lit by a procedural 1024x512 HDR sky.  One step = one frame.
 value   samples/s of the wavefront renderer (one CUDA graph per frame),
         CUDA events on the launch stream, max over ranks.
 config.megakernel_samples_per_s  the plain per-pixel megakernel on the same
-        frame; both draw the same random numbers per pixel and sample, so
-        their images agree to float rounding (equal RMSE at equal spp; the
-        measured relative RMSE between the two frames and of each against a
-        converged frame are reported).
+        frame; both draw the same random numbers per pixel and sample.
+config.equal_rmse  the error of both 256-spp frames against a converged
+        frame of the same scene: C samples per pixel (default 16,384) rendered
+        by the megakernel as frames of 256 spp with independent seeds and
+        accumulated in float64 on the host (FP64 CPU accumulation).  Relative
+        RMSE = sqrt(mean((x - r)^2)) / mean(r) over all pixels and channels,
+        with the converged frame's own variance (from the spread of its
+        frames) subtracted; the spp each renderer needs for 1 %, and the
+        samples/s ratio at equal RMSE.
 e2e     the wavefront frame through the C-ABI host entry
-        dort_gpu_render_wavefront, image copied back to host memory.
+        dort_gpu_render_wavefront, image copied back to host memory; the
+        scene's creation through dort_gpu_scene_create (what a script pays
+        once before its first frame) is reported beside it.
 roofline  the extend (closest-hit) stage: algorithmic bytes = rays x (32 B
         ray + 16 B hit + the reference traversal's N_node x 32 B + N_tri x
         36 B measured on a sample of this workload's rays).
+sub     the other workloads of the metric, measured in the same run at N=1:
+        the ray cast (Mrays/s), the batch (samples/s) and the adjoint (ms),
+        each the line its own --workload prints (fewer steps).
 
 Workload "raycast" (the ray-cast kernel configuration): a seeded soup of 1M
 random triangles (v0 ~ U[0,1]^3, edges ~ N(0, 0.01)), 16,777,216 rays per
@@ -42,8 +53,10 @@ roofline  algorithmic bytes per launch = rays x (32 B ray + 16 B hit +
 cpu_baseline  the reference's own BVH + triangle code (compiled from its
         sources into oracle/_ref) on all host cores over a bounded sample.
 
-Multi-GPU (torchrun): every rank casts its own 16M rays (weak scaling, no
-data exchange); value = all rays / max-over-ranks time.
+Multi-GPU (torchrun): every rank renders its own frame or casts its own 16M
+rays (weak scaling, no data exchange); value = all units / max-over-ranks
+time.  The converged frame, the CPU baseline and the sub-records run at N=1
+only.
 """
 from __future__ import annotations
 
@@ -202,6 +215,41 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def host_info() -> dict:
+    """The host's logical core count and CPU model (the CPU baseline's box)."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"host_cores": os.cpu_count(), "cpu_model": model}
+
+
+def ref_procs(per_proc_gb: float = 0.6) -> int:
+    """Single-threaded reference processes for the CPU baseline: one per
+    logical core, fewer if half the available memory cannot hold them (each
+    holds the 2M-triangle scene and its reference BVH, about 0.4 GB)."""
+    n = os.cpu_count() or 1
+    try:
+        import psutil
+        avail_gb = psutil.virtual_memory().available / 2**30
+        n = max(1, min(n, int(avail_gb * 0.5 / per_proc_gb)))
+    except Exception:  # noqa: BLE001 -- psutil missing: all cores
+        pass
+    return n
+
+
+class Ctx:
+    """Rank, world size, local device and process group of this process."""
+
+    def __init__(self, rank, world, local, pg):
+        self.rank, self.world, self.local, self.pg = rank, world, local, pg
+
+
 # ---- CPU leg ---------------------------------------------------------------------
 
 def cpu_sample(verts, tris, rays, budget_s: float = 15.0, threads: int | None = None):
@@ -285,6 +333,7 @@ def run_reference(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "tris": N_TRIS, "rays_per_step": N_RAYS},
         "cpu_baseline": {"value": mrays, "unit": "Mrays/s", "cores": threads, "kind": kind,
+                         **host_info(),
                          "sample": f"{len(sample)} rays per step (1/16 of the workload: "
                                    "every 16th coherent ray + diffuse rays of a smaller "
                                    "second pass), closest hit"},
@@ -296,13 +345,13 @@ def run_reference(args):
 
 # ---- GPU leg -----------------------------------------------------------------------
 
-def run_dort(args):
+def measure_raycast(args, ctx, steps, warmup, cpu_budget=15.0, e2e_steps=20):
+    """The ray-cast workload; returns its JSON line on rank 0 (else None)."""
     import torch
     import dort_b200 as db
 
-    rank, world, local, pg = dist_setup(args.gpus)
+    rank, world, local, pg = ctx.rank, ctx.world, ctx.local, ctx.pg
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
 
     def caster(verts, tris):
         sc = db.Scene(verts, tris)
@@ -327,7 +376,7 @@ def run_dort(args):
         scene.raycast_device(d_rays.data_ptr(), n, d_prim.data_ptr(), d_tb.data_ptr(),
                              stream=sh)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
 
@@ -339,7 +388,7 @@ def run_dort(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -347,11 +396,11 @@ def run_dort(args):
     ms = ev0.elapsed_time(ev1)
     clk = clocks.stop()
     ms_max = max_over_ranks(pg, ms)
-    value = job_rate(n * args.steps, world, ms_max / 1e3) / 1e6
+    value = job_rate(n * steps, world, ms_max / 1e3) / 1e6
 
     # kernel-only duration per launch (events around each launch on its stream)
     per_launch = scene.raycast_timed(d_rays.data_ptr(), n, d_prim.data_ptr(),
-                                     d_tb.data_ptr(), stream=sh, repeat=max(3, args.steps))
+                                     d_tb.data_ptr(), stream=sh, repeat=max(3, steps))
 
     # e2e through the host-pointer C-ABI entry with pinned buffers
     h_rays = torch.empty((n, 8), dtype=torch.float32, pin_memory=True)
@@ -369,7 +418,7 @@ def run_dort(args):
     if not args.no_e2e:
         e2e_step()
         barrier(pg)
-        e2e_steps = min(args.steps, 20)
+        e2e_steps = max(1, min(steps, e2e_steps))
         te0 = time.perf_counter()
         for _ in range(e2e_steps):
             e2e_step()
@@ -377,14 +426,15 @@ def run_dort(args):
         te = max_over_ranks(pg, te)
         e2e = world * n * e2e_steps / te / 1e6
 
+    line = None
     if rank == 0:
         hbm, peak_kind = peaks()
         cpu = None
         rl = None
         if world == 1 and not args.no_cpu:
-            c = cpu_sample(verts, tris, rays)
+            c = cpu_sample(verts, tris, rays, budget_s=cpu_budget)
             cpu = {"value": c["rays"] / c["seconds"] / 1e6, "unit": "Mrays/s",
-                   "cores": c["cores"], "kind": c["kind"],
+                   "cores": c["cores"], "kind": c["kind"], **host_info(),
                    "sample": f"{c['rays']} rays interleaved from the coherent and diffuse "
                              f"halves of the workload, {c['seconds']:.1f}s"}
             bytes_per_ray = 32 + 16 + c["n_node"] * 32 + c["n_tri"] * 36
@@ -398,7 +448,7 @@ def run_dort(args):
                   "kernel_ms_per_launch": per_launch}
         line = {
             "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+            "steps": steps, "warmup": warmup, "ms_per_step": ms_max / steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "tris": N_TRIS, "rays_per_step": n,
@@ -408,13 +458,11 @@ def run_dort(args):
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 16},
-            "gpu_launches": args.steps,
+            "gpu_launches": steps,
             "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
     scene.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    return line if rank == 0 else None
 
 
 # ---- pt1080p workload ------------------------------------------------------------
@@ -482,21 +530,78 @@ def pt_reference_work(sd, n=1 << 15):
     return float(nodes.mean()), float(tests.mean()), len(rays)
 
 
-def run_dort_pt(args):
+def converged_reference(sc, sd, W, H, spp_total, frame_spp, d_out, sh):
+    """A converged frame of the scene: spp_total samples per pixel rendered by
+    the per-pixel megakernel as frames of frame_spp samples with independent
+    seeds, each copied to the host and accumulated in float64.  Returns the
+    mean image, the per-pixel variance of that mean (from the spread of the
+    frames), the frame count and the seconds taken."""
+    import torch
+    import dort_b200 as db
+    frames = max(2, spp_total // frame_spp)
+    acc = np.zeros((H, W, 3), np.float64)
+    acc2 = np.zeros((H, W, 3), np.float64)
+    t0 = time.perf_counter()
+    for k in range(frames):
+        p = db.render_params(sd["camera"], W, H, frame_spp, max_depth=PT_DEPTH,
+                             seed=1_000_000 + k)
+        sc.render_device(p, d_out.data_ptr(), stream=sh)
+        img = d_out.view(H, W, 3).cpu().numpy().astype(np.float64)
+        acc += img
+        acc2 += img * img
+    torch.cuda.synchronize()
+    mean = acc / frames
+    var_frame = np.maximum(acc2 / frames - mean * mean, 0.0) * frames / (frames - 1)
+    return mean, var_frame / frames, frames, time.perf_counter() - t0
+
+
+def equal_rmse(frames: dict, ref, var_ref, ref_spp: int, spp: int, rates: dict) -> dict:
+    """Relative RMSE of each frame against the converged one (its own
+    variance subtracted), the spp each renderer needs for 1 %, and the
+    samples/s ratio at equal RMSE."""
+    mref = float(ref.mean())
+    vref = float(var_ref.mean())
+    out = {"reference": f"megakernel, {ref_spp} spp as independent 256-spp frames, float64 "
+                        "accumulation on the host",
+           "reference_spp": ref_spp,
+           "reference_rel_rmse": float(np.sqrt(vref) / mref),
+           "target_rel_rmse": 0.01}
+    need = {}
+    for name, x in frames.items():
+        raw = float(((x.astype(np.float64) - ref) ** 2).mean())
+        rel = float(np.sqrt(max(raw - vref, 0.0)) / mref)
+        out[f"rel_rmse_{name}"] = rel
+        out[f"rel_rmse_{name}_uncorrected"] = float(np.sqrt(raw) / mref)
+        # Monte Carlo error falls as 1/sqrt(spp)
+        need[name] = int(np.ceil(spp * (rel / 0.01) ** 2))
+        out[f"spp_for_1pct_{name}"] = need[name]
+    # the expected error of one frame from the reference's own spread
+    out["rel_rmse_expected_from_spread"] = float(
+        np.sqrt(vref * ref_spp / spp) / mref)
+    # both renderers trace the same paths (same random numbers), so equal spp
+    # is equal RMSE; at the spp needed for 1 % the time ratio is the rate ratio
+    out["equal_rmse_spp"] = max(spp, max(need.values()))
+    out["wavefront_over_megakernel_at_equal_rmse"] = rates["wavefront"] / rates["megakernel"]
+    return out
+
+
+def measure_pt(args, ctx):
+    """The 1080p wavefront frame; returns its JSON line on rank 0."""
     import torch
     import dort_b200 as db
     from dort_b200 import scenes
 
-    rank, world, local, pg = dist_setup(args.gpus)
+    rank, world, local, pg = ctx.rank, ctx.world, ctx.local, ctx.pg
     dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
     t0 = time.time()
     sd = scenes.wavefront_scene()
     sd["bvh_build"] = args.bvh_build
+    tc0 = time.perf_counter()
     sc = db.scene_from_dict(sd)
+    scene_create_ms = (time.perf_counter() - tc0) * 1e3
     st = sc.stats()
     log(f"[rank {rank}] scene ready in {time.time() - t0:.1f}s; nodes={st['nodes']} "
-        f"depth={st['depth']} build={st['build_ms']:.0f}ms ({st['bvh_build']} BVH "
+        f"depth={st['depth']} create={scene_create_ms:.0f}ms ({st['bvh_build']} BVH "
         f"{st['bvh_ms']:.0f}ms)")
     spp = args.spp or PT_SPP
     p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH,
@@ -562,6 +667,19 @@ def run_dort_pt(args):
         te = max_over_ranks(pg, time.perf_counter() - te0)
         e2e = world * samples * e2e_steps / te
 
+    # equal RMSE: both frames against a converged frame (N=1 only)
+    eq = None
+    if world == 1 and args.converged_spp > 0:
+        ref, var_ref, nfr, secs = converged_reference(sc, sd, PT_W, PT_H, args.converged_spp,
+                                                      PT_SPP, d_out, sh)
+        eq = equal_rmse({"wavefront": wf_img, "megakernel": mega_img}, ref, var_ref,
+                        nfr * PT_SPP, spp, {"wavefront": value, "megakernel": mega_value})
+        eq["reference_seconds"] = round(secs, 1)
+        log(f"[rank {rank}] converged frame: {nfr} x {PT_SPP} spp in {secs:.0f}s; rel RMSE "
+            f"wavefront {eq['rel_rmse_wavefront']:.4f} megakernel "
+            f"{eq['rel_rmse_megakernel']:.4f} (reference {eq['reference_rel_rmse']:.4f})")
+
+    line = None
     if rank == 0:
         rr_between = float(np.sqrt(((wf_img.astype(np.float64) - mega_img) ** 2).mean())
                            / max(float(mega_img.mean()), 1e-30))
@@ -571,16 +689,18 @@ def run_dort_pt(args):
         rays_per_frame = stages["rays"]
         if world == 1 and not args.no_cpu:
             n_node, n_tri, nwork = pt_reference_work(sd)
-            procs = min(os.cpu_count() or 1, 16)
+            procs = ref_procs()
             pool = ref_pt_pool(procs)
             ref_pt_step(pool, procs, 0)                  # builds + warms the workers
             secs = ref_pt_step(pool, procs, 1)
             pool.close()
             cpu_value = procs * REF_SAMPLE_W * REF_SAMPLE_H / secs
             cpu = {"value": cpu_value, "unit": "samples/s", "cores": procs, "kind": "reference",
-                   "sample": f"{procs} single-threaded reference PathRenderer processes, each "
-                             f"one {REF_SAMPLE_W}x{REF_SAMPLE_H} frame at 1 spp of the same "
-                             f"scene and camera ({secs:.1f}s); GGX conductor timed as Phong"}
+                   **host_info(),
+                   "sample": f"{procs} single-threaded reference PathRenderer processes (one "
+                             f"per logical core), each one {REF_SAMPLE_W}x{REF_SAMPLE_H} frame "
+                             f"at 1 spp of the same scene and camera ({secs:.1f}s); GGX "
+                             "conductor timed as Phong"}
             # dominant stage: the extend (closest-hit) stage, over the frame's
             # extension rays (counted by the staged run)
             ext_rays = stages["extend_rays"]
@@ -603,6 +723,11 @@ def run_dort_pt(args):
                   "kernel": "wf_extend (closest hit)", "bytes_per_ray": bytes_per_ray,
                   "n_node": n_node, "n_tri": n_tri, "work_sample_rays": nwork,
                   "extend_rays_per_frame": ext_rays,
+                  # the same stage against the DRAM traffic it really moves
+                  # (the tree is L2-resident): measured bytes per ray over the
+                  # stage time
+                  "measured_dram_gbs": ext_rays * EXTEND_TRAFFIC_BYTES / EXTEND_TRAFFIC_RAYS
+                                       / (stages["extend"] / 1e3) / 1e9,
                   "stage_ms_per_frame": {k: stages[k] for k in
                                          ("regen", "extend", "shade", "shadow", "neeb")}}
         line = {
@@ -616,6 +741,7 @@ def run_dort_pt(args):
                        "megakernel_samples_per_s": mega_value,
                        "wavefront_over_megakernel": value / mega_value,
                        "rel_rmse_wavefront_vs_megakernel": rr_between,
+                       "equal_rmse": eq,
                        "rays_per_frame": rays_per_frame,
                        "mrays_per_s": rays_per_frame * args.steps * world / (ms_max / 1e3) / 1e6,
                        "queue_capacity": tuning["queue_capacity"],
@@ -626,19 +752,41 @@ def run_dort_pt(args):
                        "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2),
                        "l2": "frame state (path queues ~11 GB, image 25 MB) larger than L2"},
             "roofline": rl, "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "samples/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": PT_W * PT_H * 12},
+            # per frame the caller passes its render parameters and reads the
+            # image back; the scene (vertices, indices, materials, sky) goes to
+            # the device once, at dort_gpu_scene_create
+            "e2e": {"value": e2e, "unit": "samples/s",
+                    "h2d_bytes_per_step": ctypes_sizeof_params(),
+                    "d2h_bytes_per_step": PT_W * PT_H * 12,
+                    "scene_create_ms": round(scene_create_ms, 1),
+                    "scene_h2d_bytes": scene_input_bytes(sd),
+                    "scene_device_bytes": int(st["device_bytes"])},
             "gpu_launches": args.steps * int(stages["waves"] * 6 + 2),
             "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
     sc.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    return line
+
+
+def ctypes_sizeof_params() -> int:
+    import ctypes
+    from dort_b200 import _abi
+    return ctypes.sizeof(_abi.RenderParams)
+
+
+def scene_input_bytes(sd: dict) -> int:
+    """Bytes of the host arrays a scene description hands to
+    dort_gpu_scene_create."""
+    n = 0
+    for k in ("verts", "tris", "tri_material", "tri_emission", "sky_rgb"):
+        v = sd.get(k)
+        if v is not None:
+            n += int(np.asarray(v).nbytes)
+    return n
 
 
 def run_reference_pt(args):
-    procs = min(os.cpu_count() or 1, 16)
+    procs = ref_procs()
     pool = ref_pt_pool(procs)
     for w in range(args.warmup):
         ref_pt_step(pool, procs, w)
@@ -656,7 +804,7 @@ def run_reference_pt(args):
         "config": {"workload": PT_WORKLOAD, "width": PT_W, "height": PT_H, "spp": PT_SPP,
                    "max_depth": PT_DEPTH},
         "cpu_baseline": {"value": value, "unit": "samples/s", "cores": procs,
-                         "kind": "reference",
+                         "kind": "reference", **host_info(),
                          "sample": f"per step {procs} single-threaded reference PathRenderer "
                                    f"processes each render one {REF_SAMPLE_W}x{REF_SAMPLE_H} "
                                    "1-spp frame of the same scene and camera (the reference's "
@@ -675,13 +823,13 @@ BATCH_WORKLOAD = ("batch: 64 seeded jobs, random-triangle soups of 10k-500k tris
                   "depth 8-16, one wavefront launch (one CUDA graph) for all jobs")
 
 
-def run_dort_batch(args):
+def measure_batch(args, ctx, steps, warmup, mega_warmup=True):
+    """The batch workload; returns its JSON line on rank 0."""
     import torch
     import dort_b200 as db
     from dort_b200 import scenes
 
-    rank, world, local, pg = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
+    rank, world, local, pg = ctx.rank, ctx.world, ctx.local, ctx.pg
     t0 = time.time()
     specs = scenes.batch_jobs(count=64, seed=rank_seed(4, rank))
     jobs = []
@@ -698,7 +846,7 @@ def run_dort_batch(args):
         f"{built} BVH builds {bvh_ms:.0f} ms), {samples / 1e9:.2f}G samples")
     b = db.Batch(jobs, {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"})
     stream = torch.cuda.current_stream()
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         b.render(stream.cuda_stream)
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
@@ -707,7 +855,7 @@ def run_dort_batch(args):
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         b.render(stream.cuda_stream)
     ev1.record(stream)
     torch.cuda.synchronize()
@@ -715,38 +863,40 @@ def run_dort_batch(args):
     ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
     clk = clocks.stop()
     st = b.stats()
-    value = world * samples * args.steps / (ms / 1e3)
+    value = world * samples * steps / (ms / 1e3)
     # the plain per-pixel megakernel, one launch per job
     outs = [torch.empty(p.width * p.height * 3, dtype=torch.float32, device="cuda")
             for _, p in jobs]
-    for (sc, p), o in zip(jobs, outs):
-        sc.render_device(p, o.data_ptr(), stream.cuda_stream)
-    torch.cuda.synchronize()
+    if mega_warmup:
+        for (sc, p), o in zip(jobs, outs):
+            sc.render_device(p, o.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
     ev0.record(stream)
     for (sc, p), o in zip(jobs, outs):
         sc.render_device(p, o.data_ptr(), stream.cuda_stream)
     ev1.record(stream)
     torch.cuda.synchronize()
     mega_ms = max_over_ranks(pg, ev0.elapsed_time(ev1))
+    line = None
     if rank == 0:
         line = {
             "metric": "batched samples/s, wavefront batch vs per-job megakernel", "value": value,
-            "unit": "samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "unit": "samples/s", "n_gpus": world, "steps": steps, "warmup": warmup,
+            "ms_per_step": ms / steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": BATCH_WORKLOAD, "jobs": len(jobs), "samples": samples,
                        "megakernel_samples_per_s": world * samples / (mega_ms / 1e3),
-                       "batch_over_megakernel": (mega_ms / (ms / args.steps)),
+                       "batch_over_megakernel": (mega_ms / (ms / steps)),
                        "rays_per_batch": st["rays"], "waves": st["waves"],
                        "bvh_build": built, "bvh_build_ms_total": round(bvh_ms, 1),
                        "scene_create_s_total": round(create_s, 3)},
             "roofline": None, "cpu_baseline": None,
-            "e2e": None, "gpu_launches": args.steps * int(st["waves"] * 6 + 2), "clocks": clk,
+            "e2e": None, "gpu_launches": steps * int(st["waves"] * 6 + 2), "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
     b.close()
-    if pg is not None:
-        pg.destroy_process_group()
+    for sc, _ in jobs:
+        sc.close()
+    return line
 
 
 # ---- adjoint workload ---------------------------------------------------------------
@@ -756,13 +906,13 @@ ADJ_WORKLOAD = ("adjoint: 512x512, 64 spp, depth 6, 500k random tris with per-tr
                 "render + path-replay backward for albedo and emission gradients")
 
 
-def run_dort_adjoint(args):
+def measure_adjoint(args, ctx, steps, warmup):
+    """The adjoint workload; returns its JSON line on rank 0."""
     import torch
     import dort_b200 as db
     from dort_b200 import scenes
 
-    rank, world, local, pg = dist_setup(args.gpus)
-    torch.cuda.set_device(local)
+    rank, world, local, pg = ctx.rank, ctx.world, ctx.local, ctx.pg
     sd = scenes.adjoint_scene()
     sc = db.scene_from_dict(sd)
     p = db.render_params(sd["camera"], 512, 512, 64, max_depth=6, seed=rank_seed(1, rank))
@@ -776,23 +926,24 @@ def run_dort_adjoint(args):
         loss, g = db.loss_l2(img, target)
         return sc.adjoint_backward(p, g, alb, em)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
     barrier(pg)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         step()
     torch.cuda.synchronize()
     dt = max_over_ranks(pg, time.perf_counter() - t0)
     clk = clocks.stop()
+    line = None
     if rank == 0:
-        ms = dt / args.steps * 1e3
+        ms = dt / steps * 1e3
         line = {
             "metric": "adjoint ms (forward + backward, host arrays)", "value": ms, "unit": "ms",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
             "config": {"workload": ADJ_WORKLOAD, "tris": int(len(sd["tris"]))},
@@ -800,10 +951,42 @@ def run_dort_adjoint(args):
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": int(2 * alb.nbytes * 2 +
                                                                           512 * 512 * 12 * 2),
                     "d2h_bytes_per_step": int(alb.nbytes * 2 + 512 * 512 * 12)},
-            "gpu_launches": args.steps * 4, "clocks": clk,
+            "gpu_launches": steps * 4, "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
     sc.close()
+    return line
+
+
+def run_dort(args):
+    """The GPU arm: one process per GPU; rank 0 prints one JSON line."""
+    import torch
+    rank, world, local, pg = dist_setup(args.gpus)
+    torch.cuda.set_device(local)
+    ctx = Ctx(rank, world, local, pg)
+    if args.workload == "pt1080p":
+        line = measure_pt(args, ctx)
+        if world == 1 and not args.no_sub:
+            # the metric's other parts, fewer steps each, after the frame
+            sub = {}
+            for name, fn in (("raycast", lambda: measure_raycast(args, ctx, 20, 3, cpu_budget=8.0,
+                                                                 e2e_steps=5)),
+                             ("adjoint", lambda: measure_adjoint(args, ctx, 3, 1)),
+                             ("batch", lambda: measure_batch(args, ctx, 1, 1,
+                                                             mega_warmup=False))):
+                t0 = time.time()
+                sub[name] = fn()
+                log(f"[rank {rank}] sub-record {name} in {time.time() - t0:.0f}s")
+                torch.cuda.empty_cache()
+            if line is not None:
+                line["sub"] = sub
+    elif args.workload == "batch":
+        line = measure_batch(args, ctx, args.steps, args.warmup)
+    elif args.workload == "adjoint":
+        line = measure_adjoint(args, ctx, args.steps, args.warmup)
+    else:
+        line = measure_raycast(args, ctx, args.steps, args.warmup)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
 
@@ -811,12 +994,17 @@ def run_dort_adjoint(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=0, help="timed steps (default: 5 for pt1080p, 100 for raycast)")
+    ap.add_argument("--steps", type=int, default=0,
+                    help="timed steps (default: 5 for pt1080p, 100 for raycast)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dort", choices=["dort", "reference"])
     ap.add_argument("--workload", default="pt1080p",
                     choices=["pt1080p", "raycast", "batch", "adjoint"])
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
+    ap.add_argument("--converged-spp", type=int, default=16384,
+                    help="pt1080p: samples per pixel of the converged frame (0: skip)")
+    ap.add_argument("--no-sub", action="store_true",
+                    help="pt1080p: skip the ray-cast, adjoint and batch sub-records")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--sort-rays", default="off", choices=["on", "off"],
@@ -839,14 +1027,7 @@ def main():
             print(json.dumps({"impl": "reference", "unavailable":
                               f"the reference has no {args.workload} renderer"}), flush=True)
         return
-    if args.workload == "pt1080p":
-        run_dort_pt(args)
-    elif args.workload == "batch":
-        run_dort_batch(args)
-    elif args.workload == "adjoint":
-        run_dort_adjoint(args)
-    else:
-        run_dort(args)
+    run_dort(args)
 
 
 if __name__ == "__main__":

@@ -263,10 +263,11 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
                   min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
                   sample_all_lights: bool = False, direct_strategy: str = "mis",
                   seed: int = 42, renderer: str = "pt",
-                  use_t1_paths: bool = True) -> _abi.RenderParams:
+                  use_t1_paths: bool = True, roulette: bool = True) -> _abi.RenderParams:
     """dort.render.make parameters (lua_render.cpp:102-160) with its defaults;
     `renderer` "pt" (the path tracer), "lt" / "light" (the light tracer) or
-    "bdpt" (the bidirectional path tracer, with use_t1_paths)."""
+    "bdpt" (the bidirectional path tracer, with use_t1_paths).  roulette=False
+    turns off the path tracer's Russian roulette (for derivative checks)."""
     p = _abi.RenderParams()
     p.struct_size = ctypes.sizeof(_abi.RenderParams)
     p.width, p.height, p.iterations = width, height, iterations
@@ -276,7 +277,8 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     p.seed = seed
     p.renderer = {"pt": _abi.RENDERER_PT, "path": _abi.RENDERER_PT, "lt": _abi.RENDERER_LT,
                   "light": _abi.RENDERER_LT, "bdpt": _abi.RENDERER_BDPT}[renderer]
-    p.renderer_flags = 0 if use_t1_paths else _abi.BDPT_NO_T1_PATHS
+    p.renderer_flags = ((0 if use_t1_paths else _abi.BDPT_NO_T1_PATHS) |
+                        (0 if roulette else _abi.PT_NO_ROULETTE))
     c = p.camera
     c.origin = (ctypes.c_float * 3)(*camera["origin"])
     c.right = (ctypes.c_float * 3)(*camera["right"])
@@ -302,6 +304,37 @@ def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
     t.sort_rays = 0 if sort_rays is None else (1 if sort_rays else 2)
     t.max_waves = max_waves
     return t
+
+
+def bsdf_probe(material: dict, wo, wi=None, u=None, device: bool = True) -> dict:
+    """dort_gpu_bsdf_probe: the BxDF code of one material (a dict as in
+    scene_desc's materials) on local-frame directions.  Returns f and pdf of
+    (wi, wo) when wi is given, and the sampled direction, its f and pdf when
+    the uniforms u (n x 3) are given.  device=False runs the code compiled for
+    the host."""
+    m = _abi.Material()
+    m.kind = material.get("kind", MAT_LAMBERT)
+    m.color = (ctypes.c_float * 3)(*material.get("color", (0.0, 0.0, 0.0)))
+    m.color2 = (ctypes.c_float * 3)(*material.get("color2", (0.0, 0.0, 0.0)))
+    p = list(material.get("param", ())) + [0.0] * 4
+    m.param = (ctypes.c_float * 4)(*p[:4])
+    wo = np.ascontiguousarray(wo, np.float32).reshape(-1, 3)
+    n = len(wo)
+    out = {}
+    if wi is not None:
+        wi = np.ascontiguousarray(wi, np.float32).reshape(-1, 3)
+        out["f"] = np.zeros((n, 3), np.float32)
+        out["pdf"] = np.zeros(n, np.float32)
+    if u is not None:
+        u = np.ascontiguousarray(u, np.float32).reshape(-1, 3)
+        out["wi"] = np.zeros((n, 3), np.float32)
+        out["sf"] = np.zeros((n, 3), np.float32)
+        out["spdf"] = np.zeros(n, np.float32)
+    _abi.check(_abi.lib().dort_gpu_bsdf_probe(
+        ctypes.byref(m), n, _ptr(wo), _ptr(wi), _ptr(u), _ptr(out.get("f")),
+        _ptr(out.get("pdf")), _ptr(out.get("wi")), _ptr(out.get("sf")),
+        _ptr(out.get("spdf")), int(device)))
+    return out
 
 
 def debug_fail_alloc(after: int) -> None:

@@ -34,6 +34,7 @@ CAMERA_PINHOLE, CAMERA_ORTHO, CAMERA_THIN_LENS = 0, 1, 2
 BVH_BUILD_DEFAULT, BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_PLOC = 0, 1, 2, 3
 RENDERER_PT, RENDERER_LT, RENDERER_BDPT = 0, 1, 2
 BDPT_NO_T1_PATHS = 1
+PT_NO_ROULETTE = 2
 ABI_VERSION = 2
 
 
@@ -189,6 +190,9 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_batch_destroy.argtypes = [c_p]
         L.dort_gpu_scene_bvh_cost.restype = c_i32
         L.dort_gpu_scene_bvh_cost.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_bsdf_probe.restype = c_i32
+        L.dort_gpu_bsdf_probe.argtypes = [ctypes.POINTER(Material), c_size, c_p, c_p, c_p, c_p,
+                                          c_p, c_p, c_p, c_p, c_i32]
         L.dort_gpu_debug_fail_alloc.restype = c_i32
         L.dort_gpu_debug_fail_alloc.argtypes = [ctypes.c_longlong]
         L.dort_gpu_check_device_bvh.restype = c_i32

@@ -940,7 +940,7 @@ DG_HD PathResult pt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel
     thr = thr * contrib;
     if(bounces == pp.max_depth && !last_delta) {
       break;
-    } else if(bounces >= 2 && bounces > pp.min_depth) {
+    } else if(bounces >= 2 && bounces > pp.min_depth && pp.roulette) {
       float survive = clampf(average(contrib), 0.1f, 0.99f);
       if(r2.b > survive) { break; }
       thr = thr * (1.f / survive);

@@ -179,6 +179,11 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   pp.seed = rp->seed;
   pp.renderer = rp->renderer;
   pp.use_t1 = (rp->renderer_flags & DORT_BDPT_NO_T1_PATHS) ? 0u : 1u;
+  pp.roulette = (rp->renderer_flags & DORT_PT_NO_ROULETTE) ? 0u : 1u;
+  if(rp->renderer_flags & ~(DORT_BDPT_NO_T1_PATHS | DORT_PT_NO_ROULETTE)) {
+    err = "unknown renderer_flags bits";
+    return false;
+  }
   // world -> camera: the inverse of the camera's linear part [right up forward]
   double m[3][3];
   for(int a = 0; a < 3; ++a) {

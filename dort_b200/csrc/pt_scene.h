@@ -118,6 +118,7 @@ struct PtParams {
   uint32_t renderer;         // RENDERER_PT, RENDERER_LT, RENDERER_BDPT
   float cam_inv[9];          // rows of [right up forward]^-1 (world to camera)
   uint32_t use_t1;           // bdpt: connect light subpaths to the camera (t = 1)
+  uint32_t roulette;         // pt: Russian roulette after bounce 2 (the reference's rule)
 };
 
 enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1, RENDERER_BDPT = 2 };

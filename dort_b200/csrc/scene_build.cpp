@@ -170,6 +170,10 @@ void shape_local_bounds(const DevShape& s, float lo[3], float hi[3]) {
 
 }  // namespace
 
+bool material_to_device(const dort_material& in, DevMaterial& m, std::string& err) {
+  return resolve_material(in, m, err);
+}
+
 bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& err,
                       bool allow_device_bvh) {
   if(desc->struct_size != sizeof(dort_scene_desc)) {

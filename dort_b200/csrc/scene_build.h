@@ -31,6 +31,9 @@ struct HostScene {
   float centroid[3] = {0.f, 0.f, 0.f};
 };
 
+// The device form of one material (validated; false + message on error).
+bool material_to_device(const dort_material& in, DevMaterial& m, std::string& err);
+
 // Analytic shapes are intersected as a list after the BVH.
 constexpr uint32_t kMaxShapes = 4096;
 

@@ -649,7 +649,7 @@ __global__ void wf_shade(J jobs, WfDev w) {
           thr = thr * contrib;
           if(bounces == pp.max_depth && !last_delta) {
             finished = true;
-          } else if(bounces >= 2 && bounces > pp.min_depth) {
+          } else if(bounces >= 2 && bounces > pp.min_depth && pp.roulette) {
             float survive = clampf(average(contrib), 0.1f, 0.99f);
             if(r2.b > survive) {
               finished = true;

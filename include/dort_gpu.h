@@ -314,6 +314,12 @@ enum dort_renderer { DORT_RENDERER_PT = 0, DORT_RENDERER_LT = 1, DORT_RENDERER_B
 
 /* dort_render_params.renderer_flags */
 #define DORT_BDPT_NO_T1_PATHS 1u   /* bdpt: use_t1_paths = false */
+#define DORT_PT_NO_ROULETTE 2u     /* pt: no Russian roulette (paths run to max_depth);
+                                      the reference always plays it
+                                      (path_renderer.cpp:101-106).  Same expected
+                                      image; for derivative checks, where a
+                                      roulette decision that flips under a small
+                                      parameter change makes a sample jump */
 
 typedef struct dort_render_params {
   uint32_t struct_size;        /* sizeof(dort_render_params) */
@@ -490,6 +496,21 @@ int dort_gpu_scene_bvh_cost(const dort_scene* scene, double out[4]);
  * out[4] = device build milliseconds, out[5] = SAH levels or PLOC iterations,
  * out[6] = depth, out[7] = surface area cost.  Needs a GPU. */
 int dort_gpu_check_device_bvh(const dort_scene_desc* desc, double out[8]);
+
+/* No reference counterpart.  The BxDF code of one material evaluated and
+ * sampled for directions in the local shading frame (z = the normal), for
+ * checking the formulas and samplers: for i < n, with wo[3i..3i+2] the fixed
+ * direction (towards the viewer),
+ *   wi (optional): out_f[3i..] = f(wi, wo) (RGB), out_pdf[i] = the density
+ *                  of sampling wi given wo;
+ *   u (optional):  three uniforms per entry; out_wi[3i..] = the sampled
+ *                  direction, out_sf[3i..] = its f, out_spdf[i] = its pdf
+ *                  (0: no sample).
+ * All arrays are host memory.  on_device = 1 runs the code on the current
+ * GPU, 0 the same code compiled for the host.  The renderers never call it. */
+int dort_gpu_bsdf_probe(const dort_material* material, size_t n, const float* wo,
+                        const float* wi, const float* u, float* out_f, float* out_pdf,
+                        float* out_wi, float* out_sf, float* out_spdf, int on_device);
 
 /* No reference counterpart.  Failure injection for tests of the error paths:
  * after this call the library's next `after` allocations succeed and the one

@@ -51,6 +51,22 @@ void orc_raycast_brute(const float* verts, const uint32_t* tri_idx,
 int orc_triangle_hit(const float* p0, const float* p1, const float* p2,
     const float* ray, float* out_tb);
 
+/* Float64 "pt" estimator and its gradient (pt64.c) on Lambert triangle
+ * scenes with triangle emitters and a pinhole camera, using the device's
+ * random-number streams.  albedo / emission: tri_count * 3 (the values in
+ * effect); light_power_emission: the emission the scene was created with
+ * (fixes which triangles are lights and the light-choice distribution);
+ * camera: origin, right, up, forward (12 floats).  out_image (w * h * 3) is
+ * the rendered image; with dl_dimage (w * h * 3) the gradients of the loss
+ * are added to d_albedo / d_emission (tri_count * 3, either may be NULL).
+ * Returns 0, or -1 on a bad index. */
+int orc_pt64(const float* verts, uint32_t vert_count, const uint32_t* tris, uint32_t tri_count,
+    const float* albedo, const float* emission, const float* light_power_emission,
+    const float* camera, float fov, uint32_t width, uint32_t height, uint32_t spp,
+    uint32_t min_depth, uint32_t max_depth, uint64_t seed, uint32_t no_roulette,
+    const float* dl_dimage, double* out_image, double* d_albedo, double* d_emission,
+    uint64_t* out_rays);
+
 #ifdef __cplusplus
 }
 #endif

@@ -62,6 +62,9 @@ def lib():
         L.orc_raycast_brute.argtypes = [_P, _P, _u32, _P, _u64, _P, _P]
         L.orc_triangle_hit.restype = _i32
         L.orc_triangle_hit.argtypes = [_P, _P, _P, _P, _P]
+        L.orc_pt64.restype = _i32
+        L.orc_pt64.argtypes = [_P, _u32, _P, _u32, _P, _P, _P, _P, ctypes.c_float, _u32, _u32,
+                               _u32, _u32, _u32, _u64, _u32, _P, _P, _P, _P, _P]
         _lib = L
     return _lib
 
@@ -81,6 +84,45 @@ def ref():
         R.dref_raycast.argtypes = [_P, _P, _u64, _i32, _u32, _P, _P, _P, _P]
         _ref = R
     return _ref
+
+
+def _ggx_lib():
+    R = ref()
+    for name in ("dref_ggx_d", "dref_ggx_g1", "dref_ggx_sample_m"):
+        getattr(R, name).restype = None
+    R.dref_ggx_d.argtypes = [ctypes.c_float, ctypes.c_size_t, _P, _P]
+    R.dref_ggx_g1.argtypes = [ctypes.c_float, ctypes.c_size_t, _P, _P, _P]
+    R.dref_ggx_sample_m.argtypes = [ctypes.c_float, ctypes.c_size_t, _P, _P, _P]
+    return R
+
+
+def ref_ggx_d(alpha: float, m) -> np.ndarray:
+    """The reference's MicrofacetDistrib(GGX, alpha).d(m) in float
+    (microfacet.cpp:19-36)."""
+    m = np.ascontiguousarray(m, np.float32).reshape(-1, 3)
+    out = np.zeros(len(m), np.float32)
+    _ggx_lib().dref_ggx_d(alpha, len(m), _ptr(m), _ptr(out))
+    return out
+
+
+def ref_ggx_g1(alpha: float, v, m) -> np.ndarray:
+    """The reference's MicrofacetDistrib(GGX, alpha).g1(v, m)
+    (microfacet.cpp:38-58)."""
+    v = np.ascontiguousarray(v, np.float32).reshape(-1, 3)
+    m = np.ascontiguousarray(m, np.float32).reshape(-1, 3)
+    out = np.zeros(len(v), np.float32)
+    _ggx_lib().dref_ggx_g1(alpha, len(v), _ptr(v), _ptr(m), _ptr(out))
+    return out
+
+
+def ref_ggx_sample_m(alpha: float, uv) -> tuple[np.ndarray, np.ndarray]:
+    """The reference's MicrofacetDistrib(GGX, alpha).sample_m(uv, pdf)
+    (microfacet.cpp:64-86): half vectors and pdfs."""
+    uv = np.ascontiguousarray(uv, np.float32).reshape(-1, 2)
+    m = np.zeros((len(uv), 3), np.float32)
+    pdf = np.zeros(len(uv), np.float32)
+    _ggx_lib().dref_ggx_sample_m(alpha, len(uv), _ptr(uv), _ptr(m), _ptr(pdf))
+    return m, pdf
 
 
 def _mesh_args(verts, tris):
@@ -144,6 +186,33 @@ def triangle_hit(p0, p1, p2, ray):
     tb = np.zeros(3, np.float32)
     ok = lib().orc_triangle_hit(*[_ptr(x) for x in a], _ptr(tb))
     return bool(ok), tb
+
+
+def pt64(scene: dict, width: int, height: int, spp: int, max_depth: int, seed: int,
+         albedo, emission, dl_dimage=None, min_depth: int = 0, no_roulette: bool = False):
+    """The float64 restatement of the "pt" estimator (oracle/pt64.c) on a
+    Lambert triangle scene with triangle emitters (the adjoint workload's
+    kind): the image, and with dl_dimage the loss gradients with respect to
+    per-triangle albedo and emission.  `scene` carries verts, tris, camera and
+    tri_emission (the emission it was created with); albedo / emission are
+    the per-triangle values in effect."""
+    v, t = _mesh_args(scene["verts"], scene["tris"])
+    alb = np.ascontiguousarray(albedo, np.float32).reshape(-1, 3)
+    em = np.ascontiguousarray(emission, np.float32).reshape(-1, 3)
+    em0 = np.ascontiguousarray(scene["tri_emission"], np.float32).reshape(-1, 3)
+    cam = pack_camera(scene["camera"])
+    img = np.zeros((height, width, 3), np.float64)
+    g = None if dl_dimage is None else np.ascontiguousarray(dl_dimage, np.float32)
+    da = np.zeros((len(t), 3), np.float64) if g is not None else None
+    de = np.zeros((len(t), 3), np.float64) if g is not None else None
+    rays = ctypes.c_uint64(0)
+    rc = lib().orc_pt64(_ptr(v), len(v), _ptr(t), len(t), _ptr(alb), _ptr(em), _ptr(em0),
+                        _ptr(cam), ctypes.c_float(scene["camera"]["fov"]), width, height, spp,
+                        min_depth, max_depth, seed, int(no_roulette), _ptr(g), _ptr(img),
+                        _ptr(da), _ptr(de), ctypes.byref(rays))
+    if rc != 0:
+        raise ValueError("orc_pt64: bad triangle index")
+    return img, da, de
 
 
 class RefBvh:

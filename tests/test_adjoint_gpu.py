@@ -1,19 +1,28 @@
-"""Adjoint (path replay backpropagation) against central finite differences.
+"""Adjoint (path replay backpropagation) against central finite differences
+and against the float64 CPU gradient.
 
 The backward pass uses the forward pass's seed, so the gradient is that of
 the loss of this estimator with its random numbers held fixed (common random
 numbers).  Central differences of the same estimator along a random
-direction v must then match <grad, v>.  With max_depth <= 2 no Russian
-roulette decision exists and the only difference is float rounding: the bar
-is 2 % relative.  At the workload's depth 6, roulette probabilities depend on
-the albedo and are held fixed by the adjoint (unbiased in expectation); the
-bar there is statistical.
+direction v must then match <grad, v> within 2 %:
+  * at max_depth 2, where no Russian roulette decision exists;
+  * at the workload's depth 6 with roulette off (DORT_PT_NO_ROULETTE): a
+    roulette decision depends on the albedo, so under a perturbation a
+    decision can flip and its sample jump, which finite differences see and
+    the gradient (decisions held fixed, unbiased in expectation) does not;
+  * at the full workload size (500k triangles, 512 x 512, 64 spp, depth 6).
+With roulette on, the gradient is checked statistically (seed averages).
+
+The float64 CPU gradient (oracle/pt64.c: the same estimator on the same
+random numbers, each path term differentiated directly) must equal the GPU's
+path-replay gradient to 2 % in norm (with roulette on: the same decisions).
 """
 import numpy as np
 import pytest
 
 import dort_b200 as db
 from dort_b200 import scenes
+from oracle import pyoracle as po
 
 pytestmark = pytest.mark.gpu
 
@@ -112,3 +121,85 @@ def test_l2_loss(cuda):
     loss, g = db.loss_l2(a, b)
     np.testing.assert_allclose(loss, ((a.astype(np.float64) - b) ** 2).sum(), rtol=1e-6)
     np.testing.assert_allclose(g, 2 * (a - b), rtol=1e-6)
+
+
+@pytest.mark.parametrize("roulette", [True, False])
+def test_gradient_equals_the_float64_cpu_gradient(cuda, roulette):
+    w, spp, depth = 24, 8, 6
+    sd = scenes.adjoint_scene(n_tris=2000)
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], w, w, spp, max_depth=depth, seed=13, roulette=roulette)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    rng = np.random.default_rng(4)
+    target = rng.uniform(0.0, 0.3, (w, w, 3)).astype(np.float32)
+    img = sc.adjoint_forward(p, alb, em)
+    _, g = db.loss_l2(img, target)
+    da, de = sc.adjoint_backward(p, g, alb, em)
+    img64, da64, de64 = po.pt64(sd, w, w, spp, depth, 13, alb, em, dl_dimage=g,
+                                no_roulette=not roulette)
+    assert np.sqrt(((img - img64) ** 2).mean()) / img64.mean() < 1e-3
+    for got, want in ((da, da64), (de, de64)):
+        assert np.abs(want).sum() > 0
+        err = np.linalg.norm(got.astype(np.float64) - want) / np.linalg.norm(want)
+        assert err < 0.02, err
+    # the light gradients one by one
+    lights = sd["lights"]
+    np.testing.assert_allclose(de[lights], de64[lights], rtol=0.02,
+                               atol=0.02 * np.abs(de64[lights]).max())
+
+
+@pytest.mark.parametrize("which", ["albedo", "emission"])
+def test_directional_derivative_matches_fd_depth6_no_roulette(cuda, which):
+    sd, sc, p = _setup(n_tris=20000, w=48, spp=16, depth=6)
+    p = db.render_params(sd["camera"], 48, 48, 16, max_depth=6, seed=7, roulette=False)
+    alb0, em0 = sd["tri_albedo"], sd["tri_emission"]
+    rng = np.random.default_rng(8)
+    alb_t = np.clip(alb0 * rng.uniform(0.7, 1.3, alb0.shape), 0, 1).astype(np.float32)
+    target = sc.adjoint_forward(p, alb_t, em0)
+    loss, g, img = _loss(sc, p, alb0, em0, target)
+    da, de = sc.adjoint_backward(p, g, alb0, em0)
+    if which == "albedo":
+        v = rng.normal(size=alb0.shape).astype(np.float32) * (alb0 > 0)
+        h = 1e-2
+        lp = _loss(sc, p, (alb0 + h * v).astype(np.float32), em0, target)[0]
+        lm = _loss(sc, p, (alb0 - h * v).astype(np.float32), em0, target)[0]
+        analytic = float((da.astype(np.float64) * v).sum())
+    else:
+        v = np.zeros_like(em0)
+        v[sd["lights"]] = rng.normal(size=(len(sd["lights"]), 3))
+        h = 1e-1
+        lp = _loss(sc, p, alb0, (em0 + h * v).astype(np.float32), target)[0]
+        lm = _loss(sc, p, alb0, (em0 - h * v).astype(np.float32), target)[0]
+        analytic = float((de.astype(np.float64) * v).sum())
+    fd = (lp - lm) / (2 * h)
+    assert abs(fd) > 0
+    assert abs(analytic - fd) <= 0.02 * abs(fd), (analytic, fd)
+
+
+def test_workload_size_fd_no_roulette(cuda):
+    """The adjoint workload itself: 500k triangles, 512 x 512, 64 spp, depth 6."""
+    sd = scenes.adjoint_scene()
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], 512, 512, 64, max_depth=6, seed=1, roulette=False)
+    alb0, em0 = sd["tri_albedo"], sd["tri_emission"]
+    rng = np.random.default_rng(9)
+    target = sc.adjoint_forward(p, np.clip(alb0 * rng.uniform(0.8, 1.2, alb0.shape), 0, 1)
+                                .astype(np.float32), em0)
+    loss, g, img = _loss(sc, p, alb0, em0, target)
+    da, de = sc.adjoint_backward(p, g, alb0, em0)
+    assert np.isfinite(da).all() and np.isfinite(de).all()
+    v = rng.normal(size=alb0.shape).astype(np.float32) * (alb0 > 0)
+    h = 1e-2
+    lp = _loss(sc, p, (alb0 + h * v).astype(np.float32), em0, target)[0]
+    lm = _loss(sc, p, (alb0 - h * v).astype(np.float32), em0, target)[0]
+    fd = (lp - lm) / (2 * h)
+    analytic = float((da.astype(np.float64) * v).sum())
+    assert abs(analytic - fd) <= 0.02 * abs(fd), (analytic, fd)
+    ve = np.zeros_like(em0)
+    ve[sd["lights"]] = rng.normal(size=(len(sd["lights"]), 3))
+    h = 1e-1
+    lp = _loss(sc, p, alb0, (em0 + h * ve).astype(np.float32), target)[0]
+    lm = _loss(sc, p, alb0, (em0 - h * ve).astype(np.float32), target)[0]
+    fd = (lp - lm) / (2 * h)
+    analytic = float((de.astype(np.float64) * ve).sum())
+    assert abs(analytic - fd) <= 0.02 * abs(fd), (analytic, fd)
