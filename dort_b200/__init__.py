@@ -25,7 +25,7 @@ __all__ = ["Scene", "DortError", "MISS", "host_check_raycast", "scene_desc", "ch
 # optional scene-dict keys passed through to scene_desc
 SCENE_KEYS = ("tri_material", "materials", "tri_emission", "sky_rgb", "sky_const",
               "sky_scale", "sky_up", "sky_fwd", "shapes", "delta_lights", "tri_light_verts",
-              "bvh_build")
+              "bvh_build", "watertight")
 
 _BVH_BUILD = {None: _abi.BVH_BUILD_DEFAULT, "default": _abi.BVH_BUILD_DEFAULT,
               "host": _abi.BVH_BUILD_HOST, "device": _abi.BVH_BUILD_DEVICE,
@@ -55,14 +55,16 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
                sky_rgb=None, sky_const=(0.0, 0.0, 0.0), sky_scale=(0.0, 0.0, 0.0),
                sky_up=(0.0, 0.0, 0.0), sky_fwd=(0.0, 0.0, 0.0),
                bvh_width: int = 8, shapes=None, delta_lights=None, tri_light_verts=None,
-               bvh_build: str | None = None, **_ignored) -> _DescHolder:
+               bvh_build: str | None = None, watertight: bool = False,
+               **_ignored) -> _DescHolder:
     """SceneDesc for the arrays given.  `shapes`: dicts with kind (SHAPE_*),
     material, param (up to 4), to_world (3x4), emission (RGB) and optionally
     light_to_world (3x4); `delta_lights`: dicts with kind (LIGHT_POINT /
     LIGHT_DIRECTIONAL), rgb and vec; `bvh_build`: "host" (binned SAH on the
     host), "device" (the same on the device), "ploc" (Morton order + PLOC on
     the device: fastest build, slower traversal) or None (the library's
-    default, "device")."""
+    default, "device"); `watertight`: hits by the watertight ray/triangle test
+    (DORT_SCENE_WATERTIGHT) instead of the reference's Moller-Trumbore."""
     h = _DescHolder()
     d = h.desc
     verts = np.ascontiguousarray(verts, np.float32).reshape(-1, 3)
@@ -98,6 +100,7 @@ def scene_desc(verts, tris, tri_material=None, materials=None, tri_emission=None
     if bvh_build not in _BVH_BUILD:
         raise ValueError(f"bvh_build must be one of {sorted(k for k in _BVH_BUILD if k)}")
     d.bvh_build = _BVH_BUILD[bvh_build]
+    d.flags = _abi.SCENE_WATERTIGHT if watertight else 0
     if shapes:
         arr = (_abi.Shape * len(shapes))()
         for i, sh in enumerate(shapes):
@@ -424,9 +427,10 @@ def check_device_bvh(verts, tris, bvh_width: int = 8, bvh_build: str | None = No
             "iterations": int(out[5]), "depth": int(out[6]), "sah": out[7]}
 
 
-def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8):
+def host_check_raycast(verts, tris, rays, any_hit: bool = False, bvh_width: int = 8,
+                       watertight: bool = False):
     """Runs the device traversal code compiled for the host (diagnostic)."""
-    h = scene_desc(verts, tris, bvh_width=bvh_width)
+    h = scene_desc(verts, tris, bvh_width=bvh_width, watertight=watertight)
     rays = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
     n = len(rays)
     prim = np.zeros(n, np.uint32)

@@ -35,6 +35,7 @@ BVH_BUILD_DEFAULT, BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_PLOC = 0, 1, 2, 3
 RENDERER_PT, RENDERER_LT, RENDERER_BDPT = 0, 1, 2
 BDPT_NO_T1_PATHS = 1
 PT_NO_ROULETTE = 2
+SCENE_WATERTIGHT = 1
 ABI_VERSION = 2
 
 
@@ -73,7 +74,8 @@ class SceneDesc(ctypes.Structure):
         ("light_count", c_u32),
         ("bvh_build", c_u32),
         ("tri_light_verts", c_p),
-        ("reserved", c_u32 * 2),
+        ("flags", c_u32),
+        ("reserved", c_u32 * 1),
     ]
 
 

@@ -411,7 +411,9 @@ DG_HD Hit trace_shapes(const PtScene& sc, V3 o, float t_min, V3 d,
 // its index and b1 = the cube face.
 template<bool ANY_HIT, bool G>
 DG_HD Hit scene_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
-  Hit h = trace_ray<ANY_HIT, false>(sc.trace, o.x, o.y, o.z, t_min, d.x, d.y, d.z, t_max);
+  // the general instantiation also serves scenes built watertight
+  Hit h = trace_ray<ANY_HIT, false, G ? kTriByScene : kTriMt>(sc.trace, o.x, o.y, o.z, t_min,
+                                                             d.x, d.y, d.z, t_max);
   if(!G || sc.shape_count == 0 || (ANY_HIT && h.prim != kMiss)) { return h; }
   return trace_shapes<ANY_HIT>(sc, o, t_min, d, t_max, h);
 }

@@ -14,6 +14,7 @@ struct TraceScene {
   const float4* tris;   // 3 x float4 per LeafTri
   uint32_t node_count;
   uint32_t tri_count;
+  uint32_t watertight;  // leaf triangles hold (p0, p1, p2) for the watertight test
 };
 
 // BxDF flag bits as the reference's BxdfFlags (include/dort/bsdf.hpp:8-28).
@@ -126,7 +127,7 @@ enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1, RENDERER_BDPT = 2 };
 // Whether rendering `sc` with `pp` needs the general instantiation of the
 // path code (pt.cuh, template flag G).
 inline bool scene_needs_general(const PtScene& sc, const PtParams& pp) {
-  return sc.general != 0 || pp.camera != CAMERA_PINHOLE;
+  return sc.general != 0 || pp.camera != CAMERA_PINHOLE || sc.trace.watertight != 0;
 }
 
 }  // namespace dort_gpu

@@ -15,7 +15,7 @@ namespace dort_gpu {
 
 constexpr int kRaycastBlock = 128;
 
-template<bool ANY_HIT>
+template<bool ANY_HIT, int WT = kTriMt>
 __global__ void __launch_bounds__(kRaycastBlock)
 raycast_kernel(TraceScene sc, const float4* __restrict__ rays, uint32_t ray_count,
                uint32_t* __restrict__ out_prim, float* __restrict__ out_tb,
@@ -30,7 +30,7 @@ raycast_kernel(TraceScene sc, const float4* __restrict__ rays, uint32_t ray_coun
     if(i < ray_count) {
       float4 r0 = __ldcs(rays + 2 * size_t(i));
       float4 r1 = __ldcs(rays + 2 * size_t(i) + 1);
-      Hit h = trace_ray<ANY_HIT>(sc, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w);
+      Hit h = trace_ray<ANY_HIT, true, WT>(sc, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w);
       if(ANY_HIT) {
         out_prim[i] = h.prim != kMiss ? 1u : 0u;
       } else {
@@ -65,13 +65,23 @@ int launch_raycast(dort_scene* s, const float* d_rays, size_t n, int any_hit,
   int drc = require_scene_device(s);
   if(drc != DORT_OK) { return drc; }
   DG_CUDA(cudaMemsetAsync(s->d_work, 0, sizeof(uint32_t), stream));
-  const void* kfn = any_hit ? reinterpret_cast<const void*>(&raycast_kernel<true>)
-                            : reinterpret_cast<const void*>(&raycast_kernel<false>);
-  static int blocks_any = 0, blocks_closest = 0;
-  int& blocks = any_hit ? blocks_any : blocks_closest;
+  const bool wt = s->trace.watertight != 0;
+  const void* kfn =
+      wt ? (any_hit ? reinterpret_cast<const void*>(&raycast_kernel<true, kTriWatertight>)
+                    : reinterpret_cast<const void*>(&raycast_kernel<false, kTriWatertight>))
+         : (any_hit ? reinterpret_cast<const void*>(&raycast_kernel<true>)
+                    : reinterpret_cast<const void*>(&raycast_kernel<false>));
+  static int blocks_cache[4] = {0, 0, 0, 0};
+  int& blocks = blocks_cache[(wt ? 2 : 0) + (any_hit ? 1 : 0)];
   if(blocks == 0) { blocks = persistent_blocks(kfn, kRaycastBlock); }
   const float4* r4 = reinterpret_cast<const float4*>(d_rays);
-  if(any_hit) {
+  if(wt && any_hit) {
+    raycast_kernel<true, kTriWatertight><<<blocks, kRaycastBlock, 0, stream>>>(
+        s->trace, r4, uint32_t(n), d_prim, d_tb, s->d_work);
+  } else if(wt) {
+    raycast_kernel<false, kTriWatertight><<<blocks, kRaycastBlock, 0, stream>>>(
+        s->trace, r4, uint32_t(n), d_prim, d_tb, s->d_work);
+  } else if(any_hit) {
     raycast_kernel<true><<<blocks, kRaycastBlock, 0, stream>>>(
         s->trace, r4, uint32_t(n), d_prim, d_tb, s->d_work);
   } else {

@@ -1,4 +1,5 @@
 // Scene creation / destruction and the error plumbing of the C ABI.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <new>
@@ -160,6 +161,22 @@ static int device_bvh(dort_scene* s, const dort_scene_desc* desc) {
   return DORT_OK;
 }
 
+// Watertight scenes: each leaf triangle's (p0, e1, e2) becomes its three
+// input vertices (p0, p1, p2), taken from the shading records (by original
+// triangle index), so that triangles sharing an edge hold identical
+// coordinates for it.
+__global__ void leaf_tris_to_vertices(float4* tris, uint32_t count, const float4* shade) {
+  for(uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    float4 a = tris[3 * size_t(i)];
+    uint32_t id = __float_as_uint(a.w);
+    float4 p0 = shade[3 * size_t(id)], p1 = shade[3 * size_t(id) + 1];
+    float4 p2 = shade[3 * size_t(id) + 2];
+    tris[3 * size_t(i)] = make_float4(p0.x, p0.y, p0.z, a.w);
+    tris[3 * size_t(i) + 1] = make_float4(p1.x, p1.y, p1.z, 0.f);
+    tris[3 * size_t(i) + 2] = make_float4(p2.x, p2.y, p2.z, 0.f);
+  }
+}
+
 static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostScene& hs) {
   int rc;
   if(hs.device_bvh) {
@@ -182,8 +199,17 @@ static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostSc
 
   PtScene& pt = s->pt;
   std::memset(&pt, 0, sizeof(pt));
-  pt.trace = s->trace;
   if((rc = upload(s, hs.shade, &pt.shade)) != DORT_OK) { return rc; }
+  if(desc->flags & DORT_SCENE_WATERTIGHT) {
+    if(s->trace.tri_count) {
+      leaf_tris_to_vertices<<<std::min<uint32_t>((s->trace.tri_count + 255) / 256, 4096), 256>>>(
+          const_cast<float4*>(s->trace.tris), s->trace.tri_count, pt.shade);
+      DG_CUDA(cudaGetLastError());
+      DG_CUDA(cudaDeviceSynchronize());
+    }
+    s->trace.watertight = 1;
+  }
+  pt.trace = s->trace;
   if((rc = upload(s, hs.mats, &pt.mats)) != DORT_OK) { return rc; }
   pt.mat_count = uint32_t(hs.mats.size());
   if((rc = upload(s, hs.lights, &pt.lights)) != DORT_OK) { return rc; }

@@ -180,6 +180,10 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
     err = "dort_scene_desc.struct_size mismatch (ABI version)";
     return false;
   }
+  if(desc->flags & ~DORT_SCENE_WATERTIGHT) {
+    err = "unknown dort_scene_desc.flags bits";
+    return false;
+  }
   uint32_t n = desc->tri_count;
   if(n > 0 && (!desc->verts || !desc->tris)) {
     err = "verts and tris are required when tri_count > 0";

@@ -7,8 +7,9 @@
 // (triangle.cpp:14-46, 102-134).
 //
 // Traversal: node groups (base index, 8 child-hit bits << 24 | internal-slot
-// mask) on a per-thread stack; child slots are visited in an order fixed by
-// the ray octant (slot bit index XOR octant), so no per-node sort is needed.
+// mask) on a per-thread stack whose first entries sit in shared memory; child
+// slots are visited in an order fixed by the ray octant (slot bit index XOR
+// octant), so no per-node sort is needed.
 // Child boxes are tested with fused multiply-adds on the quantized planes and
 // a relative widening of 2^-20 that covers the rounding of that arithmetic;
 // together with the one-step quantization margin the test never culls a box
@@ -138,6 +139,77 @@ DG_HD bool mt_fast(float4 a, float4 e1, float4 e2, float ox, float oy, float oz,
   return true;
 }
 
+// Watertight ray/triangle test: Woop, Benthin and Wald, "Watertight
+// Ray/Triangle Intersection", JCGT 2(1), 2013.  The ray's dominant axis
+// becomes z and a shear maps the ray onto the z axis; the triangle's edge
+// functions U, V, W are then 2-D cross products of the sheared vertices.  An
+// edge shared by two triangles gets the same operands in both, so its
+// function is computed identically (exactly negated) in both and a ray can
+// pass through neither: no leak at edges or vertices.  Products and
+// differences are rounded separately (no contraction) so that the negation
+// is exact; an edge function that comes out exactly zero is recomputed in
+// double.  Barycentrics: b1 = V / det (weight of p1), b2 = W / det (p2).
+struct WtRay {
+  uint32_t kx, ky, kz;   // dominant axis kz; kx, ky keep the winding
+  float sx, sy, sz;      // shear: d[kx] / d[kz], d[ky] / d[kz], 1 / d[kz]
+};
+
+DG_HD float wt_sel(float x, float y, float z, uint32_t k) {
+  return k == 0 ? x : (k == 1 ? y : z);
+}
+
+DG_HD WtRay wt_setup(float dx, float dy, float dz) {
+  WtRay r;
+  float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+  r.kz = ax > ay ? (ax > az ? 0u : 2u) : (ay > az ? 1u : 2u);
+  r.kx = r.kz == 2u ? 0u : r.kz + 1u;
+  r.ky = r.kx == 2u ? 0u : r.kx + 1u;
+  float dk = wt_sel(dx, dy, dz, r.kz);
+  if(dk < 0.f) { uint32_t t = r.kx; r.kx = r.ky; r.ky = t; }
+  r.sx = wt_sel(dx, dy, dz, r.kx) / dk;
+  r.sy = wt_sel(dx, dy, dz, r.ky) / dk;
+  r.sz = 1.f / dk;
+  return r;
+}
+
+DG_HD bool wt_hit(const WtRay& r, float4 p0, float4 p1, float4 p2, float ox, float oy, float oz,
+                  float t_min, float t_max, float& out_t, float& out_b1, float& out_b2) {
+  // vertices relative to the origin, permuted (kx, ky, kz)
+  float ax = DG_SUB(wt_sel(p0.x, p0.y, p0.z, r.kx), wt_sel(ox, oy, oz, r.kx));
+  float ay = DG_SUB(wt_sel(p0.x, p0.y, p0.z, r.ky), wt_sel(ox, oy, oz, r.ky));
+  float az = DG_SUB(wt_sel(p0.x, p0.y, p0.z, r.kz), wt_sel(ox, oy, oz, r.kz));
+  float bx = DG_SUB(wt_sel(p1.x, p1.y, p1.z, r.kx), wt_sel(ox, oy, oz, r.kx));
+  float by = DG_SUB(wt_sel(p1.x, p1.y, p1.z, r.ky), wt_sel(ox, oy, oz, r.ky));
+  float bz = DG_SUB(wt_sel(p1.x, p1.y, p1.z, r.kz), wt_sel(ox, oy, oz, r.kz));
+  float cx = DG_SUB(wt_sel(p2.x, p2.y, p2.z, r.kx), wt_sel(ox, oy, oz, r.kx));
+  float cy = DG_SUB(wt_sel(p2.x, p2.y, p2.z, r.ky), wt_sel(ox, oy, oz, r.ky));
+  float cz = DG_SUB(wt_sel(p2.x, p2.y, p2.z, r.kz), wt_sel(ox, oy, oz, r.kz));
+  // shear into the ray's frame
+  float Ax = DG_SUB(ax, DG_MUL(r.sx, az)), Ay = DG_SUB(ay, DG_MUL(r.sy, az));
+  float Bx = DG_SUB(bx, DG_MUL(r.sx, bz)), By = DG_SUB(by, DG_MUL(r.sy, bz));
+  float Cx = DG_SUB(cx, DG_MUL(r.sx, cz)), Cy = DG_SUB(cy, DG_MUL(r.sy, cz));
+  float U = DG_SUB(DG_MUL(Cx, By), DG_MUL(Cy, Bx));
+  float V = DG_SUB(DG_MUL(Ax, Cy), DG_MUL(Ay, Cx));
+  float W = DG_SUB(DG_MUL(Bx, Ay), DG_MUL(By, Ax));
+  if(U == 0.f || V == 0.f || W == 0.f) {
+    U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+    V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+    W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+  }
+  if((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) { return false; }
+  float det = DG_ADD(DG_ADD(U, V), W);
+  if(det == 0.f) { return false; }
+  float T = DG_ADD(DG_ADD(DG_MUL(U, DG_MUL(r.sz, az)), DG_MUL(V, DG_MUL(r.sz, bz))),
+                   DG_MUL(W, DG_MUL(r.sz, cz)));
+  float inv = DG_RCP(det);
+  float t = DG_MUL(T, inv);
+  if(!(t >= t_min && t <= t_max)) { return false; }
+  out_t = t;
+  out_b1 = DG_MUL(V, inv);
+  out_b2 = DG_MUL(W, inv);
+  return true;
+}
+
 DG_HD float byte_to_float(uint32_t w, int j) {
   return DG_BYTE_F(w, j);
 }
@@ -260,6 +332,7 @@ struct TravState {
   float nox, noy, noz;   // -o * inv: one FMA per plane
 #endif
   uint32_t oct_inv, oct_inv4;
+  WtRay wt;              // the watertight test's ray frame (WT traversals)
   uint2 group;           // current node group: (base, child-hit bits << 24 | internal mask)
   int sp;                // entries on the caller's stack
   Hit best;              // closest hit so far (best.t = t_max while none)
@@ -284,20 +357,77 @@ DG_HD void trav_init(TravState& s, const TraceScene& sc, float ox, float oy, flo
   s.noy = -oy * s.iy;
   s.noz = -oz * s.iz;
 #endif
+  s.wt = wt_setup(dx, dy, dz);
   s.sp = 0;
   // root group: internal bit 31 with an empty internal-slot mask -> node 0;
   // an empty tree starts finished
   s.group = make_uint2(0u, sc.node_count ? 0x80000000u : 0u);
 }
 
+// Traversal stacks.  A node group is pushed per level descended, so a ray's
+// stack holds at most the tree's depth (<= kTraceStack) entries; the trees
+// of the benchmark scenes are 8 levels deep.
+//
+// ShortStack (device, the default): the first kShortStack entries of every
+// thread sit in shared memory, one column per thread (entry k of thread t at
+// k * kShortStackThreads + t: a warp's 8-byte accesses fall in distinct
+// banks whatever depth each lane is at), deeper entries in local memory.
+// Pushes and pops then leave the L1 data cache to the node and triangle
+// fetches.  Blocks wider than kShortStackThreads keep the whole stack in
+// local memory.  Built with DORT_LOCAL_STACK, every entry is in local memory
+// (LocalStack).
+struct LocalStack {
+  uint2 e[kTraceStack];
+  DG_HD void init() {}
+  DG_HD void push(int sp, uint2 v) { e[sp] = v; }
+  DG_HD uint2 pop(int sp) { return e[sp]; }
+};
+
+#if defined(__CUDA_ARCH__) && !defined(DORT_LOCAL_STACK)
+constexpr int kShortStack = 8;
+constexpr int kShortStackThreads = 128;
+
+// One array per block for every traversal of the kernel (a thread runs one
+// traversal at a time).
+__device__ __forceinline__ uint2* short_stack_block() {
+  __shared__ uint2 s[kShortStack * kShortStackThreads];
+  return s;
+}
+
+struct ShortStack {
+  uint32_t col;        // this thread's column in the block's array
+  int lim;             // entries below lim live in shared memory (0: none)
+  uint2 deep[kTraceStack];
+  __device__ __forceinline__ void init() {
+    const uint32_t nt = blockDim.x * blockDim.y * blockDim.z;
+    col = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    lim = nt <= kShortStackThreads ? kShortStack : 0;
+  }
+  __device__ __forceinline__ void push(int sp, uint2 v) {
+    if(sp < lim) { short_stack_block()[sp * kShortStackThreads + col] = v; } else { deep[sp] = v; }
+  }
+  __device__ __forceinline__ uint2 pop(int sp) {
+    return sp < lim ? short_stack_block()[sp * kShortStackThreads + col] : deep[sp];
+  }
+};
+using TraceStack = ShortStack;
+#else
+using TraceStack = LocalStack;
+#endif
+
+// Triangle tests of a traversal (WT): kTriMt = Moller-Trumbore on the leaf
+// layout (p0, e1, e2), kTriWatertight = wt_hit on the layout (p0, p1, p2) of
+// scenes built watertight, kTriByScene = whichever the scene was built for
+// (TraceScene::watertight).
+enum : int { kTriMt = 0, kTriWatertight = 1, kTriByScene = 2 };
+
 // One traversal step; returns true when the ray is finished (s.best holds
 // the closest hit, or for ANY_HIT the first hit found, or prim = kMiss).
-// `stack` has kTraceStack entries.
-template<bool ANY_HIT, bool EXACT_MT>
-DG_HD bool trav_step(TravState& s, const TraceScene& sc, uint2* stack) {
+template<bool ANY_HIT, bool EXACT_MT, class Stack, int WT = kTriMt>
+DG_HD bool trav_step(TravState& s, const TraceScene& sc, Stack& stack) {
   if((s.group.y & 0xff000000u) == 0u) {
     if(s.sp == 0) { return true; }
-    s.group = stack[--s.sp];
+    s.group = stack.pop(--s.sp);
   }
   uint32_t bit = 31u - DG_CLZ(s.group.y & 0xff000000u);
   s.group.y &= ~(1u << bit);
@@ -324,7 +454,7 @@ DG_HD bool trav_step(TravState& s, const TraceScene& sc, uint2* stack) {
     if(s.group.y & 0xff000000u) {
       // sp < kTraceStack: each push descends one level and the builder
       // bounds the depth by kMaxWideDepth.
-      stack[s.sp++] = s.group;
+      stack.push(s.sp++, s.group);
     }
     s.group = make_uint2(child_base, child_hits | imask);
   }
@@ -336,9 +466,14 @@ DG_HD bool trav_step(TravState& s, const TraceScene& sc, uint2* stack) {
     const float4* tp = sc.tris + 3 * size_t(tri_base + b);
     float4 a = DG_LDG(tp), e1 = DG_LDG(tp + 1), e2 = DG_LDG(tp + 2);
     float t, b1, b2;
-    bool h = EXACT_MT
-        ? mt_exact(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2)
-        : mt_fast(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2);
+    bool h;
+    if(WT == kTriWatertight || (WT == kTriByScene && sc.watertight)) {
+      h = wt_hit(s.wt, a, e1, e2, s.ox, s.oy, s.oz, s.t_min, s.best.t, t, b1, b2);
+    } else {
+      h = EXACT_MT
+          ? mt_exact(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2)
+          : mt_fast(a, e1, e2, s.ox, s.oy, s.oz, s.dx, s.dy, s.dz, s.t_min, s.best.t, t, b1, b2);
+    }
     if(h) {
       uint32_t id = DG_AS_UINT(a.w);
       if(ANY_HIT) {
@@ -356,13 +491,14 @@ DG_HD bool trav_step(TravState& s, const TraceScene& sc, uint2* stack) {
 // Closest hit (ANY_HIT = false) or any hit (ANY_HIT = true) of one ray.
 // Returns the hit with prim = kMiss on a miss.  For any hit, prim = the first
 // triangle found to intersect.
-template<bool ANY_HIT, bool EXACT_MT = true>
+template<bool ANY_HIT, bool EXACT_MT = true, int WT = kTriMt>
 DG_HD Hit trace_ray(const TraceScene& sc, float ox, float oy, float oz, float t_min,
                     float dx, float dy, float dz, float t_max) {
   TravState s;
   trav_init(s, sc, ox, oy, oz, t_min, dx, dy, dz, t_max);
-  uint2 stack[kTraceStack];
-  while(!trav_step<ANY_HIT, EXACT_MT>(s, sc, stack)) {}
+  TraceStack stack;
+  stack.init();
+  while(!trav_step<ANY_HIT, EXACT_MT, TraceStack, WT>(s, sc, stack)) {}
   return s.best;
 }
 

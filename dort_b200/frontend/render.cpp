@@ -1,6 +1,7 @@
 // Rendering and images in the Lua front-end: dort.render (lua_render.cpp:
 // make / render_sync / get_image over the C ABI's wavefront and per-pixel
-// renderers), dort.image (lua_image.cpp: Radiance HDR read / write, PNG
+// renderers; the adjoint pair, which the reference does not have, beside
+// them), dort.image (lua_image.cpp: Radiance HDR read / write, PNG
 // write, the tone maps, bias_variance and the reference's image test
 // test_convergence), and the small modules dort.sampler, dort.filter,
 // dort.chrono, dort.stats and dort.env.
@@ -221,6 +222,59 @@ static int image_write_rgbe(lua_State* l) {
   return 0;
 }
 
+// Portable float map (PF, little-endian, bottom row first): signed floats,
+// for images that are gradients rather than radiance (the adjoint's).
+static bool write_pfm_file(const char* path, const Image& img) {
+  std::FILE* f = std::fopen(path, "wb");
+  if(!f) { return false; }
+  std::fprintf(f, "PF\n%u %u\n-1.0\n", img.w, img.h);
+  for(uint32_t y = img.h; y-- > 0;) {
+    std::fwrite(&img.px[3 * size_t(y) * img.w], sizeof(float), 3 * size_t(img.w), f);
+  }
+  return std::fclose(f) == 0;
+}
+
+static int image_write_pfm(lua_State* l) {
+  const char* path = luaL_checkstring(l, 1);
+  auto img = check_image_kind(l, 2, true);
+  if(!write_pfm_file(path, *img)) { return luaL_error(l, "Could not open file for writing: %s", path); }
+  return 0;
+}
+
+static std::shared_ptr<Image> new_hdr_image(uint32_t w, uint32_t h) {
+  auto img = std::make_shared<Image>();
+  img->w = w;
+  img->h = h;
+  img->hdr = true;
+  img->px.assign(size_t(w) * h * 3, 0.f);
+  return img;
+}
+
+// a * x + y over two HDR images of one size (a gradient step)
+static int image_axpy(lua_State* l) {
+  float a = float(luaL_checknumber(l, 1));
+  auto x = check_image_kind(l, 2, true);
+  auto y = check_image_kind(l, 3, true);
+  if(x->w != y->w || x->h != y->h) { return luaL_error(l, "axpy: images of different sizes"); }
+  auto out = new_hdr_image(x->w, x->h);
+  for(size_t i = 0; i < out->px.size(); ++i) { out->px[i] = a * x->px[i] + y->px[i]; }
+  push_image(l, out);
+  return 1;
+}
+
+// every channel clamped to [lo, hi]
+static int image_clamp(lua_State* l) {
+  auto x = check_image_kind(l, 1, true);
+  float lo = float(luaL_checknumber(l, 2)), hi = float(luaL_checknumber(l, 3));
+  auto out = new_hdr_image(x->w, x->h);
+  for(size_t i = 0; i < out->px.size(); ++i) {
+    float v = x->px[i];
+    out->px[i] = v < lo ? lo : (v > hi ? hi : v);
+  }
+  push_image(l, out);
+  return 1;
+}
+
 template<class F>
 static std::shared_ptr<Image> map_channels(const Image& in, F f) {
   auto out = std::make_shared<Image>();
@@ -373,7 +427,8 @@ int open_image(lua_State* l) {
       {"read", image_read}, {"write_png", image_write_png}, {"write_rgbe", image_write_rgbe},
       {"tonemap_srgb", image_tonemap_srgb}, {"tonemap_gamma", image_tonemap_gamma},
       {"get_res", image_get_res}, {"bias_variance", image_bias_variance},
-      {"test_convergence", image_test_convergence}, {nullptr, nullptr}};
+      {"test_convergence", image_test_convergence}, {"write_pfm", image_write_pfm},
+      {"axpy", image_axpy}, {"clamp", image_clamp}, {nullptr, nullptr}};
   luaL_newlib(l, funs);
   return 1;
 }
@@ -494,6 +549,8 @@ static int render_make(lua_State* l) {
     else if(st == "bsdf") { rp.direct_strategy = DORT_DIRECT_BSDF; }
     else if(st == "light") { rp.direct_strategy = DORT_DIRECT_LIGHT; }
     else { return luaL_error(l, "Unknown direct strategy '%s'", st.c_str()); }
+    // not a reference parameter: off for derivative checks (DORT_PT_NO_ROULETTE)
+    if(!param_bool_opt(l, p, "roulette", true)) { rp.renderer_flags |= DORT_PT_NO_ROULETTE; }
   } else if(method == "lt" || method == "light") {
     // lua_render.cpp:146-150: path lengths min_depth + 2 .. max_depth + 2
     rp.renderer = DORT_RENDERER_LT;
@@ -569,6 +626,124 @@ static int render_get_image(lua_State* l) {
   return 1;
 }
 
+// ---- the adjoint (no reference counterpart) ----------------------------------------------
+//
+// Gradients of an image loss with respect to per-triangle Lambert albedo and
+// emitted radiance (dort_gpu_adjoint_forward / _backward).  Per-triangle
+// values travel as HDR images of tri_count x 1 pixels, in the order the scene
+// flattened its triangles.
+//   dort.render.triangle_params(scene)          -> albedo, emission
+//   dort.render.adjoint_forward(job, {albedo =, emission =})   -> image
+//   dort.render.adjoint_backward(job, {dl_dimage =, albedo =, emission =})
+//                                                -> d_albedo, d_emission
+//   dort.render.loss_l2(image, target)          -> loss, dloss_dimage
+// Without `emission`, the backward pass differentiates at the emission the
+// scene was built with.
+
+static uint32_t scene_tri_count(const Scene& sc) { return uint32_t(sc.flat.tris.size() / 3); }
+
+static bool scene_has_emitters(const Scene& sc) {
+  for(float v : sc.flat.tri_emission) {
+    if(v != 0.f) { return true; }
+  }
+  return false;
+}
+
+static const float* tri_image(lua_State* l, int p, const char* key, const Scene& sc,
+                              std::shared_ptr<Image>& keep) {
+  if(!param_take(l, p, key)) { return nullptr; }
+  keep = check_image_kind(l, -1, true);
+  lua_pop(l, 1);
+  if(keep->w != scene_tri_count(sc) || keep->h != 1) {
+    luaL_error(l, "%s must be a %u x 1 image (one pixel per triangle)", key, scene_tri_count(sc));
+  }
+  return keep->px.data();
+}
+
+static int render_triangle_params(lua_State* l) {
+  auto scene = check_shared<Scene>(l, 1, SCENE_T);
+  const FlatScene& f = scene->flat;
+  uint32_t n = scene_tri_count(*scene);
+  auto alb = new_hdr_image(n, 1), em = new_hdr_image(n, 1);
+  for(uint32_t t = 0; t < n && !f.materials.empty(); ++t) {
+    const dort_material& m = f.materials[f.tri_material.empty() ? 0 : f.tri_material[t]];
+    if(m.kind == DORT_MAT_LAMBERT) {
+      for(int c = 0; c < 3; ++c) { alb->px[3 * size_t(t) + c] = m.color[c]; }
+    }
+  }
+  for(size_t i = 0; i < f.tri_emission.size() && i < em->px.size(); ++i) {
+    em->px[i] = f.tri_emission[i];
+  }
+  push_image(l, alb);
+  push_image(l, em);
+  return 2;
+}
+
+static std::shared_ptr<RenderJob> check_adjoint_job(lua_State* l, int idx) {
+  auto job = check_shared<RenderJob>(l, idx, JOB_T);
+  if(job->params.renderer != DORT_RENDERER_PT) {
+    luaL_error(l, "the adjoint differentiates the \"pt\" renderer only");
+  }
+  if(!job->scene->handle) { luaL_error(l, "the adjoint needs a GPU (record mode has none)"); }
+  return job;
+}
+
+static int render_adjoint_forward(lua_State* l) {
+  auto job = check_adjoint_job(l, 1);
+  int p = params_index(l, 2);
+  std::shared_ptr<Image> ka, ke;
+  const float* alb = tri_image(l, p, "albedo", *job->scene, ka);
+  const float* em = tri_image(l, p, "emission", *job->scene, ke);
+  params_check_unused(l, p);
+  auto img = new_hdr_image(job->params.width, job->params.height);
+  if(dort_gpu_adjoint_forward(job->scene->handle, &job->params, alb, em, img->px.data()) !=
+     DORT_OK) {
+    return luaL_error(l, "%s", dort_gpu_last_error());
+  }
+  push_image(l, img);
+  return 1;
+}
+
+static int render_adjoint_backward(lua_State* l) {
+  auto job = check_adjoint_job(l, 1);
+  int p = params_index(l, 2);
+  if(!param_take(l, p, "dl_dimage")) { return luaL_error(l, "dl_dimage is required"); }
+  auto g = check_image_kind(l, -1, true);
+  lua_pop(l, 1);
+  if(g->w != job->params.width || g->h != job->params.height) {
+    return luaL_error(l, "dl_dimage must have the render's size");
+  }
+  std::shared_ptr<Image> ka, ke;
+  const float* alb = tri_image(l, p, "albedo", *job->scene, ka);
+  const float* em = tri_image(l, p, "emission", *job->scene, ke);
+  params_check_unused(l, p);
+  const bool lights = scene_has_emitters(*job->scene);
+  if(!em && lights) { em = job->scene->flat.tri_emission.data(); }
+  uint32_t n = scene_tri_count(*job->scene);
+  auto da = new_hdr_image(n, 1), de = new_hdr_image(n, 1);
+  if(dort_gpu_adjoint_backward(job->scene->handle, &job->params, alb, em, g->px.data(),
+                               da->px.data(), lights ? de->px.data() : nullptr) != DORT_OK) {
+    return luaL_error(l, "%s", dort_gpu_last_error());
+  }
+  push_image(l, da);
+  push_image(l, de);
+  return 2;
+}
+
+static int render_loss_l2(lua_State* l) {
+  auto a = check_image_kind(l, 1, true);
+  auto b = check_image_kind(l, 2, true);
+  if(a->w != b->w || a->h != b->h) { return luaL_error(l, "loss_l2: images of different sizes"); }
+  auto g = new_hdr_image(a->w, a->h);
+  double loss = 0.0;
+  if(dort_gpu_loss_l2(a->px.data(), b->px.data(), a->px.size(), &loss, g->px.data()) != DORT_OK) {
+    return luaL_error(l, "%s", dort_gpu_last_error());
+  }
+  lua_pushnumber(l, loss);
+  push_image(l, g);
+  return 2;
+}
+
 static int render_unsupported(lua_State* l) {
   return luaL_error(l, "asynchronous rendering and previews need a GUI and are not supported");
 }
@@ -580,7 +755,9 @@ int open_render(lua_State* l) {
       {"make", render_make}, {"render_sync", render_sync}, {"get_image", render_get_image},
       {"render_async", render_unsupported}, {"image_to_pixbuf", render_unsupported},
       {"cancel", render_unsupported}, {"get_preview", render_unsupported},
-      {"get_progress", render_unsupported}, {nullptr, nullptr}};
+      {"get_progress", render_unsupported}, {"triangle_params", render_triangle_params},
+      {"adjoint_forward", render_adjoint_forward}, {"adjoint_backward", render_adjoint_backward},
+      {"loss_l2", render_loss_l2}, {nullptr, nullptr}};
   luaL_newlib(l, funs);
   return 1;
 }

@@ -118,3 +118,30 @@ def write_png(path: str, img) -> None:
         f.write(chunk(b"IHDR", struct.pack(">IIBBBBB", w, h, 8, 2, 0, 0, 0)))
         f.write(chunk(b"IDAT", zlib.compress(raw, 6)))
         f.write(chunk(b"IEND", b""))
+
+
+def write_pfm(path: str, img) -> None:
+    """Portable float map (little-endian, bottom row first): signed float RGB,
+    the format the Lua front-end's dort.image.write_pfm writes."""
+    a = np.asarray(img, np.float32)
+    h, w = a.shape[:2]
+    with open(path, "wb") as f:
+        f.write(b"PF\n%d %d\n-1.0\n" % (w, h))
+        f.write(np.ascontiguousarray(a[::-1]).astype("<f4").tobytes())
+
+
+def read_pfm(path: str) -> np.ndarray:
+    """Portable float map -> float RGB [h, w, 3] (row 0 at the top)."""
+    data = open(path, "rb").read()
+    lines, pos = [], 0
+    while len(lines) < 3:
+        end = data.index(b"\n", pos)
+        lines.append(data[pos:end].strip())
+        pos = end + 1
+    if lines[0] != b"PF":
+        raise ValueError(f"{path}: not an RGB portable float map")
+    w, h = (int(x) for x in lines[1].split())
+    scale = float(lines[2])
+    dt = "<f4" if scale < 0 else ">f4"
+    a = np.frombuffer(data, dt, 3 * w * h, pos).reshape(h, w, 3)
+    return a[::-1].astype(np.float32)

@@ -211,8 +211,20 @@ typedef struct dort_scene_desc {
   uint32_t light_count;
   uint32_t bvh_build;              /* DORT_BVH_BUILD_* */
   const float* tri_light_verts;    /* tri_count * 9, or NULL: see below */
-  uint32_t reserved[2];
+  uint32_t flags;                  /* DORT_SCENE_* */
+  uint32_t reserved[1];
 } dort_scene_desc;
+
+/* dort_scene_desc.flags
+ * DORT_SCENE_WATERTIGHT: ray/triangle hits by the watertight test of Woop,
+ * Benthin and Wald (JCGT 2013) instead of the reference's Moller-Trumbore
+ * (triangle.cpp:14-46, 102-134): a ray through an edge or a vertex shared by
+ * triangles hits one of them, never slips between them.  Off by default (the
+ * reference's arithmetic, bit-exact t / b1 / b2).  Hits away from edges are
+ * the same triangles; t, b1, b2 agree to float rounding.  The leaf triangles
+ * then store their three vertices; the path tracers use their general
+ * instantiation for such scenes. */
+#define DORT_SCENE_WATERTIGHT 1u
 
 typedef struct dort_scene dort_scene;
 

@@ -254,3 +254,125 @@ def test_frontend_bdpt_debug_images_are_refused(tmp_path):
                          capture_output=True, text=True, timeout=120)
     assert out.returncode == 1
     assert "debug_image_dir" in out.stderr
+
+
+ADJOINT_LUA = r'''
+local _ENV = require "dort/dsl"
+local scene = define_scene(function()
+  material(lambert_material { albedo = rgb(0.7, 0.6, 0.5) })
+  local floor = mesh {
+    points = { point(-4, 0, -4), point(4, 0, -4), point(4, 0, 4), point(-4, 0, 4) },
+    vertices = { 0, 1, 2,  0, 2, 3 },
+  }
+  add_triangle(floor, 0)
+  add_triangle(floor, 3)
+  block(function()
+    material(lambert_material { albedo = rgb(0.3, 0.5, 0.7) })
+    local wall = mesh {
+      points = { point(-3, 0, 2), point(3, 0, 2), point(3, 4, 3), point(-3, 4, 3) },
+      vertices = { 0, 1, 2,  0, 2, 3 },
+    }
+    add_triangle(wall, 0)
+    add_triangle(wall, 3)
+  end)
+  block(function()
+    material(lambert_material { albedo = rgb(0) })
+    local lamp = mesh {
+      points = { point(1, 4, -1), point(1, 4, 1), point(-1, 4, 1), point(-1, 4, -1) },
+      vertices = { 2, 1, 0,  3, 2, 0 },
+    }
+    for _, index in ipairs({0, 3}) do
+      local shape = triangle(lamp, index)
+      local light = diffuse_light { radiance = rgb(10, 9, 8), shape = shape }
+      add_light(light)
+      add_shape(shape, light)
+    end
+  end)
+  camera(pinhole_camera {
+    transform = look_at(point(0, 3, -8), point(0, 1, 0), vector(0, 1, 0)) * scale(1, -1, 1),
+    fov = 0.8,
+  })
+end)
+local job = dort.render.make(scene, { x_res = 48, y_res = 32, iterations = 8, max_depth = 4,
+  sampler = random_sampler { seed = 7 } })
+local albedo, emission = dort.render.triangle_params(scene)
+local target = dort.render.adjoint_forward(job, { albedo = dort.image.axpy(-0.2, albedo, albedo) })
+local image = dort.render.adjoint_forward(job, { albedo = albedo })
+local loss, dl_dimage = dort.render.loss_l2(image, target)
+local d_albedo, d_emission = dort.render.adjoint_backward(job,
+  { dl_dimage = dl_dimage, albedo = albedo })
+local out = dort.env.get_argv()[1]
+dort.image.write_pfm(out .. "/image.pfm", image)
+dort.image.write_pfm(out .. "/d_albedo.pfm", d_albedo)
+dort.image.write_pfm(out .. "/d_emission.pfm", d_emission)
+dort.image.write_pfm(out .. "/albedo.pfm", albedo)
+print(string.format("loss %.9g", loss))
+'''
+
+
+def _scene_from_record(rec: dict) -> dict:
+    """The Python scene dict of a recorded flat scene (triangles only)."""
+    cam = rec["camera"]
+    return {"verts": np.asarray(rec["verts"], np.float32).reshape(-1, 3),
+            "tris": np.asarray(rec["tris"], np.uint32).reshape(-1, 3),
+            "tri_material": np.asarray(rec["tri_material"], np.uint32),
+            "materials": [{"kind": m["kind"], "color": tuple(m["color"]),
+                           "color2": tuple(m["color2"]), "param": tuple(m["param"])}
+                          for m in rec["materials"]],
+            "tri_emission": np.asarray(rec["tri_emission"], np.float32).reshape(-1, 3),
+            "camera": {"origin": cam["origin"], "right": cam["right"], "up": cam["up"],
+                       "forward": cam["forward"], "fov": cam["fov"], "kind": cam["kind"]}}
+
+
+@needs_frontend
+def test_adjoint_script_records_and_refuses_without_a_gpu(tmp_path):
+    """In record mode (no GPU) the script's scene records, its per-triangle
+    parameters come out, and the adjoint itself stops with a clear error."""
+    script = tmp_path / "adjoint.lua"
+    script.write_text(ADJOINT_LUA)
+    env = dict(os.environ, DORT_LUA_RECORD=str(tmp_path / "rec.json"))
+    out = subprocess.run([DORT, str(script), str(tmp_path)], env=env, capture_output=True,
+                         text=True, timeout=120)
+    assert out.returncode == 1
+    assert "the adjoint needs a GPU" in out.stderr
+    sd = _scene_from_record(json.load(open(tmp_path / "rec.json")))
+    assert len(sd["tris"]) == 6 and sd["tri_emission"][4:].min() > 0
+
+
+@needs_frontend
+@pytest.mark.gpu
+def test_script_adjoint_matches_the_python_api(tmp_path, cuda):
+    import dort_b200 as db
+    from dort_b200.image import read_pfm
+    script = tmp_path / "adjoint.lua"
+    script.write_text(ADJOINT_LUA)
+    # the flat scene, recorded without GPU work (the adjoint calls then stop
+    # the script, after define_scene, which is all the record needs)
+    env = dict(os.environ, DORT_LUA_RECORD=str(tmp_path / "rec.json"))
+    subprocess.run([DORT, str(script), str(tmp_path)], env=env, capture_output=True, text=True,
+                   timeout=120)
+    rec = json.load(open(tmp_path / "rec.json"))
+    out = subprocess.run([DORT, str(script), str(tmp_path)], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr
+    lua_loss = float(out.stdout.split("loss")[1])
+    img, da, de, alb = (read_pfm(str(tmp_path / f"{k}.pfm")) for k in
+                        ("image", "d_albedo", "d_emission", "albedo"))
+    sd = _scene_from_record(rec)
+    n = len(sd["tris"])
+    assert alb.shape == (1, n, 3) and da.shape == (1, n, 3)
+    # the per-triangle albedo of the scene's materials (emissive triangles 0)
+    mats = np.asarray([m["color"] for m in sd["materials"]], np.float32)
+    np.testing.assert_array_equal(alb[0], mats[sd["tri_material"]])
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], 48, 32, 8, max_depth=4, seed=7)
+    a = alb[0]
+    target = sc.adjoint_forward(p, (a + np.float32(-0.2) * a).astype(np.float32), None)
+    py_img = sc.adjoint_forward(p, a, None)
+    loss, g = db.loss_l2(py_img, target)
+    pda, pde = sc.adjoint_backward(p, g, a, sd["tri_emission"])
+    np.testing.assert_allclose(img, py_img, rtol=1e-5, atol=1e-6)
+    assert abs(lua_loss - loss) <= 1e-5 * abs(loss)
+    np.testing.assert_allclose(da[0], pda, rtol=1e-3, atol=1e-5 * np.abs(pda).max())
+    np.testing.assert_allclose(de[0], pde, rtol=1e-3, atol=1e-5 * np.abs(pde).max())
+    assert np.abs(pda).max() > 0 and np.abs(pde[sd["tri_emission"].sum(1) > 0]).min() > 0

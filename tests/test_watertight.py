@@ -1,0 +1,127 @@
+"""The watertight ray/triangle test (DORT_SCENE_WATERTIGHT; Woop, Benthin and
+Wald, JCGT 2013) against the reference's Moller-Trumbore.
+
+* Closed mesh: rays from inside a closed icosphere aimed exactly at its
+  vertices and at the midpoints of its edges.  Every such ray meets the mesh;
+  the watertight test finds a hit for all of them, Moller-Trumbore in float
+  lets some slip between the triangles that share the edge or vertex (counted
+  as the reason for the option).
+* Away from edges the two tests agree: the same triangle, t to float
+  rounding.  Every disagreement is classified: a ray whose hit lies within
+  1e-4 (barycentric) of an edge, or whose two hits tie in t.
+CPU cases run the device traversal compiled for the host; GPU cases the
+device ray cast.
+"""
+import numpy as np
+import pytest
+
+import dort_b200 as db
+from dort_b200 import scenes
+
+
+def closed_mesh_rays(freq=24, origin=(0.0, 0.0, 0.0)):
+    v, t = scenes.icosphere(freq)
+    v = v.astype(np.float32)
+    t = t.astype(np.uint32)
+    e = np.concatenate([t[:, [0, 1]], t[:, [1, 2]], t[:, [2, 0]]])
+    targets = np.concatenate([v, ((v[e[:, 0]] + v[e[:, 1]]) * np.float32(0.5))]).astype(np.float32)
+    o = np.asarray(origin, np.float32)
+    rays = np.zeros((len(targets), 8), np.float32)
+    rays[:, 0:3] = o
+    rays[:, 4:7] = targets - o
+    rays[:, 7] = np.inf
+    return v, t, rays
+
+
+def near_edge(tb, eps=1e-4):
+    b1, b2 = tb[:, 1], tb[:, 2]
+    return np.minimum(np.minimum(b1, b2), 1.0 - b1 - b2) < eps
+
+
+def classify(prim_mt, tb_mt, prim_wt, tb_wt):
+    """Counts of the rays on which the two tests disagree, by kind; every
+    disagreement must fall in one of the explained kinds."""
+    miss = db.MISS
+    d = prim_mt != prim_wt
+    out = {"rays": int(len(prim_mt)), "differ": int(d.sum())}
+    mt_miss = d & (prim_mt == miss)
+    wt_miss = d & (prim_wt == miss)
+    both = d & ~mt_miss & ~wt_miss
+    tie = both & (np.abs(tb_mt[:, 0] - tb_wt[:, 0]) <= 1e-5 * np.abs(tb_wt[:, 0]))
+    out["mt_slips_at_edge"] = int((mt_miss & near_edge(tb_wt)).sum())
+    out["wt_misses_mt_edge_hit"] = int((wt_miss & near_edge(tb_mt)).sum())
+    out["same_t_other_triangle"] = int(tie.sum())
+    other = both & ~tie
+    out["nearer_hit_at_edge"] = int((other & (near_edge(tb_mt) | near_edge(tb_wt))).sum())
+    out["unexplained"] = out["differ"] - (out["mt_slips_at_edge"] + out["wt_misses_mt_edge_hit"]
+                                          + out["same_t_other_triangle"]
+                                          + out["nearer_hit_at_edge"])
+    return out
+
+
+@pytest.mark.parametrize("origin", [(0.0, 0.0, 0.0), (0.1, -0.2, 0.05)])
+def test_host_closed_mesh_does_not_leak(origin):
+    v, t, rays = closed_mesh_rays(origin=origin)
+    pw, _, _ = db.host_check_raycast(v, t, rays, watertight=True)
+    pm, _, _ = db.host_check_raycast(v, t, rays)
+    assert int((pw == db.MISS).sum()) == 0
+    assert int((pm == db.MISS).sum()) > 0      # the reference's test does leak here
+
+
+def test_host_agrees_with_mt_away_from_edges():
+    sv, st = scenes.random_triangles(20000, seed=3)
+    rays = np.concatenate([scenes.pinhole_rays(128, 128),
+                           scenes.pinhole_rays(64, 64, eye=(0.2, 0.8, -1.2))])
+    pm, tbm, _ = db.host_check_raycast(sv, st, rays)
+    pw, tbw, _ = db.host_check_raycast(sv, st, rays, watertight=True)
+    c = classify(pm, tbm, pw, tbw)
+    assert c["unexplained"] == 0, c
+    same = (pm == pw) & (pm != db.MISS)
+    np.testing.assert_allclose(tbw[same, 0], tbm[same, 0], rtol=1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("origin", [(0.0, 0.0, 0.0), (0.1, -0.2, 0.05)])
+def test_device_closed_mesh_does_not_leak(cuda, origin):
+    v, t, rays = closed_mesh_rays(freq=64, origin=origin)
+    wt = db.Scene(v, t, watertight=True)
+    mt = db.Scene(v, t)
+    pw, _ = wt.raycast(rays)
+    pm, _ = mt.raycast(rays)
+    assert int((pw == db.MISS).sum()) == 0
+    assert int((pm == db.MISS).sum()) > 0
+    assert np.all(wt.raycast(rays, any_hit=True) == 1)
+    # the host-compiled traversal of the same tree agrees ray by ray
+    ph, _, _ = db.host_check_raycast(v, t, rays[:20000], watertight=True)
+    assert np.array_equal(ph, pw[:20000])
+
+
+@pytest.mark.gpu
+def test_device_disagreements_on_the_ray_cast_workload_are_all_at_edges(cuda):
+    verts, tris = scenes.random_triangles(200_000, seed=1)
+    mt = db.Scene(verts, tris)
+    wt = db.Scene(verts, tris, watertight=True)
+    coh = scenes.pinhole_rays(1024, 512)
+    dif = scenes.diffuse_rays(verts, tris, len(coh), lambda r: mt.raycast(r), seed=2)
+    rays = np.ascontiguousarray(np.concatenate([coh, dif]))
+    pm, tbm = mt.raycast(rays)
+    pw, tbw = wt.raycast(rays)
+    c = classify(pm, tbm, pw, tbw)
+    assert c["unexplained"] == 0, c
+    assert c["differ"] <= 1e-3 * len(rays), c
+    same = (pm == pw) & (pm != db.MISS)
+    np.testing.assert_allclose(tbw[same, 0], tbm[same, 0], rtol=1e-5)
+
+
+@pytest.mark.gpu
+def test_watertight_scene_renders_the_same_image(cuda):
+    sd = scenes.cornell_box()
+    a = db.scene_from_dict(sd)
+    b = db.scene_from_dict(sd, watertight=True)
+    p = db.render_params(sd["camera"], 64, 64, 64, max_depth=8, seed=3)
+    ia, _ = a.render(p)
+    ib, _ = b.render(p)
+    iw, _ = b.render_wavefront(p)
+    rr = np.sqrt(((ia.astype(np.float64) - ib) ** 2).mean()) / ia.mean()
+    assert rr < 0.02, rr
+    assert np.sqrt(((iw.astype(np.float64) - ib) ** 2).mean()) / ib.mean() < 2e-3
