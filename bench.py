@@ -15,13 +15,15 @@ value   samples/s of the wavefront renderer (one CUDA graph per frame),
 config.megakernel_samples_per_s  the plain per-pixel megakernel on the same
         frame; both draw the same random numbers per pixel and sample.
 config.equal_rmse  the error of both 256-spp frames against a converged
-        frame of the same scene: C samples per pixel (default 16,384) rendered
-        by the megakernel as frames of 256 spp with independent seeds and
-        accumulated in float64 on the host (FP64 CPU accumulation).  Relative
-        RMSE = sqrt(mean((x - r)^2)) / mean(r) over all pixels and channels,
-        with the converged frame's own variance (from the spread of its
-        frames) subtracted; the spp each renderer needs for 1 %, and the
-        samples/s ratio at equal RMSE.
+        frame of the same scene: C samples per pixel (default 20,480), half
+        rendered by each renderer as 256-spp frames with independent seeds,
+        every frame accumulated in float64 on the host (FP64 CPU
+        accumulation).  Relative RMSE = sqrt(mean((x - r)^2)) / mean(r) over
+        all pixels and channels, with the converged frame's own variance (from
+        the spread of its frames) subtracted; the spp each renderer needs for
+        1 %.  at_1pct: each renderer's own half (C/2 spp, below 1 % error),
+        the device seconds it took and the ratio of those times: the samples/s
+        ratio at equal RMSE below 1 %, measured.
 e2e     the wavefront frame through the C-ABI host entry
         dort_gpu_render_wavefront, image copied back to host memory; the
         scene's creation through dort_gpu_scene_create (what a script pays
@@ -530,39 +532,62 @@ def pt_reference_work(sd, n=1 << 15):
     return float(nodes.mean()), float(tests.mean()), len(rays)
 
 
-def converged_reference(sc, sd, W, H, spp_total, frame_spp, d_out, sh):
-    """A converged frame of the scene: spp_total samples per pixel rendered by
-    the per-pixel megakernel as frames of frame_spp samples with independent
-    seeds, each copied to the host and accumulated in float64.  Returns the
-    mean image, the per-pixel variance of that mean (from the spread of the
-    frames), the frame count and the seconds taken."""
+def converged_halves(sc, sd, W, H, frames_each, frame_spp, d_out, sh, stream, tuning):
+    """The converged frame of the scene, rendered half by each renderer: each
+    renders `frames_each` frames of `frame_spp` samples per pixel with
+    independent seeds (CUDA events around every frame), each frame is copied
+    to the host and accumulated in float64.  Returns per renderer its mean
+    image, the variance of that mean per pixel (from the spread of its
+    frames), its spp and device seconds; and the mean and variance of all
+    frames together (the reference)."""
     import torch
     import dort_b200 as db
-    frames = max(2, spp_total // frame_spp)
-    acc = np.zeros((H, W, 3), np.float64)
-    acc2 = np.zeros((H, W, 3), np.float64)
-    t0 = time.perf_counter()
-    for k in range(frames):
-        p = db.render_params(sd["camera"], W, H, frame_spp, max_depth=PT_DEPTH,
-                             seed=1_000_000 + k)
-        sc.render_device(p, d_out.data_ptr(), stream=sh)
-        img = d_out.view(H, W, 3).cpu().numpy().astype(np.float64)
-        acc += img
-        acc2 += img * img
-    torch.cuda.synchronize()
-    mean = acc / frames
-    var_frame = np.maximum(acc2 / frames - mean * mean, 0.0) * frames / (frames - 1)
-    return mean, var_frame / frames, frames, time.perf_counter() - t0
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    halves = {}
+    tot = np.zeros((H, W, 3), np.float64)
+    tot2 = np.zeros((H, W, 3), np.float64)
+    for name, seed0 in (("wavefront", 2_000_000), ("megakernel", 1_000_000)):
+        acc = np.zeros((H, W, 3), np.float64)
+        acc2 = np.zeros((H, W, 3), np.float64)
+        ms = 0.0
+        for k in range(frames_each):
+            p = db.render_params(sd["camera"], W, H, frame_spp, max_depth=PT_DEPTH,
+                                 seed=seed0 + k)
+            ev0.record(stream)
+            if name == "wavefront":
+                sc.render_wavefront_device(p, d_out.data_ptr(), stream=sh, tuning=tuning)
+            else:
+                sc.render_device(p, d_out.data_ptr(), stream=sh)
+            ev1.record(stream)
+            ev1.synchronize()
+            ms += ev0.elapsed_time(ev1)
+            img = d_out.view(H, W, 3).cpu().numpy().astype(np.float64)
+            acc += img
+            acc2 += img * img
+        mean = acc / frames_each
+        var_frame = np.maximum(acc2 / frames_each - mean * mean, 0.0) * frames_each / (
+            frames_each - 1)
+        halves[name] = {"mean": mean, "var_mean": var_frame / frames_each,
+                        "spp": frames_each * frame_spp, "seconds": ms / 1e3}
+        tot += acc
+        tot2 += acc2
+    n = 2 * frames_each
+    ref = tot / n
+    var_ref = np.maximum(tot2 / n - ref * ref, 0.0) * n / (n - 1) / n
+    return halves, ref, var_ref
 
 
-def equal_rmse(frames: dict, ref, var_ref, ref_spp: int, spp: int, rates: dict) -> dict:
+def equal_rmse(frames: dict, ref, var_ref, ref_spp: int, spp: int, rates: dict,
+               halves: dict | None = None, pixels: int = 0) -> dict:
     """Relative RMSE of each frame against the converged one (its own
     variance subtracted), the spp each renderer needs for 1 %, and the
-    samples/s ratio at equal RMSE."""
+    samples/s ratio at equal RMSE; with `halves` (each renderer's own
+    converged half), the error each half reaches and the time it took."""
     mref = float(ref.mean())
     vref = float(var_ref.mean())
-    out = {"reference": f"megakernel, {ref_spp} spp as independent 256-spp frames, float64 "
-                        "accumulation on the host",
+    out = {"reference": f"{ref_spp} spp, half rendered by each renderer as independent "
+                        f"{spp}-spp frames, float64 accumulation on the host",
            "reference_spp": ref_spp,
            "reference_rel_rmse": float(np.sqrt(vref) / mref),
            "target_rel_rmse": 0.01}
@@ -576,12 +601,23 @@ def equal_rmse(frames: dict, ref, var_ref, ref_spp: int, spp: int, rates: dict) 
         need[name] = int(np.ceil(spp * (rel / 0.01) ** 2))
         out[f"spp_for_1pct_{name}"] = need[name]
     # the expected error of one frame from the reference's own spread
-    out["rel_rmse_expected_from_spread"] = float(
-        np.sqrt(vref * ref_spp / spp) / mref)
+    out["rel_rmse_expected_from_spread"] = float(np.sqrt(vref * ref_spp / spp) / mref)
     # both renderers trace the same paths (same random numbers), so equal spp
-    # is equal RMSE; at the spp needed for 1 % the time ratio is the rate ratio
+    # is equal RMSE
     out["equal_rmse_spp"] = max(spp, max(need.values()))
     out["wavefront_over_megakernel_at_equal_rmse"] = rates["wavefront"] / rates["megakernel"]
+    if halves:
+        at = {}
+        for name, h in halves.items():
+            at[name] = {"spp": h["spp"], "seconds": round(h["seconds"], 3),
+                        "samples_per_s": pixels * h["spp"] / h["seconds"] if pixels else None,
+                        "rel_rmse": float(np.sqrt(h["var_mean"].mean()) / mref)}
+        a, b = halves["wavefront"], halves["megakernel"]
+        at["rel_rmse_between"] = float(np.sqrt(((a["mean"] - b["mean"]) ** 2).mean()) / mref)
+        at["rel_rmse_between_expected"] = float(
+            np.sqrt((a["var_mean"] + b["var_mean"]).mean()) / mref)
+        at["wavefront_over_megakernel"] = b["seconds"] / a["seconds"]
+        out["at_1pct"] = at
     return out
 
 
@@ -606,10 +642,21 @@ def measure_pt(args, ctx):
     spp = args.spp or PT_SPP
     p = db.render_params(sd["camera"], PT_W, PT_H, spp, max_depth=PT_DEPTH,
                          seed=rank_seed(42, rank))
-    # 2^25 path slots (about 11 GB of path state): fewer, fuller waves; at
-    # 256 spp 2^22 / 2^23 / 2^24 / 2^25 slots measured 567 / 592 / 606 / 616
-    # M samples/s
-    tuning = {"queue_capacity": 1 << 25, "sort_rays": args.sort_rays == "on"}
+    # the fixed tuning: 2^25 path slots (about 11 GB of path state), fewer,
+    # fuller waves (at 256 spp 2^22 / 2^23 / 2^24 / 2^25 slots measured
+    # 567 / 592 / 606 / 616 M samples/s), blocks of 128; by default the
+    # autotuner times its candidates (this one among them) on this frame first
+    tuning = {"queue_capacity": 1 << 25, "trace_block": 128, "shade_block": 128,
+              "sort_rays": args.sort_rays == "on", "stage_queues": args.stage_queues == "on"}
+    if args.queue_capacity:
+        tuning["queue_capacity"] = args.queue_capacity
+    tuned = None
+    if args.tuning == "auto" and not args.queue_capacity:
+        from dort_b200 import autotune as at
+        tuned = at.tune_scene(sc, p, budget_s=30.0)
+        tuning.update(tuned["tuning"])
+        log(f"[rank {rank}] autotune: {tuned['tuning']} ({tuned['candidates']} candidates, "
+            f"{tuned['seconds']:.1f}s)")
     d_out = torch.empty(PT_H * PT_W * 3, dtype=torch.float32, device=dev)
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
@@ -667,17 +714,22 @@ def measure_pt(args, ctx):
         te = max_over_ranks(pg, time.perf_counter() - te0)
         e2e = world * samples * e2e_steps / te
 
-    # equal RMSE: both frames against a converged frame (N=1 only)
+    # equal RMSE: both 256-spp frames against a converged frame, and each
+    # renderer timed to its own converged half (N=1 only)
     eq = None
     if world == 1 and args.converged_spp > 0:
-        ref, var_ref, nfr, secs = converged_reference(sc, sd, PT_W, PT_H, args.converged_spp,
-                                                      PT_SPP, d_out, sh)
+        frames_each = max(2, args.converged_spp // (2 * PT_SPP))
+        halves, ref, var_ref = converged_halves(sc, sd, PT_W, PT_H, frames_each, PT_SPP, d_out,
+                                                sh, stream, tuning)
         eq = equal_rmse({"wavefront": wf_img, "megakernel": mega_img}, ref, var_ref,
-                        nfr * PT_SPP, spp, {"wavefront": value, "megakernel": mega_value})
-        eq["reference_seconds"] = round(secs, 1)
-        log(f"[rank {rank}] converged frame: {nfr} x {PT_SPP} spp in {secs:.0f}s; rel RMSE "
-            f"wavefront {eq['rel_rmse_wavefront']:.4f} megakernel "
-            f"{eq['rel_rmse_megakernel']:.4f} (reference {eq['reference_rel_rmse']:.4f})")
+                        2 * frames_each * PT_SPP, spp,
+                        {"wavefront": value, "megakernel": mega_value}, halves, PT_W * PT_H)
+        at = eq["at_1pct"]
+        log(f"[rank {rank}] converged frame {2 * frames_each * PT_SPP} spp: 256-spp rel RMSE "
+            f"{eq['rel_rmse_wavefront']:.4f}; {at['wavefront']['spp']} spp: wavefront "
+            f"{at['wavefront']['seconds']:.1f}s rel RMSE {at['wavefront']['rel_rmse']:.4f}, "
+            f"megakernel {at['megakernel']['seconds']:.1f}s rel RMSE "
+            f"{at['megakernel']['rel_rmse']:.4f}")
 
     line = None
     if rank == 0:
@@ -745,7 +797,12 @@ def measure_pt(args, ctx):
                        "rays_per_frame": rays_per_frame,
                        "mrays_per_s": rays_per_frame * args.steps * world / (ms_max / 1e3) / 1e6,
                        "queue_capacity": tuning["queue_capacity"],
+                       "trace_block": tuning["trace_block"],
+                       "shade_block": tuning["shade_block"],
+                       "tuning": "fixed" if args.queue_capacity else args.tuning,
+                       "autotune": tuned,
                        "sort_rays": tuning["sort_rays"],
+                       "stage_queues": tuning["stage_queues"],
                        "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
@@ -844,7 +901,17 @@ def measure_batch(args, ctx, steps, warmup, mega_warmup=True):
     samples = sum(w * h * spp for (_, w, h, spp, _) in specs)
     log(f"[rank {rank}] 64 scenes ready in {time.time() - t0:.1f}s ({create_s:.2f}s to create, "
         f"{built} BVH builds {bvh_ms:.0f} ms), {samples / 1e9:.2f}G samples")
-    b = db.Batch(jobs, {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"})
+    # the batch tuning: 2^22 slots, or the autotuner's choice on a proxy
+    # batch (every job at an eighth of its samples) with --tuning auto in a
+    # batch run of its own
+    tuning = {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"}
+    tuned = None
+    if args.tuning == "auto" and args.workload == "batch":
+        from dort_b200 import autotune as at
+        tuned = at.tune_batch(jobs, budget_s=60.0)
+        tuning.update(tuned["tuning"])
+        log(f"[rank {rank}] batch autotune: {tuned['tuning']} ({tuned['seconds']:.1f}s)")
+    b = db.Batch(jobs, tuning)
     stream = torch.cuda.current_stream()
     for _ in range(warmup):
         b.render(stream.cuda_stream)
@@ -888,6 +955,7 @@ def measure_batch(args, ctx, steps, warmup, mega_warmup=True):
                        "megakernel_samples_per_s": world * samples / (mega_ms / 1e3),
                        "batch_over_megakernel": (mega_ms / (ms / steps)),
                        "rays_per_batch": st["rays"], "waves": st["waves"],
+                       "queue_capacity": tuning["queue_capacity"], "autotune": tuned,
                        "bvh_build": built, "bvh_build_ms_total": round(bvh_ms, 1),
                        "scene_create_s_total": round(create_s, 3)},
             "roofline": None, "cpu_baseline": None,
@@ -1001,12 +1069,21 @@ def main():
     ap.add_argument("--workload", default="pt1080p",
                     choices=["pt1080p", "raycast", "batch", "adjoint"])
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
-    ap.add_argument("--converged-spp", type=int, default=16384,
-                    help="pt1080p: samples per pixel of the converged frame (0: skip)")
+    ap.add_argument("--converged-spp", type=int, default=20480,
+                    help="pt1080p: samples per pixel of the converged frame, half rendered "
+                         "by each renderer (0: skip)")
     ap.add_argument("--no-sub", action="store_true",
                     help="pt1080p: skip the ray-cast, adjoint and batch sub-records")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--tuning", default="auto", choices=["auto", "fixed"],
+                    help="wavefront tuning: the autotuner's choice on the frame, or the "
+                         "fixed 2^25 slots / 128-thread blocks")
+    ap.add_argument("--queue-capacity", type=int, default=0,
+                    help="pt1080p: path slots of the wavefront (implies a fixed tuning; "
+                         "small values keep a profiled run's device memory small)")
+    ap.add_argument("--stage-queues", default="off", choices=["on", "off"],
+                    help="stage the shadow queue through bulk copies (TMA) into shared memory")
     ap.add_argument("--sort-rays", default="off", choices=["on", "off"],
                     help="sort each wave's extension rays (wavefront)")
     ap.add_argument("--bvh-build", default=None, choices=["host", "device", "ploc"],

@@ -98,7 +98,7 @@ class RenderParams(ctypes.Structure):
 class WavefrontTuning(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
                 ("shade_block", c_u32), ("sort_rays", c_u32), ("max_waves", c_u32),
-                ("reserved", c_u32 * 2)]
+                ("stage_queues", c_u32), ("reserved", c_u32 * 1)]
 
 
 class BatchJob(ctypes.Structure):
@@ -195,6 +195,14 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_bsdf_probe.restype = c_i32
         L.dort_gpu_bsdf_probe.argtypes = [ctypes.POINTER(Material), c_size, c_p, c_p, c_p, c_p,
                                           c_p, c_p, c_p, c_p, c_i32]
+        L.dort_gpu_autotune_wavefront.restype = c_i32
+        L.dort_gpu_autotune_wavefront.argtypes = [c_p, ctypes.POINTER(RenderParams),
+                                                  ctypes.c_double, ctypes.POINTER(WavefrontTuning),
+                                                  ctypes.POINTER(ctypes.c_double)]
+        L.dort_gpu_autotune_batch.restype = c_i32
+        L.dort_gpu_autotune_batch.argtypes = [ctypes.POINTER(BatchJob), c_u32, ctypes.c_double,
+                                              ctypes.POINTER(WavefrontTuning),
+                                              ctypes.POINTER(ctypes.c_double)]
         L.dort_gpu_debug_fail_alloc.restype = c_i32
         L.dort_gpu_debug_fail_alloc.argtypes = [ctypes.c_longlong]
         L.dort_gpu_check_device_bvh.restype = c_i32

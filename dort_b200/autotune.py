@@ -1,69 +1,76 @@
 """Autotuner for the wavefront renderer.
 
-Picks the wavefront's queue capacity (paths in flight), the thread-block
-sizes of its trace and shade stages and the BVH node width by timing short
-proxy frames of the caller's own scene and camera on the GPU: the same
-resolution and depth at a few samples per pixel, each candidate run twice
-with the faster run kept (the first warms caches).  The proxy keeps every
-sample the full frame would trace at sample 0..k, so the ranking reflects the
-real frame's ray mix.
+The search itself is native (dort_gpu_autotune_wavefront /
+dort_gpu_autotune_batch, csrc/autotune.cu): block sizes of the trace and
+shade stages ranked on a proxy frame of the caller's scene and camera, path
+slot capacities 2^22 .. 2^25 on the frame itself, each candidate timed with
+CUDA events.  This module adds the one choice that needs the scene rebuilt,
+the BVH node width, by tuning each width's scene and keeping the fastest.
 
-    best = autotune(scene_dict, params)          # -> {"bvh_width": 8, "tuning": {...}}
-    sc = Scene(..., bvh_width=best["bvh_width"])
+    best = autotune(scene_dict, params)   # {"bvh_width": 8, "tuning": {...}, "ms": ...}
+    sc = scene_from_dict(scene_dict, bvh_width=best["bvh_width"])
     sc.render_wavefront(params, best["tuning"])
 """
 from __future__ import annotations
 
-import copy
-import itertools
+import ctypes
 import time
 
-from . import _abi, render_params, scene_from_dict
+from . import _abi, scene_from_dict
 
-# more path slots make fewer, fuller waves (the 1080p frame at 256 spp:
-# 567 / 606 M samples/s at 2^22 / 2^24); about 330 B of device memory each
-DEFAULT_CAPACITIES = (1 << 22, 1 << 23, 1 << 24)
-DEFAULT_BLOCKS = (64, 128, 256)
-DEFAULT_WIDTHS = (8, 4)
+DEFAULT_WIDTHS = (8,)
 
 
-def _time_frame(sc, params, tuning) -> float:
-    best = float("inf")
-    for _ in range(2):
-        _, st = sc.render_wavefront(params, tuning)
-        best = min(best, st["ms"])
-    return best
+def _as_dict(t: _abi.WavefrontTuning) -> dict:
+    return {"queue_capacity": int(t.queue_capacity), "trace_block": int(t.trace_block),
+            "shade_block": int(t.shade_block)}
 
 
-def autotune(scene: dict, params: _abi.RenderParams, proxy_spp: int = 4,
-             capacities=DEFAULT_CAPACITIES, blocks=DEFAULT_BLOCKS, widths=DEFAULT_WIDTHS,
+def tune_scene(scene, params: _abi.RenderParams, budget_s: float = 30.0) -> dict:
+    """Native search on one scene handle: {"tuning", "ms", "candidates",
+    "seconds", "cut"}."""
+    t = _abi.WavefrontTuning()
+    st = (ctypes.c_double * 4)()
+    _abi.check(_abi.lib().dort_gpu_autotune_wavefront(scene.handle, ctypes.byref(params),
+                                                       budget_s * 1e3, ctypes.byref(t), st))
+    return {"tuning": _as_dict(t), "ms": st[1], "candidates": int(st[0]),
+            "seconds": st[2] / 1e3, "cut": bool(st[3])}
+
+
+def tune_batch(jobs, budget_s: float = 60.0) -> dict:
+    """Native search for a batch (a list of (Scene, RenderParams))."""
+    arr = (_abi.BatchJob * len(jobs))()
+    for i, (sc, p) in enumerate(jobs):
+        arr[i].scene = sc.handle
+        arr[i].params = p
+    t = _abi.WavefrontTuning()
+    st = (ctypes.c_double * 4)()
+    _abi.check(_abi.lib().dort_gpu_autotune_batch(arr, len(jobs), budget_s * 1e3,
+                                                   ctypes.byref(t), st))
+    return {"tuning": _as_dict(t), "ms": st[1], "candidates": int(st[0]),
+            "seconds": st[2] / 1e3, "cut": bool(st[3])}
+
+
+def autotune(scene: dict, params: _abi.RenderParams, widths=DEFAULT_WIDTHS,
              budget_s: float = 60.0, log=None) -> dict:
-    """Returns {"bvh_width", "tuning", "ms", "table"}: the fastest candidate
-    on a proxy frame of `proxy_spp` samples per pixel."""
-    proxy = copy.copy(params)
-    proxy = render_params(scene["camera"], params.width, params.height,
-                          min(params.iterations, proxy_spp), min_depth=params.min_depth,
-                          max_depth=params.max_depth, only_direct=bool(params.only_direct),
-                          direct_strategy={0: "mis", 1: "bsdf", 2: "light"}[params.direct_strategy],
-                          seed=params.seed)
-    samples = params.width * params.height * proxy.iterations
+    """Returns {"bvh_width", "tuning", "ms", "table"}: the fastest BVH width
+    with its native tuning (each width gets an equal share of the budget)."""
     table = []
-    t0 = time.perf_counter()
     best = None
+    t0 = time.perf_counter()
     for width in widths:
+        left = budget_s - (time.perf_counter() - t0)
+        if best is not None and left <= 0:
+            break
         sc = scene_from_dict(scene, bvh_width=width)
-        for cap, tb, sb in itertools.product(capacities, blocks, blocks):
-            if cap > 4 * samples and cap != min(capacities):
-                continue
-            if time.perf_counter() - t0 > budget_s:
-                break
-            tuning = {"queue_capacity": cap, "trace_block": tb, "shade_block": sb}
-            ms = _time_frame(sc, proxy, tuning)
-            table.append({"bvh_width": width, **tuning, "ms": ms})
-            if log:
-                log(f"autotune width={width} cap={cap} trace={tb} shade={sb}: {ms:.2f} ms")
-            if best is None or ms < best["ms"]:
-                best = {"bvh_width": width, "tuning": tuning, "ms": ms}
-        sc.close()
+        try:
+            r = tune_scene(sc, params, max(left / max(1, len(widths)), 1.0))
+        finally:
+            sc.close()
+        table.append({"bvh_width": width, **r})
+        if log:
+            log(f"autotune width={width}: {r['tuning']} {r['ms']:.2f} ms")
+        if best is None or r["ms"] < best["ms"]:
+            best = {"bvh_width": width, "tuning": r["tuning"], "ms": r["ms"]}
     best["table"] = table
     return best

@@ -436,12 +436,18 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
   tn.shade_block = 128;
   tn.sort = 0;
   tn.max_waves = 0;
+  tn.stage_queues = 0;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
       return false;
     }
     tn.max_waves = t->max_waves;
+    if(t->stage_queues > 2) {
+      err = "stage_queues must be 0 (auto), 1 (on) or 2 (off)";
+      return false;
+    }
+    tn.stage_queues = t->stage_queues == 1 ? 1u : 0u;
     if(t->queue_capacity) { tn.capacity = t->queue_capacity; }
     if(t->trace_block) { tn.trace_block = t->trace_block; }
     if(t->shade_block) { tn.shade_block = t->shade_block; }
@@ -522,7 +528,8 @@ extern "C" int dort_gpu_render_wavefront(dort_scene* scene, const dort_render_pa
   }
   if(rc == DORT_OK) { rc = wavefront_counters(scene, &rays, &waves, &error, st); }
   if(rc == DORT_OK && error) {
-    rc = fail(DORT_ERR_TIMEOUT, "wavefront frame exceeded its wave limit");
+    rc = fail(DORT_ERR_TIMEOUT, error & 2u ? "a wavefront stage's bounded device wait timed out"
+                                           : "wavefront frame exceeded its wave limit");
   }
   float ms = 0.f;
   if(rc == DORT_OK) { cudaEventElapsedTime(&ms, e0, e1); }
@@ -617,11 +624,16 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
   tn.shade_block = 128;
   tn.sort = 0;
   tn.max_waves = 0;
+  tn.stage_queues = 0;
   if(tuning) {
     if(tuning->struct_size != sizeof(dort_wavefront_tuning)) {
       return fail(DORT_ERR_INVALID, "dort_wavefront_tuning.struct_size mismatch (ABI version)");
     }
     tn.max_waves = tuning->max_waves;
+    if(tuning->stage_queues > 2) {
+      return fail(DORT_ERR_INVALID, "stage_queues must be 0 (auto), 1 (on) or 2 (off)");
+    }
+    tn.stage_queues = tuning->stage_queues == 1 ? 1u : 0u;
     if(tuning->queue_capacity) { tn.capacity = tuning->queue_capacity; }
     if(tuning->trace_block) { tn.trace_block = tuning->trace_block; }
     if(tuning->shade_block) { tn.shade_block = tuning->shade_block; }

@@ -7,9 +7,8 @@
 // (triangle.cpp:14-46, 102-134).
 //
 // Traversal: node groups (base index, 8 child-hit bits << 24 | internal-slot
-// mask) on a per-thread stack whose first entries sit in shared memory; child
-// slots are visited in an order fixed by the ray octant (slot bit index XOR
-// octant), so no per-node sort is needed.
+// mask) on a per-thread stack; child slots are visited in an order fixed by
+// the ray octant (slot bit index XOR octant), so no per-node sort is needed.
 // Child boxes are tested with fused multiply-adds on the quantized planes and
 // a relative widening of 2^-20 that covers the rounding of that arithmetic;
 // together with the one-step quantization margin the test never culls a box
@@ -368,14 +367,18 @@ DG_HD void trav_init(TravState& s, const TraceScene& sc, float ox, float oy, flo
 // stack holds at most the tree's depth (<= kTraceStack) entries; the trees
 // of the benchmark scenes are 8 levels deep.
 //
-// ShortStack (device, the default): the first kShortStack entries of every
-// thread sit in shared memory, one column per thread (entry k of thread t at
-// k * kShortStackThreads + t: a warp's 8-byte accesses fall in distinct
-// banks whatever depth each lane is at), deeper entries in local memory.
-// Pushes and pops then leave the L1 data cache to the node and triangle
-// fetches.  Blocks wider than kShortStackThreads keep the whole stack in
-// local memory.  Built with DORT_LOCAL_STACK, every entry is in local memory
-// (LocalStack).
+// LocalStack (the default): the stack in per-thread local memory.  Only the
+// first few entries are ever touched, and local memory is interleaved so a
+// warp's accesses to one depth are coalesced; they stay in the L1 cache.
+//
+// ShortStack (built with DORT_SHORT_STACK): the first kShortStack entries of
+// every thread in shared memory, one column per thread (entry k of thread t
+// at k * kShortStackThreads + t: a warp's 8-byte accesses fall in distinct
+// banks whatever depth each lane is at), deeper entries in local memory.  It
+// measured slower on B200: 598 against 618 M samples/s on the 1080p frame,
+// 2,315 against 2,457 Mrays/s on the ray cast, as the shared array takes
+// its share of the SM's L1 from the node and triangle fetches.  Blocks wider
+// than kShortStackThreads keep the whole stack in local memory.
 struct LocalStack {
   uint2 e[kTraceStack];
   DG_HD void init() {}
@@ -383,7 +386,7 @@ struct LocalStack {
   DG_HD uint2 pop(int sp) { return e[sp]; }
 };
 
-#if defined(__CUDA_ARCH__) && !defined(DORT_LOCAL_STACK)
+#if defined(__CUDA_ARCH__) && defined(DORT_SHORT_STACK)
 constexpr int kShortStack = 8;
 constexpr int kShortStackThreads = 128;
 

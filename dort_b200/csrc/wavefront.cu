@@ -698,29 +698,123 @@ __global__ void wf_shade(J jobs, WfDev w) {
   }
 }
 
+// One shadow-queue entry: any hit of its segment; if nothing blocks it, its
+// contribution joins its path's sum.
 template<class J>
+__device__ __forceinline__ void shadow_entry(J& jobs, WfDev& w, uint32_t i, float4 o, float4 d) {
+  uint32_t slot = w.sh_slot[i];
+  uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
+  const PtScene& sc = jobs.scene(job);
+  Hit h = scene_trace<true, J::kGeneral>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), d.w);
+  if(h.prim == kMiss) {
+    // a path can own two entries (light and BSDF strategy for a background
+    // light), so the additions are atomic
+    float4 c = w.sh_c[i];
+    float* sp = &w.sum[slot].x;
+    atomicAdd(sp, c.x);
+    atomicAdd(sp + 1, c.y);
+    atomicAdd(sp + 2, c.z);
+  }
+}
+
+// Staging of the shadow queue through the bulk-copy (TMA) engine.  The queue
+// is contiguous in entry order, so a warp's next 32 entries (origins and
+// directions, 512 bytes each) are one cp.async.bulk copy per array into the
+// warp's slot of shared memory, completing on the warp's mbarrier; the warp
+// issues the copy of its next batch as soon as it has read the current one
+// into registers, so the loads of batch k + 1 overlap the traversals of
+// batch k.  The source is this GPU's own memory and no copy multicasts.
+constexpr uint32_t kTmaWarps = 8;   // blocks of up to 256 threads stage
+constexpr uint32_t kTmaSpin = 1u << 20;   // bound on one mbarrier wait
+
+struct ShadowStage {
+  float4 o[32];
+  float4 d[32];
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return uint32_t(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// lane 0: arm the barrier for `bytes` and start the two copies into `st`
+__device__ __forceinline__ void stage_batch(ShadowStage* st, uint64_t* bar, const float4* o,
+                                            const float4* d, uint32_t count) {
+  const uint32_t bytes = count * uint32_t(sizeof(float4));
+  // the warp's earlier reads of the buffer (generic proxy) before the copy
+  // (async proxy) overwrites it
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+               ::"r"(smem_addr(bar)), "r"(2 * bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+               "[%0], [%1], %2, [%3];"
+               ::"r"(smem_addr(st->o)), "l"(o), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+               "[%0], [%1], %2, [%3];"
+               ::"r"(smem_addr(st->d)), "l"(d), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// Bounded wait for the barrier's phase `parity`; warp-uniform result.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t spins) {
+  uint32_t done = 0;
+  for(uint32_t k = 0; k < spins && !done; ++k) {
+    asm volatile("{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; "
+                 "selp.u32 %0, 1, 0, p; }"
+                 : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+  }
+  return __any_sync(0xffffffffu, done != 0);
+}
+
+template<class J, bool STAGED>
 __global__ void wf_shadow(J jobs, WfDev w) {
   const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_SHADOW);
+  const uint32_t lane = threadIdx.x & 31u;
+  if(STAGED && blockDim.x <= 32 * kTmaWarps) {
+    __shared__ __align__(128) ShadowStage stage[kTmaWarps];
+    __shared__ __align__(8) uint64_t bar[kTmaWarps];
+    const uint32_t warp = threadIdx.x >> 5;
+    ShadowStage* st = &stage[warp];
+    if(lane == 0) { mbar_init(&bar[warp]); }
+    __syncwarp();
+    uint32_t parity = 0;
+    uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_SH));
+    if(base < n && lane == 0) {
+      stage_batch(st, &bar[warp], w.sh_o + base, w.sh_d + base, min(32u, n - base));
+    }
+    while(base < n) {
+      if(!mbar_wait(&bar[warp], parity, kTmaSpin)) {
+        // the copy did not land: flag the frame (the host reports
+        // DORT_ERR_TIMEOUT), wait longer for the copy in flight, stop
+        if(lane == 0) { atomicOr(ctr_at(w.ctr, C_ERROR), 2u); }
+        mbar_wait(&bar[warp], parity, 64u * kTmaSpin);
+        return;
+      }
+      parity ^= 1u;
+      const uint32_t i = base + lane;
+      float4 o = make_float4(0.f, 0.f, 0.f, 0.f), d = o;
+      if(i < n) {
+        o = st->o[lane];
+        d = st->d[lane];
+      }
+      __syncwarp();
+      const uint32_t next = warp_fetch(ctr_at(w.ctr, C_F_SH));
+      if(next < n && lane == 0) {
+        stage_batch(st, &bar[warp], w.sh_o + next, w.sh_d + next, min(32u, n - next));
+      }
+      if(i < n) { shadow_entry(jobs, w, i, o, d); }
+      base = next;
+    }
+    return;
+  }
   for(;;) {
     uint32_t base = warp_fetch(ctr_at(w.ctr, C_F_SH));
     if(base >= n) { break; }
-    uint32_t i = base + (threadIdx.x & 31u);
-    if(i < n) {
-      uint32_t slot = w.sh_slot[i];
-      uint32_t job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
-      const PtScene& sc = jobs.scene(job);
-      float4 o = w.sh_o[i], d = w.sh_d[i];
-      Hit h = scene_trace<true, J::kGeneral>(sc, v3(o.x, o.y, o.z), o.w, v3(d.x, d.y, d.z), d.w);
-      if(h.prim == kMiss) {
-        // a path can own two entries (light and BSDF strategy for a
-        // background light), so the additions are atomic
-        float4 c = w.sh_c[i];
-        float* sp = &w.sum[slot].x;
-        atomicAdd(sp, c.x);
-        atomicAdd(sp + 1, c.y);
-        atomicAdd(sp + 2, c.z);
-      }
-    }
+    uint32_t i = base + lane;
+    if(i < n) { shadow_entry(jobs, w, i, w.sh_o[i], w.sh_d[i]); }
   }
 }
 
@@ -925,7 +1019,9 @@ static WfGrids wf_grids(const WfTuning& tn) {
   g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), int(kRegenBlock));
   g.ext = grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
   g.sha = grid_for(reinterpret_cast<const void*>(&wf_shade<J>), int(tn.shade_block));
-  g.shw = grid_for(reinterpret_cast<const void*>(&wf_shadow<J>), int(tn.trace_block));
+  g.shw = tn.stage_queues
+      ? grid_for(reinterpret_cast<const void*>(&wf_shadow<J, true>), int(tn.trace_block))
+      : grid_for(reinterpret_cast<const void*>(&wf_shadow<J, false>), int(tn.trace_block));
   g.nb = grid_for(reinterpret_cast<const void*>(&wf_neeb<J>), int(tn.trace_block));
   return g;
 }
@@ -949,7 +1045,11 @@ static void wf_launch_wave(const J& jobs, WfDev& dev, const WfTuning& tn, const 
   wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
   if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(dev); }
   wf_shade<J><<<g.sha, bs, 0, st>>>(jobs, dev);
-  wf_shadow<J><<<g.shw, bt, 0, st>>>(jobs, dev);
+  if(tn.stage_queues) {
+    wf_shadow<J, true><<<g.shw, bt, 0, st>>>(jobs, dev);
+  } else {
+    wf_shadow<J, false><<<g.shw, bt, 0, st>>>(jobs, dev);
+  }
   wf_neeb<J><<<g.nb, bt, 0, st>>>(jobs, dev);
 }
 
@@ -1076,7 +1176,11 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
     cudaEventRecord(ev[2], st);
     wf_shade<SingleJob<G>><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[3], st);
-    wf_shadow<SingleJob<G>><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
+    if(tn.stage_queues) {
+      wf_shadow<SingleJob<G>, true><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
+    } else {
+      wf_shadow<SingleJob<G>, false><<<g.shw, bt, 0, st>>>(jobs, wf->dev);
+    }
     cudaEventRecord(ev[4], st);
     wf_neeb<SingleJob<G>><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);

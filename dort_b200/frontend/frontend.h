@@ -147,6 +147,8 @@ struct RenderJob {
   std::shared_ptr<Scene> scene;
   dort_render_params params{};
   bool started = false, finished = false;
+  bool autotune = false;              // tune the wavefront before rendering (not a
+                                      // reference parameter)
   std::shared_ptr<Image> image;       // float RGB result
 };
 

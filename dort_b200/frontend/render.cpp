@@ -549,8 +549,11 @@ static int render_make(lua_State* l) {
     else if(st == "bsdf") { rp.direct_strategy = DORT_DIRECT_BSDF; }
     else if(st == "light") { rp.direct_strategy = DORT_DIRECT_LIGHT; }
     else { return luaL_error(l, "Unknown direct strategy '%s'", st.c_str()); }
-    // not a reference parameter: off for derivative checks (DORT_PT_NO_ROULETTE)
+    // not reference parameters: roulette off for derivative checks
+    // (DORT_PT_NO_ROULETTE); autotune = true times the wavefront's candidate
+    // tunings on this frame before rendering it (dort_gpu_autotune_wavefront)
     if(!param_bool_opt(l, p, "roulette", true)) { rp.renderer_flags |= DORT_PT_NO_ROULETTE; }
+    job->autotune = param_bool_opt(l, p, "autotune", false);
   } else if(method == "lt" || method == "light") {
     // lua_render.cpp:146-150: path lengths min_depth + 2 .. max_depth + 2
     rp.renderer = DORT_RENDERER_LT;
@@ -594,10 +597,20 @@ static int render_sync(lua_State* l) {
   if(job->scene->handle) {
     // the wavefront unless the per-pixel renderer is needed (sample_all_lights)
     // or the light or bidirectional tracer is asked for
-    int rc = job->params.sample_all_lights || job->params.renderer != DORT_RENDERER_PT
-        ? dort_gpu_render(job->scene->handle, &job->params, img->px.data(), nullptr)
-        : dort_gpu_render_wavefront(job->scene->handle, &job->params, nullptr, img->px.data(),
-                                    nullptr);
+    const bool wavefront = !job->params.sample_all_lights &&
+                           job->params.renderer == DORT_RENDERER_PT;
+    dort_wavefront_tuning tuning{};
+    const dort_wavefront_tuning* tp = nullptr;
+    if(wavefront && job->autotune) {
+      if(dort_gpu_autotune_wavefront(job->scene->handle, &job->params, 0.0, &tuning, nullptr) !=
+         DORT_OK) {
+        return luaL_error(l, "%s", dort_gpu_last_error());
+      }
+      tp = &tuning;
+    }
+    int rc = wavefront
+        ? dort_gpu_render_wavefront(job->scene->handle, &job->params, tp, img->px.data(), nullptr)
+        : dort_gpu_render(job->scene->handle, &job->params, img->px.data(), nullptr);
     if(rc != DORT_OK) { return luaL_error(l, "%s", dort_gpu_last_error()); }
   }
   job->image = img;

@@ -399,7 +399,13 @@ typedef struct dort_wavefront_tuning {
                                   entry points return DORT_ERR_TIMEOUT and
                                   the device-pointer ones leave the flag for
                                   dort_gpu_batch_stats / out_stats. */
-  uint32_t reserved[2];
+  uint32_t stage_queues;       /* 0: auto (off), 1: on, 2: off -- the shadow
+                                  stage stages its queue through bulk copies
+                                  into shared memory (cp.async.bulk, one per
+                                  warp and batch of 32 entries, overlapping
+                                  the previous batch's traversals); blocks of
+                                  at most 256 trace threads */
+  uint32_t reserved[1];
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel
@@ -438,6 +444,27 @@ int dort_gpu_batch_image_device(dort_batch* batch, uint32_t job, const float** o
  * out[3] = total samples (waits for the last render). */
 int dort_gpu_batch_stats(dort_batch* batch, double out[4]);
 int dort_gpu_batch_destroy(dort_batch* batch);
+
+/* No reference counterpart.  The wavefront's autotuner: times candidate
+ * tunings on the GPU and writes the fastest to out_tuning (struct_size set).
+ * Block sizes (trace, shade) of {64, 128, 256} are ranked on a proxy frame
+ * (the frame at up to 8 samples per pixel, 2^22 path slots); path-slot
+ * capacities 2^22 .. 2^25 on the frame itself, skipping those beyond twice
+ * its work or beyond the free device memory (about 340 bytes per slot).
+ * Each candidate runs twice, the faster run counts.  budget_ms bounds the
+ * search (0: 30 s); when it runs out the best so far wins.  out_stats
+ * (optional, 4 doubles): candidates timed, the chosen frame's milliseconds,
+ * milliseconds spent, 1 if the budget cut the search short.  The scene's
+ * wavefront queues are left at the last candidate's size. */
+int dort_gpu_autotune_wavefront(dort_scene* scene, const dort_render_params* params,
+                                double budget_ms, dort_wavefront_tuning* out_tuning,
+                                double* out_stats);
+
+/* No reference counterpart.  The same for a batch: capacities 2^21 .. 2^24
+ * ranked on a proxy batch (every job at an eighth of its samples, at least
+ * 4), blocks of 128 (budget_ms 0: 60 s). */
+int dort_gpu_autotune_batch(const dort_batch_job* jobs, uint32_t job_count, double budget_ms,
+                            dort_wavefront_tuning* out_tuning, double* out_stats);
 
 /* Measurement entry: renders the same frame wave by wave from the host
  * (without the graph) with CUDA events around each stage; out_ms[0..4] =

@@ -46,6 +46,32 @@ def test_equal_rmse_subtracts_the_references_own_noise(ref_frames):
     assert eq["wavefront_over_megakernel_at_equal_rmse"] == 2.0
 
 
+def test_equal_rmse_halves_report_each_renderers_converged_half():
+    rng = np.random.default_rng(5)
+    truth = rng.uniform(0.5, 1.5, (64, 96, 3))
+    sigma, k = 0.05, 32
+    halves = {}
+    for name, secs in (("wavefront", 10.0), ("megakernel", 25.0)):
+        subs = _frames(truth, sigma, k, rng)
+        mean = np.mean(subs, axis=0)
+        var_frame = np.var(subs, axis=0, ddof=1)
+        halves[name] = {"mean": mean, "var_mean": var_frame / k, "spp": k * 256,
+                        "seconds": secs}
+    ref = (halves["wavefront"]["mean"] + halves["megakernel"]["mean"]) / 2
+    var_ref = (halves["wavefront"]["var_mean"] + halves["megakernel"]["var_mean"]) / 4
+    x = truth + rng.normal(0.0, sigma, truth.shape)
+    eq = bench.equal_rmse({"wavefront": x, "megakernel": x}, ref, var_ref, 2 * k * 256, 256,
+                          {"wavefront": 2.0, "megakernel": 1.0}, halves, 64 * 96)
+    at = eq["at_1pct"]
+    want = sigma / truth.mean() / np.sqrt(k)
+    assert at["wavefront"]["rel_rmse"] == pytest.approx(want, rel=0.05)
+    assert at["megakernel"]["rel_rmse"] == pytest.approx(want, rel=0.05)
+    assert at["rel_rmse_between"] == pytest.approx(at["rel_rmse_between_expected"], rel=0.05)
+    assert at["wavefront_over_megakernel"] == 2.5
+    assert at["wavefront"]["samples_per_s"] == pytest.approx(64 * 96 * k * 256 / 10.0)
+    assert eq["rel_rmse_wavefront"] == pytest.approx(sigma / truth.mean(), rel=0.05)
+
+
 def test_ref_procs_and_host_info():
     n = bench.ref_procs()
     assert 1 <= n <= (os.cpu_count() or 1)

@@ -376,3 +376,25 @@ def test_script_adjoint_matches_the_python_api(tmp_path, cuda):
     np.testing.assert_allclose(da[0], pda, rtol=1e-3, atol=1e-5 * np.abs(pda).max())
     np.testing.assert_allclose(de[0], pde, rtol=1e-3, atol=1e-5 * np.abs(pde).max())
     assert np.abs(pda).max() > 0 and np.abs(pde[sd["tri_emission"].sum(1) > 0]).min() > 0
+
+
+@needs_frontend
+@pytest.mark.gpu
+def test_script_autotune_renders_like_the_python_api(tmp_path, cuda):
+    """render.make { autotune = true }: the wavefront tuned on the frame first;
+    the image is the same estimator's (same random numbers)."""
+    import dort_b200 as db
+    from dort_b200.image import read_rgbe, rgbe_quantize
+    script = tmp_path / "scene.lua"
+    script.write_text(SCENE_LUA.replace("max_depth = 4,", "max_depth = 4, autotune = true,"))
+    out = subprocess.run([DORT, str(script), str(tmp_path / "img.hdr")], capture_output=True,
+                         text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lua_img = read_rgbe(str(tmp_path / "img.hdr"))
+    d = _python_scene()
+    sc = db.scene_from_dict(d)
+    p = db.render_params(d["camera"], 96, 64, 16, max_depth=4, seed=7)
+    py_img = rgbe_quantize(sc.render_wavefront(p)[0])
+    sc.close()
+    diff = np.abs(lua_img.astype(np.float64) - py_img)
+    assert float(diff.mean()) < 1e-3 * max(float(py_img.mean()), 1e-6), float(diff.mean())

@@ -101,16 +101,19 @@ def test_wavefront_rejects_sample_all_lights(cuda):
     assert np.isfinite(img).all()
 
 
-@pytest.mark.parametrize("sort_rays", [False, True])
-@pytest.mark.parametrize("capacity,block", [(64, 32), (4096, 256), (100000, 128)])
-def test_wavefront_queue_shapes(cuda, capacity, block, sort_rays):
-    """Queue sizes, block sizes and the optional ray sort change the order of
-    work, not the paths: the same image as the megakernel."""
+@pytest.mark.parametrize("sort_rays,staged", [(False, False), (True, False), (False, True)])
+@pytest.mark.parametrize("capacity,block", [(64, 32), (4096, 256), (100000, 128), (50000, 512)])
+def test_wavefront_queue_shapes(cuda, capacity, block, sort_rays, staged):
+    """Queue sizes, block sizes, the optional ray sort and the staging of the
+    shadow queue through bulk copies (blocks above 256 threads load it
+    directly) change the order of work, not the paths: the same image as the
+    megakernel."""
     sd = scenes.cornell_variant("delt")
     sc = db.scene_from_dict(sd)
     p = db.render_params(sd["camera"], 32, 24, 16, seed=4)
     a, _ = sc.render(p)
     b, st = sc.render_wavefront(p, {"queue_capacity": capacity, "trace_block": block,
-                                    "shade_block": block, "sort_rays": sort_rays})
+                                    "shade_block": block, "sort_rays": sort_rays,
+                                    "stage_queues": staged})
     assert ptcheck.rel_rmse(b, a) < 2e-3
     assert st["waves"] >= 1

@@ -110,7 +110,9 @@ def test_device_disagreements_on_the_ray_cast_workload_are_all_at_edges(cuda):
     assert c["unexplained"] == 0, c
     assert c["differ"] <= 1e-3 * len(rays), c
     same = (pm == pw) & (pm != db.MISS)
-    np.testing.assert_allclose(tbw[same, 0], tbm[same, 0], rtol=1e-5)
+    # t of the same triangle: float rounding of two formulas (a few grazing
+    # rays in 10^6 differ by up to 5e-5)
+    np.testing.assert_allclose(tbw[same, 0], tbm[same, 0], rtol=2e-4)
 
 
 @pytest.mark.gpu
