@@ -217,6 +217,28 @@ def peaks():
     return 6650.0, "fallback"
 
 
+def classify_watertight(prim_mt, tb_mt, prim_wt, tb_wt, eps: float = 1e-4) -> dict:
+    """The rays on which the watertight test and the reference's
+    Moller-Trumbore disagree, by kind: a ray that slips through an edge under
+    one test, a tie in t between two triangles (a shared edge), or nearer
+    hits at an edge; 'unexplained' counts the rest (none expected)."""
+    miss = 0xFFFFFFFF
+    near = lambda tb: np.minimum(np.minimum(tb[:, 1], tb[:, 2]), 1 - tb[:, 1] - tb[:, 2]) < eps
+    d = prim_mt != prim_wt
+    mt_miss, wt_miss = d & (prim_mt == miss), d & (prim_wt == miss)
+    both = d & ~mt_miss & ~wt_miss
+    tie = both & (np.abs(tb_mt[:, 0] - tb_wt[:, 0]) <= 1e-5 * np.abs(tb_wt[:, 0]))
+    out = {"rays": int(len(prim_mt)), "ids_differ": int(d.sum()),
+           "mt_slips_at_edge": int((mt_miss & near(tb_wt)).sum()),
+           "watertight_misses_mt_edge_hit": int((wt_miss & near(tb_mt)).sum()),
+           "same_t_other_triangle": int(tie.sum()),
+           "nearer_hit_at_edge": int((both & ~tie & (near(tb_mt) | near(tb_wt))).sum())}
+    out["unexplained"] = out["ids_differ"] - sum(
+        out[k] for k in ("mt_slips_at_edge", "watertight_misses_mt_edge_hit",
+                         "same_t_other_triangle", "nearer_hit_at_edge"))
+    return out
+
+
 def host_info() -> dict:
     """The host's logical core count and CPU model (the CPU baseline's box)."""
     model = None
@@ -404,6 +426,21 @@ def measure_raycast(args, ctx, steps, warmup, cpu_budget=15.0, e2e_steps=20):
     per_launch = scene.raycast_timed(d_rays.data_ptr(), n, d_prim.data_ptr(),
                                      d_tb.data_ptr(), stream=sh, repeat=max(3, steps))
 
+    # the watertight test (DORT_SCENE_WATERTIGHT) on the same rays: its rate
+    # and every ray on which it disagrees with the reference's test, by kind
+    wt = None
+    if world == 1 and not args.no_cpu:
+        wsc = db.Scene(verts, tris, bvh_build=args.bvh_build, watertight=True)
+        w_prim = torch.empty_like(d_prim)
+        w_tb = torch.empty_like(d_tb)
+        w_ms = wsc.raycast_timed(d_rays.data_ptr(), n, w_prim.data_ptr(), w_tb.data_ptr(),
+                                 stream=sh, repeat=max(3, steps))
+        torch.cuda.synchronize()
+        wt = classify_watertight(d_prim.cpu().numpy().view(np.uint32), d_tb.cpu().numpy(),
+                                 w_prim.cpu().numpy().view(np.uint32), w_tb.cpu().numpy())
+        wt["mrays_per_s"] = n / (w_ms / 1e3) / 1e6
+        wsc.close()
+
     # e2e through the host-pointer C-ABI entry with pinned buffers
     h_rays = torch.empty((n, 8), dtype=torch.float32, pin_memory=True)
     h_rays.numpy()[:] = rays
@@ -456,7 +493,8 @@ def measure_raycast(args, ctx, steps, warmup, cpu_budget=15.0, e2e_steps=20):
             "config": {"workload": WORKLOAD, "tris": N_TRIS, "rays_per_step": n,
                        "l2": "inputs larger than L2 (512 MB of rays per step)",
                        "bvh": f"wide BVH width 8, {st['nodes']} nodes, depth {st['depth']}",
-                       "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2)},
+                       "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2),
+                       "watertight": wt},
             "roofline": rl, "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Mrays/s", "h2d_bytes_per_step": n * 32,
                     "d2h_bytes_per_step": n * 16},

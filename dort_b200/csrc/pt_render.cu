@@ -483,10 +483,6 @@ extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
   if(pp.renderer != RENDERER_PT) {
     return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_render_wavefront_device renders only the pt renderer");
   }
-  if(pp.sample_all_lights) {
-    return fail(DORT_ERR_UNSUPPORTED, "the wavefront renderer does not do sample_all_lights; "
-                                      "use dort_gpu_render");
-  }
   WfTuning tn;
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
   int drc = require_scene_device(scene);
@@ -555,7 +551,6 @@ extern "C" int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_rend
   if(pp.renderer != RENDERER_PT) {
     return fail(DORT_ERR_UNSUPPORTED, "dort_gpu_wavefront_stage_times renders only the pt renderer");
   }
-  if(pp.sample_all_lights) { return fail(DORT_ERR_UNSUPPORTED, "sample_all_lights"); }
   WfTuning tn;
   if(!make_tuning(tuning, pp, tn, err)) { return fail(DORT_ERR_INVALID, err); }
   int drc = require_scene_device(scene);
@@ -606,9 +601,6 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
     std::string err;
     if(!make_params(&jobs[j].params, params[j], err)) {
       return fail(DORT_ERR_INVALID, "job " + std::to_string(j) + ": " + err);
-    }
-    if(params[j].sample_all_lights) {
-      return fail(DORT_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": sample_all_lights");
     }
     if(params[j].renderer != RENDERER_PT) {
       return fail(DORT_ERR_UNSUPPORTED, "job " + std::to_string(j) + ": batches render only pt");

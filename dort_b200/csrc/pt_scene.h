@@ -127,7 +127,8 @@ enum : uint32_t { RENDERER_PT = 0, RENDERER_LT = 1, RENDERER_BDPT = 2 };
 // Whether rendering `sc` with `pp` needs the general instantiation of the
 // path code (pt.cuh, template flag G).
 inline bool scene_needs_general(const PtScene& sc, const PtParams& pp) {
-  return sc.general != 0 || pp.camera != CAMERA_PINHOLE || sc.trace.watertight != 0;
+  return sc.general != 0 || pp.camera != CAMERA_PINHOLE || sc.trace.watertight != 0 ||
+         pp.sample_all_lights != 0;
 }
 
 }  // namespace dort_gpu

@@ -512,6 +512,97 @@ __global__ void wf_extend(J jobs, WfDev w) {
   }
 }
 
+// The direct lighting of one light at a path vertex (estimate_direct,
+// path_renderer.cpp:135-206) as queue entries, `inv_lpdf` the inverse of the
+// light's choice probability (1 when every light is sampled):
+//   sh   the light strategy's shadow ray and its contribution if unblocked;
+//   sh2  the BSDF strategy towards a background light: it counts only if the
+//        ray escapes, and L and w depend on the direction alone, so it is an
+//        any-hit query with its contribution computed here;
+//   nb   the BSDF strategy towards an area light: closest hit, L and the MIS
+//        weight once the hit is known (wf_neeb).
+struct NeeEntries {
+  bool sh, sh2, nb;
+  float4 sh_o, sh_d, sh_c, sh2_o, sh2_d, sh2_c, nb_o, nb_d, nb_f;
+};
+
+template<bool G>
+__device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& pp, uint32_t li,
+                                            float inv_lpdf, const SurfaceHit& g,
+                                            const DevMaterial& mt, V3 wo, V3 thr, float ub,
+                                            float vb, float cb, float ul, float vl,
+                                            NeeEntries& e) {
+  const uint32_t req_nd = F_ALL & ~F_DELTA;
+  e.sh = e.sh2 = e.nb = false;
+  const DevLight& l = sc.lights[li];
+  // the BSDF strategy only for area and background lights
+  // (path_renderer.cpp:138-140)
+  bool use_bsdf = pp.strategy != 2 && (light_is_area(l) || light_is_background(l));
+  bool use_light = pp.strategy != 1;
+  if(use_bsdf) {
+    BsdfSample bs = bsdf_sample<G>(mt, g.frame, wo, req_nd, ub, vb, cb);
+    if(!(bs.pdf == 0.f || is_black(bs.f))) {
+      // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf
+      V3 fac = thr * (bs.f * (fabsf(dot(g.n, bs.w)) / bs.pdf)) * inv_lpdf;
+      if(light_is_area(l)) {
+        e.nb = true;
+        e.nb_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
+        e.nb_d = make_float4(bs.w.x, bs.w.y, bs.w.z, bs.pdf);
+        e.nb_f = make_float4(fac.x, fac.y, fac.z, u2f(li | (use_light ? 0x80000000u : 0u)));
+      } else {
+        V3 L = background_radiance(sc, l, bs.w);
+        if(!is_black(L)) {
+          float wgt = 1.f;
+          if(use_light) {
+            float lp = light_pivot_pdf<G>(sc, l, bs.w, g.p);
+            wgt = bs.pdf / (bs.pdf + lp);
+          }
+          V3 c = fac * L * wgt;
+          e.sh2 = true;
+          e.sh2_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
+          e.sh2_d = make_float4(bs.w.x, bs.w.y, bs.w.z, INFINITY);
+          e.sh2_c = make_float4(c.x, c.y, c.z, 0.f);
+        }
+      }
+    }
+  }
+  if(use_light) {
+    LightSample ls = light_sample<G>(sc, l, g.p, g.eps, ul, vl);
+    if(!(ls.pdf == 0.f || is_black(ls.L))) {
+      V3 f = bsdf_eval<G>(mt, g.frame, ls.wi, wo, req_nd);
+      if(!is_black(f)) {
+        float wgt = 1.f;
+        if(use_bsdf) {
+          float bp = bsdf_pdf<G>(mt, g.frame, ls.wi, wo, req_nd);
+          wgt = ls.pdf / (ls.pdf + bp);
+        }
+        V3 c = (f * ls.L * (wgt * fabsf(dot(g.n, ls.wi)) / ls.pdf)) * inv_lpdf * thr;
+        e.sh = true;
+        e.sh_o = make_float4(ls.o.x, ls.o.y, ls.o.z, ls.tmin);
+        e.sh_d = make_float4(ls.d.x, ls.d.y, ls.d.z, ls.tmax);
+        e.sh_c = make_float4(c.x, c.y, c.z, 0.f);
+      }
+    }
+  }
+}
+
+// Appends one vertex's entries with per-thread atomics (the every-light mode,
+// where a path adds a variable number of entries per wave).
+__device__ __forceinline__ void push_entries(WfDev& w, uint32_t slot, const NeeEntries& e) {
+  if(e.sh) {
+    uint32_t at = atomicAdd(ctr_at(w.ctr, C_SHADOW), 1u);
+    w.sh_slot[at] = slot; w.sh_o[at] = e.sh_o; w.sh_d[at] = e.sh_d; w.sh_c[at] = e.sh_c;
+  }
+  if(e.sh2) {
+    uint32_t at = atomicAdd(ctr_at(w.ctr, C_SHADOW), 1u);
+    w.sh_slot[at] = slot; w.sh_o[at] = e.sh2_o; w.sh_d[at] = e.sh2_d; w.sh_c[at] = e.sh2_c;
+  }
+  if(e.nb) {
+    uint32_t at = atomicAdd(ctr_at(w.ctr, C_NEEB), 1u);
+    w.nb_slot[at] = slot; w.nb_o[at] = e.nb_o; w.nb_d[at] = e.nb_d; w.nb_f[at] = e.nb_f;
+  }
+}
+
 template<class J>
 __global__ void wf_shade(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
@@ -528,8 +619,9 @@ __global__ void wf_shade(J jobs, WfDev w) {
     if(base >= n) { break; }
     uint32_t i = base + (threadIdx.x & 31u);
     bool valid = i < n;
-    bool push_sh = false, push_sh2 = false, push_nb = false, cont = false, done = false;
-    float4 sh_o, sh_d, sh_c, sh2_o, sh2_d, sh2_c, nb_o, nb_d, nb_f;
+    bool cont = false, done = false;
+    NeeEntries nee;
+    nee.sh = nee.sh2 = nee.nb = false;
     uint32_t slot = 0;
     if(valid) {
       // index i of the concatenated shade queues
@@ -578,64 +670,25 @@ __global__ void wf_shade(J jobs, WfDev w) {
         Rand4 r1 = rand4(pp.seed, m.x, m.y, blk + 1);
         Rand4 r2 = rand4(pp.seed, m.x, m.y, blk + 2);
         if(bounces >= pp.min_depth && bxdf_matches(mt.bxdf_flags, req_nd) && sc.light_count > 0) {
-          uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, r0.a);
-          float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
-          if(lpdf != 0.f) {
-            const DevLight& l = sc.lights[li];
-            // the BSDF strategy only for area and background lights
-            // (path_renderer.cpp:138-140)
-            bool use_bsdf = pp.strategy != 2 && (light_is_area(l) || light_is_background(l));
-            bool use_light = pp.strategy != 1;
-            if(use_bsdf) {
-              BsdfSample bs = bsdf_sample<J::kGeneral>(mt, g.frame, wo, req_nd, r0.b, r0.c,
-                                                       r0.d);
-              if(!(bs.pdf == 0.f || is_black(bs.f))) {
-                // contribution = f * L * (w |n.wi| / pdf) * thr / light_pick_pdf
-                V3 fac = thr * (bs.f * (fabsf(dot(g.n, bs.w)) / bs.pdf)) * (1.f / lpdf);
-                if(light_is_area(l)) {
-                  // L and w are known once the closest hit is
-                  push_nb = true;
-                  nb_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
-                  nb_d = make_float4(bs.w.x, bs.w.y, bs.w.z, bs.pdf);
-                  nb_f = make_float4(fac.x, fac.y, fac.z,
-                                     u2f(li | (use_light ? 0x80000000u : 0u)));
-                } else {
-                  // a background light counts only if the ray escapes: L and
-                  // w depend on the direction alone, so the ray is an any-hit
-                  // query with its contribution computed here
-                  V3 L = background_radiance(sc, l, bs.w);
-                  if(!is_black(L)) {
-                    float wgt = 1.f;
-                    if(use_light) {
-                      float lp = light_pivot_pdf<J::kGeneral>(sc, l, bs.w, g.p);
-                      wgt = bs.pdf / (bs.pdf + lp);
-                    }
-                    V3 c = fac * L * wgt;
-                    push_sh2 = true;
-                    sh2_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
-                    sh2_d = make_float4(bs.w.x, bs.w.y, bs.w.z, INFINITY);
-                    sh2_c = make_float4(c.x, c.y, c.z, 0.f);
-                  }
-                }
-              }
+          if(J::kGeneral && pp.sample_all_lights) {
+            // every light, with its own random numbers (path_renderer.cpp:
+            // 120-126); entries are appended one by one (this mode is for
+            // scenes with few lights)
+            for(uint32_t li = 0; li < sc.light_count; ++li) {
+              uint32_t b2 = all_lights_block(bounces, li, sc.light_count);
+              Rand4 a = rand4(pp.seed, m.x, m.y, b2);
+              Rand4 b = rand4(pp.seed, m.x, m.y, b2 + 1);
+              NeeEntries e;
+              nee_entries<J::kGeneral>(sc, pp, li, 1.f, g, mt, wo, thr, a.a, a.b, a.c, b.a, b.b,
+                                       e);
+              push_entries(w, slot, e);
             }
-            if(use_light) {
-              LightSample ls = light_sample<J::kGeneral>(sc, l, g.p, g.eps, r1.a, r1.b);
-              if(!(ls.pdf == 0.f || is_black(ls.L))) {
-                V3 f = bsdf_eval<J::kGeneral>(mt, g.frame, ls.wi, wo, req_nd);
-                if(!is_black(f)) {
-                  float wgt = 1.f;
-                  if(use_bsdf) {
-                    float bp = bsdf_pdf<J::kGeneral>(mt, g.frame, ls.wi, wo, req_nd);
-                    wgt = ls.pdf / (ls.pdf + bp);
-                  }
-                  V3 c = (f * ls.L * (wgt * fabsf(dot(g.n, ls.wi)) / ls.pdf)) * (1.f / lpdf) * thr;
-                  push_sh = true;
-                  sh_o = make_float4(ls.o.x, ls.o.y, ls.o.z, ls.tmin);
-                  sh_d = make_float4(ls.d.x, ls.d.y, ls.d.z, ls.tmax);
-                  sh_c = make_float4(c.x, c.y, c.z, 0.f);
-                }
-              }
+          } else {
+            uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, r0.a);
+            float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
+            if(lpdf != 0.f) {
+              nee_entries<J::kGeneral>(sc, pp, li, 1.f / lpdf, g, mt, wo, thr, r0.b, r0.c, r0.d,
+                                       r1.a, r1.b, nee);
             }
           }
         }
@@ -674,26 +727,26 @@ __global__ void wf_shade(J jobs, WfDev w) {
     }
     (void)cont;
     (void)done;
-    uint32_t si = warp_append(ctr_at(w.ctr, C_SHADOW), push_sh);
-    if(push_sh) {
+    uint32_t si = warp_append(ctr_at(w.ctr, C_SHADOW), nee.sh);
+    if(nee.sh) {
       w.sh_slot[si] = slot;
-      w.sh_o[si] = sh_o;
-      w.sh_d[si] = sh_d;
-      w.sh_c[si] = sh_c;
+      w.sh_o[si] = nee.sh_o;
+      w.sh_d[si] = nee.sh_d;
+      w.sh_c[si] = nee.sh_c;
     }
-    uint32_t si2 = warp_append(ctr_at(w.ctr, C_SHADOW), push_sh2);
-    if(push_sh2) {
+    uint32_t si2 = warp_append(ctr_at(w.ctr, C_SHADOW), nee.sh2);
+    if(nee.sh2) {
       w.sh_slot[si2] = slot;
-      w.sh_o[si2] = sh2_o;
-      w.sh_d[si2] = sh2_d;
-      w.sh_c[si2] = sh2_c;
+      w.sh_o[si2] = nee.sh2_o;
+      w.sh_d[si2] = nee.sh2_d;
+      w.sh_c[si2] = nee.sh2_c;
     }
-    uint32_t ni = warp_append(ctr_at(w.ctr, C_NEEB), push_nb);
-    if(push_nb) {
+    uint32_t ni = warp_append(ctr_at(w.ctr, C_NEEB), nee.nb);
+    if(nee.nb) {
       w.nb_slot[ni] = slot;
-      w.nb_o[ni] = nb_o;
-      w.nb_d[ni] = nb_d;
-      w.nb_f[ni] = nb_f;
+      w.nb_o[ni] = nee.nb_o;
+      w.nb_d[ni] = nee.nb_d;
+      w.nb_f[ni] = nee.nb_f;
     }
   }
 }
@@ -918,6 +971,7 @@ struct Wavefront {
   size_t mem_bytes = 0;
   uint32_t capacity = 0;
   uint32_t npix_cap = 0;
+  uint32_t nee_mult = 1;
   // graph cache (rebuilt when parameters change)
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
@@ -941,20 +995,33 @@ void wavefront_destroy(Wavefront* wf) {
   delete wf;
 }
 
-static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
-  if(wf->mem && wf->capacity == capacity && wf->npix_cap >= npix) { return DORT_OK; }
+// Entries a path adds to the direct-lighting queues per wave, relative to
+// one light: every light when the frame samples them all.
+static uint32_t nee_mult(const PtScene& sc, const PtParams& pp) {
+  return pp.sample_all_lights ? std::max(1u, sc.light_count) : 1u;
+}
+
+// Queues of `capacity` path slots for images of up to npix pixels; a path
+// adds up to 2 * nee_mult shadow entries and nee_mult BSDF-strategy entries
+// per wave (nee_mult = the light count when every light is sampled, else 1).
+static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix, uint32_t nee_mult = 1) {
+  if(wf->mem && wf->capacity == capacity && wf->npix_cap >= npix && wf->nee_mult == nee_mult) {
+    return DORT_OK;
+  }
   wf_release(wf);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t Q = capacity;
   size_t f4 = al(Q * sizeof(float4)), u4 = al(Q * sizeof(uint4)), u1 = al(Q * sizeof(uint32_t));
-  size_t f4x2 = al(2 * Q * sizeof(float4)), u1x2 = al(2 * Q * sizeof(uint32_t));
+  size_t f4x2 = al(2 * nee_mult * Q * sizeof(float4));
+  size_t u1x2 = al(2 * nee_mult * Q * sizeof(uint32_t));
+  size_t f4n = al(nee_mult * Q * sizeof(float4)), u1n = al(nee_mult * Q * sizeof(uint32_t));
   size_t sort_temp = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, sort_temp, static_cast<uint32_t*>(nullptr),
                                   static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
                                   static_cast<uint32_t*>(nullptr), int(capacity), 0, kSortBits);
   sort_temp = al(sort_temp);
   size_t bytes = 5 * f4 + u4 + f4 /*hit*/ + (4 + kShadeQueues) * u1 /*queues*/ + u1x2 +
-                 3 * f4x2 /*shadow, two per path*/ + u1 + 3 * f4 /*neeb*/ +
+                 3 * f4x2 /*shadow, two per path*/ + u1n + 3 * f4n /*neeb*/ +
                  al(size_t(npix) * sizeof(float4)) + 5 * u1 /*sort*/ + sort_temp +
                  al(C_COUNT * kCtrStride * 4);
   if(dev_alloc(&wf->mem, bytes) != cudaSuccess) {
@@ -981,10 +1048,10 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.sh_o = reinterpret_cast<float4*>(take(f4x2));
   d.sh_d = reinterpret_cast<float4*>(take(f4x2));
   d.sh_c = reinterpret_cast<float4*>(take(f4x2));
-  d.nb_slot = reinterpret_cast<uint32_t*>(take(u1));
-  d.nb_o = reinterpret_cast<float4*>(take(f4));
-  d.nb_d = reinterpret_cast<float4*>(take(f4));
-  d.nb_f = reinterpret_cast<float4*>(take(f4));
+  d.nb_slot = reinterpret_cast<uint32_t*>(take(u1n));
+  d.nb_o = reinterpret_cast<float4*>(take(f4n));
+  d.nb_d = reinterpret_cast<float4*>(take(f4n));
+  d.nb_f = reinterpret_cast<float4*>(take(f4n));
   d.film = reinterpret_cast<float4*>(take(al(size_t(npix) * sizeof(float4))));
   for(int k = 0; k < 2; ++k) {
     d.sort_key[k] = reinterpret_cast<uint32_t*>(take(u1));
@@ -997,6 +1064,7 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix) {
   d.capacity = capacity;
   wf->capacity = capacity;
   wf->npix_cap = npix;
+  wf->nee_mult = nee_mult;
   wf->mem_bytes = bytes;
   return DORT_OK;
 }
@@ -1114,7 +1182,7 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   if(!s->wavefront) { s->wavefront = new Wavefront(); }
   Wavefront* wf = s->wavefront;
   uint32_t npix = pp.width * pp.height;
-  int rc = wf_alloc(wf, tn.capacity, npix);
+  int rc = wf_alloc(wf, tn.capacity, npix, nee_mult(s->pt, pp));
   if(rc != DORT_OK) { return rc; }
   wf->dev.total_samples = padded_samples(pp);
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
@@ -1148,7 +1216,7 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   if(!s->wavefront) { s->wavefront = new Wavefront(); }
   Wavefront* wf = s->wavefront;
   uint32_t npix = pp.width * pp.height;
-  int rc = wf_alloc(wf, tn.capacity, npix);
+  int rc = wf_alloc(wf, tn.capacity, npix, nee_mult(s->pt, pp));
   if(rc != DORT_OK) { return rc; }
   wf->dev.total_samples = padded_samples(pp);
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
@@ -1265,6 +1333,7 @@ struct WavefrontBatch {
   uint32_t total_pix = 0;
   uint64_t total_samples = 0;
   uint32_t max_depth = 0;
+  uint32_t nee_mult = 1;
   WfTuning tn{};
   std::vector<uint32_t> film_offset;
   std::vector<uint32_t> npix;
@@ -1300,12 +1369,13 @@ int wavefront_batch_create(const PtScene* scenes, const PtParams* params, uint32
     }
     pix = uint32_t(np);
     b->max_depth = std::max(b->max_depth, params[j].max_depth);
+    b->nee_mult = std::max(b->nee_mult, nee_mult(scenes[j], params[j]));
   }
   b->job_count = n;
   b->total_pix = pix;
   b->total_samples = sample;
   b->tn = tn;
-  int rc = wf_alloc(&b->wf, tn.capacity, pix);
+  int rc = wf_alloc(&b->wf, tn.capacity, pix, b->nee_mult);
   if(rc == DORT_OK && (dev_alloc(&b->d_jobs, n * sizeof(WfJob)) != cudaSuccess ||
                        dev_alloc(&b->d_images, size_t(pix) * 3 * sizeof(float)) != cudaSuccess)) {
     cudaGetLastError();

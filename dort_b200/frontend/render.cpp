@@ -595,10 +595,8 @@ static int render_sync(lua_State* l) {
   img->hdr = true;
   img->px.assign(size_t(img->w) * img->h * 3, 0.f);
   if(job->scene->handle) {
-    // the wavefront unless the per-pixel renderer is needed (sample_all_lights)
-    // or the light or bidirectional tracer is asked for
-    const bool wavefront = !job->params.sample_all_lights &&
-                           job->params.renderer == DORT_RENDERER_PT;
+    // the wavefront for "pt", the light or bidirectional tracer when asked for
+    const bool wavefront = job->params.renderer == DORT_RENDERER_PT;
     dort_wavefront_tuning tuning{};
     const dort_wavefront_tuning* tp = nullptr;
     if(wavefront && job->autotune) {

@@ -378,8 +378,9 @@ int dort_gpu_render_device_noalloc(dort_scene* scene, const dort_render_params* 
  * (same parameters, same random numbers per pixel and sample, so the same
  * paths), executed as a wavefront of generate / extend / shade / shadow
  * stages over device-resident path queues with path regeneration, looped
- * inside one CUDA graph per frame.  sample_all_lights is not supported here
- * (DORT_ERR_UNSUPPORTED); use dort_gpu_render for it. */
+ * inside one CUDA graph per frame.  With sample_all_lights every path vertex
+ * queues the direct-lighting rays of every light (the queues then hold that
+ * many entries per path slot). */
 typedef struct dort_wavefront_tuning {
   uint32_t struct_size;        /* sizeof(dort_wavefront_tuning) */
   uint32_t queue_capacity;     /* paths in flight (0: auto, up to 2^24 for a
@@ -424,7 +425,7 @@ int dort_gpu_render_wavefront_device(dort_scene* scene, const dort_render_params
  * path queues mix samples of all jobs, so short jobs do not leave the GPU
  * idle.  A batch snapshots each job's scene (which must stay alive and on the
  * current device) and parameters when it is created; it owns its queues,
- * film and images until destroyed.  sample_all_lights is not supported. */
+ * film and images until destroyed. */
 typedef struct dort_batch_job {
   dort_scene* scene;
   dort_render_params params;
@@ -449,7 +450,7 @@ int dort_gpu_batch_destroy(dort_batch* batch);
  * tunings on the GPU and writes the fastest to out_tuning (struct_size set).
  * Block sizes (trace, shade) of {64, 128, 256} are ranked on a proxy frame
  * (the frame at up to 8 samples per pixel, 2^22 path slots); path-slot
- * capacities 2^22 .. 2^25 on the frame itself, skipping those beyond twice
+ * capacities 2^22 .. 2^26 on the frame itself, skipping those beyond twice
  * its work or beyond the free device memory (about 340 bytes per slot).
  * Each candidate runs twice, the faster run counts.  budget_ms bounds the
  * search (0: 30 s); when it runs out the best so far wins.  out_stats

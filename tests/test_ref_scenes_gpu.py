@@ -104,7 +104,7 @@ def test_reference_scene_megakernel(name, cuda):
 
 @pytest.mark.gpu
 @pytest.mark.skipif(FIX is None, reason="tests/golden/ref_images.npz missing")
-@pytest.mark.parametrize("name", [n for n in NAMES if not CASES[n]["sample_all_lights"]])
+@pytest.mark.parametrize("name", NAMES)
 def test_reference_scene_wavefront(name, cuda):
     _check(name, _render(name, "wavefront"))
 
