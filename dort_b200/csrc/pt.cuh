@@ -556,23 +556,35 @@ DG_HD float env_dir_pdf(const DevEnv& e, V3 d) {
   if(st == 0.f) { return 0.f; }
   return env_dir_uv_pdf(e, du, dv) / (2.f * kPi * kPi * st);
 }
-// PiecewiseDistrib2d::sample_cdf_slice (piecewise_distrib_2d.cpp:47-70)
-DG_HD float env_sample_slice(const float* cdf, uint32_t n_plus_1, float u, uint32_t& idx) {
-  uint32_t begin = 0, end = n_plus_1 - 1;
-  while(begin + 1 < end) {
-    uint32_t mid = begin + (end - begin) / 2;
-    if(DG_LDG(cdf + mid) < u) { begin = mid; } else { end = mid; }
+// One draw from an alias table of n entries (scene_build.cpp build_alias):
+// u picks an entry and its fraction decides between the entry and its alias;
+// the fraction, rescaled, is returned in `rest` as a fresh uniform (about 14
+// bits for tables of 1024 entries: the position inside a texel).
+DG_HD uint32_t alias_draw(const float2* t, uint32_t n, float u, float& rest) {
+  float x = u * float(n);
+  uint32_t i = x < float(n) ? uint32_t(x) : n - 1u;
+  float f = x - float(i);
+  float2 a = DG_LDG(t + i);
+  if(f < a.x) {
+    rest = f / a.x;
+    return i;
   }
-  float c0 = DG_LDG(cdf + begin), c1 = DG_LDG(cdf + begin + 1);
-  idx = begin;
-  return float(begin) + (u - c0) / (c1 - c0);
+  rest = (f - a.x) / (1.f - a.x);
+  return DG_AS_UINT(a.y);
 }
+
+// A direction of the environment light drawn from its texel distribution:
+// the row by its alias table, the column by the row's, the point inside the
+// texel uniform (the distribution PiecewiseDistrib2d::sample draws by
+// inverting its CDFs, piecewise_distrib_2d.cpp:37-70, in two table reads
+// instead of two binary searches).
 DG_HD V3 env_sample_dir(const DevEnv& e, float u, float v, float& du, float& dv, float& pdf) {
-  uint32_t yi, xi;
-  float y = env_sample_slice(e.marginal_cdf, e.h + 1, v, yi);
-  float x = env_sample_slice(e.cond_cdf + size_t(e.w + 1) * yi, e.w + 1, u, xi);
-  du = x / float(e.w);
-  dv = y / float(e.h);
+  float rx, ry;
+  uint32_t yi = alias_draw(e.row_alias, e.h, v, ry);
+  uint32_t xi = alias_draw(e.col_alias + size_t(e.w) * yi, e.w, u, rx);
+  const float below_one = 0.99999994f;
+  du = (float(xi) + fminf(rx, below_one)) / float(e.w);
+  dv = (float(yi) + fminf(ry, below_one)) / float(e.h);
   float st;
   V3 d = env_dir_from_uv(e, du, dv, st);
   pdf = st == 0.f ? 0.f : env_dir_uv_pdf(e, du, dv) / (2.f * kPi * kPi * st);

@@ -70,9 +70,11 @@ struct DevShape {
 // (piecewise_distrib_2d.cpp).
 struct DevEnv {
   const float* rgb;          // w * h * 3
-  const float* marginal_cdf; // h + 1
-  const float* cond_cdf;     // (w + 1) * h
   const float* pdfs;         // w * h
+  // the same distribution as alias tables: rows (h entries), then the
+  // columns of each row (w * h); (probability, alias index as float bits)
+  const float2* row_alias;
+  const float2* col_alias;
   uint32_t w, h;
   float scale[3];
   float up[3], s[3], t[3];

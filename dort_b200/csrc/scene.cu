@@ -220,9 +220,9 @@ static int scene_upload(dort_scene* s, const dort_scene_desc* desc, const HostSc
   pt.bg_light[1] = hs.bg_light[1];
   pt.env = hs.env;
   if((rc = upload(s, hs.env_rgb, &pt.env.rgb)) != DORT_OK) { return rc; }
-  if((rc = upload(s, hs.env_marginal, &pt.env.marginal_cdf)) != DORT_OK) { return rc; }
-  if((rc = upload(s, hs.env_cond, &pt.env.cond_cdf)) != DORT_OK) { return rc; }
   if((rc = upload(s, hs.env_pdfs, &pt.env.pdfs)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.env_row_alias, &pt.env.row_alias)) != DORT_OK) { return rc; }
+  if((rc = upload(s, hs.env_col_alias, &pt.env.col_alias)) != DORT_OK) { return rc; }
   if((rc = upload(s, hs.shapes, &pt.shapes)) != DORT_OK) { return rc; }
   pt.shape_count = uint32_t(hs.shapes.size());
   pt.shape_base = hs.shape_base;

@@ -170,6 +170,39 @@ void shape_local_bounds(const DevShape& s, float lo[3], float hi[3]) {
 
 }  // namespace
 
+// Alias table (Vose's method: M. D. Vose, "A Linear Algorithm for Generating
+// Random Numbers with a Given Distribution", IEEE TSE 17(9), 1991) of the
+// weights w[0..n): entry i = (probability of keeping i, the other index);
+// picking i uniformly and keeping it with that probability, else taking its
+// alias, draws index k with probability w[k] / sum(w).  Weights that sum to
+// zero give every entry probability 1 (the table is then never used).
+static void build_alias(const double* w, uint32_t n, float2* out) {
+  double sum = 0.0;
+  for(uint32_t i = 0; i < n; ++i) { sum += w[i]; }
+  std::vector<double> q(n);
+  std::vector<uint32_t> small, large;
+  for(uint32_t i = 0; i < n; ++i) {
+    q[i] = sum > 0.0 ? w[i] * double(n) / sum : 1.0;
+    (q[i] < 1.0 ? small : large).push_back(i);
+  }
+  for(uint32_t i = 0; i < n; ++i) {
+    uint32_t self = i;
+    float bits;
+    std::memcpy(&bits, &self, 4);
+    out[i] = make_float2(1.f, bits);
+  }
+  while(!small.empty() && !large.empty()) {
+    uint32_t s = small.back(), l = large.back();
+    small.pop_back();
+    large.pop_back();
+    float bits;
+    std::memcpy(&bits, &l, 4);
+    out[s] = make_float2(float(q[s]), bits);
+    q[l] = (q[l] + q[s]) - 1.0;
+    (q[l] < 1.0 ? small : large).push_back(l);
+  }
+}
+
 bool material_to_device(const dort_material& in, DevMaterial& m, std::string& err) {
   return resolve_material(in, m, err);
 }
@@ -487,26 +520,32 @@ bool build_host_scene(const dort_scene_desc* desc, HostScene& hs, std::string& e
         vweight += ct;
       }
     }
-    // PiecewiseDistrib2d (piecewise_distrib_2d.cpp:4-35)
+    // PiecewiseDistrib2d (piecewise_distrib_2d.cpp:4-35): texel probability
+    // value / sum (its pdf over (u, v) is that times w * h); rows chosen by
+    // their sums, columns within a row by their values
     hs.env_pdfs.assign(size_t(w) * h, 0.f);
-    hs.env_marginal.assign(h + 1, 0.f);
-    hs.env_cond.assign(size_t(w + 1) * h, 0.f);
     float sum = 0.f;
     for(uint32_t y = 0; y < h; ++y) {
       float ysum = 0.f;
-      hs.env_cond[size_t(w + 1) * y] = 0.f;
-      for(uint32_t x = 0; x < w; ++x) {
-        ysum += values[size_t(y) * w + x];
-        hs.env_cond[size_t(w + 1) * y + x + 1] = ysum;
-      }
-      float inv = 1.f / ysum;
-      for(uint32_t x = 0; x <= w; ++x) { hs.env_cond[size_t(w + 1) * y + x] *= inv; }
+      for(uint32_t x = 0; x < w; ++x) { ysum += values[size_t(y) * w + x]; }
       sum += ysum;
-      hs.env_marginal[y + 1] = sum;
     }
     float inv_sum = 1.f / sum;
-    for(uint32_t y = 0; y <= h; ++y) { hs.env_marginal[y] *= inv_sum; }
     for(size_t i = 0; i < values.size(); ++i) { hs.env_pdfs[i] = values[i] * inv_sum; }
+    // the same row and column distributions as alias tables (O(1) sampling)
+    std::vector<double> rw(h), cw(w);
+    hs.env_row_alias.resize(h);
+    hs.env_col_alias.resize(size_t(w) * h);
+    for(uint32_t y = 0; y < h; ++y) {
+      double rs = 0.0;
+      for(uint32_t x = 0; x < w; ++x) {
+        cw[x] = values[size_t(y) * w + x];
+        rs += cw[x];
+      }
+      rw[y] = rs;
+      build_alias(cw.data(), w, hs.env_col_alias.data() + size_t(y) * w);
+    }
+    build_alias(rw.data(), h, hs.env_row_alias.data());
     hs.env.w = w;
     hs.env.h = h;
     for(int a = 0; a < 3; ++a) { hs.env.scale[a] = scale[a]; }
@@ -551,9 +590,9 @@ PtScene host_view(const HostScene& hs) {
   sc.bg_light[1] = hs.bg_light[1];
   sc.env = hs.env;
   sc.env.rgb = hs.env_rgb.empty() ? nullptr : hs.env_rgb.data();
-  sc.env.marginal_cdf = hs.env_marginal.empty() ? nullptr : hs.env_marginal.data();
-  sc.env.cond_cdf = hs.env_cond.empty() ? nullptr : hs.env_cond.data();
   sc.env.pdfs = hs.env_pdfs.empty() ? nullptr : hs.env_pdfs.data();
+  sc.env.row_alias = hs.env_row_alias.empty() ? nullptr : hs.env_row_alias.data();
+  sc.env.col_alias = hs.env_col_alias.empty() ? nullptr : hs.env_col_alias.data();
   sc.shapes = hs.shapes.empty() ? nullptr : hs.shapes.data();
   sc.shape_count = uint32_t(hs.shapes.size());
   for(int a = 0; a < 3; ++a) { sc.centroid[a] = hs.centroid[a]; }

@@ -20,7 +20,8 @@ struct HostScene {
   std::vector<float> light_cdf;
   uint32_t bg_count = 0;
   uint32_t bg_light[2] = {0, 0};
-  std::vector<float> env_rgb, env_marginal, env_cond, env_pdfs;
+  std::vector<float> env_rgb, env_pdfs;
+  std::vector<float2> env_row_alias, env_col_alias;
   std::vector<DevShape> shapes;
   std::vector<DevShape> light_shapes;
   uint32_t general = 0;   // needs the general path instantiation (pt.cuh)
