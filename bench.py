@@ -685,7 +685,8 @@ def measure_pt(args, ctx):
     # 567 / 592 / 606 / 616 M samples/s), blocks of 128; by default the
     # autotuner times its candidates (this one among them) on this frame first
     tuning = {"queue_capacity": 1 << 25, "trace_block": 128, "shade_block": 128,
-              "sort_rays": args.sort_rays == "on", "stage_queues": args.stage_queues == "on"}
+              "sort_rays": args.sort_rays == "on", "stage_queues": args.stage_queues == "on",
+              "refill_lanes": args.refill}
     if args.queue_capacity:
         tuning["queue_capacity"] = args.queue_capacity
     tuned = None
@@ -841,6 +842,7 @@ def measure_pt(args, ctx):
                        "autotune": tuned,
                        "sort_rays": tuning["sort_rays"],
                        "stage_queues": tuning["stage_queues"],
+                       "refill_lanes": tuning["refill_lanes"] or "auto",
                        "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
@@ -1122,6 +1124,8 @@ def main():
                          "small values keep a profiled run's device memory small)")
     ap.add_argument("--stage-queues", default="off", choices=["on", "off"],
                     help="stage the shadow queue through bulk copies (TMA) into shared memory")
+    ap.add_argument("--refill", type=int, default=0,
+                    help="pt1080p extension-stage lane refill threshold 1..32 (0: the library's)")
     ap.add_argument("--sort-rays", default="off", choices=["on", "off"],
                     help="sort each wave's extension rays (wavefront)")
     ap.add_argument("--bvh-build", default=None, choices=["host", "device", "ploc"],

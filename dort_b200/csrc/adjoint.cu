@@ -1,11 +1,10 @@
 // Adjoint of the path tracer: gradients of an image loss with respect to
 // per-triangle Lambert albedo and per-triangle emitted radiance, by path
 // replay backpropagation (Vicini, Speierer, Jakob, "Path Replay
-// Backpropagation", SIGGRAPH 2021).  No path vertex is stored: every sample
-// is traced twice from its counter-based random numbers,
-//   pass 1: the sample value L (as the forward render computes it);
-//   pass 2: the same path again, with an observer that keeps the sum A of
-//           the terms seen so far and attributes derivatives:
+// Backpropagation", SIGGRAPH 2021).  Every sample is traced from its
+// counter-based random numbers with an observer that keeps the sum A of the
+// terms seen so far and attributes derivatives once the sample value L is
+// known:
 //     - a Lambert vertex on triangle t: every later term of the sample is
 //       linear in that vertex's albedo, so dL/d(albedo_t) += (L - A) / albedo_t
 //       (per channel);
@@ -16,6 +15,13 @@
 // weights) are held fixed, which keeps the gradient estimate unbiased.  The
 // image gradient dLoss/dI weights each sample by dLoss/dI(pixel) / spp, and
 // gradients are accumulated with float atomics.
+//
+// One pass per sample: the observer (AdjointLog) records each term's
+// triangle and factor in a short per-thread log and applies them after the
+// path ends, when L is known -- a sample the film drops adds nothing.  A
+// path with more terms than the log holds is traced a second time with an
+// observer that applies each term as it comes (AdjointTape, given L from
+// the first pass): the replay of the paper, which stores no vertex at all.
 //
 // No reference counterpart: the reference renderer has no derivatives.
 #include <cstring>
@@ -79,10 +85,86 @@ struct AdjointTape {
   }
 };
 
+// Terms of one sample, recorded during its path and applied at its end.
+// Entries are float4 (x, y, z, tag), tag = kind << 30 | primitive; a vertex
+// takes two entries (A at the vertex, then the albedo).
+constexpr uint32_t kAdjLog = 32;
+enum : uint32_t { kEvEmission = 0u, kEvDirect = 1u, kEvVertex = 2u };
+constexpr uint32_t kEvPrimMask = (1u << 30) - 1u;
+
+struct AdjointLog {
+  float4 ev[kAdjLog];
+  uint32_t n;
+  bool overflow;
+  bool want_albedo, want_emission;
+  uint32_t tri_count;
+  V3 acc;
+
+  DG_HD void init(bool albedo, bool emission, uint32_t tris) {
+    n = 0;
+    overflow = false;
+    want_albedo = albedo;
+    want_emission = emission;
+    tri_count = tris;
+    acc = v3(0.f, 0.f, 0.f);
+  }
+  DG_HD void push(uint32_t kind, uint32_t prim, V3 v) {
+    if(n >= kAdjLog || prim > kEvPrimMask) { overflow = true; return; }
+    ev[n++] = make_float4(v.x, v.y, v.z, DG_AS_FLOAT(kind << 30 | prim));
+  }
+  DG_HD void emission(uint32_t tri, V3 thr, V3 Le) {
+    acc = acc + thr * Le;
+    if(want_emission && !is_black(Le) && tri < tri_count) { push(kEvEmission, tri, thr); }
+  }
+  DG_HD void background(V3 c) { acc = acc + c; }
+  DG_HD void vertex(uint32_t tri, const DevMaterial& m) {
+    if(!want_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags || tri >= tri_count) { return; }
+    if(n + 2 > kAdjLog) { overflow = true; return; }
+    push(kEvVertex, tri, acc);
+    push(kEvVertex, tri, v3(m.c[0], m.c[1], m.c[2]));
+  }
+  DG_HD void direct(uint32_t light_tri, V3 c) {
+    acc = acc + c;
+    if(want_emission && light_tri != kMiss) { push(kEvDirect, light_tri, c); }
+  }
+  // The recorded terms' derivatives for a sample of value L (the same
+  // expressions as AdjointTape's).
+  __device__ void apply(V3 L, V3 adj, const float* tri_emission, float* d_albedo,
+                        float* d_emission) const {
+    for(uint32_t i = 0; i < n; ++i) {
+      const float4 e = ev[i];
+      const uint32_t tag = DG_AS_UINT(e.w), kind = tag >> 30;
+      const size_t prim = tag & kEvPrimMask;
+      if(kind == kEvEmission) {
+        float* g = d_emission + 3 * prim;
+        atomicAdd(g, adj.x * e.x);
+        atomicAdd(g + 1, adj.y * e.y);
+        atomicAdd(g + 2, adj.z * e.z);
+      } else if(kind == kEvDirect) {
+        const float* le = tri_emission + 3 * prim;
+        float* g = d_emission + 3 * prim;
+        if(le[0] > 0.f) { atomicAdd(g, adj.x * e.x / le[0]); }
+        if(le[1] > 0.f) { atomicAdd(g + 1, adj.y * e.y / le[1]); }
+        if(le[2] > 0.f) { atomicAdd(g + 2, adj.z * e.z / le[2]); }
+      } else {
+        const float4 c = ev[++i];
+        const V3 rem = L - v3(e.x, e.y, e.z);
+        float* g = d_albedo + 3 * prim;
+        if(c.x > 0.f) { atomicAdd(g, adj.x * rem.x / c.x); }
+        if(c.y > 0.f) { atomicAdd(g + 1, adj.y * rem.y / c.y); }
+        if(c.z > 0.f) { atomicAdd(g + 2, adj.z * rem.z / c.z); }
+      }
+    }
+  }
+};
+
 constexpr int kAdjBlock = 128;
+#ifndef DORT_ADJ_MIN_BLOCKS
+#define DORT_ADJ_MIN_BLOCKS 1
+#endif
 
 template<bool G>
-__global__ void __launch_bounds__(kAdjBlock)
+__global__ void __launch_bounds__(kAdjBlock, DORT_ADJ_MIN_BLOCKS)
 adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
                uint32_t per_slice, const float* __restrict__ dl_dimage,
                float* __restrict__ d_albedo, float* __restrict__ d_emission) {
@@ -111,12 +193,17 @@ adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
       fx = float(x) + j.a;
       fy = float(y) + j.b;
     }
-    NoTape none;
-    PathResult r1 = pt_sample<NoTape, G>(sc, pp, pixel, s, fx, fy, none);
+    AdjointLog log;
+    log.init(d_albedo != nullptr, d_emission != nullptr, sc.shape_base);
+    PathResult r1 = pt_sample<AdjointLog, G>(sc, pp, pixel, s, fx, fy, log);
     V3 L = r1.L;
     // samples the film drops have no gradient (renderer.cpp:36-41)
     if(!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) || L.x < 0.f || L.y < 0.f ||
        L.z < 0.f) {
+      continue;
+    }
+    if(!log.overflow) {
+      log.apply(L, adj, sc.tri_emission, d_albedo, d_emission);
       continue;
     }
     AdjointTape tape;

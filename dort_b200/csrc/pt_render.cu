@@ -424,19 +424,22 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
 
 #include "wavefront.h"
 
-static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTuning& tn,
+// The lane-refill threshold of the extension stage when the caller leaves
+// it automatic.
+constexpr uint32_t kDefaultRefill = 32;
+
+// A caller's tuning over the defaults (default_capacity path slots, 128
+// threads per block, no ray sort, no queue staging, the automatic wave
+// bound); false with err set on an invalid field.
+static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacity, WfTuning& tn,
                         std::string& err) {
-  uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  uint64_t total = tiles * 32 * pp.spp;
-  // default: up to 2^24 path slots (about 5.5 GB of path state); more slots
-  // make fewer, fuller waves (1080p at 256 spp: 567 M samples/s at 2^22,
-  // 606 M at 2^24)
-  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 24));
+  tn.capacity = default_capacity;
   tn.trace_block = 128;
   tn.shade_block = 128;
   tn.sort = 0;
   tn.max_waves = 0;
   tn.stage_queues = 0;
+  tn.refill = kDefaultRefill;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
@@ -456,6 +459,11 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
       return false;
     }
     if(t->sort_rays == 1) { tn.sort = 1; }
+    if(t->refill_lanes > 32) {
+      err = "refill_lanes must be 0 (auto) or 1..32";
+      return false;
+    }
+    if(t->refill_lanes) { tn.refill = t->refill_lanes; }
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
   if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
@@ -469,6 +477,16 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
     }
   }
   return true;
+}
+
+static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTuning& tn,
+                        std::string& err) {
+  uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
+  uint64_t total = tiles * 32 * pp.spp;
+  // default: up to 2^24 path slots (about 5.5 GB of path state); more slots
+  // make fewer, fuller waves (1080p at 256 spp: 567 M samples/s at 2^22,
+  // 606 M at 2^24)
+  return read_tuning(t, uint32_t(std::min<uint64_t>(total, 1u << 24)), tn, err);
 }
 
 extern "C" int dort_gpu_render_wavefront_device(dort_scene* scene,
@@ -609,39 +627,11 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
     total += uint64_t(params[j].width) * params[j].height * params[j].spp;
   }
   WfTuning tn;
+  std::string terr;
   // batches keep 2^22 slots: the batch workload measured 192 M samples/s at
   // 2^22 and 187 M at 2^24
-  tn.capacity = uint32_t(std::min<uint64_t>(total, 1u << 22));
-  tn.trace_block = 128;
-  tn.shade_block = 128;
-  tn.sort = 0;
-  tn.max_waves = 0;
-  tn.stage_queues = 0;
-  if(tuning) {
-    if(tuning->struct_size != sizeof(dort_wavefront_tuning)) {
-      return fail(DORT_ERR_INVALID, "dort_wavefront_tuning.struct_size mismatch (ABI version)");
-    }
-    tn.max_waves = tuning->max_waves;
-    if(tuning->stage_queues > 2) {
-      return fail(DORT_ERR_INVALID, "stage_queues must be 0 (auto), 1 (on) or 2 (off)");
-    }
-    tn.stage_queues = tuning->stage_queues == 1 ? 1u : 0u;
-    if(tuning->queue_capacity) { tn.capacity = tuning->queue_capacity; }
-    if(tuning->trace_block) { tn.trace_block = tuning->trace_block; }
-    if(tuning->shade_block) { tn.shade_block = tuning->shade_block; }
-    if(tuning->sort_rays > 2) {
-      return fail(DORT_ERR_INVALID, "sort_rays must be 0 (auto), 1 (on) or 2 (off)");
-    }
-    if(tuning->sort_rays == 1) { tn.sort = 1; }
-  }
-  tn.capacity = (tn.capacity + 31u) & ~31u;
-  if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
-    return fail(DORT_ERR_INVALID, "queue_capacity must be 32..2^26");
-  }
-  for(uint32_t b : {tn.trace_block, tn.shade_block}) {
-    if(b < 32 || b > 1024 || b % 32 != 0) {
-      return fail(DORT_ERR_INVALID, "block sizes must be multiples of 32 in 32..1024");
-    }
+  if(!read_tuning(tuning, uint32_t(std::min<uint64_t>(total, 1u << 22)), tn, terr)) {
+    return fail(DORT_ERR_INVALID, terr);
   }
   auto* batch = new dort_batch();
   int rc = wavefront_batch_create(scenes.data(), params.data(), job_count, tn, &batch->impl);

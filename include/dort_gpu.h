@@ -406,7 +406,11 @@ typedef struct dort_wavefront_tuning {
                                   warp and batch of 32 entries, overlapping
                                   the previous batch's traversals); blocks of
                                   at most 256 trace threads */
-  uint32_t reserved[1];
+  uint32_t refill_lanes;       /* 0: auto; 1..32: the extension stage hands a
+                                  finished lane the queue's next ray once at
+                                  least this many of its warp's 32 lanes are
+                                  idle (32: a warp takes new rays only when
+                                  all its rays have finished) */
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel

@@ -123,9 +123,11 @@ def test_l2_loss(cuda):
     np.testing.assert_allclose(g, 2 * (a - b), rtol=1e-6)
 
 
-@pytest.mark.parametrize("roulette", [True, False])
-def test_gradient_equals_the_float64_cpu_gradient(cuda, roulette):
-    w, spp, depth = 24, 8, 6
+@pytest.mark.parametrize("roulette,depth", [(True, 6), (False, 6), (False, 14)])
+def test_gradient_equals_the_float64_cpu_gradient(cuda, roulette, depth):
+    """depth 14 without roulette: long paths record more terms than the
+    per-sample log holds, and those samples take the two-pass replay."""
+    w, spp = 24, 8
     sd = scenes.adjoint_scene(n_tris=2000)
     sc = db.scene_from_dict(sd)
     p = db.render_params(sd["camera"], w, w, spp, max_depth=depth, seed=13, roulette=roulette)
@@ -203,3 +205,18 @@ def test_workload_size_fd_no_roulette(cuda):
     fd = (lp - lm) / (2 * h)
     analytic = float((de.astype(np.float64) * ve).sum())
     assert abs(analytic - fd) <= 0.02 * abs(fd), (analytic, fd)
+
+
+def test_wavefront_renders_with_the_triangle_overrides(cuda):
+    """The per-triangle albedo / emission set by the adjoint entry points
+    belong to the scene: a wavefront frame rendered after them uses them
+    (its cached graph is rebuilt), and after they are replaced, the new ones."""
+    sd, sc, p = _setup(n_tris=2000, w=32, spp=16, depth=4)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    plain, _ = sc.render_wavefront(p)
+    for k in (0.5, 0.25):
+        a = (alb * k).astype(np.float32)
+        img = sc.adjoint_forward(p, a, em)
+        wf, _ = sc.render_wavefront(p)
+        assert np.sqrt(((wf - img) ** 2).mean()) / img.mean() < 2e-3
+        assert img.mean() < 0.9 * plain.mean()

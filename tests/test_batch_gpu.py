@@ -51,9 +51,15 @@ def test_batch_mixed_materials_and_sky(cuda):
 
 
 def test_batch_rejects_bad_jobs(cuda):
+    """Batches render the path tracer only; a light-tracer job is refused
+    (DORT_ERR_UNSUPPORTED), and so is an out-of-range tuning field."""
     sd = scenes.cornell_box()
     sc = db.scene_from_dict(sd)
-    p = db.render_params(sd["camera"], 8, 8, 2, sample_all_lights=True)
+    p = db.render_params(sd["camera"], 8, 8, 2, renderer="lt")
     with pytest.raises(db.DortError) as ex:
         db.Batch([(sc, p)])
     assert ex.value.status == -5
+    p = db.render_params(sd["camera"], 8, 8, 2)
+    with pytest.raises(db.DortError) as ex:
+        db.Batch([(sc, p)], {"refill_lanes": 33})
+    assert ex.value.status == -1 and "refill_lanes" in str(ex.value)
