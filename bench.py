@@ -82,6 +82,18 @@ N_RAYS = 16 * 1024 * 1024
 # profiles/raycast_kernel_1Mtri_16Mrays.md (dram__bytes_read.sum +
 # dram__bytes_write.sum); reported as the roofline's traffic.
 RAYCAST_TRAFFIC_BYTES = 800.7e6
+# The bound that applies to the ray cast beside the HBM roofline (whose
+# algorithmic bytes count the reference's binary-tree work, more than the
+# wide tree does, so its frac exceeds 1): issue slots.  Figures of one
+# launch under ncu --set full (profiles/raycast_kernel_1Mtri_16Mrays.md).
+RAYCAST_LIMITER = {
+    "bound": "issue slots (divergent traversal)",
+    "source": "ncu --set full of one raycast_kernel launch, "
+              "profiles/raycast_kernel_1Mtri_16Mrays.md",
+    "issue_slots_busy": 0.739, "simt_efficiency": 11.6 / 32, "achieved_occupancy": 0.496,
+    "dram_throughput": 0.013,
+    "top_stall": "long_scoreboard, 3.85 cycles per issue",
+}
 WORKLOAD = "raycast: 1M random tris (SAH BVH), 16M rays (8M coherent pinhole 4096x2048 + 8M diffuse bounce), closest hit"
 
 
@@ -484,7 +496,12 @@ def measure_raycast(args, ctx, steps, warmup, cpu_budget=15.0, e2e_steps=20):
                                     "(profiles/raycast_kernel_1Mtri_16Mrays.md)",
                   "peak_source": peak_kind,
                   "bytes_per_ray": bytes_per_ray, "n_node": c["n_node"], "n_tri": c["n_tri"],
-                  "kernel_ms_per_launch": per_launch}
+                  "kernel_ms_per_launch": per_launch,
+                  "frac_note": "algorithmic bytes are the reference's binary-BVH work per "
+                               "ray; the 8-wide tree visits fewer nodes, so frac can exceed "
+                               "1; the applicable bound is in limiter",
+                  "measured_dram_gbs": RAYCAST_TRAFFIC_BYTES / (per_launch / 1e3) / 1e9,
+                  "limiter": RAYCAST_LIMITER}
         line = {
             "metric": "Mrays/s", "value": value, "unit": "Mrays/s", "n_gpus": world,
             "steps": steps, "warmup": warmup, "ms_per_step": ms_max / steps,
@@ -518,6 +535,18 @@ REF_SAMPLE_W, REF_SAMPLE_H = 480, 270
 # per ray; reported as the roofline's traffic.
 EXTEND_TRAFFIC_BYTES = 777.0e6
 EXTEND_TRAFFIC_RAYS = 4194304
+# The bound that applies to the extension stage beside the HBM roofline:
+# issue slots and latency.  Figures of one wf_extend launch under
+# ncu --set full (profiles/wf_extend_pt1080p.md): smsp__issue_active,
+# smsp__thread_inst_executed_per_inst_executed / 32, sm__warps_active,
+# lts__throughput and gpu__dram_throughput as fractions of their peaks.
+EXTEND_LIMITER = {
+    "bound": "issue slots and node-fetch latency (divergent traversal)",
+    "source": "ncu --set full of one wf_extend launch, profiles/wf_extend_pt1080p.md",
+    "issue_slots_busy": 0.453, "simt_efficiency": 9.34 / 32, "achieved_occupancy": 0.374,
+    "l2_throughput": 0.178, "dram_throughput": 0.082,
+    "top_stall": "long_scoreboard (L1/L2 node and stack loads), 9.24 cycles per issue",
+}
 
 _ref_worker_scene = None
 
@@ -685,8 +714,7 @@ def measure_pt(args, ctx):
     # 567 / 592 / 606 / 616 M samples/s), blocks of 128; by default the
     # autotuner times its candidates (this one among them) on this frame first
     tuning = {"queue_capacity": 1 << 25, "trace_block": 128, "shade_block": 128,
-              "sort_rays": args.sort_rays == "on", "stage_queues": args.stage_queues == "on",
-              "refill_lanes": args.refill}
+              "sort_rays": args.sort_rays == "on", "stage_queues": args.stage_queues == "on"}
     if args.queue_capacity:
         tuning["queue_capacity"] = args.queue_capacity
     tuned = None
@@ -820,7 +848,8 @@ def measure_pt(args, ctx):
                   "measured_dram_gbs": ext_rays * EXTEND_TRAFFIC_BYTES / EXTEND_TRAFFIC_RAYS
                                        / (stages["extend"] / 1e3) / 1e9,
                   "stage_ms_per_frame": {k: stages[k] for k in
-                                         ("regen", "extend", "shade", "shadow", "neeb")}}
+                                         ("regen", "extend", "shade", "shadow", "neeb")},
+                  "limiter": EXTEND_LIMITER}
         line = {
             "metric": "samples/s at 1080p equal-RMSE, wavefront vs plain GPU",
             "value": value, "unit": "samples/s", "n_gpus": world, "steps": args.steps,
@@ -842,7 +871,6 @@ def measure_pt(args, ctx):
                        "autotune": tuned,
                        "sort_rays": tuning["sort_rays"],
                        "stage_queues": tuning["stage_queues"],
-                       "refill_lanes": tuning["refill_lanes"] or "auto",
                        "extend_rays_per_frame": stages["extend_rays"],
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
@@ -1065,6 +1093,69 @@ def measure_adjoint(args, ctx, steps, warmup):
     return line
 
 
+C1_W, C1_H, C1_SPP, C1_DEPTH = 256, 256, 64, 8
+C1_WORKLOAD = ("cornell: Cornell box (10 wall tris, two 12-tri boxes, 0.5 x 0.5 quad light), "
+               "256x256, 64 spp, max depth 8")
+
+
+def measure_cornell(args, ctx, steps, warmup):
+    """The Cornell-box configuration (256 x 256, 64 spp, depth 8) with the
+    renderer --renderer names: pt (the megakernel, or --engine wavefront),
+    lt or bdpt; device output, CUDA events; returns its JSON line on rank 0."""
+    import torch
+    import dort_b200 as db
+    from dort_b200 import scenes
+
+    rank, world, local, pg = ctx.rank, ctx.world, ctx.local, ctx.pg
+    dev = torch.device("cuda", local)
+    sd = scenes.cornell_box()
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], C1_W, C1_H, C1_SPP, max_depth=C1_DEPTH,
+                         seed=rank_seed(42, rank), renderer=args.renderer)
+    d_out = torch.empty(C1_W * C1_H * 3, dtype=torch.float32, device=dev)
+    sh = torch.cuda.current_stream(dev).cuda_stream
+    wavefront = args.renderer == "pt" and args.engine == "wavefront"
+
+    def frame():
+        if wavefront:
+            sc.render_wavefront_device(p, d_out.data_ptr(), sh)
+        else:
+            sc.render_device(p, d_out.data_ptr(), sh)
+
+    for _ in range(warmup):
+        frame()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier(pg)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        frame()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(pg, e0.elapsed_time(e1) / 1e3) * 1e3
+    clk = clocks.stop()
+    img = d_out.view(C1_H, C1_W, 3).cpu().numpy()
+    line = None
+    if rank == 0:
+        samples = C1_W * C1_H * C1_SPP * steps * world
+        line = {
+            "metric": "samples/s", "value": samples / (ms / 1e3), "unit": "samples/s",
+            "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms / steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": C1_WORKLOAD, "renderer": args.renderer,
+                       "engine": "wavefront" if wavefront else "megakernel",
+                       "image_mean": float(img.mean()),
+                       "l2": "inputs are a few KB (L2-resident by design of the workload)"},
+            "roofline": None, "cpu_baseline": None, "e2e": None,
+            "gpu_launches": steps * (1 if not wavefront else 0), "clocks": clk,
+        }
+    sc.close()
+    return line
+
+
 def run_dort(args):
     """The GPU arm: one process per GPU; rank 0 prints one JSON line."""
     import torch
@@ -1091,6 +1182,8 @@ def run_dort(args):
         line = measure_batch(args, ctx, args.steps, args.warmup)
     elif args.workload == "adjoint":
         line = measure_adjoint(args, ctx, args.steps, args.warmup)
+    elif args.workload == "cornell":
+        line = measure_cornell(args, ctx, args.steps, args.warmup)
     else:
         line = measure_raycast(args, ctx, args.steps, args.warmup)
     if rank == 0 and line is not None:
@@ -1107,7 +1200,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dort", choices=["dort", "reference"])
     ap.add_argument("--workload", default="pt1080p",
-                    choices=["pt1080p", "raycast", "batch", "adjoint"])
+                    choices=["pt1080p", "raycast", "batch", "adjoint", "cornell"])
+    ap.add_argument("--renderer", default="pt", choices=["pt", "lt", "bdpt"],
+                    help="cornell workload: the renderer")
+    ap.add_argument("--engine", default="megakernel", choices=["megakernel", "wavefront"],
+                    help="cornell workload with the pt renderer: megakernel or wavefront")
     ap.add_argument("--spp", type=int, default=0, help="pt1080p samples per pixel (default 256)")
     ap.add_argument("--converged-spp", type=int, default=20480,
                     help="pt1080p: samples per pixel of the converged frame, half rendered "
@@ -1124,8 +1221,6 @@ def main():
                          "small values keep a profiled run's device memory small)")
     ap.add_argument("--stage-queues", default="off", choices=["on", "off"],
                     help="stage the shadow queue through bulk copies (TMA) into shared memory")
-    ap.add_argument("--refill", type=int, default=0,
-                    help="pt1080p extension-stage lane refill threshold 1..32 (0: the library's)")
     ap.add_argument("--sort-rays", default="off", choices=["on", "off"],
                     help="sort each wave's extension rays (wavefront)")
     ap.add_argument("--bvh-build", default=None, choices=["host", "device", "ploc"],
@@ -1134,7 +1229,8 @@ def main():
     if args.warmup < 3:
         args.warmup = 3
     if args.steps <= 0:
-        args.steps = {"pt1080p": 5, "raycast": 100, "batch": 2, "adjoint": 5}[args.workload]
+        args.steps = {"pt1080p": 5, "raycast": 100, "batch": 2, "adjoint": 5,
+                      "cornell": 20}[args.workload]
     if args.impl == "reference":
         if int(os.environ.get("RANK", "0")) != 0:
             return
@@ -1143,8 +1239,10 @@ def main():
         elif args.workload == "pt1080p":
             run_reference_pt(args)
         else:
-            print(json.dumps({"impl": "reference", "unavailable":
-                              f"the reference has no {args.workload} renderer"}), flush=True)
+            why = ("the reference has no batched or adjoint renderer"
+                   if args.workload in ("batch", "adjoint") else
+                   "the reference arm times the pt1080p and raycast workloads only")
+            print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
         return
     run_dort(args)
 

@@ -159,8 +159,13 @@ struct AdjointLog {
 };
 
 constexpr int kAdjBlock = 128;
+// Resident blocks per SM the register allocation must allow: 3 caps the
+// kernel at 168 registers (214 unbounded, 2 blocks), with a few bytes of
+// spill; the adjoint workload (512 x 512, 64 spp, depth 6, 500k triangles)
+// measured 295 ms against 339 ms per forward + backward.  4 blocks (128
+// registers) spill hundreds of bytes per thread.
 #ifndef DORT_ADJ_MIN_BLOCKS
-#define DORT_ADJ_MIN_BLOCKS 1
+#define DORT_ADJ_MIN_BLOCKS 3
 #endif
 
 template<bool G>

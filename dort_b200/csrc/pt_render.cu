@@ -424,10 +424,6 @@ extern "C" int dort_gpu_host_check_render(const dort_scene_desc* desc,
 
 #include "wavefront.h"
 
-// The lane-refill threshold of the extension stage when the caller leaves
-// it automatic.
-constexpr uint32_t kDefaultRefill = 32;
-
 // A caller's tuning over the defaults (default_capacity path slots, 128
 // threads per block, no ray sort, no queue staging, the automatic wave
 // bound); false with err set on an invalid field.
@@ -439,7 +435,6 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
   tn.sort = 0;
   tn.max_waves = 0;
   tn.stage_queues = 0;
-  tn.refill = kDefaultRefill;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
@@ -459,11 +454,6 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
       return false;
     }
     if(t->sort_rays == 1) { tn.sort = 1; }
-    if(t->refill_lanes > 32) {
-      err = "refill_lanes must be 0 (auto) or 1..32";
-      return false;
-    }
-    if(t->refill_lanes) { tn.refill = t->refill_lanes; }
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
   if(tn.capacity < 32 || tn.capacity > (1u << 26)) {

@@ -1,14 +1,10 @@
 // Ray-cast kernels and their C-ABI entry points.
 //
 // One thread per ray inside a persistent grid (one wave of resident blocks);
-// rays come from a device work counter.  A lane whose ray has finished takes
-// the next ray as soon as at least kRaycastRefill of its warp's 32 lanes are
-// idle (persistent threads with dynamic ray fetch, after Aila and Laine,
-// "Understanding the efficiency of ray traversal on GPUs", HPG 2009), so a
-// warp does not idle until its slowest ray is done; the traversal advances
-// one node step per iteration and the warp re-forms after each.  Rays are
-// read as two 16-byte loads, results written as one u32 + three floats per
-// ray.
+// each warp takes 32 consecutive rays at a time from a device work counter,
+// so warps whose rays finish early pick up new ones instead of idling until
+// the slowest ray of a static block is done.  Rays are read as two 16-byte
+// loads, results written as one u32 + three floats per ray.
 #include <cstring>
 #include <string>
 
@@ -18,13 +14,7 @@
 namespace dort_gpu {
 
 constexpr int kRaycastBlock = 128;
-#ifndef DORT_RAYCAST_REFILL
-#define DORT_RAYCAST_REFILL 32
-#endif
-// idle lanes of a warp that trigger a refill (32: only a fully idle warp
-// takes new rays)
-constexpr uint32_t kRaycastRefill = DORT_RAYCAST_REFILL;
-// The work counter may run past ray_count by one fetch per warp; entries
+// The work counter runs past ray_count by at most one fetch per warp; entries
 // are limited so that it cannot wrap.
 constexpr size_t kRaycastMaxRays = 0xff000000u;
 
@@ -34,47 +24,26 @@ raycast_kernel(TraceScene sc, const float4* __restrict__ rays, uint32_t ray_coun
                uint32_t* __restrict__ out_prim, float* __restrict__ out_tb,
                uint32_t* __restrict__ work) {
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t below = (1u << lane) - 1u;
-  TravState s;
-  TraceStack stack;
-  stack.init();
-  uint32_t ray = 0;
-  bool live = false;
-  bool drained = false;   // warp-uniform: no rays left to fetch
   for(;;) {
-    const uint32_t idle = ~__ballot_sync(0xffffffffu, live);
-    if(idle == 0xffffffffu || (!drained && uint32_t(__popc(idle)) >= kRaycastRefill)) {
-      if(drained) { break; }
-      const uint32_t cnt = __popc(idle);
-      uint32_t base = 0;
-      if(lane == 0) { base = atomicAdd(work, cnt); }
-      base = __shfl_sync(0xffffffffu, base, 0);
-      drained = uint64_t(base) + cnt >= ray_count;
-      if(!live) {
-        const uint32_t i = base + __popc(idle & below);
-        if(i < ray_count) {
-          const float4 r0 = __ldcs(rays + 2 * size_t(i));
-          const float4 r1 = __ldcs(rays + 2 * size_t(i) + 1);
-          trav_init(s, sc, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w);
-          ray = i;
-          live = true;
-        }
-      }
-      if(__ballot_sync(0xffffffffu, live) == 0u) { break; }
-    }
-    if(live && trav_step<ANY_HIT, true, TraceStack, WT>(s, sc, stack)) {
-      const Hit& h = s.best;
+    uint32_t base = 0;
+    if(lane == 0) { base = atomicAdd(work, 32u); }
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if(base >= ray_count) { break; }
+    uint32_t i = base + lane;
+    if(i < ray_count) {
+      float4 r0 = __ldcs(rays + 2 * size_t(i));
+      float4 r1 = __ldcs(rays + 2 * size_t(i) + 1);
+      Hit h = trace_ray<ANY_HIT, true, WT>(sc, r0.x, r0.y, r0.z, r0.w, r1.x, r1.y, r1.z, r1.w);
       if(ANY_HIT) {
-        out_prim[ray] = h.prim != kMiss ? 1u : 0u;
+        out_prim[i] = h.prim != kMiss ? 1u : 0u;
       } else {
-        out_prim[ray] = h.prim;
+        out_prim[i] = h.prim;
         if(h.prim != kMiss) {
-          out_tb[3 * size_t(ray)] = h.t;
-          out_tb[3 * size_t(ray) + 1] = h.b1;
-          out_tb[3 * size_t(ray) + 2] = h.b2;
+          out_tb[3 * size_t(i)] = h.t;
+          out_tb[3 * size_t(i) + 1] = h.b1;
+          out_tb[3 * size_t(i) + 2] = h.b2;
         }
       }
-      live = false;
     }
   }
 }

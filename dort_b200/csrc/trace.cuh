@@ -320,10 +320,11 @@ DG_HD uint32_t node_hitmask_f(const uint4* np, uint4 h0, float ix, float iy, flo
 }
 
 // Traversal state of one ray.  trav_step advances it by one node (the
-// node's child boxes, then the triangles of its leaf children), so a kernel
-// can hand a lane whose ray has finished a new ray between steps (see
-// raycast_kernel) instead of letting it idle until the warp's slowest ray is
-// done.  trace_ray runs the steps of one ray to the end.
+// node's child boxes, then the triangles of its leaf children); trace_ray
+// runs the steps of one ray to the end.  (Handing a finished lane a new ray
+// between steps, with a warp vote per step, measured slower than running
+// each warp's 32 rays to the end: 1,882 against 2,460 Mrays/s on the ray
+// cast at the best threshold, and a slower extension stage at every one.)
 struct TravState {
   float ox, oy, oz, dx, dy, dz, t_min;
   float ix, iy, iz;

@@ -512,83 +512,6 @@ __global__ void wf_extend(J jobs, WfDev w) {
   }
 }
 
-// The extension stage with lane refill (persistent threads with dynamic ray
-// fetch, after Aila and Laine, "Understanding the efficiency of ray
-// traversal on GPUs", HPG 2009): a lane whose ray has finished takes the
-// next ray of the queue as soon as at least `refill_at` of its warp's 32
-// lanes are idle, instead of idling until the warp's slowest ray ends.  The
-// traversal runs one node step per iteration (trav_step), so a warp
-// re-forms after every step.  refill_at = 32 is wf_extend's schedule (a
-// warp refills only when all its rays have finished).  Finished rays join
-// their shade queues at the next refill, where the whole warp takes part.
-template<class J>
-__global__ void wf_extend_refill(J jobs, WfDev w, uint32_t refill_at) {
-  constexpr int kWt = J::kGeneral ? kTriByScene : kTriMt;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t below = (1u << lane) - 1u;
-  const uint32_t cur = wave_of(w) & 1u;
-  const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + cur);
-  const uint32_t* act = w.sorted ? w.sort_val[1] : w.active[cur];
-  uint32_t* cursor = ctr_at(w.ctr, C_F_EXT);
-  TravState s;
-  TraceStack stack;
-  stack.init();
-  uint32_t slot = 0, job = 0;
-  uint32_t kind = kShadeQueues;   // < kShadeQueues: a finished ray not yet queued
-  bool live = false;
-  bool drained = false;           // warp-uniform: the queue has no rays left
-  for(;;) {
-    const uint32_t idle = ~__ballot_sync(0xffffffffu, live);
-    if(idle == 0xffffffffu || (!drained && uint32_t(__popc(idle)) >= refill_at)) {
-      if(!w.sorted) {
-#pragma unroll
-        for(uint32_t k = 0; k < kShadeQueues; ++k) {
-          bool mine = kind == k;
-          uint32_t at = warp_append(ctr_at(w.ctr, C_KQ0 + k), mine);
-          if(mine) { w.kq[k][at] = slot; }
-        }
-      }
-      kind = kShadeQueues;
-      if(drained) { break; }   // every lane idle, nothing left to fetch
-      const uint32_t cnt = __popc(idle);
-      uint32_t base = 0;
-      if(lane == 0) { base = atomicAdd(cursor, cnt); }
-      base = __shfl_sync(0xffffffffu, base, 0);
-      drained = base + cnt >= n;
-      if(!live) {
-        const uint32_t i = base + __popc(idle & below);
-        if(i < n) {
-          slot = act[i];
-          job = J::kBatched ? (w.meta[slot].w >> 8) : 0u;
-          const float4 o = w.ray_o[slot], d = w.ray_d[slot];
-          trav_init(s, jobs.scene(job).trace, o.x, o.y, o.z, o.w, d.x, d.y, d.z, INFINITY);
-          live = true;
-        }
-      }
-      if(__ballot_sync(0xffffffffu, live) == 0u) { break; }
-    }
-    if(live && trav_step<false, false, TraceStack, kWt>(s, jobs.scene(job).trace, stack)) {
-      const PtScene& sc = jobs.scene(job);
-      Hit h = s.best;
-      if(J::kGeneral && sc.shape_count) {
-        h = trace_shapes<false>(sc, v3(s.ox, s.oy, s.oz), s.t_min, v3(s.dx, s.dy, s.dz),
-                                INFINITY, h);
-      }
-      w.hit[slot] = make_float4(h.t, h.b1, h.b2, u2f(h.prim));
-      kind = kMissQueue;
-      if(h.prim != kMiss) {
-        kind = __ldg(&sc.mats[prim_material<J::kGeneral>(sc, h.prim)].kind);
-        if(kind >= kMissQueue) { kind = DORT_MAT_LAMBERT; }
-      }
-      if(w.sorted) {
-        w.hit_kind[slot] = kind;
-        kind = kShadeQueues;
-      }
-      live = false;
-    }
-  }
-}
-
 // The direct lighting of one light at a path vertex (estimate_direct,
 // path_renderer.cpp:135-206) as queue entries, `inv_lpdf` the inverse of the
 // light's choice probability (1 when every light is sampled):
@@ -1163,9 +1086,7 @@ template<class J>
 static WfGrids wf_grids(const WfTuning& tn) {
   WfGrids g;
   g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), int(kRegenBlock));
-  g.ext = tn.refill < 32
-      ? grid_for(reinterpret_cast<const void*>(&wf_extend_refill<J>), int(tn.trace_block))
-      : grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
+  g.ext = grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
   g.sha = grid_for(reinterpret_cast<const void*>(&wf_shade<J>), int(tn.shade_block));
   g.shw = tn.stage_queues
       ? grid_for(reinterpret_cast<const void*>(&wf_shadow<J, true>), int(tn.trace_block))
@@ -1191,11 +1112,7 @@ static void wf_launch_extend(const J& jobs, WfDev& dev, const WfTuning& tn, cons
                              cudaStream_t st) {
   int bt = int(tn.trace_block);
   if(tn.sort) { wf_sort<J>(jobs, dev, g, st); }
-  if(tn.refill < 32) {
-    wf_extend_refill<J><<<g.ext, bt, 0, st>>>(jobs, dev, tn.refill);
-  } else {
-    wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
-  }
+  wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
   if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(dev); }
 }
 

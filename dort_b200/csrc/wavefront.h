@@ -16,7 +16,6 @@ struct WfTuning {
   uint32_t sort;          // 1: sort each wave's rays by direction octant and origin cell
   uint32_t max_waves;     // waves a frame may take (0: the automatic bound)
   uint32_t stage_queues;  // 1: stage the shadow queue through bulk copies (TMA)
-  uint32_t refill;        // 1..31: lane-refill threshold of the extension stage; 32: off
 };
 
 struct Wavefront;

@@ -255,6 +255,8 @@ int dort_gpu_scene_stats(const dort_scene* scene, double out[8]);
  * (mesh_bvh_primitive.cpp:34-45): out_prim[i] = 1 if some triangle is hit
  * with t in [t_min, t_max], else 0; out_tb may be NULL.
  *
+ * ray_count is at most 2^32 - 2^24 (DORT_ERR_INVALID above).
+ *
  * Host-pointer form: rays, out_prim and out_tb are host arrays. */
 int dort_gpu_raycast(dort_scene* scene, const float* rays, size_t ray_count,
                      int any_hit, uint32_t* out_prim, float* out_tb);
@@ -406,11 +408,7 @@ typedef struct dort_wavefront_tuning {
                                   warp and batch of 32 entries, overlapping
                                   the previous batch's traversals); blocks of
                                   at most 256 trace threads */
-  uint32_t refill_lanes;       /* 0: auto; 1..32: the extension stage hands a
-                                  finished lane the queue's next ray once at
-                                  least this many of its warp's 32 lanes are
-                                  idle (32: a warp takes new rays only when
-                                  all its rays have finished) */
+  uint32_t reserved[1];
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel

@@ -39,6 +39,16 @@ def rel_rmse(x, ref):
     return float(np.sqrt(((x - ref) ** 2).mean()) / ref.mean())
 
 
+def forked_pixels(x, ref, tol=1e-4):
+    """Pixels of two renders of the same paths (same random numbers) that
+    differ by more than tol x the reference's mean.  Two kernels compile
+    the same arithmetic with different fused multiply-adds, so a path that
+    grazes an edge or a critical angle can take another branch in one of
+    them; every other pixel agrees to float rounding."""
+    d = np.abs(np.asarray(x, np.float64) - ref).max(axis=-1)
+    return int((d > tol * float(np.mean(ref))).sum())
+
+
 def compare_blocks(A0, A1, B0, B1):
     """compare() on images already reduced to block means."""
     A0, A1, B0, B1 = (np.asarray(x, np.float64) for x in (A0, A1, B0, B1))

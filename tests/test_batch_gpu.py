@@ -51,8 +51,8 @@ def test_batch_mixed_materials_and_sky(cuda):
 
 
 def test_batch_rejects_bad_jobs(cuda):
-    """Batches render the path tracer only; a light-tracer job is refused
-    (DORT_ERR_UNSUPPORTED), and so is an out-of-range tuning field."""
+    """Batches render the path tracer only: a light-tracer job is refused
+    (DORT_ERR_UNSUPPORTED); an out-of-range tuning field is invalid."""
     sd = scenes.cornell_box()
     sc = db.scene_from_dict(sd)
     p = db.render_params(sd["camera"], 8, 8, 2, renderer="lt")
@@ -61,5 +61,5 @@ def test_batch_rejects_bad_jobs(cuda):
     assert ex.value.status == -5
     p = db.render_params(sd["camera"], 8, 8, 2)
     with pytest.raises(db.DortError) as ex:
-        db.Batch([(sc, p)], {"refill_lanes": 33})
-    assert ex.value.status == -1 and "refill_lanes" in str(ex.value)
+        db.Batch([(sc, p)], {"stage_queues": None, "sort_rays": None, "trace_block": 48})
+    assert ex.value.status == -1 and "block sizes" in str(ex.value)

@@ -113,14 +113,18 @@ def test_wavefront_sample_all_lights_equals_megakernel(cuda, variant):
     a, sa = sc.render(p)
     b, sb = sc.render_wavefront(p)
     assert a.mean() > 0
-    assert ptcheck.rel_rmse(b, a) < 2e-3
+    # the same paths: at most a pixel or two whose path forks at a float
+    # rounding difference between the two kernels
+    assert ptcheck.forked_pixels(b, a) <= 2
     assert abs(sa["rays"] - sb["rays"]) <= 0.001 * sa["rays"]
-    # and in a batch, beside a job that picks one light
+    # and in a batch, beside a job that picks one light: the batch's frames
+    # equal the wavefront's single frames
     p1 = db.render_params(sd["camera"], 40, 24, 8, max_depth=6, seed=9)
     bt = db.Batch([(sc, p), (sc, p1)])
     bt.render()
-    assert ptcheck.rel_rmse(bt.image(0), a) < 2e-3
-    assert ptcheck.rel_rmse(bt.image(1), sc.render(p1)[0]) < 2e-3
+    assert ptcheck.forked_pixels(bt.image(0), b) == 0
+    assert ptcheck.forked_pixels(bt.image(1), sc.render_wavefront(p1)[0]) == 0
+    assert ptcheck.forked_pixels(bt.image(1), sc.render(p1)[0]) <= 2
     bt.close()
 
 
@@ -140,26 +144,3 @@ def test_wavefront_queue_shapes(cuda, capacity, block, sort_rays, staged):
                                     "stage_queues": staged})
     assert ptcheck.rel_rmse(b, a) < 2e-3
     assert st["waves"] >= 1
-
-
-@pytest.mark.parametrize("refill,sort_rays", [(1, False), (8, False), (16, False), (31, False),
-                                              (8, True)])
-def test_wavefront_lane_refill(cuda, refill, sort_rays):
-    """The extension stage's lane refill (a finished lane takes the next ray
-    once `refill` lanes of its warp are idle) changes which lane traces which
-    ray, not the rays: the megakernel's image, and the same for a batch."""
-    sd = scenes.cornell_variant("delt")
-    sc = db.scene_from_dict(sd)
-    p = db.render_params(sd["camera"], 32, 24, 16, seed=4)
-    a, _ = sc.render(p)
-    b, st = sc.render_wavefront(p, {"queue_capacity": 4096, "refill_lanes": refill,
-                                    "sort_rays": sort_rays})
-    assert ptcheck.rel_rmse(b, a) < 2e-3
-    sd2 = scenes.cornell_box()
-    sc2 = db.scene_from_dict(sd2)
-    p2 = db.render_params(sd2["camera"], 24, 16, 8, seed=5)
-    bt = db.Batch([(sc, p), (sc2, p2)], {"refill_lanes": refill})
-    bt.render()
-    assert ptcheck.rel_rmse(bt.image(0), a) < 2e-3
-    assert ptcheck.rel_rmse(bt.image(1), sc2.render(p2)[0]) < 2e-3
-    bt.close()
