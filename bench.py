@@ -1074,6 +1074,20 @@ def measure_adjoint(args, ctx, steps, warmup):
     torch.cuda.synchronize()
     dt = max_over_ranks(pg, time.perf_counter() - t0)
     clk = clocks.stop()
+    # the step's parts, timed apart after the timed steps (host clock, each
+    # call returns host arrays): forward render, loss, backward
+    img = sc.adjoint_forward(p, alb, em)
+    loss, g = db.loss_l2(img, target)
+    parts = {}
+    for name, fn in (("forward", lambda: sc.adjoint_forward(p, alb, em)),
+                     ("loss", lambda: db.loss_l2(img, target)),
+                     ("backward", lambda: sc.adjoint_backward(p, g, alb, em))):
+        torch.cuda.synchronize()
+        tp = time.perf_counter()
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        parts[name] = round((time.perf_counter() - tp) / 2 * 1e3, 2)
     line = None
     if rank == 0:
         ms = dt / steps * 1e3
@@ -1082,7 +1096,8 @@ def measure_adjoint(args, ctx, steps, warmup):
             "n_gpus": world, "steps": steps, "warmup": warmup, "ms_per_step": ms,
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": ADJ_WORKLOAD, "tris": int(len(sd["tris"]))},
+            "config": {"workload": ADJ_WORKLOAD, "tris": int(len(sd["tris"])),
+                       "parts_ms": parts},
             "roofline": None, "cpu_baseline": None,
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": int(2 * alb.nbytes * 2 +
                                                                           512 * 512 * 12 * 2),
@@ -1169,7 +1184,7 @@ def run_dort(args):
             sub = {}
             for name, fn in (("raycast", lambda: measure_raycast(args, ctx, 20, 3, cpu_budget=8.0,
                                                                  e2e_steps=5)),
-                             ("adjoint", lambda: measure_adjoint(args, ctx, 3, 1)),
+                             ("adjoint", lambda: measure_adjoint(args, ctx, 3, 3)),
                              ("batch", lambda: measure_batch(args, ctx, 1, 1,
                                                              mega_warmup=False))):
                 t0 = time.time()

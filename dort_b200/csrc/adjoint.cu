@@ -25,7 +25,10 @@
 //
 // No reference counterpart: the reference renderer has no derivatives.
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "common.h"
 #include "launch_plan.h"
@@ -311,19 +314,25 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   }
   size_t npix = size_t(pp.width) * pp.height;
   size_t tbytes = size_t(scene->tri_count) * 3 * sizeof(float);
-  float *d_img = nullptr, *d_ga = nullptr, *d_ge = nullptr;
-  auto cleanup = [&]() {
-    if(d_img) { cudaFree(d_img); }
-    if(d_ga) { cudaFree(d_ga); }
-    if(d_ge) { cudaFree(d_ge); }
-  };
-  if(dev_alloc(&d_img, npix * 3 * sizeof(float)) != cudaSuccess ||
-     (d_albedo && dev_alloc(&d_ga, tbytes ? tbytes : 4) != cudaSuccess) ||
-     (d_emission && dev_alloc(&d_ge, tbytes ? tbytes : 4) != cudaSuccess)) {
-    cudaGetLastError();
-    cleanup();
-    return fail(DORT_ERR_OOM, "cudaMalloc for the adjoint failed");
+  // dLoss/dimage, then the albedo and emission gradients, in one grow-only
+  // buffer held by the scene (256-byte aligned parts)
+  auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
+  const size_t img_bytes = align(npix * 3 * sizeof(float)), tri_bytes = align(tbytes);
+  const size_t need = img_bytes + 2 * tri_bytes;
+  if(scene->adjoint_bytes < need) {
+    if(scene->d_adjoint) { cudaFree(scene->d_adjoint); }
+    scene->d_adjoint = nullptr;
+    scene->adjoint_bytes = 0;
+    if(dev_alloc(&scene->d_adjoint, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DORT_ERR_OOM, "cudaMalloc for the adjoint failed");
+    }
+    scene->adjoint_bytes = need;
   }
+  char* base = static_cast<char*>(scene->d_adjoint);
+  float* d_img = reinterpret_cast<float*>(base);
+  float* d_ga = d_albedo ? reinterpret_cast<float*>(base + img_bytes) : nullptr;
+  float* d_ge = d_emission ? reinterpret_cast<float*>(base + img_bytes + tri_bytes) : nullptr;
   cudaStream_t st = 0;
   bool ok = cudaMemcpyAsync(d_img, dl_dimage, npix * 3 * sizeof(float),
                             cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -334,7 +343,6 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   MegaPlan plan;
   if(megakernel_plan(scene->device, dev, sms, pp.width, pp.height, pp.spp, 0, &plan) != 0) {
-    cleanup();
     return fail(DORT_ERR_INVALID, plan.why);
   }
   const uint32_t slices = plan.slices, per = plan.per, per_slice = plan.per_slice;
@@ -357,7 +365,6 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
     ok = cudaMemcpyAsync(d_emission, d_ge, tbytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
   }
   ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
-  cleanup();
   if(!ok) {
     return fail(DORT_ERR_CUDA, std::string("adjoint failed: ") +
                                cudaGetErrorString(cudaGetLastError()));
@@ -372,13 +379,33 @@ extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t 
     return fail(DORT_ERR_INVALID, "null argument");
   }
   if(count > 0xffffffffull) { return fail(DORT_ERR_INVALID, "count exceeds 2^32 - 1"); }
-  float *d_a = nullptr, *d_b = nullptr, *d_g = nullptr;
-  double* d_l = nullptr;
+  // image, target and gradient (256-byte aligned) and the loss, in a
+  // grow-only buffer per device kept for the process; one call at a time
+  static std::mutex mu;
+  static std::vector<std::pair<void*, size_t>> scratch;
+  std::lock_guard<std::mutex> lock(mu);
+  int dev = 0;
+  DG_CUDA(cudaGetDevice(&dev));
+  if(scratch.size() <= size_t(dev)) { scratch.resize(size_t(dev) + 1, {nullptr, 0}); }
   size_t bytes = count * sizeof(float);
-  bool ok = dev_alloc(&d_a, bytes ? bytes : 4) == cudaSuccess &&
-            dev_alloc(&d_b, bytes ? bytes : 4) == cudaSuccess &&
-            dev_alloc(&d_g, bytes ? bytes : 4) == cudaSuccess &&
-            dev_alloc(&d_l, sizeof(double)) == cudaSuccess;
+  const size_t part = (bytes + 255) & ~size_t(255);
+  const size_t need = 3 * part + sizeof(double);
+  auto& buf = scratch[size_t(dev)];
+  if(buf.second < need) {
+    if(buf.first) { cudaFree(buf.first); }
+    buf = {nullptr, 0};
+    if(dev_alloc(&buf.first, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(DORT_ERR_OOM, "cudaMalloc for the loss failed");
+    }
+    buf.second = need;
+  }
+  char* base = static_cast<char*>(buf.first);
+  float* d_a = reinterpret_cast<float*>(base);
+  float* d_b = reinterpret_cast<float*>(base + part);
+  float* d_g = reinterpret_cast<float*>(base + 2 * part);
+  double* d_l = reinterpret_cast<double*>(base + 3 * part);
+  bool ok = true;
   cudaStream_t st = 0;
   ok = ok && cudaMemcpyAsync(d_a, image, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
   ok = ok && cudaMemcpyAsync(d_b, target, bytes, cudaMemcpyHostToDevice, st) == cudaSuccess;
@@ -392,10 +419,6 @@ extern "C" int dort_gpu_loss_l2(const float* image, const float* target, size_t 
   ok = ok && cudaMemcpyAsync(out_loss, d_l, sizeof(double), cudaMemcpyDeviceToHost, st) ==
                  cudaSuccess;
   ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
-  if(d_a) { cudaFree(d_a); }
-  if(d_b) { cudaFree(d_b); }
-  if(d_g) { cudaFree(d_g); }
-  if(d_l) { cudaFree(d_l); }
   if(!ok) {
     cudaGetLastError();
     return fail(DORT_ERR_CUDA, "l2 loss failed");

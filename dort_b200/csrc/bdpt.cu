@@ -12,9 +12,13 @@
 namespace dort_gpu {
 
 constexpr int kBdptBlock = 128;
+// Resident blocks per SM the register allocation must allow.
+#ifndef DORT_BDPT_MIN_BLOCKS
+#define DORT_BDPT_MIN_BLOCKS 1
+#endif
 
 template<bool G>
-__global__ void __launch_bounds__(kBdptBlock)
+__global__ void __launch_bounds__(kBdptBlock, DORT_BDPT_MIN_BLOCKS)
 bdpt_kernel(PtScene sc, PtParams pp, uint64_t total, float4* __restrict__ acc,
             float* __restrict__ splat, unsigned long long* __restrict__ counters) {
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;

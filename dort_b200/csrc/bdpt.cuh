@@ -15,6 +15,46 @@ namespace dort_gpu {
 
 constexpr uint32_t kBdptVerts = 16;   // vertices per walk: max_depth <= 13
 
+// Out-of-line entry points for the ray, surface, BSDF and light queries
+// that the walks, the (s, t) connections and the MIS weight share.  Each is
+// called from several places of one sample; inlined at every call site, the
+// kernel's code outgrew the SM's instruction cache (ncu on the Cornell
+// workload: "no_instruction" the top stall at 48 cycles per issued
+// instruction, 7 % of issue slots busy).  One copy of each, reached by a
+// call, keeps the loop's code small.
+template<bool ANY_HIT, bool G>
+DG_HD __noinline__ Hit bd_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
+  return scene_trace<ANY_HIT, G>(sc, o, t_min, d, t_max);
+}
+template<bool G>
+DG_HD __noinline__ bool bd_visible(const PtScene& sc, V3 a, float ea, V3 b, float eb) {
+  return lt_visible<G>(sc, a, ea, b, eb);
+}
+template<bool G>
+DG_HD __noinline__ SurfaceHit bd_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+  return surface_at<G>(sc, h, o, d);
+}
+template<bool G>
+DG_HD __noinline__ V3 bd_bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+                                   uint32_t req) {
+  return bsdf_eval<G>(m, fr, wi, wo, req);
+}
+template<bool G>
+DG_HD __noinline__ float bd_bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+                                     uint32_t req) {
+  return bsdf_pdf<G>(m, fr, wi, wo, req);
+}
+template<bool G>
+DG_HD __noinline__ BsdfSample bd_bsdf_sample(const DevMaterial& m, const Frame& fr, V3 w,
+                                             uint32_t req, float u, float v, float c) {
+  return bsdf_sample<G>(m, fr, w, req, u, v, c);
+}
+template<bool G>
+DG_HD __noinline__ LightSample bd_light_sample(const PtScene& sc, const DevLight& l, V3 p,
+                                               float eps, float u, float v) {
+  return light_sample<G>(sc, l, p, eps, u, v);
+}
+
 // Light flags (light.hpp:9-29).
 enum : uint32_t {
   LF_DELTA_POS = 1, LF_DELTA_DIR = 2, LF_AREA = 4, LF_BACKGROUND = 8, LF_DISTANT = 16,
@@ -199,18 +239,18 @@ DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, B
   for(uint32_t b = 0; b <= c.pp.max_depth && n < kBdptVerts; ++b) {
     BVert& prev = lw[n - 1];
     ++rays;
-    Hit h = scene_trace<false, G>(sc, o, eps, d, INFINITY);
+    Hit h = bd_trace<false, G>(sc, o, eps, d, INFINITY);
     if(h.prim == kMiss) { break; }
-    SurfaceHit g = surface_at<G>(sc, h, o, d);
+    SurfaceHit g = bd_surface<G>(sc, h, o, d);
     DevMaterial m = material_at(sc, g);
     V3 wi = -d;
     Rand4 ra = rand4(c.pp.seed, c.pixel, c.sample, kBdLightWalk + 2 * b);
     Rand4 rb = rand4(c.pp.seed, c.pixel, c.sample, kBdLightWalk + 2 * b + 1);
     // Bsdf::sample_camera_f: the same sampling from either side here
-    BsdfSample bs = bsdf_sample<G>(m, g.frame, wi, F_ALL, ra.a, ra.b, ra.c);
+    BsdfSample bs = bd_bsdf_sample<G>(m, g.frame, wi, F_ALL, ra.a, ra.b, ra.c);
     if(bs.pdf == 0.f) { break; }
     V3 wo = normalize(bs.w);
-    float bwd_dir_pdf = bsdf_pdf<G>(m, g.frame, wi, wo, F_ALL);   // light_f_pdf(wi, wo)
+    float bwd_dir_pdf = bd_bsdf_pdf<G>(m, g.frame, wi, wo, F_ALL);   // light_f_pdf(wi, wo)
     float dist2 = length_sq(g.p - prev.p);
     if(dist2 < 1e-9f) { break; }
     V3 scale = prev_f * (fabsf(dot(prev.nn, wi)) / fwd_dir_pdf);
@@ -267,7 +307,7 @@ DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
       scale = scale * (1.f / rr);
     }
     ++rays;
-    Hit h = scene_trace<false, G>(sc, o, eps, d, INFINITY);
+    Hit h = bd_trace<false, G>(sc, o, eps, d, INFINITY);
     if(h.prim == kMiss) {
       // a virtual vertex on the background light picked by power
       // (background_light_distrib)
@@ -288,10 +328,10 @@ DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
       cw[n++] = zb;
       break;
     }
-    SurfaceHit g = surface_at<G>(sc, h, o, d);
+    SurfaceHit g = bd_surface<G>(sc, h, o, d);
     DevMaterial m = material_at(sc, g);
     V3 wo = -d;
-    BsdfSample bs = bsdf_sample<G>(m, g.frame, wo, F_ALL, ra.a, ra.b, ra.c);
+    BsdfSample bs = bd_bsdf_sample<G>(m, g.frame, wo, F_ALL, ra.a, ra.b, ra.c);
     float dist2 = length_sq(g.p - prev.p);
     if(dist2 < 1e-9f) { break; }
     BVert z = bvert_surface(g);
@@ -306,7 +346,7 @@ DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
       break;
     }
     V3 wi = normalize(bs.w);
-    float bwd_dir_pdf = bsdf_pdf<G>(m, g.frame, wo, wi, F_ALL);   // camera_f_pdf(wo, wi)
+    float bwd_dir_pdf = bd_bsdf_pdf<G>(m, g.frame, wo, wi, F_ALL);   // camera_f_pdf(wo, wi)
     prev.bwd_pdf = bwd_dir_pdf * fabsf(dot(prev.nn, wo)) / dist2;
     prev_f = bs.f;
     fwd_dir_pdf = bs.pdf;
@@ -386,7 +426,7 @@ DG_HD float bdpt_weight(const BdptCtx& c, const DevLight& light, const BdptPath&
       const BVert& xi = x.at(i - 2);
       V3 bwi = normalize(xi.p - xm.p), bwo = normalize(xo.p - xm.p);
       DevMaterial m = bvert_material(sc, xm);
-      float dir_pdf = bsdf_pdf<G>(m, bvert_frame(xm), bwo, bwi, F_ALL);   // camera_f_pdf
+      float dir_pdf = bd_bsdf_pdf<G>(m, bvert_frame(xm), bwo, bwi, F_ALL);   // camera_f_pdf
       float d2 = length_sq(xo.p - xm.p);
       if(d2 == 0.f) { return 0.f; }
       return dir_pdf * fabsf(dot(bwo, xo.nn)) / d2;
@@ -418,7 +458,7 @@ DG_HD float bdpt_weight(const BdptCtx& c, const DevLight& light, const BdptPath&
       const BVert& xo = x.at(i + 2);
       V3 bwi = normalize(xi.p - xm.p), bwo = normalize(xo.p - xm.p);
       DevMaterial m = bvert_material(sc, xm);
-      float dir_pdf = bsdf_pdf<G>(m, bvert_frame(xm), bwi, bwo, F_ALL);   // light_f_pdf
+      float dir_pdf = bd_bsdf_pdf<G>(m, bvert_frame(xm), bwi, bwo, F_ALL);   // light_f_pdf
       if(i == 0 && (lf & LF_DISTANT)) { return dir_pdf; }
       return dir_pdf * fabsf(dot(xi.nn, bwi)) / length_sq(xi.p - xm.p);
     }
@@ -499,13 +539,13 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         float cam_pdf;
         V3 cp = camera_sample_point<G>(pp, rc.a, rc.b, cam_pdf);
         if(cam_pdf == 0.f) { continue; }
-        LightSample ls = light_sample<G>(sc, sc.lights[light_i], cp, 0.f, rc.c, rc.d);
+        LightSample ls = bd_light_sample<G>(sc, sc.lights[light_i], cp, 0.f, rc.c, rc.d);
         if(ls.pdf == 0.f || is_black(ls.L)) { continue; }
         float We = camera_eval_importance<G>(pp, cp, ls.wi, sfx, sfy);
         if(We == 0.f) { continue; }
         if(pick == 0.f) { continue; }
         ++rays;
-        Hit h = scene_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
+        Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
         if(h.prim != kMiss) { continue; }
         contrib = ls.L * (We / (cam_pdf * ls.pdf * pick));
       } else if(s == 0 && t >= 2 && last_camera.bg != 0) {
@@ -528,15 +568,15 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         new_light = li;
         if(lp == 0.f) { continue; }
         const DevLight& l2 = sc.lights[li];
-        LightSample ls = light_sample<G>(sc, l2, last_camera.p, last_camera.eps, rc.b, rc.c);
+        LightSample ls = bd_light_sample<G>(sc, l2, last_camera.p, last_camera.eps, rc.b, rc.c);
         if(is_black(ls.L) || ls.pdf == 0.f) { continue; }
         ++rays;
-        Hit h = scene_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
+        Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
         if(h.prim != kMiss) { continue; }
         V3 bwo = normalize(cw[t - 2].p - last_camera.p);
         DevMaterial m = bvert_material(sc, last_camera);
         Frame fr = bvert_frame(last_camera);
-        V3 f = bsdf_eval<G>(m, fr, ls.wi, bwo, F_ALL);
+        V3 f = bd_bsdf_eval<G>(m, fr, ls.wi, bwo, F_ALL);
         if(is_black(f)) { continue; }
         first_light = bvert_empty();
         if(light_flags(l2) & LF_DISTANT) {
@@ -549,7 +589,7 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
           first_light.fwd_pdf = ls.pdf * fabsf(dot(ls.nn, ls.wi)) / length_sq(ls.p - last_camera.p);
         }
         first_light.delta = (light_flags(l2) & LF_DELTA_DIR) ? 1u : 0u;
-        first_light.bwd_pdf = bsdf_pdf<G>(m, fr, ls.wi, bwo, F_ALL);
+        first_light.bwd_pdf = bd_bsdf_pdf<G>(m, fr, ls.wi, bwo, F_ALL);
         fl = &first_light;
         contrib = last_camera.alpha * f * ls.L *
                   (fabsf(dot(last_camera.nn, ls.wi)) / (lp * ls.pdf));
@@ -565,10 +605,10 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         V3 wi = normalize(lw[s - 2].p - last_light.p);
         V3 wo = normalize(cam.p - last_light.p);
         DevMaterial m = bvert_material(sc, last_light);
-        V3 f = bsdf_eval<G>(m, bvert_frame(last_light), wi, wo, F_ALL);
+        V3 f = bd_bsdf_eval<G>(m, bvert_frame(last_light), wi, wo, F_ALL);
         if(is_black(f)) { continue; }
         ++rays;
-        if(!lt_visible<G>(sc, last_light.p, last_light.eps, cam.p, 0.f)) { continue; }
+        if(!bd_visible<G>(sc, last_light.p, last_light.eps, cam.p, 0.f)) { continue; }
         first_camera = bvert_empty();
         first_camera.p = cam.p;
         first_camera.fwd_pdf = cam.pdf;
@@ -580,17 +620,17 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
         // s >= 2 && t >= 2
         const BVert& last_light = lw[s - 1];
         ++rays;
-        if(!lt_visible<G>(sc, last_light.p, last_light.eps, last_camera.p, last_camera.eps)) {
+        if(!bd_visible<G>(sc, last_light.p, last_light.eps, last_camera.p, last_camera.eps)) {
           continue;
         }
         V3 lwi = normalize(lw[s - 2].p - last_light.p);
         V3 cwo = normalize(cw[t - 2].p - last_camera.p);
         V3 wo = normalize(last_camera.p - last_light.p);
         DevMaterial ml = bvert_material(sc, last_light);
-        V3 fl = bsdf_eval<G>(ml, bvert_frame(last_light), lwi, wo, F_ALL);
+        V3 fl = bd_bsdf_eval<G>(ml, bvert_frame(last_light), lwi, wo, F_ALL);
         if(is_black(fl)) { continue; }
         DevMaterial mc = bvert_material(sc, last_camera);
-        V3 fc = bsdf_eval<G>(mc, bvert_frame(last_camera), -wo, cwo, F_ALL);
+        V3 fc = bd_bsdf_eval<G>(mc, bvert_frame(last_camera), -wo, cwo, F_ALL);
         if(is_black(fc)) { continue; }
         float geom = fabsf(dot(wo, last_light.nn)) * fabsf(dot(wo, last_camera.nn)) /
                      length_sq(last_light.p - last_camera.p);

@@ -110,4 +110,7 @@ struct dort_scene {
   // device image of the host-pointer render entry points (grow-only)
   void* d_image = nullptr;
   size_t image_bytes = 0;
+  // the adjoint's image gradient and triangle gradients (grow-only)
+  void* d_adjoint = nullptr;
+  size_t adjoint_bytes = 0;
 };

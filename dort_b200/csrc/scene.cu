@@ -102,6 +102,9 @@ static void scene_free_device(dort_scene* s) {
   if(s->d_image) { cudaFree(s->d_image); }
   s->d_image = nullptr;
   s->image_bytes = 0;
+  if(s->d_adjoint) { cudaFree(s->d_adjoint); }
+  s->d_adjoint = nullptr;
+  s->adjoint_bytes = 0;
   s->d_work = nullptr;
 }
 

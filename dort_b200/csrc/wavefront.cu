@@ -473,8 +473,14 @@ __global__ void wf_classify(WfDev w) {
   }
 }
 
+#ifdef DORT_TRACE_MAXNREG
+#define DORT_TRACE_REGS __maxnreg__(DORT_TRACE_MAXNREG)
+#else
+#define DORT_TRACE_REGS
+#endif
+
 template<class J>
-__global__ void wf_extend(J jobs, WfDev w) {
+__global__ void DORT_TRACE_REGS wf_extend(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
   const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_ACT0 + cur);
   const uint32_t* act = w.sorted ? w.sort_val[1] : w.active[cur];
@@ -823,7 +829,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32
 }
 
 template<class J, bool STAGED>
-__global__ void wf_shadow(J jobs, WfDev w) {
+__global__ void DORT_TRACE_REGS wf_shadow(J jobs, WfDev w) {
   const uint32_t n = *(volatile uint32_t*)ctr_at(w.ctr, C_SHADOW);
   const uint32_t lane = threadIdx.x & 31u;
   if(STAGED && blockDim.x <= 32 * kTmaWarps) {
@@ -912,9 +918,12 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
         wgt = d.w / (d.w + lp);
       }
       V3 c = v3(f.x, f.y, f.z) * L * wgt;
-      uint32_t slot = w.nb_slot[i];
-      float4 s = w.sum[slot];
-      w.sum[slot] = make_float4(s.x + c.x, s.y + c.y, s.z + c.z, 0.f);
+      // with sample_all_lights a path owns one entry per area light, which
+      // may run in the same wave of this kernel: the additions are atomic
+      float* sp = &w.sum[w.nb_slot[i]].x;
+      atomicAdd(sp, c.x);
+      atomicAdd(sp + 1, c.y);
+      atomicAdd(sp + 2, c.z);
     }
 }
 

@@ -145,3 +145,27 @@ def test_wavefront_wave_bound_reports_timeout_then_renders(cuda):
     b.render()
     assert b.stats()["error"] == 1.0
     b.close()
+
+
+@pytest.mark.gpu
+def test_adjoint_allocation_failure_then_recover(cuda):
+    """The adjoint's gradient buffers are the scene's (grown on demand): a
+    failed allocation returns DORT_ERR_OOM and the next call computes the
+    same gradients as a scene that never failed."""
+    sd = scenes.adjoint_scene(n_tris=2000)
+    p = db.render_params(sd["camera"], 24, 24, 4, max_depth=3, seed=2)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    ref_sc = db.scene_from_dict(sd)
+    img = ref_sc.adjoint_forward(p, alb, em)
+    _, g = db.loss_l2(img, np.zeros_like(img))
+    ref_a, ref_e = ref_sc.adjoint_backward(p, g, alb, em)
+    sc = db.scene_from_dict(sd)
+    sc.adjoint_forward(p, alb, em)          # the per-triangle buffers exist now
+    db.debug_fail_alloc(0)
+    with pytest.raises(db.DortError) as e:
+        sc.adjoint_backward(p, g, alb, em)
+    assert e.value.status == OOM
+    db.debug_fail_alloc(-1)
+    da, de = sc.adjoint_backward(p, g, alb, em)
+    np.testing.assert_allclose(da, ref_a, rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(de, ref_e, rtol=1e-4, atol=1e-7)
