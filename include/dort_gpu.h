@@ -482,8 +482,11 @@ int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* 
 /* ---- adjoint --------------------------------------------------------------
  * No reference counterpart.  Differentiable rendering of the "pt" estimator
  * with respect to per-triangle Lambert albedo and per-triangle emitted
- * radiance, by path replay backpropagation (every sample is re-traced from its
- * random numbers; nothing per vertex is stored).
+ * radiance, by path replay backpropagation: the backward pass re-traces every
+ * sample from its random numbers (nothing is kept between the forward and the
+ * backward call), keeping the path's terms in a short per-path log until the
+ * sample's value is known; a path with more terms than the log holds is
+ * traced a second time instead.
  *
  * tri_albedo (tri_count * 3, or NULL) replaces the albedo of every triangle
  * whose material is Lambert; tri_emission (tri_count * 3, or NULL) replaces

@@ -167,5 +167,7 @@ def test_adjoint_allocation_failure_then_recover(cuda):
     assert e.value.status == OOM
     db.debug_fail_alloc(-1)
     da, de = sc.adjoint_backward(p, g, alb, em)
-    np.testing.assert_allclose(da, ref_a, rtol=1e-4, atol=1e-7)
-    np.testing.assert_allclose(de, ref_e, rtol=1e-4, atol=1e-7)
+    # float atomics add in any order: equal to rounding, in norm
+    for got, want in ((da, ref_a), (de, ref_e)):
+        assert np.abs(want).sum() > 0
+        assert np.linalg.norm(got - want) <= 1e-4 * np.linalg.norm(want)
