@@ -242,6 +242,15 @@ class Scene:
                                                         _ptr(de)))
         return da, de
 
+    def adjoint_stats(self) -> dict:
+        """dort_gpu_adjoint_stats: the last backward pass's engine ("wavefront",
+        "megakernel" or "wavefront+megakernel"), samples traced a second time,
+        wavefront rays and waves."""
+        st = (ctypes.c_double * 4)()
+        _abi.check(_abi.lib().dort_gpu_adjoint_stats(self.handle, st))
+        return {"engine": ("wavefront", "megakernel", "wavefront+megakernel")[int(st[0])],
+                "retraced": int(st[1]), "rays": st[2], "waves": int(st[3])}
+
     def render_device_noalloc(self, params: _abi.RenderParams, d_out: int, stream: int = 0):
         """dort_gpu_render_device_noalloc: no device allocation in the call."""
         _abi.check(_abi.lib().dort_gpu_render_device_noalloc(
@@ -266,11 +275,14 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
                   min_depth: int = 0, max_depth: int = 5, only_direct: bool = False,
                   sample_all_lights: bool = False, direct_strategy: str = "mis",
                   seed: int = 42, renderer: str = "pt",
-                  use_t1_paths: bool = True, roulette: bool = True) -> _abi.RenderParams:
+                  use_t1_paths: bool = True, roulette: bool = True,
+                  adjoint_megakernel: bool = False) -> _abi.RenderParams:
     """dort.render.make parameters (lua_render.cpp:102-160) with its defaults;
     `renderer` "pt" (the path tracer), "lt" / "light" (the light tracer) or
     "bdpt" (the bidirectional path tracer, with use_t1_paths).  roulette=False
-    turns off the path tracer's Russian roulette (for derivative checks)."""
+    turns off the path tracer's Russian roulette (for derivative checks);
+    adjoint_megakernel=True runs the adjoint's backward pass as a megakernel
+    instead of the wavefront."""
     p = _abi.RenderParams()
     p.struct_size = ctypes.sizeof(_abi.RenderParams)
     p.width, p.height, p.iterations = width, height, iterations
@@ -281,7 +293,8 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
     p.renderer = {"pt": _abi.RENDERER_PT, "path": _abi.RENDERER_PT, "lt": _abi.RENDERER_LT,
                   "light": _abi.RENDERER_LT, "bdpt": _abi.RENDERER_BDPT}[renderer]
     p.renderer_flags = ((0 if use_t1_paths else _abi.BDPT_NO_T1_PATHS) |
-                        (0 if roulette else _abi.PT_NO_ROULETTE))
+                        (0 if roulette else _abi.PT_NO_ROULETTE) |
+                        (_abi.ADJOINT_MEGAKERNEL if adjoint_megakernel else 0))
     c = p.camera
     c.origin = (ctypes.c_float * 3)(*camera["origin"])
     c.right = (ctypes.c_float * 3)(*camera["right"])
@@ -341,6 +354,12 @@ def bsdf_probe(material: dict, wo, wi=None, u=None, device: bool = True) -> dict
         _ptr(out.get("pdf")), _ptr(out.get("wi")), _ptr(out.get("sf")),
         _ptr(out.get("spdf")), int(device)))
     return out
+
+
+def debug_adjoint_list(entries: int) -> None:
+    """dort_gpu_debug_adjoint_list: caps the backward pass's list of samples
+    traced a second time (negative: the default); for tests."""
+    _abi.check(_abi.lib().dort_gpu_debug_adjoint_list(int(entries)))
 
 
 def debug_fail_alloc(after: int) -> None:

@@ -35,6 +35,7 @@ BVH_BUILD_DEFAULT, BVH_BUILD_HOST, BVH_BUILD_DEVICE, BVH_BUILD_PLOC = 0, 1, 2, 3
 RENDERER_PT, RENDERER_LT, RENDERER_BDPT = 0, 1, 2
 BDPT_NO_T1_PATHS = 1
 PT_NO_ROULETTE = 2
+ADJOINT_MEGAKERNEL = 4
 SCENE_WATERTIGHT = 1
 ABI_VERSION = 2
 
@@ -172,6 +173,10 @@ def lib() -> ctypes.CDLL:
         L.dort_gpu_adjoint_backward.restype = c_i32
         L.dort_gpu_adjoint_backward.argtypes = [c_p, ctypes.POINTER(RenderParams), c_p, c_p, c_p,
                                                 c_p, c_p]
+        L.dort_gpu_debug_adjoint_list.restype = c_i32
+        L.dort_gpu_debug_adjoint_list.argtypes = [ctypes.c_longlong]
+        L.dort_gpu_adjoint_stats.restype = c_i32
+        L.dort_gpu_adjoint_stats.argtypes = [c_p, ctypes.POINTER(ctypes.c_double)]
         L.dort_gpu_loss_l2.restype = c_i32
         L.dort_gpu_loss_l2.argtypes = [c_p, c_p, c_size, ctypes.POINTER(ctypes.c_double), c_p]
         L.dort_gpu_render_device_noalloc.restype = c_i32

@@ -24,16 +24,20 @@
 // the first pass): the replay of the paper, which stores no vertex at all.
 //
 // No reference counterpart: the reference renderer has no derivatives.
+#include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
 
+#include "adjoint.cuh"
 #include "common.h"
 #include "launch_plan.h"
 #include "pt.cuh"
 #include "scene_build.h"
+#include "wavefront.h"
 
 namespace dort_gpu {
 
@@ -69,7 +73,7 @@ struct AdjointTape {
   }
   DG_HD void background(V3 c) { acc = acc + c; }
   DG_HD void vertex(uint32_t tri, const DevMaterial& m) {
-    if(!d_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags || tri >= tri_count) { return; }
+    if(!d_albedo || !adj_albedo_vertex(m, tri, tri_count)) { return; }
     V3 rem = L - acc;
     float* g = d_albedo + 3 * size_t(tri);
     if(m.c[0] > 0.f) { ADJ_ADD(g, adj.x * rem.x / m.c[0]); }
@@ -88,13 +92,7 @@ struct AdjointTape {
   }
 };
 
-// Terms of one sample, recorded during its path and applied at its end.
-// Entries are float4 (x, y, z, tag), tag = kind << 30 | primitive; a vertex
-// takes two entries (A at the vertex, then the albedo).
-constexpr uint32_t kAdjLog = 32;
-enum : uint32_t { kEvEmission = 0u, kEvDirect = 1u, kEvVertex = 2u };
-constexpr uint32_t kEvPrimMask = (1u << 30) - 1u;
-
+// Terms of one sample in a per-thread log (adjoint.cuh's entries).
 struct AdjointLog {
   float4 ev[kAdjLog];
   uint32_t n;
@@ -113,7 +111,7 @@ struct AdjointLog {
   }
   DG_HD void push(uint32_t kind, uint32_t prim, V3 v) {
     if(n >= kAdjLog || prim > kEvPrimMask) { overflow = true; return; }
-    ev[n++] = make_float4(v.x, v.y, v.z, DG_AS_FLOAT(kind << 30 | prim));
+    ev[n++] = adj_entry(kind, prim, v);
   }
   DG_HD void emission(uint32_t tri, V3 thr, V3 Le) {
     acc = acc + thr * Le;
@@ -121,7 +119,7 @@ struct AdjointLog {
   }
   DG_HD void background(V3 c) { acc = acc + c; }
   DG_HD void vertex(uint32_t tri, const DevMaterial& m) {
-    if(!want_albedo || m.kind != DORT_MAT_LAMBERT || !m.bxdf_flags || tri >= tri_count) { return; }
+    if(!want_albedo || !adj_albedo_vertex(m, tri, tri_count)) { return; }
     if(n + 2 > kAdjLog) { overflow = true; return; }
     push(kEvVertex, tri, acc);
     push(kEvVertex, tri, v3(m.c[0], m.c[1], m.c[2]));
@@ -130,38 +128,20 @@ struct AdjointLog {
     acc = acc + c;
     if(want_emission && light_tri != kMiss) { push(kEvDirect, light_tri, c); }
   }
-  // The recorded terms' derivatives for a sample of value L (the same
-  // expressions as AdjointTape's).
   __device__ void apply(V3 L, V3 adj, const float* tri_emission, float* d_albedo,
                         float* d_emission) const {
-    for(uint32_t i = 0; i < n; ++i) {
-      const float4 e = ev[i];
-      const uint32_t tag = DG_AS_UINT(e.w), kind = tag >> 30;
-      const size_t prim = tag & kEvPrimMask;
-      if(kind == kEvEmission) {
-        float* g = d_emission + 3 * prim;
-        atomicAdd(g, adj.x * e.x);
-        atomicAdd(g + 1, adj.y * e.y);
-        atomicAdd(g + 2, adj.z * e.z);
-      } else if(kind == kEvDirect) {
-        const float* le = tri_emission + 3 * prim;
-        float* g = d_emission + 3 * prim;
-        if(le[0] > 0.f) { atomicAdd(g, adj.x * e.x / le[0]); }
-        if(le[1] > 0.f) { atomicAdd(g + 1, adj.y * e.y / le[1]); }
-        if(le[2] > 0.f) { atomicAdd(g + 2, adj.z * e.z / le[2]); }
-      } else {
-        const float4 c = ev[++i];
-        const V3 rem = L - v3(e.x, e.y, e.z);
-        float* g = d_albedo + 3 * prim;
-        if(c.x > 0.f) { atomicAdd(g, adj.x * rem.x / c.x); }
-        if(c.y > 0.f) { atomicAdd(g + 1, adj.y * rem.y / c.y); }
-        if(c.z > 0.f) { atomicAdd(g + 2, adj.z * rem.z / c.z); }
-      }
-    }
+    adj_apply(ev, 1, n, L, adj, tri_emission, d_albedo, d_emission);
   }
 };
 
 constexpr int kAdjBlock = 128;
+// Path slots of the wavefront backward pass (one per 4-sample work unit of
+// the frame, at most this many; each slot's term log takes 512 bytes).
+constexpr uint64_t kAdjSlots = uint64_t(1) << 22;
+// Entries of the list of samples traced a second time (8 bytes each).
+constexpr uint64_t kAdjListMax = uint64_t(1) << 24;
+// A smaller list for tests of the path taken when it fills (-1: none).
+std::atomic<long long> g_adj_list_cap{-1};
 // Resident blocks per SM the register allocation must allow: 3 caps the
 // kernel at 168 registers (214 unbounded, 2 blocks), with a few bytes of
 // spill; the adjoint workload (512 x 512, 64 spp, depth 6, 500k triangles)
@@ -171,6 +151,50 @@ constexpr int kAdjBlock = 128;
 #define DORT_ADJ_MIN_BLOCKS 3
 #endif
 
+// One sample's gradient: its path traced once with the term log; a path
+// whose terms overflow the log is traced again with immediate attribution.
+template<bool G>
+__device__ __forceinline__ void adjoint_sample(const PtScene& sc, const PtParams& pp,
+                                               uint32_t pixel, uint32_t s, V3 adj,
+                                               float* d_albedo, float* d_emission) {
+  const uint32_t x = pixel % pp.width, y = pixel / pp.width;
+  float fx, fy;
+  if(s == 0) {
+    fx = float(x) + 0.5f;
+    fy = float(y) + 0.5f;
+  } else {
+    Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
+    fx = float(x) + j.a;
+    fy = float(y) + j.b;
+  }
+  AdjointLog log;
+  log.init(d_albedo != nullptr, d_emission != nullptr, sc.shape_base);
+  PathResult r1 = pt_sample<AdjointLog, G>(sc, pp, pixel, s, fx, fy, log);
+  V3 L = r1.L;
+  // samples the film drops have no gradient (renderer.cpp:36-41)
+  if(!adj_kept(L)) { return; }
+  if(!log.overflow) {
+    log.apply(L, adj, sc.tri_emission, d_albedo, d_emission);
+    return;
+  }
+  AdjointTape tape;
+  tape.L = L;
+  tape.acc = v3(0.f, 0.f, 0.f);
+  tape.adj = adj;
+  tape.d_albedo = d_albedo;
+  tape.d_emission = d_emission;
+  tape.tri_emission = sc.tri_emission;
+  tape.tri_count = sc.shape_base;
+  pt_sample<AdjointTape, G>(sc, pp, pixel, s, fx, fy, tape);
+}
+
+__device__ __forceinline__ V3 pixel_adj(const float* dl_dimage, uint32_t pixel, float inv_spp) {
+  return v3(dl_dimage[3 * size_t(pixel)], dl_dimage[3 * size_t(pixel) + 1],
+            dl_dimage[3 * size_t(pixel) + 2]) * inv_spp;
+}
+
+// The backward pass as a megakernel: one thread per (pixel, slice of samples),
+// 8 x 4 pixel tiles per warp.
 template<bool G>
 __global__ void __launch_bounds__(kAdjBlock, DORT_ADJ_MIN_BLOCKS)
 adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
@@ -185,45 +209,27 @@ adjoint_replay(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
   uint32_t x = (tile % tiles_x) * 8 + lane % 8, y = (tile / tiles_x) * 4 + lane / 8;
   if(x >= pp.width || y >= pp.height) { return; }
   uint32_t pixel = y * pp.width + x;
-  float inv_spp = 1.f / float(pp.spp);
-  V3 adj = v3(dl_dimage[3 * size_t(pixel)], dl_dimage[3 * size_t(pixel) + 1],
-              dl_dimage[3 * size_t(pixel) + 2]) * inv_spp;
+  V3 adj = pixel_adj(dl_dimage, pixel, 1.f / float(pp.spp));
   if(is_black(adj)) { return; }
   uint32_t s0 = slice * spp_per_slice;
   uint32_t s1 = min(pp.spp, s0 + spp_per_slice);
   for(uint32_t s = s0; s < s1; ++s) {
-    float fx, fy;
-    if(s == 0) {
-      fx = float(x) + 0.5f;
-      fy = float(y) + 0.5f;
-    } else {
-      Rand4 j = rand4(pp.seed, pixel, s, kBlockCamera);
-      fx = float(x) + j.a;
-      fy = float(y) + j.b;
-    }
-    AdjointLog log;
-    log.init(d_albedo != nullptr, d_emission != nullptr, sc.shape_base);
-    PathResult r1 = pt_sample<AdjointLog, G>(sc, pp, pixel, s, fx, fy, log);
-    V3 L = r1.L;
-    // samples the film drops have no gradient (renderer.cpp:36-41)
-    if(!(isfinite(L.x) && isfinite(L.y) && isfinite(L.z)) || L.x < 0.f || L.y < 0.f ||
-       L.z < 0.f) {
-      continue;
-    }
-    if(!log.overflow) {
-      log.apply(L, adj, sc.tri_emission, d_albedo, d_emission);
-      continue;
-    }
-    AdjointTape tape;
-    tape.L = L;
-    tape.acc = v3(0.f, 0.f, 0.f);
-    tape.adj = adj;
-    tape.d_albedo = d_albedo;
-    tape.d_emission = d_emission;
-    tape.tri_emission = sc.tri_emission;
-    tape.tri_count = sc.shape_base;
-    pt_sample<AdjointTape, G>(sc, pp, pixel, s, fx, fy, tape);
+    adjoint_sample<G>(sc, pp, pixel, s, adj, d_albedo, d_emission);
   }
+}
+
+// The samples the wavefront backward could not log (list of pixel, sample).
+template<bool G>
+__global__ void __launch_bounds__(kAdjBlock, DORT_ADJ_MIN_BLOCKS)
+adjoint_replay_list(PtScene sc, PtParams pp, const uint2* __restrict__ list, uint32_t n,
+                    const float* __restrict__ dl_dimage, float* __restrict__ d_albedo,
+                    float* __restrict__ d_emission) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) { return; }
+  const uint2 e = list[i];
+  V3 adj = pixel_adj(dl_dimage, e.x, 1.f / float(pp.spp));
+  if(is_black(adj)) { return; }
+  adjoint_sample<G>(sc, pp, e.x, e.y, adj, d_albedo, d_emission);
 }
 
 __global__ void l2_loss_grad(const float* __restrict__ img, const float* __restrict__ target,
@@ -314,11 +320,22 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   }
   size_t npix = size_t(pp.width) * pp.height;
   size_t tbytes = size_t(scene->tri_count) * 3 * sizeof(float);
-  // dLoss/dimage, then the albedo and emission gradients, in one grow-only
-  // buffer held by the scene (256-byte aligned parts)
+  const bool megakernel = (params->renderer_flags & DORT_ADJOINT_MEGAKERNEL) != 0;
+  // the wavefront's path slots: one per 4-sample work unit, at most 2^22
+  const uint64_t units = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4) * 32 *
+                         ((uint64_t(pp.spp) + 3) / 4);
+  const uint32_t capacity = uint32_t((std::min<uint64_t>(units, kAdjSlots) + 31) & ~uint64_t(31));
+  // samples whose terms overflow the wavefront's log, traced again: a list
+  // of up to every sample of the frame, at most 2^24
+  uint32_t overflow_cap = uint32_t(std::min<uint64_t>(uint64_t(npix) * pp.spp, kAdjListMax));
+  const long long cap_override = g_adj_list_cap.load();
+  if(cap_override >= 0) { overflow_cap = uint32_t(std::min<long long>(cap_override, overflow_cap)); }
+  // dLoss/dimage, the albedo and emission gradients, the overflow list and
+  // its count, in one grow-only buffer held by the scene (256-byte aligned)
   auto align = [](size_t x) { return (x + 255) & ~size_t(255); };
   const size_t img_bytes = align(npix * 3 * sizeof(float)), tri_bytes = align(tbytes);
-  const size_t need = img_bytes + 2 * tri_bytes;
+  const size_t list_bytes = align(size_t(overflow_cap) * sizeof(uint2));
+  const size_t need = img_bytes + 2 * tri_bytes + list_bytes + 256;
   if(scene->adjoint_bytes < need) {
     if(scene->d_adjoint) { cudaFree(scene->d_adjoint); }
     scene->d_adjoint = nullptr;
@@ -333,30 +350,92 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
   float* d_img = reinterpret_cast<float*>(base);
   float* d_ga = d_albedo ? reinterpret_cast<float*>(base + img_bytes) : nullptr;
   float* d_ge = d_emission ? reinterpret_cast<float*>(base + img_bytes + tri_bytes) : nullptr;
+  uint2* d_list = reinterpret_cast<uint2*>(base + img_bytes + 2 * tri_bytes);
+  uint32_t* d_list_n = reinterpret_cast<uint32_t*>(base + img_bytes + 2 * tri_bytes + list_bytes);
   cudaStream_t st = 0;
+  auto zero_gradients = [&]() {
+    bool z = true;
+    if(d_ga) { z = z && cudaMemsetAsync(d_ga, 0, tbytes, st) == cudaSuccess; }
+    if(d_ge) { z = z && cudaMemsetAsync(d_ge, 0, tbytes, st) == cudaSuccess; }
+    return z;
+  };
   bool ok = cudaMemcpyAsync(d_img, dl_dimage, npix * 3 * sizeof(float),
                             cudaMemcpyHostToDevice, st) == cudaSuccess;
-  if(d_ga) { ok = ok && cudaMemsetAsync(d_ga, 0, tbytes, st) == cudaSuccess; }
-  if(d_ge) { ok = ok && cudaMemsetAsync(d_ge, 0, tbytes, st) == cudaSuccess; }
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  MegaPlan plan;
-  if(megakernel_plan(scene->device, dev, sms, pp.width, pp.height, pp.spp, 0, &plan) != 0) {
-    return fail(DORT_ERR_INVALID, plan.why);
-  }
-  const uint32_t slices = plan.slices, per = plan.per, per_slice = plan.per_slice;
-  uint64_t threads = uint64_t(slices) * per_slice;
-  if(ok) {
-    uint32_t grid = uint32_t((threads + kAdjBlock - 1) / kAdjBlock);
-    if(scene_needs_general(scene->pt, pp)) {
-      adjoint_replay<true><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, slices, per, per_slice,
-                                                         d_img, d_ga, d_ge);
-    } else {
-      adjoint_replay<false><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, slices, per, per_slice,
-                                                          d_img, d_ga, d_ge);
+  ok = ok && zero_gradients();
+  const bool general = scene_needs_general(scene->pt, pp);
+  // the megakernel form: one thread per (pixel, slice of samples)
+  auto run_megakernel = [&]() -> int {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    MegaPlan plan;
+    if(megakernel_plan(scene->device, dev, sms, pp.width, pp.height, pp.spp, 0, &plan) != 0) {
+      return fail(DORT_ERR_INVALID, plan.why);
     }
-    ok = cudaGetLastError() == cudaSuccess;
+    const uint64_t threads = uint64_t(plan.slices) * plan.per_slice;
+    const uint32_t grid = uint32_t((threads + kAdjBlock - 1) / kAdjBlock);
+    if(general) {
+      adjoint_replay<true><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, plan.slices, plan.per,
+                                                         plan.per_slice, d_img, d_ga, d_ge);
+    } else {
+      adjoint_replay<false><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, plan.slices, plan.per,
+                                                          plan.per_slice, d_img, d_ga, d_ge);
+    }
+    return cudaGetLastError() == cudaSuccess ? DORT_OK
+                                             : fail(DORT_ERR_CUDA, "adjoint launch failed");
+  };
+  for(double& v : scene->adjoint_stats) { v = 0.0; }
+  if(ok && megakernel) {
+    scene->adjoint_stats[0] = 1.0;
+    rc = run_megakernel();
+    if(rc != DORT_OK) { return rc; }
+  } else if(ok) {
+    ok = cudaMemsetAsync(d_list_n, 0, sizeof(uint32_t), st) == cudaSuccess;
+    WfTuning tn{};
+    tn.capacity = capacity;
+    tn.trace_block = 128;
+    tn.shade_block = 128;
+    if(ok) {
+      rc = wavefront_adjoint(scene, pp, tn, d_img, d_ga, d_ge, d_list, overflow_cap, d_list_n,
+                             st);
+      if(rc != DORT_OK) { return rc; }
+    }
+    uint32_t listed = 0;
+    ok = ok && cudaMemcpyAsync(&listed, d_list_n, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                               st) == cudaSuccess;
+    ok = ok && cudaStreamSynchronize(st) == cudaSuccess;
+    if(ok) {
+      uint64_t rays = 0;
+      uint32_t waves = 0, error = 0;
+      rc = wavefront_adjoint_counters(scene, &rays, &waves, &error, st);
+      if(rc != DORT_OK) { return rc; }
+      if(error) {
+        return fail(DORT_ERR_TIMEOUT, "the adjoint's wavefront reached its wave bound");
+      }
+      scene->adjoint_stats[1] = double(listed);
+      scene->adjoint_stats[2] = double(rays);
+      scene->adjoint_stats[3] = double(waves);
+    }
+    if(ok && listed > overflow_cap) {
+      // more overflowing samples than the list holds: the megakernel form
+      // for every sample instead
+      scene->adjoint_stats[0] = 2.0;
+      ok = zero_gradients();
+      if(ok) {
+        rc = run_megakernel();
+        if(rc != DORT_OK) { return rc; }
+      }
+    } else if(ok && listed > 0) {
+      const uint32_t grid = (listed + kAdjBlock - 1) / kAdjBlock;
+      if(general) {
+        adjoint_replay_list<true><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, d_list, listed,
+                                                                d_img, d_ga, d_ge);
+      } else {
+        adjoint_replay_list<false><<<grid, kAdjBlock, 0, st>>>(scene->pt, pp, d_list, listed,
+                                                                 d_img, d_ga, d_ge);
+      }
+      ok = cudaGetLastError() == cudaSuccess;
+    }
   }
   if(ok && d_albedo) {
     ok = cudaMemcpyAsync(d_albedo, d_ga, tbytes, cudaMemcpyDeviceToHost, st) == cudaSuccess;
@@ -369,6 +448,19 @@ extern "C" int dort_gpu_adjoint_backward(dort_scene* scene, const dort_render_pa
     return fail(DORT_ERR_CUDA, std::string("adjoint failed: ") +
                                cudaGetErrorString(cudaGetLastError()));
   }
+  return DORT_OK;
+} DORT_ABI_CATCH
+
+extern "C" int dort_gpu_debug_adjoint_list(long long entries) try {
+  clear_error();
+  g_adj_list_cap.store(entries < 0 ? -1 : entries);
+  return DORT_OK;
+} DORT_ABI_CATCH
+
+extern "C" int dort_gpu_adjoint_stats(dort_scene* scene, double* out_stats) try {
+  clear_error();
+  if(!scene || !out_stats) { return fail(DORT_ERR_INVALID, "null argument"); }
+  for(int k = 0; k < 4; ++k) { out_stats[k] = scene->adjoint_stats[k]; }
   return DORT_OK;
 } DORT_ABI_CATCH
 

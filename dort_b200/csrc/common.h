@@ -101,6 +101,7 @@ struct dort_scene {
   uint32_t bvh_iterations = 0;          // SAH levels / PLOC iterations of a device build
   std::vector<void*> allocations;       // every device buffer owned by the scene
   dort_gpu::Wavefront* wavefront = nullptr;  // wavefront queues + frame graph (lazy)
+  dort_gpu::Wavefront* adj_wavefront = nullptr;  // the adjoint's backward pass (lazy)
   float* d_tri_albedo = nullptr;        // per-triangle overrides (adjoint), lazy
   float* d_tri_emission = nullptr;
   uint32_t* d_work = nullptr;           // work counters of persistent kernels (scratch)
@@ -113,4 +114,7 @@ struct dort_scene {
   // the adjoint's image gradient and triangle gradients (grow-only)
   void* d_adjoint = nullptr;
   size_t adjoint_bytes = 0;
+  // the last backward pass: engine (0 wavefront, 1 megakernel, 2 wavefront
+  // then megakernel), samples traced a second time, rays, waves
+  double adjoint_stats[4] = {0.0, 0.0, 0.0, 0.0};
 };

@@ -180,7 +180,8 @@ bool make_params(const dort_render_params* rp, PtParams& pp, std::string& err) {
   pp.renderer = rp->renderer;
   pp.use_t1 = (rp->renderer_flags & DORT_BDPT_NO_T1_PATHS) ? 0u : 1u;
   pp.roulette = (rp->renderer_flags & DORT_PT_NO_ROULETTE) ? 0u : 1u;
-  if(rp->renderer_flags & ~(DORT_BDPT_NO_T1_PATHS | DORT_PT_NO_ROULETTE)) {
+  if(rp->renderer_flags &
+     ~(DORT_BDPT_NO_T1_PATHS | DORT_PT_NO_ROULETTE | DORT_ADJOINT_MEGAKERNEL)) {
     err = "unknown renderer_flags bits";
     return false;
   }

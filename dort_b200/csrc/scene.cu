@@ -94,6 +94,7 @@ extern "C" int dort_gpu_debug_fail_alloc(long long after) try {
 
 static void scene_free_device(dort_scene* s) {
   if(s->wavefront) { wavefront_destroy(s->wavefront); s->wavefront = nullptr; }
+  if(s->adj_wavefront) { wavefront_destroy(s->adj_wavefront); s->adj_wavefront = nullptr; }
   for(void* p : s->allocations) { cudaFree(p); }
   s->allocations.clear();
   if(s->d_stage) { cudaFree(s->d_stage); }

@@ -28,6 +28,7 @@
 #include <cstring>
 #include <string>
 
+#include "adjoint.cuh"
 #include "common.h"
 #include "pt.cuh"
 #include "scene_build.h"
@@ -136,6 +137,11 @@ struct WfDev {
   uint32_t capacity;
   uint64_t total_samples;   // work units (see kChunk) of all jobs
   uint32_t max_waves;
+  // the adjoint's term log (adjoint.cuh): entry k of slot s at
+  // adj_log[k * capacity + s], adj_n[s] entries so far (above kAdjLog: the
+  // sample overflowed); null outside the adjoint
+  float4* adj_log;
+  uint32_t* adj_n;
 };
 
 // Where a path's scene and render parameters come from.  A single frame
@@ -147,6 +153,7 @@ template<bool G>
 struct SingleJob {
   static constexpr bool kBatched = false;
   static constexpr bool kGeneral = G;
+  static constexpr bool kAdjoint = false;
   PtScene sc;
   PtParams pp;
   __device__ __forceinline__ uint32_t job_of_sample(uint64_t) const { return 0; }
@@ -168,6 +175,7 @@ template<bool G>
 struct JobTable {
   static constexpr bool kBatched = true;
   static constexpr bool kGeneral = G;
+  static constexpr bool kAdjoint = false;
   const WfJob* jobs;
   uint32_t count;
   __device__ __forceinline__ uint32_t job_of_sample(uint64_t sid) const {
@@ -184,6 +192,44 @@ struct JobTable {
   __device__ __forceinline__ uint32_t film_offset(uint32_t j) const { return jobs[j].film_offset; }
 };
 
+// The backward pass of the adjoint as a wavefront: a single frame whose
+// paths record their terms in the slot's log (shade: emission and Lambert
+// vertices; shadow and BSDF-strategy stages: direct-lighting terms from
+// light triangles) and whose regeneration stage turns a finished sample's
+// log into gradients.  Samples whose terms overflow the log are listed as
+// (pixel, sample) for a second trace (adjoint.cu).
+template<bool G>
+struct AdjointJob : SingleJob<G> {
+  static constexpr bool kAdjoint = true;
+  const float* dl_dimage;   // dLoss/dI (width * height * 3)
+  float* d_albedo;          // gradients (tri_count * 3 each), either may be null
+  float* d_emission;
+  uint2* overflow;          // (pixel, sample) of the samples that overflowed
+  uint32_t* overflow_n;     // their count (may exceed overflow_cap: then all are lost)
+  uint32_t overflow_cap;
+};
+
+// One log entry of `slot` (entries = 1, or 2 for a vertex); the stages that
+// may append to a slot concurrently (several shadow entries per path) pass
+// atomic.
+template<bool ATOMIC>
+__device__ __forceinline__ uint32_t adj_reserve(WfDev& w, uint32_t slot, uint32_t entries) {
+  if(ATOMIC) { return atomicAdd(&w.adj_n[slot], entries); }
+  const uint32_t k = w.adj_n[slot];
+  w.adj_n[slot] = k + entries;
+  return k;
+}
+
+template<bool ATOMIC>
+__device__ __forceinline__ void adj_record(WfDev& w, uint32_t slot, uint32_t kind,
+                                           uint32_t prim, V3 v) {
+  // a primitive index that does not fit the tag overflows the sample
+  const uint32_t k = adj_reserve<ATOMIC>(w, slot, prim > kEvPrimMask ? kAdjLog + 1 : 1u);
+  if(prim <= kEvPrimMask && k < kAdjLog) {
+    w.adj_log[size_t(k) * w.capacity + slot] = adj_entry(kind, prim, v);
+  }
+}
+
 __device__ __forceinline__ uint32_t wave_of(const WfDev& w) {
   return *(volatile uint32_t*)ctr_at(w.ctr, C_WAVES);
 }
@@ -193,6 +239,7 @@ __global__ void wf_init(WfDev w, uint32_t npix) {
   for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < w.capacity; i += stride) {
     w.meta[i] = make_uint4(0u, 0u, 0u, SLOT_FREE);
     w.finished[0][i] = uint32_t(i);    // every slot starts on the free list
+    if(w.adj_n) { w.adj_n[i] = 0u; }
   }
   for(uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < npix; i += stride) {
     w.film[i] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -273,6 +320,29 @@ __device__ __forceinline__ uint32_t regen_scan(uint32_t* cnt) {
   return t;
 }
 
+// The end of a sample in the adjoint's backward pass: its log becomes
+// gradients (samples the film drops have none), or the sample is listed for
+// a second trace when its terms overflowed the log; the log is emptied for
+// the slot's next sample.
+template<class J>
+__device__ __forceinline__ void adj_finish(const J& jobs, WfDev& w, uint32_t slot,
+                                           uint32_t pixel, uint32_t sample, V3 L) {
+  const uint32_t n = w.adj_n[slot];
+  w.adj_n[slot] = 0u;
+  if(n == 0u || !adj_kept(L)) { return; }
+  const float inv_spp = 1.f / float(jobs.pp.spp);
+  const V3 adj = v3(jobs.dl_dimage[3 * size_t(pixel)], jobs.dl_dimage[3 * size_t(pixel) + 1],
+                    jobs.dl_dimage[3 * size_t(pixel) + 2]) * inv_spp;
+  if(is_black(adj)) { return; }
+  if(n > kAdjLog) {
+    const uint32_t k = atomicAdd(jobs.overflow_n, 1u);
+    if(k < jobs.overflow_cap) { jobs.overflow[k] = make_uint2(pixel, sample); }
+    return;
+  }
+  adj_apply(w.adj_log + slot, w.capacity, n, L, adj, jobs.sc.tri_emission, jobs.d_albedo,
+            jobs.d_emission);
+}
+
 template<class J>
 __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32_t slot,
                                            uint32_t cur, bool from_free, RegenShared& sh) {
@@ -295,6 +365,7 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
        s.z >= 0.f) {
       a = make_float4(a.x + s.x, a.y + s.y, a.z + s.z, a.w + 1.f);
     }
+    if constexpr(J::kAdjoint) { adj_finish(jobs, w, slot, m.x, m.y, v3(s.x, s.y, s.z)); }
     uint32_t next_s = m.y + 1u;
     uint32_t unit_end = min(pp.spp, (m.y / kChunk + 1u) * kChunk);
     if(next_s < unit_end) {
@@ -570,7 +641,7 @@ __device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& p
           e.sh2 = true;
           e.sh2_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
           e.sh2_d = make_float4(bs.w.x, bs.w.y, bs.w.z, INFINITY);
-          e.sh2_c = make_float4(c.x, c.y, c.z, 0.f);
+          e.sh2_c = make_float4(c.x, c.y, c.z, u2f(kMiss));
         }
       }
     }
@@ -589,7 +660,8 @@ __device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& p
         e.sh = true;
         e.sh_o = make_float4(ls.o.x, ls.o.y, ls.o.z, ls.tmin);
         e.sh_d = make_float4(ls.d.x, ls.d.y, ls.d.z, ls.tmax);
-        e.sh_c = make_float4(c.x, c.y, c.z, 0.f);
+        // .w: the light's triangle (the adjoint's emission gradient)
+        e.sh_c = make_float4(c.x, c.y, c.z, u2f(l.kind == LIGHT_TRI ? l.tri : kMiss));
       }
     }
   }
@@ -661,7 +733,13 @@ __global__ void wf_shade(J jobs, WfDev w) {
         if(hit) {
           if(g.light) {
             const DevLight& l = sc.lights[g.light - 1];
-            sum = sum + thr * area_eval_radiance(sc, l, g.p, g.n, o);
+            const V3 Le = area_eval_radiance(sc, l, g.p, g.n, o);
+            if constexpr(J::kAdjoint) {
+              if(jobs.d_emission && !is_black(Le) && g.tri < sc.shape_base) {
+                adj_record<false>(w, slot, kEvEmission, g.tri, thr);
+              }
+            }
+            sum = sum + thr * Le;
           }
         } else {
           for(uint32_t k = 0; k < sc.bg_count; ++k) {
@@ -674,6 +752,17 @@ __global__ void wf_shade(J jobs, WfDev w) {
       if(!finished) {
         V3 wo = normalize(-d);
         DevMaterial mt = material_at(sc, g);
+        if constexpr(J::kAdjoint) {
+          // a Lambert vertex: the sum of the terms so far and its albedo
+          if(jobs.d_albedo && adj_albedo_vertex(mt, g.tri, sc.shape_base)) {
+            const uint32_t k = adj_reserve<false>(w, slot, 2u);
+            if(k + 2u <= kAdjLog) {
+              w.adj_log[size_t(k) * w.capacity + slot] = adj_entry(kEvVertex, g.tri, sum);
+              w.adj_log[size_t(k + 1u) * w.capacity + slot] =
+                  adj_entry(kEvVertex, g.tri, v3(mt.c[0], mt.c[1], mt.c[2]));
+            }
+          }
+        }
         uint32_t blk = bounce_block(bounces);
         Rand4 r0 = rand4(pp.seed, m.x, m.y, blk);
         Rand4 r1 = rand4(pp.seed, m.x, m.y, blk + 1);
@@ -776,6 +865,12 @@ __device__ __forceinline__ void shadow_entry(J& jobs, WfDev& w, uint32_t i, floa
     atomicAdd(sp, c.x);
     atomicAdd(sp + 1, c.y);
     atomicAdd(sp + 2, c.z);
+    if constexpr(J::kAdjoint) {
+      const uint32_t light_tri = f2u(c.w);
+      if(jobs.d_emission && light_tri != kMiss) {
+        adj_record<true>(w, slot, kEvDirect, light_tri, v3(c.x, c.y, c.z));
+      }
+    }
   }
 }
 
@@ -880,8 +975,9 @@ __global__ void DORT_TRACE_REGS wf_shadow(J jobs, WfDev w) {
   }
 }
 
-template<bool G>
-__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i);
+template<bool G, bool ADJ>
+__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i,
+                                              bool want_emission);
 
 template<class J>
 __global__ void wf_neeb(J jobs, WfDev w) {
@@ -892,13 +988,16 @@ __global__ void wf_neeb(J jobs, WfDev w) {
     uint32_t i = base + (threadIdx.x & 31u);
     if(i < n) {
       uint32_t job = J::kBatched ? (w.meta[w.nb_slot[i]].w >> 8) : 0u;
-      neeb_one_impl<J::kGeneral>(jobs.scene(job), w, i);
+      bool want_emission = false;
+      if constexpr(J::kAdjoint) { want_emission = jobs.d_emission != nullptr; }
+      neeb_one_impl<J::kGeneral, J::kAdjoint>(jobs.scene(job), w, i, want_emission);
     }
   }
 }
 
-template<bool G>
-__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i) {
+template<bool G, bool ADJ>
+__device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint32_t i,
+                                              bool want_emission) {
     float4 o = w.nb_o[i], d = w.nb_d[i], f = w.nb_f[i];
     uint32_t lw = f2u(f.w);
     const uint32_t li = lw & 0x7fffffffu;
@@ -927,6 +1026,9 @@ __device__ __forceinline__ void neeb_one_impl(const PtScene& sc, WfDev& w, uint3
       atomicAdd(sp, c.x);
       atomicAdd(sp + 1, c.y);
       atomicAdd(sp + 2, c.z);
+      if(ADJ && want_emission && l.kind == LIGHT_TRI) {
+        adj_record<true>(w, w.nb_slot[i], kEvDirect, l.tri, c);
+      }
     }
 }
 
@@ -992,6 +1094,10 @@ struct Wavefront {
   const void* jobs_cached = nullptr;
   WfTuning tune_cached{};
   bool valid = false;
+  // the adjoint's term log (allocated by the adjoint's backward pass only)
+  void* adj_mem = nullptr;
+  uint32_t adj_capacity = 0;
+  uint64_t adj_key[6] = {0, 0, 0, 0, 0, 0};   // the adjoint buffers the graph was given
 };
 
 static void wf_release(Wavefront* wf) {
@@ -999,6 +1105,10 @@ static void wf_release(Wavefront* wf) {
   if(wf->exec) { cudaGraphExecDestroy(wf->exec); wf->exec = nullptr; }
   if(wf->graph) { cudaGraphDestroy(wf->graph); wf->graph = nullptr; }
   if(wf->mem) { cudaFree(wf->mem); wf->mem = nullptr; }
+  if(wf->adj_mem) { cudaFree(wf->adj_mem); wf->adj_mem = nullptr; }
+  wf->adj_capacity = 0;
+  wf->dev.adj_log = nullptr;
+  wf->dev.adj_n = nullptr;
   wf->valid = false;
 }
 
@@ -1235,6 +1345,73 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   wf_resolve<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, d_out);
   DG_CUDA(cudaGetLastError());
   return DORT_OK;
+}
+
+// The adjoint's backward pass (AdjointJob): one wavefront frame whose paths
+// log their terms; the slot logs hold kAdjLog entries of 16 bytes per slot.
+int wavefront_adjoint(dort_scene* s, const PtParams& pp, const WfTuning& tn, const float* d_dl,
+                      float* d_ga, float* d_ge, uint2* d_overflow, uint32_t overflow_cap,
+                      uint32_t* d_overflow_n, cudaStream_t st) {
+  if(!s->adj_wavefront) { s->adj_wavefront = new Wavefront(); }
+  Wavefront* wf = s->adj_wavefront;
+  const uint32_t npix = pp.width * pp.height;
+  int rc = wf_alloc(wf, tn.capacity, npix, nee_mult(s->pt, pp));
+  if(rc != DORT_OK) { return rc; }
+  if(!wf->adj_mem || wf->adj_capacity != tn.capacity) {
+    if(wf->adj_mem) { cudaFree(wf->adj_mem); wf->adj_mem = nullptr; }
+    const size_t log_bytes = size_t(kAdjLog) * tn.capacity * sizeof(float4);
+    if(dev_alloc(&wf->adj_mem, log_bytes + size_t(tn.capacity) * sizeof(uint32_t)) !=
+       cudaSuccess) {
+      cudaGetLastError();
+      wf->adj_capacity = 0;
+      wf->dev.adj_log = nullptr;
+      wf->dev.adj_n = nullptr;
+      return fail(DORT_ERR_OOM, "cudaMalloc of the adjoint's term log failed");
+    }
+    wf->adj_capacity = tn.capacity;
+    wf->dev.adj_log = static_cast<float4*>(wf->adj_mem);
+    wf->dev.adj_n = reinterpret_cast<uint32_t*>(static_cast<char*>(wf->adj_mem) + log_bytes);
+    wf->valid = false;
+  }
+  wf->dev.total_samples = padded_samples(pp);
+  wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
+  const uint64_t key[6] = {uint64_t(uintptr_t(d_dl)), uint64_t(uintptr_t(d_ga)),
+                           uint64_t(uintptr_t(d_ge)), uint64_t(uintptr_t(d_overflow)),
+                           uint64_t(uintptr_t(d_overflow_n)), overflow_cap};
+  if(!wf->valid || std::memcmp(&wf->pp_cached, &pp, sizeof(PtParams)) != 0 ||
+     std::memcmp(&wf->sc_cached, &s->pt, sizeof(PtScene)) != 0 ||
+     std::memcmp(&wf->tune_cached, &tn, sizeof(WfTuning)) != 0 ||
+     std::memcmp(wf->adj_key, key, sizeof(key)) != 0) {
+    auto build = [&](auto job) {
+      job.sc = s->pt;
+      job.pp = pp;
+      job.dl_dimage = d_dl;
+      job.d_albedo = d_ga;
+      job.d_emission = d_ge;
+      job.overflow = d_overflow;
+      job.overflow_n = d_overflow_n;
+      job.overflow_cap = overflow_cap;
+      return wf_build_graph(wf, job, tn);
+    };
+    rc = scene_needs_general(s->pt, pp) ? build(AdjointJob<true>{}) : build(AdjointJob<false>{});
+    if(rc != DORT_OK) { return rc; }
+    wf->pp_cached = pp;
+    std::memcpy(&wf->sc_cached, &s->pt, sizeof(PtScene));
+    std::memcpy(wf->adj_key, key, sizeof(key));
+    wf->jobs_cached = nullptr;
+  }
+  wf_init<<<(std::max(tn.capacity, npix) + 255) / 256, 256, 0, st>>>(wf->dev, npix);
+  DG_CUDA(cudaGetLastError());
+  DG_CUDA(cudaGraphLaunch(wf->exec, st));
+  return DORT_OK;
+}
+
+int wavefront_counters_of(Wavefront* wf, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                          cudaStream_t st);
+
+int wavefront_adjoint_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                               cudaStream_t st) {
+  return wavefront_counters_of(s->adj_wavefront, rays, waves, error, st);
 }
 
 // The same frame as wavefront_render, run wave by wave from the host without

@@ -36,5 +36,15 @@ int wavefront_batch_counters(WavefrontBatch* b, uint64_t* rays, uint32_t* waves,
                              uint32_t* error, cudaStream_t st);
 int wavefront_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
                        cudaStream_t st);
+// The adjoint's backward pass as a wavefront frame (the scene's second
+// wavefront state): gradients added into d_ga / d_ge (either may be null);
+// samples whose terms overflowed the per-slot log are listed in d_overflow
+// as (pixel, sample), their count in *d_overflow_n (which may exceed
+// overflow_cap: the list then holds the first overflow_cap).
+int wavefront_adjoint(dort_scene* s, const PtParams& pp, const WfTuning& tn, const float* d_dl,
+                      float* d_ga, float* d_ge, uint2* d_overflow, uint32_t overflow_cap,
+                      uint32_t* d_overflow_n, cudaStream_t st);
+int wavefront_adjoint_counters(dort_scene* s, uint64_t* rays, uint32_t* waves, uint32_t* error,
+                               cudaStream_t st);
 
 }  // namespace dort_gpu

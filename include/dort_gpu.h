@@ -334,6 +334,10 @@ enum dort_renderer { DORT_RENDERER_PT = 0, DORT_RENDERER_LT = 1, DORT_RENDERER_B
                                       image; for derivative checks, where a
                                       roulette decision that flips under a small
                                       parameter change makes a sample jump */
+#define DORT_ADJOINT_MEGAKERNEL 4u /* dort_gpu_adjoint_backward: one thread per
+                                      (pixel, slice of samples) instead of the
+                                      wavefront (same gradients; ignored by the
+                                      renders) */
 
 typedef struct dort_render_params {
   uint32_t struct_size;        /* sizeof(dort_render_params) */
@@ -500,6 +504,17 @@ int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* 
  *           dLoss/d Le (host, tri_count * 3 each; either may be NULL), for
  *           the same parameters and seed as the forward call.
  * loss_l2:  loss = sum (image - target)^2 and its image gradient, on the GPU. */
+/* The scene's last backward pass (4 doubles): engine (0: wavefront, 1:
+ * megakernel, 2: wavefront whose overflowing samples outnumbered its list,
+ * then the megakernel), samples traced a second time because their terms
+ * overflowed the wavefront's per-path log, wavefront rays, waves. */
+int dort_gpu_adjoint_stats(dort_scene* scene, double* out_stats);
+
+/* Testing aid: the list of samples a wavefront backward pass traces a second
+ * time holds at most `entries` samples (a negative value restores the
+ * default), so that tests reach the path taken when it fills. */
+int dort_gpu_debug_adjoint_list(long long entries);
+
 int dort_gpu_adjoint_forward(dort_scene* scene, const dort_render_params* params,
                              const float* tri_albedo, const float* tri_emission,
                              float* out_image);

@@ -220,3 +220,80 @@ def test_wavefront_renders_with_the_triangle_overrides(cuda):
         wf, _ = sc.render_wavefront(p)
         assert np.sqrt(((wf - img) ** 2).mean()) / img.mean() < 2e-3
         assert img.mean() < 0.9 * plain.mean()
+
+
+@pytest.mark.parametrize("roulette", [True, False])
+def test_wavefront_backward_equals_megakernel_backward(cuda, roulette):
+    """The backward pass as a wavefront (per-slot term logs, applied by the
+    regeneration stage) and as a megakernel trace the same paths: the same
+    gradients to float rounding (atomics add in any order; a path that forks
+    at a rounding difference between the two kernels is rare)."""
+    sd, sc, p = _setup(n_tris=20000, w=48, spp=16, depth=6)
+    pw = db.render_params(sd["camera"], 48, 48, 16, max_depth=6, seed=11, roulette=roulette)
+    pm = db.render_params(sd["camera"], 48, 48, 16, max_depth=6, seed=11, roulette=roulette,
+                          adjoint_megakernel=True)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    rng = np.random.default_rng(12)
+    target = rng.uniform(0.0, 0.3, (48, 48, 3)).astype(np.float32)
+    img = sc.adjoint_forward(pw, alb, em)
+    _, g = db.loss_l2(img, target)
+    wa, we = sc.adjoint_backward(pw, g, alb, em)
+    st = sc.adjoint_stats()
+    assert st["engine"] == "wavefront" and st["retraced"] == 0 and st["waves"] > 0
+    ma, me = sc.adjoint_backward(pm, g, alb, em)
+    assert sc.adjoint_stats()["engine"] == "megakernel"
+    for got, want in ((wa, ma), (we, me)):
+        assert np.abs(want).sum() > 0
+        assert np.linalg.norm(got - want) <= 5e-3 * np.linalg.norm(want)
+
+
+def _closed_box():
+    """The Cornell box closed by a front wall, the camera inside it: without
+    roulette every path runs to max_depth."""
+    sd = scenes.cornell_box()
+    P = np.array([[552.8, 0, 0], [0, 0, 0], [556, 548.8, 0], [0, 548.8, 0]], np.float32) * 0.01
+    base = len(sd["verts"])
+    sd["verts"] = np.concatenate([sd["verts"], P]).astype(np.float32)
+    sd["tris"] = np.concatenate([sd["tris"], np.array([[base, base + 1, base + 3],
+                                                       [base, base + 3, base + 2]],
+                                                      np.uint32)]).astype(np.uint32)
+    sd["tri_material"] = np.concatenate([sd["tri_material"],
+                                         np.zeros(2, np.uint32)]).astype(np.uint32)
+    sd["tri_emission"] = np.concatenate([sd["tri_emission"],
+                                         np.zeros((2, 3), np.float32)]).astype(np.float32)
+    sd["camera"] = scenes.look_at_camera((2.78, 2.73, 0.2), (2.78, 2.73, 5.0), (0.0, 1.0, 0.0),
+                                         1.2)
+    return sd
+
+
+@pytest.mark.parametrize("list_cap,engine", [(None, "wavefront"), (100, "wavefront+megakernel")])
+def test_wavefront_backward_log_overflow(cuda, list_cap, engine):
+    """In a closed box without roulette every path reaches depth 14 and
+    records more terms than a slot's log holds: those samples are traced
+    again from a list, or, when they outnumber the list (capped here), the
+    megakernel form runs for every sample.  Both give the megakernel's
+    gradients."""
+    sd = _closed_box()
+    sc = db.scene_from_dict(sd)
+    n = len(sd["tris"])
+    rng = np.random.default_rng(6)
+    alb = rng.uniform(0.3, 0.8, (n, 3)).astype(np.float32)
+    em = sd["tri_emission"]
+    args = dict(max_depth=14, seed=5, roulette=False)
+    pw = db.render_params(sd["camera"], 32, 32, 4, **args)
+    pm = db.render_params(sd["camera"], 32, 32, 4, adjoint_megakernel=True, **args)
+    img = sc.adjoint_forward(pw, alb, em)
+    _, g = db.loss_l2(img, np.zeros_like(img))
+    if list_cap is not None:
+        db.debug_adjoint_list(list_cap)
+    try:
+        wa, we = sc.adjoint_backward(pw, g, alb, em)
+    finally:
+        db.debug_adjoint_list(-1)
+    st = sc.adjoint_stats()
+    assert st["engine"] == engine, st
+    assert st["retraced"] > 0.9 * 32 * 32 * 4, st
+    ma, me = sc.adjoint_backward(pm, g, alb, em)
+    for got, want in ((wa, ma), (we, me)):
+        assert np.abs(want).sum() > 0
+        assert np.linalg.norm(got - want) <= 5e-3 * np.linalg.norm(want)
