@@ -311,17 +311,20 @@ def render_params(camera: dict, width: int, height: int, iterations: int = 1,
 def wavefront_tuning(queue_capacity: int = 0, trace_block: int = 0,
                      shade_block: int = 0, sort_rays: bool | None = None,
                      max_waves: int = 0,
-                     stage_queues: bool | None = None) -> _abi.WavefrontTuning:
+                     stage_queues: bool | None = None,
+                     deterministic: bool | None = None) -> _abi.WavefrontTuning:
     """dort_wavefront_tuning; zeros select the library's automatic choices.
     max_waves caps the waves of a frame (a frame that reaches it stops with
     DORT_ERR_TIMEOUT); stage_queues stages the shadow queue through bulk
-    copies (TMA) into shared memory."""
+    copies (TMA) into shared memory; deterministic adds the frame's per-unit
+    sums in a fixed order (the same frame renders to the same bits)."""
     t = _abi.WavefrontTuning()
     t.struct_size = ctypes.sizeof(_abi.WavefrontTuning)
     t.queue_capacity, t.trace_block, t.shade_block = queue_capacity, trace_block, shade_block
     t.sort_rays = 0 if sort_rays is None else (1 if sort_rays else 2)
     t.max_waves = max_waves
     t.stage_queues = 0 if stage_queues is None else (1 if stage_queues else 2)
+    t.deterministic = 0 if deterministic is None else (1 if deterministic else 2)
     return t
 
 

@@ -99,7 +99,7 @@ class RenderParams(ctypes.Structure):
 class WavefrontTuning(ctypes.Structure):
     _fields_ = [("struct_size", c_u32), ("queue_capacity", c_u32), ("trace_block", c_u32),
                 ("shade_block", c_u32), ("sort_rays", c_u32), ("max_waves", c_u32),
-                ("stage_queues", c_u32), ("reserved", c_u32 * 1)]
+                ("stage_queues", c_u32), ("deterministic", c_u32)]
 
 
 class BatchJob(ctypes.Structure):

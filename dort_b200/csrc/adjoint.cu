@@ -294,6 +294,17 @@ extern "C" int dort_gpu_adjoint_forward(dort_scene* scene, const dort_render_par
   if(rc != DORT_OK) { return rc; }
   rc = set_tri_params(scene, tri_albedo, tri_emission);
   if(rc != DORT_OK) { return rc; }
+  // the path tracer renders as a wavefront whose sums are added in a fixed
+  // order, so that the same parameters give the same image (finite
+  // differences of the loss rely on it); DORT_ADJOINT_MEGAKERNEL keeps the
+  // megakernel, the other renderers render as dort_gpu_render does
+  if(params->renderer == DORT_RENDERER_PT && params->struct_size == sizeof(dort_render_params) &&
+     !(params->renderer_flags & DORT_ADJOINT_MEGAKERNEL)) {
+    dort_wavefront_tuning t{};
+    t.struct_size = sizeof(t);
+    t.deterministic = 1;
+    return dort_gpu_render_wavefront(scene, params, &t, out_image, nullptr);
+  }
   return dort_gpu_render(scene, params, out_image, nullptr);
 } DORT_ABI_CATCH
 

@@ -436,6 +436,7 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
   tn.sort = 0;
   tn.max_waves = 0;
   tn.stage_queues = 0;
+  tn.deterministic = 0;
   if(t) {
     if(t->struct_size != sizeof(dort_wavefront_tuning)) {
       err = "dort_wavefront_tuning.struct_size mismatch (ABI version)";
@@ -455,6 +456,11 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
       return false;
     }
     if(t->sort_rays == 1) { tn.sort = 1; }
+    if(t->deterministic > 2) {
+      err = "deterministic must be 0 (auto), 1 (on) or 2 (off)";
+      return false;
+    }
+    tn.deterministic = t->deterministic == 1 ? 1u : 0u;
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
   if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
@@ -623,6 +629,9 @@ extern "C" int dort_gpu_batch_create(const dort_batch_job* jobs, uint32_t job_co
   // 2^22 and 187 M at 2^24
   if(!read_tuning(tuning, uint32_t(std::min<uint64_t>(total, 1u << 22)), tn, terr)) {
     return fail(DORT_ERR_INVALID, terr);
+  }
+  if(tn.deterministic) {
+    return fail(DORT_ERR_UNSUPPORTED, "deterministic sums are for single frames, not batches");
   }
   auto* batch = new dort_batch();
   int rc = wavefront_batch_create(scenes.data(), params.data(), job_count, tn, &batch->impl);

@@ -142,6 +142,11 @@ struct WfDev {
   // sample overflowed); null outside the adjoint
   float4* adj_log;
   uint32_t* adj_n;
+  // deterministic sums (single frames): the sum of work unit u of pixel p at
+  // unit_film[u * npix + p], added in unit order by the resolve; null: the
+  // units are added to film by atomics
+  float4* unit_film;
+  uint32_t npix;
 };
 
 // Where a path's scene and render parameters come from.  A single frame
@@ -374,7 +379,9 @@ __device__ __forceinline__ void regen_slot(J& jobs, WfDev& w, bool valid, uint32
       m = make_uint4(m.x, next_s, oct << kOctShift, SLOT_ACTIVE | (job << 8));
       started = true;
     } else {
-      if(a.w > 0.f || a.x != 0.f || a.y != 0.f || a.z != 0.f) {
+      if(!J::kBatched && w.unit_film) {
+        w.unit_film[size_t(m.y / kChunk) * w.npix + m.x] = a;
+      } else if(a.w > 0.f || a.x != 0.f || a.y != 0.f || a.z != 0.f) {
         atomicAdd(w.film + jobs.film_offset(job) + m.x, a);
       }
       live -= 1;
@@ -1076,6 +1083,22 @@ __global__ void wf_resolve(WfDev w, uint32_t npix, float* __restrict__ out) {
   }
 }
 
+// The deterministic resolve: every pixel's unit sums in unit order.
+__global__ void wf_resolve_units(WfDev w, uint32_t npix, uint32_t units,
+                                 float* __restrict__ out) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if(p >= npix) { return; }
+  float4 a = make_float4(0.f, 0.f, 0.f, 0.f);
+  for(uint32_t u = 0; u < units; ++u) {
+    const float4 b = w.unit_film[size_t(u) * npix + p];
+    a = make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+  }
+  const float inv = a.w != 0.f ? 1.f / a.w : 0.f;
+  out[3 * size_t(p)] = a.x * inv;
+  out[3 * size_t(p) + 1] = a.y * inv;
+  out[3 * size_t(p) + 2] = a.z * inv;
+}
+
 // ---- host side --------------------------------------------------------------------
 
 struct Wavefront {
@@ -1094,6 +1117,9 @@ struct Wavefront {
   const void* jobs_cached = nullptr;
   WfTuning tune_cached{};
   bool valid = false;
+  // per-unit sums of deterministic frames (grow-only)
+  void* unit_mem = nullptr;
+  size_t unit_bytes = 0;
   // the adjoint's term log (allocated by the adjoint's backward pass only)
   void* adj_mem = nullptr;
   uint32_t adj_capacity = 0;
@@ -1107,6 +1133,9 @@ static void wf_release(Wavefront* wf) {
   if(wf->mem) { cudaFree(wf->mem); wf->mem = nullptr; }
   if(wf->adj_mem) { cudaFree(wf->adj_mem); wf->adj_mem = nullptr; }
   wf->adj_capacity = 0;
+  if(wf->unit_mem) { cudaFree(wf->unit_mem); wf->unit_mem = nullptr; }
+  wf->unit_bytes = 0;
+  wf->dev.unit_film = nullptr;
   wf->dev.adj_log = nullptr;
   wf->dev.adj_n = nullptr;
   wf->valid = false;
@@ -1323,6 +1352,25 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   uint32_t npix = pp.width * pp.height;
   int rc = wf_alloc(wf, tn.capacity, npix, nee_mult(s->pt, pp));
   if(rc != DORT_OK) { return rc; }
+  const uint32_t units = (pp.spp + kChunk - 1) / kChunk;
+  float4* unit_film = nullptr;
+  if(tn.deterministic) {
+    const size_t need = size_t(npix) * units * sizeof(float4);
+    if(wf->unit_bytes < need) {
+      if(wf->unit_mem) { cudaFree(wf->unit_mem); }
+      wf->unit_mem = nullptr;
+      wf->unit_bytes = 0;
+      if(dev_alloc(&wf->unit_mem, need) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DORT_ERR_OOM, "cudaMalloc of the per-unit sums failed");
+      }
+      wf->unit_bytes = need;
+    }
+    unit_film = static_cast<float4*>(wf->unit_mem);
+  }
+  if(wf->dev.unit_film != unit_film || wf->dev.npix != npix) { wf->valid = false; }
+  wf->dev.unit_film = unit_film;
+  wf->dev.npix = npix;
   wf->dev.total_samples = padded_samples(pp);
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
   // the graph holds the scene view by value: a change to it (per-triangle
@@ -1342,7 +1390,11 @@ int wavefront_render(dort_scene* s, const PtParams& pp, const WfTuning& tn, floa
   wf_init<<<(std::max(tn.capacity, npix) + 255) / 256, 256, 0, st>>>(wf->dev, npix);
   DG_CUDA(cudaGetLastError());
   DG_CUDA(cudaGraphLaunch(wf->exec, st));
-  wf_resolve<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, d_out);
+  if(unit_film) {
+    wf_resolve_units<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, units, d_out);
+  } else {
+    wf_resolve<<<(npix + 255) / 256, 256, 0, st>>>(wf->dev, npix, d_out);
+  }
   DG_CUDA(cudaGetLastError());
   return DORT_OK;
 }
@@ -1428,6 +1480,13 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   uint32_t npix = pp.width * pp.height;
   int rc = wf_alloc(wf, tn.capacity, npix, nee_mult(s->pt, pp));
   if(rc != DORT_OK) { return rc; }
+  // film sums by atomics here (wf_resolve); the cached graph is rebuilt by
+  // the next frame that wants per-unit sums
+  if(wf->dev.unit_film) {
+    wf->dev.unit_film = nullptr;
+    wf->valid = false;
+  }
+  wf->dev.npix = npix;
   wf->dev.total_samples = padded_samples(pp);
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
   SingleJob<G> jobs{s->pt, pp};

@@ -16,6 +16,7 @@ struct WfTuning {
   uint32_t sort;          // 1: sort each wave's rays by direction octant and origin cell
   uint32_t max_waves;     // waves a frame may take (0: the automatic bound)
   uint32_t stage_queues;  // 1: stage the shadow queue through bulk copies (TMA)
+  uint32_t deterministic; // 1: per-unit sums added in unit order (single frames)
 };
 
 struct Wavefront;

@@ -334,10 +334,11 @@ enum dort_renderer { DORT_RENDERER_PT = 0, DORT_RENDERER_LT = 1, DORT_RENDERER_B
                                       image; for derivative checks, where a
                                       roulette decision that flips under a small
                                       parameter change makes a sample jump */
-#define DORT_ADJOINT_MEGAKERNEL 4u /* dort_gpu_adjoint_backward: one thread per
-                                      (pixel, slice of samples) instead of the
-                                      wavefront (same gradients; ignored by the
-                                      renders) */
+#define DORT_ADJOINT_MEGAKERNEL 4u /* the adjoint's forward and backward
+                                      passes as megakernels (one thread per
+                                      pixel and slice of samples) instead of
+                                      wavefronts (the same estimator; ignored
+                                      by the renders) */
 
 typedef struct dort_render_params {
   uint32_t struct_size;        /* sizeof(dort_render_params) */
@@ -412,7 +413,15 @@ typedef struct dort_wavefront_tuning {
                                   warp and batch of 32 entries, overlapping
                                   the previous batch's traversals); blocks of
                                   at most 256 trace threads */
-  uint32_t reserved[1];
+  uint32_t deterministic;      /* 0: auto (off), 1: on, 2: off -- the frame's
+                                  sums in a fixed order: every 4-sample work
+                                  unit's sum is stored apart (16 bytes per
+                                  pixel and unit) and the resolve adds them in
+                                  unit order, so that the same frame renders
+                                  to the same bits (a path's shadow-ray
+                                  additions are ordered too unless it has two
+                                  in one wave: a background light under the
+                                  MIS BSDF strategy, or sample_all_lights) */
 } dort_wavefront_tuning;
 
 /* out_stats (optional, 4 doubles): rays traced, samples kept, kernel
@@ -498,7 +507,10 @@ int dort_gpu_wavefront_stage_times(dort_scene* scene, const dort_render_params* 
  * when the scene is created).  Both stay in effect for later renders of the
  * scene until replaced; NULL removes an override.
  *
- * forward:  renders the image (as dort_gpu_render) with the overrides.
+ * forward:  renders the image with the overrides: the path tracer as
+ *           dort_gpu_render_wavefront with deterministic sums (the same
+ *           parameters give the same image), or as dort_gpu_render with
+ *           DORT_ADJOINT_MEGAKERNEL; the other renderers as dort_gpu_render.
  * backward: given dLoss/dImage (width * height * 3, host), writes
  *           d_albedo[t*3+c] = dLoss/d albedo and d_emission[t*3+c] =
  *           dLoss/d Le (host, tri_count * 3 each; either may be NULL), for

@@ -297,3 +297,20 @@ def test_wavefront_backward_log_overflow(cuda, list_cap, engine):
     for got, want in ((wa, ma), (we, me)):
         assert np.abs(want).sum() > 0
         assert np.linalg.norm(got - want) <= 5e-3 * np.linalg.norm(want)
+
+
+def test_forward_is_deterministic_and_equals_megakernel_forward(cuda):
+    """The forward pass renders the path tracer as a wavefront with
+    deterministic sums: repeated calls give the same bits (finite
+    differences of the loss rely on it), and the megakernel form
+    (DORT_ADJOINT_MEGAKERNEL) the same image up to rounding."""
+    sd, sc, p = _setup(n_tris=20000, w=40, spp=12, depth=6)
+    alb, em = sd["tri_albedo"], sd["tri_emission"]
+    a = sc.adjoint_forward(p, alb, em)
+    b = sc.adjoint_forward(p, alb, em)
+    assert np.array_equal(a, b)
+    pm = db.render_params(sd["camera"], 40, 40, 12, max_depth=2, seed=7, adjoint_megakernel=True)
+    m = sc.adjoint_forward(pm, alb, em)
+    pw = db.render_params(sd["camera"], 40, 40, 12, max_depth=2, seed=7)
+    w = sc.adjoint_forward(pw, alb, em)
+    assert np.sqrt(((w - m) ** 2).mean()) / m.mean() < 1e-3

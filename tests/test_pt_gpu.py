@@ -144,3 +144,24 @@ def test_wavefront_queue_shapes(cuda, capacity, block, sort_rays, staged):
                                     "stage_queues": staged})
     assert ptcheck.rel_rmse(b, a) < 2e-3
     assert st["waves"] >= 1
+
+
+def test_wavefront_deterministic_sums(cuda):
+    """With deterministic sums (per-unit sums added in unit order) the same
+    frame renders to the same bits, the megakernel's image up to rounding;
+    batches refuse the option."""
+    sd = scenes.cornell_box()
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], 40, 32, 23, max_depth=5, seed=21)
+    a, _ = sc.render_wavefront(p, {"deterministic": True})
+    b, _ = sc.render_wavefront(p, {"deterministic": True, "queue_capacity": 1024})
+    c, _ = sc.render_wavefront(p, {"deterministic": True})
+    assert np.array_equal(a, c) and np.array_equal(a, b)
+    m, _ = sc.render(p)
+    assert ptcheck.forked_pixels(a, m) <= 2
+    # and the atomic film again afterwards
+    d, _ = sc.render_wavefront(p)
+    assert ptcheck.forked_pixels(d, m) <= 2
+    with pytest.raises(db.DortError) as e:
+        db.Batch([(sc, p)], {"deterministic": True})
+    assert e.value.status == -5
