@@ -613,7 +613,7 @@ struct NeeEntries {
   float4 sh_o, sh_d, sh_c, sh2_o, sh2_d, sh2_c, nb_o, nb_d, nb_f;
 };
 
-template<bool G>
+template<bool G, bool ADJ = false>
 __device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& pp, uint32_t li,
                                             float inv_lpdf, const SurfaceHit& g,
                                             const DevMaterial& mt, V3 wo, V3 thr, float ub,
@@ -648,7 +648,7 @@ __device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& p
           e.sh2 = true;
           e.sh2_o = make_float4(g.p.x, g.p.y, g.p.z, g.eps);
           e.sh2_d = make_float4(bs.w.x, bs.w.y, bs.w.z, INFINITY);
-          e.sh2_c = make_float4(c.x, c.y, c.z, u2f(kMiss));
+          e.sh2_c = make_float4(c.x, c.y, c.z, ADJ ? u2f(kMiss) : 0.f);
         }
       }
     }
@@ -667,8 +667,9 @@ __device__ __forceinline__ void nee_entries(const PtScene& sc, const PtParams& p
         e.sh = true;
         e.sh_o = make_float4(ls.o.x, ls.o.y, ls.o.z, ls.tmin);
         e.sh_d = make_float4(ls.d.x, ls.d.y, ls.d.z, ls.tmax);
-        // .w: the light's triangle (the adjoint's emission gradient)
-        e.sh_c = make_float4(c.x, c.y, c.z, u2f(l.kind == LIGHT_TRI ? l.tri : kMiss));
+        // .w: for the adjoint, the light's triangle (its emission gradient)
+        e.sh_c = make_float4(c.x, c.y, c.z,
+                             ADJ ? u2f(l.kind == LIGHT_TRI ? l.tri : kMiss) : 0.f);
       }
     }
   }
@@ -691,8 +692,14 @@ __device__ __forceinline__ void push_entries(WfDev& w, uint32_t slot, const NeeE
   }
 }
 
+#ifdef DORT_SHADE_MAXNREG
+#define DORT_SHADE_REGS __maxnreg__(DORT_SHADE_MAXNREG)
+#else
+#define DORT_SHADE_REGS
+#endif
+
 template<class J>
-__global__ void wf_shade(J jobs, WfDev w) {
+__global__ void DORT_SHADE_REGS wf_shade(J jobs, WfDev w) {
   const uint32_t cur = wave_of(w) & 1u;
   uint32_t qn[kShadeQueues];
   uint32_t n = 0;
@@ -784,16 +791,16 @@ __global__ void wf_shade(J jobs, WfDev w) {
               Rand4 a = rand4(pp.seed, m.x, m.y, b2);
               Rand4 b = rand4(pp.seed, m.x, m.y, b2 + 1);
               NeeEntries e;
-              nee_entries<J::kGeneral>(sc, pp, li, 1.f, g, mt, wo, thr, a.a, a.b, a.c, b.a, b.b,
-                                       e);
+              nee_entries<J::kGeneral, J::kAdjoint>(sc, pp, li, 1.f, g, mt, wo, thr, a.a, a.b,
+                                                    a.c, b.a, b.b, e);
               push_entries(w, slot, e);
             }
           } else {
             uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, r0.a);
             float lpdf = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
             if(lpdf != 0.f) {
-              nee_entries<J::kGeneral>(sc, pp, li, 1.f / lpdf, g, mt, wo, thr, r0.b, r0.c, r0.d,
-                                       r1.a, r1.b, nee);
+              nee_entries<J::kGeneral, J::kAdjoint>(sc, pp, li, 1.f / lpdf, g, mt, wo, thr, r0.b,
+                                                    r0.c, r0.d, r1.a, r1.b, nee);
             }
           }
         }
@@ -1229,20 +1236,40 @@ static int grid_for(const void* kernel, int block) {
   return sms * std::max(per_sm, 1);
 }
 
+// Grid and block of every stage kernel.  A block size the tuning asks for
+// that a kernel's registers do not allow (threads x registers above the
+// SM's register file) is lowered to the kernel's limit, a multiple of 32.
 struct WfGrids {
   int regen, ext, sha, shw, nb;
+  int b_ext, b_sha, b_shw, b_nb;
 };
+
+static int fit_block(const void* kernel, int block) {
+  cudaFuncAttributes a{};
+  if(cudaFuncGetAttributes(&a, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return block;
+  }
+  return std::min(block, std::max(32, a.maxThreadsPerBlock & ~31));
+}
 
 template<class J>
 static WfGrids wf_grids(const WfTuning& tn) {
   WfGrids g;
+  const void* ext = reinterpret_cast<const void*>(&wf_extend<J>);
+  const void* sha = reinterpret_cast<const void*>(&wf_shade<J>);
+  const void* shw = tn.stage_queues ? reinterpret_cast<const void*>(&wf_shadow<J, true>)
+                                    : reinterpret_cast<const void*>(&wf_shadow<J, false>);
+  const void* nb = reinterpret_cast<const void*>(&wf_neeb<J>);
+  g.b_ext = fit_block(ext, int(tn.trace_block));
+  g.b_sha = fit_block(sha, int(tn.shade_block));
+  g.b_shw = fit_block(shw, int(tn.trace_block));
+  g.b_nb = fit_block(nb, int(tn.trace_block));
   g.regen = grid_for(reinterpret_cast<const void*>(&wf_regen<J>), int(kRegenBlock));
-  g.ext = grid_for(reinterpret_cast<const void*>(&wf_extend<J>), int(tn.trace_block));
-  g.sha = grid_for(reinterpret_cast<const void*>(&wf_shade<J>), int(tn.shade_block));
-  g.shw = tn.stage_queues
-      ? grid_for(reinterpret_cast<const void*>(&wf_shadow<J, true>), int(tn.trace_block))
-      : grid_for(reinterpret_cast<const void*>(&wf_shadow<J, false>), int(tn.trace_block));
-  g.nb = grid_for(reinterpret_cast<const void*>(&wf_neeb<J>), int(tn.trace_block));
+  g.ext = grid_for(ext, g.b_ext);
+  g.sha = grid_for(sha, g.b_sha);
+  g.shw = grid_for(shw, g.b_shw);
+  g.nb = grid_for(nb, g.b_nb);
   return g;
 }
 
@@ -1261,32 +1288,29 @@ static void wf_sort(const J& jobs, WfDev& dev, const WfGrids& g, cudaStream_t st
 template<class J>
 static void wf_launch_extend(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
                              cudaStream_t st) {
-  int bt = int(tn.trace_block);
   if(tn.sort) { wf_sort<J>(jobs, dev, g, st); }
-  wf_extend<J><<<g.ext, bt, 0, st>>>(jobs, dev);
+  wf_extend<J><<<g.ext, g.b_ext, 0, st>>>(jobs, dev);
   if(tn.sort) { wf_classify<<<g.regen, 256, 0, st>>>(dev); }
 }
 
 template<class J>
 static void wf_launch_shadow(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
                              cudaStream_t st) {
-  int bt = int(tn.trace_block);
   if(tn.stage_queues) {
-    wf_shadow<J, true><<<g.shw, bt, 0, st>>>(jobs, dev);
+    wf_shadow<J, true><<<g.shw, g.b_shw, 0, st>>>(jobs, dev);
   } else {
-    wf_shadow<J, false><<<g.shw, bt, 0, st>>>(jobs, dev);
+    wf_shadow<J, false><<<g.shw, g.b_shw, 0, st>>>(jobs, dev);
   }
 }
 
 template<class J>
 static void wf_launch_wave(const J& jobs, WfDev& dev, const WfTuning& tn, const WfGrids& g,
                            cudaStream_t st) {
-  int bt = int(tn.trace_block), bs = int(tn.shade_block);
   wf_regen<J><<<g.regen, kRegenBlock, 0, st>>>(jobs, dev);
   wf_launch_extend<J>(jobs, dev, tn, g, st);
-  wf_shade<J><<<g.sha, bs, 0, st>>>(jobs, dev);
+  wf_shade<J><<<g.sha, g.b_sha, 0, st>>>(jobs, dev);
   wf_launch_shadow<J>(jobs, dev, tn, g, st);
-  wf_neeb<J><<<g.nb, bt, 0, st>>>(jobs, dev);
+  wf_neeb<J><<<g.nb, g.b_nb, 0, st>>>(jobs, dev);
 }
 
 template<class J>
@@ -1491,7 +1515,6 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
   wf->dev.max_waves = wave_bound(wf->dev.total_samples, tn.capacity, pp.max_depth, tn.max_waves);
   SingleJob<G> jobs{s->pt, pp};
   WfGrids g = wf_grids<SingleJob<G>>(tn);
-  int bt = int(tn.trace_block), bs = int(tn.shade_block);
   wf->dev.sorted = tn.sort;
   // more[0]: loop flag; more[1..6]: the counters C_ACT0 .. C_NEEB of the wave
   uint32_t* more = nullptr;
@@ -1509,11 +1532,11 @@ static int stage_times_g(dort_scene* s, const PtParams& pp, const WfTuning& tn, 
     // the sort counts as part of the extension stage
     wf_launch_extend<SingleJob<G>>(jobs, wf->dev, tn, g, st);
     cudaEventRecord(ev[2], st);
-    wf_shade<SingleJob<G>><<<g.sha, bs, 0, st>>>(jobs, wf->dev);
+    wf_shade<SingleJob<G>><<<g.sha, g.b_sha, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[3], st);
     wf_launch_shadow<SingleJob<G>>(jobs, wf->dev, tn, g, st);
     cudaEventRecord(ev[4], st);
-    wf_neeb<SingleJob<G>><<<g.nb, bt, 0, st>>>(jobs, wf->dev);
+    wf_neeb<SingleJob<G>><<<g.nb, g.b_nb, 0, st>>>(jobs, wf->dev);
     cudaEventRecord(ev[5], st);
     cudaMemcpy2DAsync(more + 1, sizeof(uint32_t), wf->dev.ctr, kCtrStride * sizeof(uint32_t),
                       sizeof(uint32_t), C_NEEB + 1, cudaMemcpyDeviceToHost, st);

@@ -395,7 +395,9 @@ typedef struct dort_wavefront_tuning {
                                   holds about 330 bytes of device memory;
                                   more slots, fewer and fuller waves) */
   uint32_t trace_block;        /* threads per block, trace stages (0: auto) */
-  uint32_t shade_block;        /* threads per block, shade stage (0: auto) */
+  uint32_t shade_block;        /* threads per block, shade stage (0: auto);
+                                  a size above what a stage kernel's registers
+                                  allow is lowered to that kernel's limit */
   uint32_t sort_rays;          /* 0: auto (off), 1: on, 2: off -- sort each
                                   wave's extension rays by direction octant
                                   and origin cell before tracing them */
