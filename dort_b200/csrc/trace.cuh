@@ -9,10 +9,10 @@
 // Traversal: node groups (base index, 8 child-hit bits << 24 | internal-slot
 // mask) on a per-thread stack; child slots are visited in an order fixed by
 // the ray octant (slot bit index XOR octant), so no per-node sort is needed.
-// Child boxes are tested with fused multiply-adds on the quantized planes and
-// a relative widening of 2^-20 that covers the rounding of that arithmetic;
-// together with the one-step quantization margin the test never culls a box
-// containing a hit.
+// Child boxes are tested with fused multiply-adds on the planes (rounded
+// outward) and a relative widening that covers the rounding of that
+// arithmetic (DG_BOX_HIT); together with the one-step quantization margin the
+// test never culls a box containing a hit.
 //
 // Triangle test: the reference's Moller-Trumbore operations in the
 // reference's order with explicit round-to-nearest intrinsics (no fused
@@ -42,6 +42,20 @@
 #define DG_BYTE_F(w, j) __uint2float_rn(((w) >> (8 * (j))) & 0xffu)
 #define DG_FMA(a, b, c) fmaf(a, b, c)
 #define DG_RCP_FAST(a) __frcp_rn(a)
+// three-input float max / min (one instruction on sm_100a; exact, like two
+// fmaxf / fminf)
+__device__ __forceinline__ float dg_max3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+__device__ __forceinline__ float dg_min3(float a, float b, float c) {
+  float d;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+#define DG_MAX3(a, b, c) dg_max3(a, b, c)
+#define DG_MIN3(a, b, c) dg_min3(a, b, c)
 #else
 namespace dort_gpu {
 inline float host_as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
@@ -61,6 +75,8 @@ inline uint32_t host_as_uint(float f) { uint32_t u; std::memcpy(&u, &f, 4); retu
 #define DG_BYTE_F(w, j) (float(((w) >> (8 * (j))) & 0xffu))
 #define DG_FMA(a, b, c) std::fma(a, b, c)
 #define DG_RCP_FAST(a) (1.f / (a))
+#define DG_MAX3(a, b, c) fmaxf(fmaxf(a, b), c)
+#define DG_MIN3(a, b, c) fminf(fminf(a, b), c)
 #endif
 #define DG_HD __host__ __device__ __forceinline__
 
@@ -213,8 +229,17 @@ DG_HD float byte_to_float(uint32_t w, int j) {
   return DG_BYTE_F(w, j);
 }
 
-// Widening factor for the slab test: 2^-20 relative (> 8 ulp).
-#define DORT_SLAB_WIDEN 9.5367431640625e-7f
+// Widening of the slab test.  The plane distances t carry a relative
+// rounding error below 2^-20 of |t| (> 8 ulp).  Widening both ends by that,
+// tnear - |tnear| 2^-20 <= tfar + |tfar| 2^-20, takes two fused multiply-adds
+// per child; the test used, tnear <= tfar + |tfar| 2^-18, takes one and
+// accepts every box the two-sided form accepts, for every sign of tnear and
+// tfar (the widening only decides where tnear > tfar: with both >= 0 the
+// two-sided form needs tnear <= tfar (1 + 2^-20) / (1 - 2^-20) < tfar (1 +
+// 2^-18); with both < 0, |tfar| > |tnear| and 2^-18 |tfar| exceeds the two
+// margins together; with tnear >= 0 > tfar both forms reject).
+#define DORT_SLAB_FAR_WIDEN 3.814697265625e-6f
+#define DG_BOX_HIT(tn, tf) ((tn) <= DG_FMA(fabsf(tf), DORT_SLAB_FAR_WIDEN, (tf)))
 
 // Tests the 8 child boxes of one node; returns the hit mask: bits 24..31 =
 // internal children (bit 24 + (slot ^ oct_inv)), bits 0..23 = triangles
@@ -255,10 +280,9 @@ DG_HD uint32_t node_hitmask(
       float tfx = fmaf(byte_to_float(far_x[h], j), adj_ix, adj_ox);
       float tfy = fmaf(byte_to_float(far_y[h], j), adj_iy, adj_oy);
       float tfz = fmaf(byte_to_float(far_z[h], j), adj_iz, adj_oz);
-      float tnear = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, t_min));
-      float tfar = fminf(fminf(tfx, tfy), fminf(tfz, t_max));
-      bool hit = fmaf(-fabsf(tnear), DORT_SLAB_WIDEN, tnear) <=
-                 fmaf(fabsf(tfar), DORT_SLAB_WIDEN, tfar);
+      float tnear = DG_MAX3(tnx, tny, fmaxf(tnz, t_min));
+      float tfar = DG_MIN3(tfx, tfy, fminf(tfz, t_max));
+      bool hit = DG_BOX_HIT(tnear, tfar);
       if(hit) {
         uint32_t bits = (child_bits4 >> (8 * j)) & 0xffu;
         uint32_t bidx = (bit_index4 >> (8 * j)) & 0xffu;
@@ -303,12 +327,11 @@ DG_HD uint32_t node_hitmask_f(const uint4* np, uint4 h0, float ix, float iy, flo
     const float nza[4] = {nz.x, nz.y, nz.z, nz.w}, fza[4] = {fz.x, fz.y, fz.z, fz.w};
 #pragma unroll
     for(int j = 0; j < 4; ++j) {
-      float tnear = fmaxf(fmaxf(fmaf(nxa[j], ix, nox), fmaf(nya[j], iy, noy)),
-                          fmaxf(fmaf(nza[j], iz, noz), t_min));
-      float tfar = fminf(fminf(fmaf(fxa[j], ix, nox), fmaf(fya[j], iy, noy)),
-                         fminf(fmaf(fza[j], iz, noz), t_max));
-      bool hit = fmaf(-fabsf(tnear), DORT_SLAB_WIDEN, tnear) <=
-                 fmaf(fabsf(tfar), DORT_SLAB_WIDEN, tfar);
+      float tnear = DG_MAX3(fmaf(nxa[j], ix, nox), fmaf(nya[j], iy, noy),
+                            fmaxf(fmaf(nza[j], iz, noz), t_min));
+      float tfar = DG_MIN3(fmaf(fxa[j], ix, nox), fmaf(fya[j], iy, noy),
+                           fminf(fmaf(fza[j], iz, noz), t_max));
+      bool hit = DG_BOX_HIT(tnear, tfar);
       if(hit) {
         uint32_t bits = (child_bits4 >> (8 * j)) & 0xffu;
         uint32_t bidx = (bit_index4 >> (8 * j)) & 0xffu;
