@@ -7,7 +7,9 @@
 // within the depth limits is connected (path_contrib, :292-468) and weighted
 // by the balance heuristic over the strategies that could have made the same
 // path (path_weight, :470-678); t = 1 connections splat onto the film.  The
-// walks live in local arrays of kBdptVerts vertices.
+// walks are written through a vertex sink (a local array for the host check,
+// device memory for the GPU's connection-parallel kernels in bdpt.cu), and
+// one connection function serves both.
 #pragma once
 #include "lt.cuh"
 
@@ -197,6 +199,54 @@ DG_HD BVert bvert_empty() {
   return v;
 }
 
+// Where a walk's vertices live.
+//   LocalWalk  an array of one sample's vertices (the host check).
+//   SoaWalk    the device's connection-parallel form: vertex k of sample i of
+//              a chunk as five float4 words, word w at (5 k + w) * stride + i,
+//              so that the lanes of a warp (consecutive samples) store and
+//              load whole lines.  get() reads through the read-only path: a
+//              walk is read only by launches after the one that wrote it.
+struct LocalWalk {
+  BVert* v;
+  DG_HD void put(uint32_t k, const BVert& x) const { v[k] = x; }
+  DG_HD BVert get(uint32_t k) const { return v[k]; }
+};
+
+struct SoaWalk {
+  float4* base;
+  uint32_t stride, i;
+  DG_HD void put(uint32_t k, const BVert& x) const {
+    float4* q = base + size_t(5 * k) * stride + i;
+    const size_t st = stride;
+    q[0] = make_float4(x.p.x, x.p.y, x.p.z, x.eps);
+    q[st] = make_float4(x.nn.x, x.nn.y, x.nn.z, x.fwd_pdf);
+    q[2 * st] = make_float4(x.s.x, x.s.y, x.s.z, x.bwd_pdf);
+    q[3 * st] = make_float4(x.alpha.x, x.alpha.y, x.alpha.z, DG_AS_FLOAT(x.mat));
+    q[4 * st] = make_float4(DG_AS_FLOAT(x.prim), DG_AS_FLOAT(x.light), DG_AS_FLOAT(x.bg),
+                            DG_AS_FLOAT(x.delta));
+  }
+  DG_HD BVert get(uint32_t k) const {
+    const float4* q = base + size_t(5 * k) * stride + i;
+    const size_t st = stride;
+    float4 a = DG_LDG(q), b = DG_LDG(q + st), c = DG_LDG(q + 2 * st);
+    float4 d = DG_LDG(q + 3 * st), e = DG_LDG(q + 4 * st);
+    BVert v;
+    v.p = v3(a.x, a.y, a.z);
+    v.eps = a.w;
+    v.nn = v3(b.x, b.y, b.z);
+    v.fwd_pdf = b.w;
+    v.s = v3(c.x, c.y, c.z);
+    v.bwd_pdf = c.w;
+    v.alpha = v3(d.x, d.y, d.z);
+    v.mat = DG_AS_UINT(d.w);
+    v.prim = DG_AS_UINT(e.x);
+    v.light = DG_AS_UINT(e.y);
+    v.bg = DG_AS_UINT(e.z);
+    v.delta = DG_AS_UINT(e.w);
+    return v;
+  }
+};
+
 // Dimension blocks of one BDPT sample:
 //   0                 film jitter (a, b); the thin lens's lens point (c, d)
 //   1, 2              light pick, light ray position and direction
@@ -213,8 +263,10 @@ struct BdptCtx {
 };
 
 // random_light_walk (bdpt_renderer.cpp:96-180); returns the vertex count.
-template<bool G>
-DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, BVert* lw,
+// The walk's last vertex stays in registers until the next one is made (it
+// receives its backward pdf then), so every vertex is stored once.
+template<bool G, class W>
+DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, const W& lw,
                                uint32_t& rays) {
   const PtScene& sc = c.sc;
   const DevLight& l = sc.lights[light_i];
@@ -224,20 +276,18 @@ DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, B
   if(!light_sample_ray<G>(sc, l, r1.b, r1.c, r1.d, r2.a, ray)) { return 0; }
   if(ray.pos_pdf == 0.f || ray.dir_pdf == 0.f) { return 0; }
   const bool distant = (light_flags(l) & LF_DISTANT) != 0;
-  BVert y0 = bvert_empty();
-  y0.p = ray.o;
-  y0.eps = ray.eps;
-  y0.nn = ray.nn;
-  y0.fwd_pdf = ray.pos_pdf;
-  y0.alpha = ray.L * (1.f / (ray.pos_pdf * pick));
-  lw[0] = y0;
+  BVert prev = bvert_empty();
+  prev.p = ray.o;
+  prev.eps = ray.eps;
+  prev.nn = ray.nn;
+  prev.fwd_pdf = ray.pos_pdf;
+  prev.alpha = ray.L * (1.f / (ray.pos_pdf * pick));
   uint32_t n = 1;
   V3 prev_f = v3(1.f, 1.f, 1.f);
   float fwd_dir_pdf = ray.dir_pdf;
   V3 o = ray.o, d = ray.d;
   float eps = ray.eps;
   for(uint32_t b = 0; b <= c.pp.max_depth && n < kBdptVerts; ++b) {
-    BVert& prev = lw[n - 1];
     ++rays;
     Hit h = bd_trace<false, G>(sc, o, eps, d, INFINITY);
     if(h.prim == kMiss) { break; }
@@ -245,7 +295,6 @@ DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, B
     DevMaterial m = material_at(sc, g);
     V3 wi = -d;
     Rand4 ra = rand4(c.pp.seed, c.pixel, c.sample, kBdLightWalk + 2 * b);
-    Rand4 rb = rand4(c.pp.seed, c.pixel, c.sample, kBdLightWalk + 2 * b + 1);
     // Bsdf::sample_camera_f: the same sampling from either side here
     BsdfSample bs = bd_bsdf_sample<G>(m, g.frame, wi, F_ALL, ra.a, ra.b, ra.c);
     if(bs.pdf == 0.f) { break; }
@@ -265,38 +314,41 @@ DG_HD uint32_t bdpt_light_walk(const BdptCtx& c, uint32_t light_i, float pick, B
     y.delta = (bs.flags & F_DELTA) ? 1u : 0u;
     if(is_black(y.alpha)) { break; }
     prev.bwd_pdf = bwd_dir_pdf * fabsf(dot(prev.nn, wi)) / dist2;
+    lw.put(n - 1, prev);
+    prev = y;
+    ++n;
     prev_f = bs.f;
     fwd_dir_pdf = bs.pdf;
     o = y.p;
     d = wo;
     eps = g.eps;
-    lw[n++] = y;
-    (void)rb;
   }
+  lw.put(n - 1, prev);
   return n;
 }
 
 // random_camera_walk (bdpt_renderer.cpp:182-290); returns the vertex count.
-template<bool G>
-DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
-                                uint32_t& rays) {
+// `emit` collects bit k for a vertex k that is emissive (an area light hit)
+// and bit 16 + k for a virtual background vertex.
+template<bool G, class W>
+DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, const W& cw,
+                                uint32_t& rays, uint32_t& emit) {
   const PtScene& sc = c.sc;
+  emit = 0;
   V3 o, d;
   float pos_pdf, dir_pdf;
   float We = camera_ray_importance<G>(c.pp, c.pixel, c.sample, fx, fy, o, d, pos_pdf, dir_pdf);
   if(pos_pdf == 0.f || dir_pdf == 0.f) { return 0; }
-  BVert z0 = bvert_empty();
-  z0.p = o;
-  z0.nn = d;
-  z0.fwd_pdf = pos_pdf;
-  z0.alpha = v3(We, We, We) * (1.f / pos_pdf);
-  cw[0] = z0;
+  BVert prev = bvert_empty();
+  prev.p = o;
+  prev.nn = d;
+  prev.fwd_pdf = pos_pdf;
+  prev.alpha = v3(We, We, We) * (1.f / pos_pdf);
   uint32_t n = 1;
   V3 prev_f = v3(1.f, 1.f, 1.f);
   float fwd_dir_pdf = dir_pdf;
   float eps = 0.f;
   for(uint32_t b = 0; b <= c.pp.max_depth && n < kBdptVerts; ++b) {
-    BVert& prev = cw[n - 1];
     if(is_black(prev.alpha)) { break; }
     Rand4 ra = rand4(c.pp.seed, c.pixel, c.sample, kBdCameraWalk + 2 * b);
     Rand4 rb = rand4(c.pp.seed, c.pixel, c.sample, kBdCameraWalk + 2 * b + 1);
@@ -325,7 +377,10 @@ DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
       zb.bg = sc.bg_light[k] + 1u;
       zb.fwd_pdf = fwd_dir_pdf;
       zb.alpha = prev.alpha * scale * (1.f / bg_pdf);
-      cw[n++] = zb;
+      cw.put(n - 1, prev);
+      prev = zb;
+      emit |= 1u << (16 + n);
+      ++n;
       break;
     }
     SurfaceHit g = bd_surface<G>(sc, h, o, d);
@@ -340,43 +395,55 @@ DG_HD uint32_t bdpt_camera_walk(const BdptCtx& c, float fx, float fy, BVert* cw,
     z.alpha = prev.alpha * scale;
     z.delta = (bs.flags & F_DELTA) ? 1u : 0u;
     if(is_black(z.alpha) && z.light == 0) { break; }
+    if(z.light != 0) { emit |= 1u << n; }
     if(bs.pdf == 0.f) {
       prev.bwd_pdf = 0.f;
-      cw[n++] = z;
+      cw.put(n - 1, prev);
+      prev = z;
+      ++n;
       break;
     }
     V3 wi = normalize(bs.w);
     float bwd_dir_pdf = bd_bsdf_pdf<G>(m, g.frame, wo, wi, F_ALL);   // camera_f_pdf(wo, wi)
     prev.bwd_pdf = bwd_dir_pdf * fabsf(dot(prev.nn, wo)) / dist2;
+    cw.put(n - 1, prev);
+    prev = z;
+    ++n;
     prev_f = bs.f;
     fwd_dir_pdf = bs.pdf;
     o = z.p;
     d = wi;
     eps = g.eps;
-    cw[n++] = z;
   }
+  cw.put(n - 1, prev);
   return n;
 }
 
 // The path of s light and t camera vertices, as path_weight indexes it:
 // x[0 .. s-1] = light vertices, x[s .. s+t-1] = camera vertices in reverse.
+// A connection that makes its own end vertex (s = 1: a new light sample;
+// t = 1: a new camera point) puts it in place of the walk's first one.
+template<class W>
 struct BdptPath {
-  const BVert* lw;
-  const BVert* cw;
-  const BVert* first_light;    // replaces lw[0] (s == 1)
-  const BVert* first_camera;   // replaces cw[0] (t == 1)
+  W lw, cw;
+  const BVert* first_light;    // replaces light vertex 0 if set
+  const BVert* first_camera;   // replaces camera vertex 0 if set
   uint32_t s, t;
-  DG_HD const BVert& light_at(uint32_t i) const { return i == 0 ? *first_light : lw[i]; }
-  DG_HD const BVert& camera_at(uint32_t i) const { return i == 0 ? *first_camera : cw[i]; }
-  DG_HD const BVert& at(uint32_t i) const {
+  DG_HD BVert light_at(uint32_t i) const {
+    return (i == 0 && first_light) ? *first_light : lw.get(i);
+  }
+  DG_HD BVert camera_at(uint32_t i) const {
+    return (i == 0 && first_camera) ? *first_camera : cw.get(i);
+  }
+  DG_HD BVert at(uint32_t i) const {
     return i < s ? light_at(i) : camera_at(t - (i - s + 1));
   }
 };
 
 // path_weight (bdpt_renderer.cpp:470-678): the balance heuristic over the
 // strategies (s', t') with s' + t' = s + t.
-template<bool G>
-DG_HD float bdpt_weight(const BdptCtx& c, const DevLight& light, const BdptPath& x) {
+template<bool G, class P>
+DG_HD float bdpt_weight(const BdptCtx& c, const DevLight& light, const P& x) {
   const PtScene& sc = c.sc;
   const PtParams& pp = c.pp;
   const uint32_t s = x.s, t = x.t;
@@ -492,8 +559,199 @@ DG_HD float bdpt_weight(const BdptCtx& c, const DevLight& light, const BdptPath&
   return 1.f / inv_sum;
 }
 
-// One pixel sample (sample_path, bdpt_renderer.cpp:40-94): the camera-side
-// value is returned, t = 1 splats go straight to the film.
+// One sample's data beside its walks: vertex counts, the light picked for
+// the light walk with its probability, the film position.
+struct BdptSampleData {
+  uint32_t ns, nt, light_i;
+  float pick, fx, fy;
+};
+
+// Connection cases, by the code each runs (the branches of sample_path's
+// connection loop, bdpt_renderer.cpp:292-468):
+//   kBdCaseS0  s = 0: the camera walk's vertex t - 1 is emissive (no ray)
+//   kBdCaseS1  s = 1, t >= 2: a new light sample seen from camera vertex t - 1
+//   kBdCaseT1  t = 1: a new camera point seen from light vertex s - 1 (a
+//              film splat)
+//   kBdCaseST  s >= 2, t >= 2: the two walks' end vertices joined
+// kBdCaseAll compiles every branch (the host's loop over one sample).
+enum : uint32_t {
+  kBdCaseS0 = 0, kBdCaseS1 = 1, kBdCaseT1 = 2, kBdCaseST = 3, kBdCases = 4, kBdCaseAll = 4
+};
+
+// The case of connection (s, t), or kBdCases when the loop skips it before
+// drawing its random numbers or always rejects it: `emit` is the camera
+// walk's mask (bdpt_camera_walk).
+DG_HD uint32_t bdpt_pair_case(const PtParams& pp, bool use_t1, uint32_t emit, uint32_t s,
+                              uint32_t t) {
+  if(t == 1 && !use_t1) { return kBdCases; }
+  if(s + t < pp.min_depth + 2 || s + t > pp.max_depth + 2) { return kBdCases; }
+  const bool bg = (emit >> (16 + t - 1)) & 1u, light = (emit >> (t - 1)) & 1u;
+  if(s > 0 && bg) { return kBdCases; }
+  if(s == 0) { return (bg || light) ? kBdCaseS0 : kBdCases; }   // t >= 2 as s + t >= 2
+  if(t == 1) { return kBdCaseT1; }
+  return s == 1 ? kBdCaseS1 : kBdCaseST;
+}
+
+// One connection (s, t) of a sample: false if it adds nothing, else its
+// weighted contribution `wc` and, for t = 1, the film position it splats to.
+// The body of sample_path's connection loop (bdpt_renderer.cpp:292-468).
+template<bool G, uint32_t CASE, class W>
+DG_HD bool bdpt_connect(const BdptCtx& c, const W& lw, const W& cw, const BdptSampleData& sd,
+                        uint32_t s, uint32_t t, V3& wc, float& sfx, float& sfy, uint32_t& rays) {
+  constexpr bool kAll = CASE == kBdCaseAll;
+  const PtScene& sc = c.sc;
+  const PtParams& pp = c.pp;
+  const uint32_t light_i = sd.light_i;
+  Rand4 rc = rand4(pp.seed, c.pixel, c.sample, kBdConnect + 32 * s + t);
+  const BVert last_camera = cw.get(t - 1);
+  uint32_t new_light = light_i;
+  // the connection's own end vertices where it makes new ones (s = 1 light
+  // sample, t = 1 camera point), else the walks' first vertices
+  BVert first_light, first_camera;
+  const BVert* fl = nullptr;
+  const BVert* fc = nullptr;
+  sfx = sd.fx;
+  sfy = sd.fy;
+  V3 contrib = v3(0.f, 0.f, 0.f);
+  if(s > 0 && last_camera.bg != 0) {
+    return false;
+  } else if(s == 1 && t == 1) {
+    if constexpr(kAll || CASE == kBdCaseT1) {
+      if(G && pp.camera == CAMERA_ORTHO) { return false; }   // CAMERA_DIR_BY_POS_DELTA
+      float cam_pdf;
+      V3 cp = camera_sample_point<G>(pp, rc.a, rc.b, cam_pdf);
+      if(cam_pdf == 0.f) { return false; }
+      LightSample ls = bd_light_sample<G>(sc, sc.lights[light_i], cp, 0.f, rc.c, rc.d);
+      if(ls.pdf == 0.f || is_black(ls.L)) { return false; }
+      float We = camera_eval_importance<G>(pp, cp, ls.wi, sfx, sfy);
+      if(We == 0.f) { return false; }
+      if(sd.pick == 0.f) { return false; }
+      ++rays;
+      Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
+      if(h.prim != kMiss) { return false; }
+      contrib = ls.L * (We / (cam_pdf * ls.pdf * sd.pick));
+    } else {
+      return false;
+    }
+  } else if(s == 0) {
+    if constexpr(kAll || CASE == kBdCaseS0) {
+      const BVert prev_camera = cw.get(t - 2);
+      if(last_camera.bg != 0) {
+        const DevLight& bl = sc.lights[last_camera.bg - 1u];
+        V3 Le = background_radiance(sc, bl, normalize(last_camera.p - prev_camera.p));
+        if(is_black(Le)) { return false; }
+        new_light = last_camera.bg - 1u;
+        contrib = Le * last_camera.alpha;
+      } else if(last_camera.light != 0) {
+        const DevLight& al = sc.lights[last_camera.light - 1u];
+        V3 Le = area_eval_radiance(sc, al, last_camera.p, last_camera.nn, prev_camera.p);
+        if(is_black(Le)) { return false; }
+        new_light = last_camera.light - 1u;
+        contrib = Le * last_camera.alpha;
+      } else {
+        return false;
+      }
+    } else {
+      return false;
+    }
+  } else if(s == 1) {
+    if constexpr(kAll || CASE == kBdCaseS1) {
+      uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, rc.a);
+      float lp = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
+      new_light = li;
+      if(lp == 0.f) { return false; }
+      const DevLight& l2 = sc.lights[li];
+      LightSample ls = bd_light_sample<G>(sc, l2, last_camera.p, last_camera.eps, rc.b, rc.c);
+      if(is_black(ls.L) || ls.pdf == 0.f) { return false; }
+      ++rays;
+      Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
+      if(h.prim != kMiss) { return false; }
+      V3 bwo = normalize(cw.get(t - 2).p - last_camera.p);
+      DevMaterial m = bvert_material(sc, last_camera);
+      Frame fr = bvert_frame(last_camera);
+      V3 f = bd_bsdf_eval<G>(m, fr, ls.wi, bwo, F_ALL);
+      if(is_black(f)) { return false; }
+      first_light = bvert_empty();
+      if(light_flags(l2) & LF_DISTANT) {
+        first_light.p = last_camera.p + ls.wi;
+        first_light.fwd_pdf = ls.pdf;
+      } else {
+        first_light.p = ls.p;
+        first_light.eps = ls.p_eps;
+        first_light.nn = ls.nn;
+        first_light.fwd_pdf = ls.pdf * fabsf(dot(ls.nn, ls.wi)) / length_sq(ls.p - last_camera.p);
+      }
+      first_light.delta = (light_flags(l2) & LF_DELTA_DIR) ? 1u : 0u;
+      first_light.bwd_pdf = bd_bsdf_pdf<G>(m, fr, ls.wi, bwo, F_ALL);
+      fl = &first_light;
+      contrib = last_camera.alpha * f * ls.L *
+                (fabsf(dot(last_camera.nn, ls.wi)) / (lp * ls.pdf));
+    } else {
+      return false;
+    }
+  } else if(t == 1) {
+    if constexpr(kAll || CASE == kBdCaseT1) {
+      const BVert last_light = lw.get(s - 1);
+      CameraPivot cam;
+      if(!camera_pivot_importance<G>(pp, last_light.p, rc.a, rc.b, cam) || cam.We == 0.f ||
+         cam.pdf == 0.f) {
+        return false;
+      }
+      sfx = cam.fx;
+      sfy = cam.fy;
+      V3 wi = normalize(lw.get(s - 2).p - last_light.p);
+      V3 wo = normalize(cam.p - last_light.p);
+      DevMaterial m = bvert_material(sc, last_light);
+      V3 f = bd_bsdf_eval<G>(m, bvert_frame(last_light), wi, wo, F_ALL);
+      if(is_black(f)) { return false; }
+      ++rays;
+      if(!bd_visible<G>(sc, last_light.p, last_light.eps, cam.p, 0.f)) { return false; }
+      first_camera = bvert_empty();
+      first_camera.p = cam.p;
+      first_camera.fwd_pdf = cam.pdf;
+      first_camera.alpha = v3(cam.We, cam.We, cam.We);
+      fc = &first_camera;
+      contrib = last_light.alpha * f *
+                (cam.We * fabsf(dot(last_light.nn, wo)) /
+                 (length_sq(cam.p - last_light.p) * cam.pdf));
+    } else {
+      return false;
+    }
+  } else {
+    // s >= 2 && t >= 2
+    if constexpr(kAll || CASE == kBdCaseST) {
+      const BVert last_light = lw.get(s - 1);
+      ++rays;
+      if(!bd_visible<G>(sc, last_light.p, last_light.eps, last_camera.p, last_camera.eps)) {
+        return false;
+      }
+      V3 lwi = normalize(lw.get(s - 2).p - last_light.p);
+      V3 cwo = normalize(cw.get(t - 2).p - last_camera.p);
+      V3 wo = normalize(last_camera.p - last_light.p);
+      DevMaterial ml = bvert_material(sc, last_light);
+      V3 fl3 = bd_bsdf_eval<G>(ml, bvert_frame(last_light), lwi, wo, F_ALL);
+      if(is_black(fl3)) { return false; }
+      DevMaterial mc = bvert_material(sc, last_camera);
+      V3 fc3 = bd_bsdf_eval<G>(mc, bvert_frame(last_camera), -wo, cwo, F_ALL);
+      if(is_black(fc3)) { return false; }
+      float geom = fabsf(dot(wo, last_light.nn)) * fabsf(dot(wo, last_camera.nn)) /
+                   length_sq(last_light.p - last_camera.p);
+      contrib = last_light.alpha * last_camera.alpha * fl3 * fc3 * geom;
+    } else {
+      return false;
+    }
+  }
+  if(is_black(contrib)) { return false; }
+  BdptPath<W> path{lw, cw, fl, fc, s, t};
+  float w = bdpt_weight<G>(c, sc.lights[new_light], path);
+  wc = contrib * w;
+  return true;
+}
+
+// One pixel sample (sample_path, bdpt_renderer.cpp:40-94) in one thread, as
+// the host check runs it: the camera-side value is returned, t = 1 splats go
+// straight to the film.  The device runs the same walks and connections
+// spread over kernels (bdpt.cu).
 template<bool G>
 DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint32_t sample,
                      float fx, float fy, bool use_t1, float* splat, uint32_t& rays) {
@@ -503,143 +761,20 @@ DG_HD V3 bdpt_sample(const PtScene& sc, const PtParams& pp, uint32_t pixel, uint
   Rand4 r1 = rand4(pp.seed, pixel, sample, 1);
   uint32_t light_i = distrib_sample(sc.light_cdf, sc.light_count + 1, r1.a);
   float pick = distrib_pdf(sc.light_cdf, sc.light_count + 1, light_i);
-  BVert lw[kBdptVerts], cw[kBdptVerts];
+  BVert lwa[kBdptVerts], cwa[kBdptVerts];
+  const LocalWalk lw{lwa}, cw{cwa};
+  uint32_t emit = 0;
   uint32_t ns = pick > 0.f ? bdpt_light_walk<G>(c, light_i, pick, lw, rays) : 0u;
-  uint32_t nt = bdpt_camera_walk<G>(c, fx, fy, cw, rays);
-  if(ns == 0) { lw[0] = bvert_empty(); }
+  uint32_t nt = bdpt_camera_walk<G>(c, fx, fy, cw, rays, emit);
+  if(ns == 0) { lwa[0] = bvert_empty(); }
   if(nt == 0) { return total; }
-  // On the device the lanes of a warp run the (s, t) loop in lock step, to
-  // the warp's largest walk lengths, so that they take the same connection
-  // case together instead of drifting apart by their own walk lengths.
-#ifdef __CUDA_ARCH__
-  const uint32_t lanes = __activemask();
-  const uint32_t s_end = __reduce_max_sync(lanes, ns), t_end = __reduce_max_sync(lanes, nt);
-#else
-  const uint32_t s_end = ns, t_end = nt;
-#endif
-  for(uint32_t s = 0; s <= s_end; ++s) {
-    for(uint32_t t = 1; t <= t_end; ++t) {
-      if(s > ns || t > nt) { continue; }
-      if(t == 1 && !use_t1) { continue; }
-      if(s + t < pp.min_depth + 2 || s + t > pp.max_depth + 2) { continue; }
-      Rand4 rc = rand4(pp.seed, pixel, sample, kBdConnect + 32 * s + t);
-      const BVert& last_camera = cw[t - 1];
-      uint32_t new_light = light_i;
-      // the connection's own end vertices where it makes new ones (s = 1
-      // light sample, t = 1 camera point), else the walks' first vertices
-      BVert first_light, first_camera;
-      const BVert* fl = &lw[0];
-      const BVert* fc = &cw[0];
-      float sfx = fx, sfy = fy;
-      V3 contrib = v3(0.f, 0.f, 0.f);
-      if(s > 0 && last_camera.bg != 0) {
-        continue;
-      } else if(s == 1 && t == 1) {
-        if(G && pp.camera == CAMERA_ORTHO) { continue; }   // CAMERA_DIR_BY_POS_DELTA
-        float cam_pdf;
-        V3 cp = camera_sample_point<G>(pp, rc.a, rc.b, cam_pdf);
-        if(cam_pdf == 0.f) { continue; }
-        LightSample ls = bd_light_sample<G>(sc, sc.lights[light_i], cp, 0.f, rc.c, rc.d);
-        if(ls.pdf == 0.f || is_black(ls.L)) { continue; }
-        float We = camera_eval_importance<G>(pp, cp, ls.wi, sfx, sfy);
-        if(We == 0.f) { continue; }
-        if(pick == 0.f) { continue; }
-        ++rays;
-        Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
-        if(h.prim != kMiss) { continue; }
-        contrib = ls.L * (We / (cam_pdf * ls.pdf * pick));
-      } else if(s == 0 && t >= 2 && last_camera.bg != 0) {
-        const DevLight& bl = sc.lights[last_camera.bg - 1u];
-        V3 Le = background_radiance(sc, bl, normalize(last_camera.p - cw[t - 2].p));
-        if(is_black(Le)) { continue; }
-        new_light = last_camera.bg - 1u;
-        contrib = Le * last_camera.alpha;
-      } else if(s == 0 && t >= 2 && last_camera.light != 0) {
-        const DevLight& al = sc.lights[last_camera.light - 1u];
-        V3 Le = area_eval_radiance(sc, al, last_camera.p, last_camera.nn, cw[t - 2].p);
-        if(is_black(Le)) { continue; }
-        new_light = last_camera.light - 1u;
-        contrib = Le * last_camera.alpha;
-      } else if(s == 0 && t >= 2) {
-        continue;
-      } else if(s == 1 && t >= 2) {
-        uint32_t li = distrib_sample(sc.light_cdf, sc.light_count + 1, rc.a);
-        float lp = distrib_pdf(sc.light_cdf, sc.light_count + 1, li);
-        new_light = li;
-        if(lp == 0.f) { continue; }
-        const DevLight& l2 = sc.lights[li];
-        LightSample ls = bd_light_sample<G>(sc, l2, last_camera.p, last_camera.eps, rc.b, rc.c);
-        if(is_black(ls.L) || ls.pdf == 0.f) { continue; }
-        ++rays;
-        Hit h = bd_trace<true, G>(sc, ls.o, ls.tmin, ls.d, ls.tmax);
-        if(h.prim != kMiss) { continue; }
-        V3 bwo = normalize(cw[t - 2].p - last_camera.p);
-        DevMaterial m = bvert_material(sc, last_camera);
-        Frame fr = bvert_frame(last_camera);
-        V3 f = bd_bsdf_eval<G>(m, fr, ls.wi, bwo, F_ALL);
-        if(is_black(f)) { continue; }
-        first_light = bvert_empty();
-        if(light_flags(l2) & LF_DISTANT) {
-          first_light.p = last_camera.p + ls.wi;
-          first_light.fwd_pdf = ls.pdf;
-        } else {
-          first_light.p = ls.p;
-          first_light.eps = ls.p_eps;
-          first_light.nn = ls.nn;
-          first_light.fwd_pdf = ls.pdf * fabsf(dot(ls.nn, ls.wi)) / length_sq(ls.p - last_camera.p);
-        }
-        first_light.delta = (light_flags(l2) & LF_DELTA_DIR) ? 1u : 0u;
-        first_light.bwd_pdf = bd_bsdf_pdf<G>(m, fr, ls.wi, bwo, F_ALL);
-        fl = &first_light;
-        contrib = last_camera.alpha * f * ls.L *
-                  (fabsf(dot(last_camera.nn, ls.wi)) / (lp * ls.pdf));
-      } else if(s >= 2 && t == 1) {
-        const BVert& last_light = lw[s - 1];
-        CameraPivot cam;
-        if(!camera_pivot_importance<G>(pp, last_light.p, rc.a, rc.b, cam) || cam.We == 0.f ||
-           cam.pdf == 0.f) {
-          continue;
-        }
-        sfx = cam.fx;
-        sfy = cam.fy;
-        V3 wi = normalize(lw[s - 2].p - last_light.p);
-        V3 wo = normalize(cam.p - last_light.p);
-        DevMaterial m = bvert_material(sc, last_light);
-        V3 f = bd_bsdf_eval<G>(m, bvert_frame(last_light), wi, wo, F_ALL);
-        if(is_black(f)) { continue; }
-        ++rays;
-        if(!bd_visible<G>(sc, last_light.p, last_light.eps, cam.p, 0.f)) { continue; }
-        first_camera = bvert_empty();
-        first_camera.p = cam.p;
-        first_camera.fwd_pdf = cam.pdf;
-        first_camera.alpha = v3(cam.We, cam.We, cam.We);
-        fc = &first_camera;
-        contrib = last_light.alpha * f *
-                  (cam.We * fabsf(dot(last_light.nn, wo)) / (length_sq(cam.p - last_light.p) * cam.pdf));
-      } else {
-        // s >= 2 && t >= 2
-        const BVert& last_light = lw[s - 1];
-        ++rays;
-        if(!bd_visible<G>(sc, last_light.p, last_light.eps, last_camera.p, last_camera.eps)) {
-          continue;
-        }
-        V3 lwi = normalize(lw[s - 2].p - last_light.p);
-        V3 cwo = normalize(cw[t - 2].p - last_camera.p);
-        V3 wo = normalize(last_camera.p - last_light.p);
-        DevMaterial ml = bvert_material(sc, last_light);
-        V3 fl = bd_bsdf_eval<G>(ml, bvert_frame(last_light), lwi, wo, F_ALL);
-        if(is_black(fl)) { continue; }
-        DevMaterial mc = bvert_material(sc, last_camera);
-        V3 fc = bd_bsdf_eval<G>(mc, bvert_frame(last_camera), -wo, cwo, F_ALL);
-        if(is_black(fc)) { continue; }
-        float geom = fabsf(dot(wo, last_light.nn)) * fabsf(dot(wo, last_camera.nn)) /
-                     length_sq(last_light.p - last_camera.p);
-        contrib = last_light.alpha * last_camera.alpha * fl * fc * geom;
-      }
-      if(is_black(contrib)) { continue; }
-      BdptPath path{lw, cw, fl, fc, s, t};
-      float w = bdpt_weight<G>(c, sc.lights[new_light], path);
-      V3 wc = contrib * w;
+  const BdptSampleData sd{ns, nt, light_i, pick, fx, fy};
+  for(uint32_t s = 0; s <= ns; ++s) {
+    for(uint32_t t = 1; t <= nt; ++t) {
+      if(bdpt_pair_case(pp, use_t1, emit, s, t) == kBdCases) { continue; }
+      V3 wc;
+      float sfx, sfy;
+      if(!bdpt_connect<G, kBdCaseAll>(c, lw, cw, sd, s, t, wc, sfx, sfy, rays)) { continue; }
       if(t == 1) {
         lt_splat(splat, pp, sfx, sfy, wc);
       } else {

@@ -136,6 +136,65 @@ def test_bdpt_entry_points(cuda):
     sc.close()
 
 
+HOST_CASES = ["box_diff_area_pin", "box_glos_sphe_pin", "box_delt_dire_pin", "box_diff_poin_pin",
+              "openbox_glos_infi_pin", "box_diff_area_orth_d2", "box_diff_area_thin_d1",
+              "simple_sphe_glos_area_fwd_pin", "simple_disk_diff_mixd_2_pin",
+              "bsdf_dielectric_1.5@square", "bsdf_phong_50@square"]
+
+
+def _device_and_host(case, d, w, h, spp, use_t1, max_depth=None, seed=17):
+    import dort_b200 as db
+    p = db.render_params(d["camera"], w, h, spp, min_depth=case["min_depth"],
+                         max_depth=case["max_depth"] if max_depth is None else max_depth,
+                         seed=seed, renderer="bdpt", use_t1_paths=use_t1)
+    sc = db.scene_from_dict(d)
+    dev, st = sc.render(p)
+    sc.close()
+    return dev, db.host_check_render(d, p), st
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", HOST_CASES)
+@pytest.mark.parametrize("use_t1", [True, False])
+def test_bdpt_device_equals_host_check(name, use_t1, cuda):
+    """The device's connection-parallel kernels (walks, one launch per
+    connection case, the ordered per-sample gather) against the same
+    estimator run one sample at a time by the host check, on the same random
+    numbers: the same image up to float rounding (the film's atomic sums,
+    fused multiply-adds) and at most a few paths that take another branch
+    at an edge or a critical angle."""
+    case = ref_scenes.case_by_name(name)
+    d = ref_scenes.build(case)
+    dev, host, st = _device_and_host(case, d, 24, 20, 16, use_t1)
+    assert st["samples"] + st["dropped"] == 24 * 20 * 16
+    assert host.mean() > 0
+    assert ptcheck.forked_pixels(dev, host, tol=1e-3) <= 3, name
+    assert abs(dev.mean() / host.mean() - 1) < 2e-3, name
+
+
+@pytest.mark.gpu
+def test_bdpt_device_equals_host_check_at_depth_13(cuda):
+    """max_depth 13, the deepest the tracer takes: 15 vertices per walk and
+    120 connection slots per sample (all four words of the gather's mask)."""
+    case = ref_scenes.case_by_name("box_diff_area_pin")
+    d = ref_scenes.build(case)
+    dev, host, _ = _device_and_host(case, d, 16, 16, 16, True, max_depth=13)
+    assert ptcheck.forked_pixels(dev, host, tol=1e-3) <= 3
+    assert abs(dev.mean() / host.mean() - 1) < 2e-3
+
+
+@pytest.mark.gpu
+def test_bdpt_frame_spanning_two_chunks(cuda):
+    """32 x 32 x 1100 samples: more than one chunk of 2^20 samples, so the
+    walk buffers, lists and slots are reused by the second chunk."""
+    case = ref_scenes.case_by_name("box_diff_area_pin")
+    d = ref_scenes.build(case)
+    dev, host, st = _device_and_host(case, d, 32, 32, 1100, True)
+    assert st["samples"] + st["dropped"] == 32 * 32 * 1100
+    assert ptcheck.forked_pixels(dev, host, tol=1e-3) <= 3
+    assert abs(dev.mean() / host.mean() - 1) < 1e-3
+
+
 def test_bdpt_fixture_is_consistent():
     """CPU: the fixture covers the reference's "bdpt" test scenes with the
     expected shapes."""
