@@ -1165,7 +1165,14 @@ def measure_cornell(args, ctx, steps, warmup):
                        "image_mean": float(img.mean()),
                        "l2": "inputs are a few KB (L2-resident by design of the workload)"},
             "roofline": None, "cpu_baseline": None, "e2e": None,
-            "gpu_launches": steps * (1 if not wavefront else 0), "clocks": clk,
+            # kernels per frame: kernel + resolve (pt megakernel, lt); bdpt: per
+            # chunk of 2^20 samples the light and camera walks, four connection
+            # cases and the gather, then the resolve; the wavefront's graph is
+            # not counted
+            "gpu_launches": (None if wavefront else steps * (
+                2 if args.renderer != "bdpt" else
+                7 * -(-(C1_W * C1_H * C1_SPP) // (1 << 20)) + 1)),
+            "clocks": clk,
         }
     sc.close()
     return line

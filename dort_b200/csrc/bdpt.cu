@@ -2,11 +2,12 @@
 // connection-parallel.  The pixel samples of a frame (W x H x iterations, in
 // the order pixel + npix * sample) are taken in chunks; per chunk:
 //
-//   bdpt_walks           one thread per sample: the light walk and the camera
-//                        walk into device memory (structure of arrays, so a
-//                        warp's stores are whole lines), and the sample's
-//                        (s, t) connections appended to one list per case
-//                        (bdpt_pair_case) with one atomic per warp and case;
+//   bdpt_light_walks,    one thread per sample: the light walk, then the
+//   bdpt_camera_walks    camera walk, into device memory (structure of
+//                        arrays, so a warp's stores are whole lines); the
+//                        camera kernel appends the sample's (s, t)
+//                        connections to one list per case (bdpt_pair_case)
+//                        with one atomic per warp and case;
 //   bdpt_connect_kernel  one launch per case, one thread per listed
 //                        connection: its rays and its MIS weight
 //                        (bdpt_connect, the host check's code); t = 1
@@ -59,7 +60,8 @@ struct BdptChunk {
   float4* lw;                 // light walks: SoaWalk, 5 D words per sample
   float4* cw;                 // camera walks
   uint4* rec0;                // pixel, sample, light index, ns | nt << 8
-  float4* rec1;               // light pick probability, film x, film y, -
+  float4* rec1;               // light pick probability, film x, film y, - (between
+                              // the walk kernels: pick, light index, ns, -)
   uint4* mask;                // slots holding a t >= 2 connection's value
   float* contrib;             // slot values: ((slot * 3 + channel) * cap + i)
   uint32_t* list[kBdCases];   // connections: i << 8 | s << 4 | t
@@ -72,10 +74,43 @@ __device__ __forceinline__ uint32_t bd_case_count(uint32_t packed, uint32_t c) {
   return (packed >> (8 * c)) & 0xffu;
 }
 
+// The light walks of a chunk: the light pick and the walk of each sample;
+// rec1 carries the pick, the light's index and the vertex count to the
+// camera walks.
 template<bool G>
 __global__ void __launch_bounds__(kBdptBlock)
-bdpt_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch,
-           unsigned long long* __restrict__ counters) {
+bdpt_light_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch,
+                 unsigned long long* __restrict__ counters) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t npix = pp.width * pp.height;
+  uint32_t rays = 0;
+  if(i < count) {
+    const uint64_t g = first + i;
+    const uint32_t pixel = uint32_t(g % npix), sample = uint32_t(g / npix);
+    uint32_t light_i = 0, ns = 0;
+    float pick = 0.f;
+    if(sc.light_count != 0) {
+      BdptCtx c{sc, pp, pixel, sample};
+      Rand4 r1 = rand4(pp.seed, pixel, sample, 1);
+      light_i = distrib_sample(sc.light_cdf, sc.light_count + 1, r1.a);
+      pick = distrib_pdf(sc.light_cdf, sc.light_count + 1, light_i);
+      const SoaWalk lw{ch.lw, ch.cap, i};
+      ns = pick > 0.f ? bdpt_light_walk<G>(c, light_i, pick, lw, rays) : 0u;
+      if(ns == 0) { lw.put(0, bvert_empty()); }
+    }
+    ch.rec1[i] = make_float4(pick, __uint_as_float(light_i), __uint_as_float(ns), 0.f);
+  }
+  unsigned long long r = rays;
+  for(int o = 16; o > 0; o >>= 1) { r += __shfl_down_sync(0xffffffffu, r, o); }
+  if((threadIdx.x & 31u) == 0 && r) { atomicAdd(&counters[0], r); }
+}
+
+// The camera walks of a chunk, then each sample's connections: counted per
+// case, their slots marked for the gather, appended to the case lists.
+template<bool G>
+__global__ void __launch_bounds__(kBdptBlock)
+bdpt_camera_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch,
+                  unsigned long long* __restrict__ counters) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool valid = i < count;
   const uint32_t npix = pp.width * pp.height;
@@ -86,20 +121,16 @@ bdpt_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch
     const uint32_t pixel = uint32_t(g % npix), sample = uint32_t(g / npix);
     Rand4 r0 = rand4(pp.seed, pixel, sample, 0);
     const float fx = float(pixel % pp.width) + r0.a, fy = float(pixel / pp.width) + r0.b;
-    uint32_t light_i = 0;
-    float pick = 0.f;
+    const float4 lr = ch.rec1[i];
+    const uint32_t light_i = __float_as_uint(lr.y);
+    ns = __float_as_uint(lr.z);
     if(sc.light_count != 0) {
       BdptCtx c{sc, pp, pixel, sample};
-      Rand4 r1 = rand4(pp.seed, pixel, sample, 1);
-      light_i = distrib_sample(sc.light_cdf, sc.light_count + 1, r1.a);
-      pick = distrib_pdf(sc.light_cdf, sc.light_count + 1, light_i);
-      const SoaWalk lw{ch.lw, ch.cap, i}, cw{ch.cw, ch.cap, i};
-      ns = pick > 0.f ? bdpt_light_walk<G>(c, light_i, pick, lw, rays) : 0u;
+      const SoaWalk cw{ch.cw, ch.cap, i};
       nt = bdpt_camera_walk<G>(c, fx, fy, cw, rays, emit);
-      if(ns == 0) { lw.put(0, bvert_empty()); }
     }
     ch.rec0[i] = make_uint4(pixel, sample, light_i, ns | (nt << 8));
-    ch.rec1[i] = make_float4(pick, fx, fy, 0.f);
+    ch.rec1[i] = make_float4(lr.x, fx, fy, 0.f);
   }
   // the sample's connections: counts per case (8 bits each: at most 120)
   // and the slots the gather sums
@@ -310,7 +341,10 @@ int launch_bdpt(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st
     const uint32_t count = uint32_t(std::min<uint64_t>(cap, total - first));
     DG_CUDA(cudaMemsetAsync(ch.count, 0, kBdCases * sizeof(uint32_t), st));
     const uint32_t blocks = (count + kBdptBlock - 1) / kBdptBlock;
-    bdpt_walks<true><<<blocks, kBdptBlock, 0, st>>>(s->pt, pp, first, count, ch, d_counters);
+    bdpt_light_walks<true><<<blocks, kBdptBlock, 0, st>>>(s->pt, pp, first, count, ch,
+                                                          d_counters);
+    bdpt_camera_walks<true><<<blocks, kBdptBlock, 0, st>>>(s->pt, pp, first, count, ch,
+                                                           d_counters);
     DG_CUDA(cudaGetLastError());
     bdpt_connect_kernel<true, kBdCaseS0><<<connect_blocks<kBdCaseS0>(sms), kBdptBlock, 0, st>>>(
         s->pt, pp, ch, splat, d_counters);

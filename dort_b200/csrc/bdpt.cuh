@@ -17,42 +17,48 @@ namespace dort_gpu {
 
 constexpr uint32_t kBdptVerts = 16;   // vertices per walk: max_depth <= 13
 
-// Out-of-line entry points for the ray, surface, BSDF and light queries
-// that the walks, the (s, t) connections and the MIS weight share.  Each is
-// called from several places of one sample; inlined at every call site, the
-// kernel's code outgrew the SM's instruction cache (ncu on the Cornell
-// workload: "no_instruction" the top stall at 48 cycles per issued
-// instruction, 7 % of issue slots busy).  One copy of each, reached by a
-// call, keeps the loop's code small.
+// The ray, surface, BSDF and light queries that the walks, the (s, t)
+// connections and the MIS weight share.  When one kernel ran a whole sample,
+// inlining them at every call site outgrew the SM's instruction cache (ncu:
+// "no_instruction" the top stall at 48 cycles per issued instruction), and
+// they were called out of line.  Each device kernel now runs one walk kind or
+// one connection case, small enough to inline them: 148.8 against 136.5 M
+// samples/s on the Cornell workload.  DORT_BD_NOINLINE keeps them out of
+// line.
+#ifdef DORT_BD_NOINLINE
+#define DORT_BD_CALL __noinline__
+#else
+#define DORT_BD_CALL
+#endif
 template<bool ANY_HIT, bool G>
-DG_HD __noinline__ Hit bd_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
+DG_HD DORT_BD_CALL Hit bd_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
   return scene_trace<ANY_HIT, G>(sc, o, t_min, d, t_max);
 }
 template<bool G>
-DG_HD __noinline__ bool bd_visible(const PtScene& sc, V3 a, float ea, V3 b, float eb) {
+DG_HD DORT_BD_CALL bool bd_visible(const PtScene& sc, V3 a, float ea, V3 b, float eb) {
   return lt_visible<G>(sc, a, ea, b, eb);
 }
 template<bool G>
-DG_HD __noinline__ SurfaceHit bd_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+DG_HD DORT_BD_CALL SurfaceHit bd_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
   return surface_at<G>(sc, h, o, d);
 }
 template<bool G>
-DG_HD __noinline__ V3 bd_bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+DG_HD DORT_BD_CALL V3 bd_bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
                                    uint32_t req) {
   return bsdf_eval<G>(m, fr, wi, wo, req);
 }
 template<bool G>
-DG_HD __noinline__ float bd_bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+DG_HD DORT_BD_CALL float bd_bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
                                      uint32_t req) {
   return bsdf_pdf<G>(m, fr, wi, wo, req);
 }
 template<bool G>
-DG_HD __noinline__ BsdfSample bd_bsdf_sample(const DevMaterial& m, const Frame& fr, V3 w,
+DG_HD DORT_BD_CALL BsdfSample bd_bsdf_sample(const DevMaterial& m, const Frame& fr, V3 w,
                                              uint32_t req, float u, float v, float c) {
   return bsdf_sample<G>(m, fr, w, req, u, v, c);
 }
 template<bool G>
-DG_HD __noinline__ LightSample bd_light_sample(const PtScene& sc, const DevLight& l, V3 p,
+DG_HD DORT_BD_CALL LightSample bd_light_sample(const PtScene& sc, const DevLight& l, V3 p,
                                                float eps, float u, float v) {
   return light_sample<G>(sc, l, p, eps, u, v);
 }
