@@ -36,7 +36,21 @@
 namespace dort_gpu {
 
 constexpr int kBdptBlock = 128;
-constexpr uint32_t kBdptChunk = 1u << 20;   // samples per chunk (< 2^24: list code)
+#ifndef DORT_BDPT_CHUNK_LOG2
+#define DORT_BDPT_CHUNK_LOG2 20
+#endif
+// samples per chunk (< 2^24: the list entries' sample field)
+constexpr uint32_t kBdptChunk = 1u << DORT_BDPT_CHUNK_LOG2;
+// Resident blocks per SM the register allocation must allow (Cornell
+// workload, A/B against the compiler's 104-128 registers): connection
+// kernels at 6 blocks +13 %, at 8 (64 registers, some spill) another +4 %;
+// walk kernels at 5 (102 registers) +8 %, at 6 less.
+#ifndef DORT_BDPT_CONNECT_MIN_BLOCKS
+#define DORT_BDPT_CONNECT_MIN_BLOCKS 8
+#endif
+#ifndef DORT_BDPT_WALK_MIN_BLOCKS
+#define DORT_BDPT_WALK_MIN_BLOCKS 5
+#endif
 
 // Connection slots of one sample: (s, t) with t >= 1 and s + t <= D =
 // max_depth + 2, numbered in the host loop's order (s outer, t inner); at
@@ -78,7 +92,7 @@ __device__ __forceinline__ uint32_t bd_case_count(uint32_t packed, uint32_t c) {
 // rec1 carries the pick, the light's index and the vertex count to the
 // camera walks.
 template<bool G>
-__global__ void __launch_bounds__(kBdptBlock)
+__global__ void __launch_bounds__(kBdptBlock, DORT_BDPT_WALK_MIN_BLOCKS)
 bdpt_light_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch,
                  unsigned long long* __restrict__ counters) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -108,7 +122,7 @@ bdpt_light_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptCh
 // The camera walks of a chunk, then each sample's connections: counted per
 // case, their slots marked for the gather, appended to the case lists.
 template<bool G>
-__global__ void __launch_bounds__(kBdptBlock)
+__global__ void __launch_bounds__(kBdptBlock, DORT_BDPT_WALK_MIN_BLOCKS)
 bdpt_camera_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptChunk ch,
                   unsigned long long* __restrict__ counters) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -198,7 +212,7 @@ bdpt_camera_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptC
 }
 
 template<bool G, uint32_t CASE>
-__global__ void __launch_bounds__(kBdptBlock)
+__global__ void __launch_bounds__(kBdptBlock, DORT_BDPT_CONNECT_MIN_BLOCKS)
 bdpt_connect_kernel(PtScene sc, PtParams pp, BdptChunk ch, float* __restrict__ splat,
                     unsigned long long* __restrict__ counters) {
   const uint32_t n = *(volatile uint32_t*)&ch.count[CASE];
