@@ -350,7 +350,10 @@ int launch_bdpt(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st
   ch.cap = cap;
   ch.D = D;
   DG_CUDA(cudaMemsetAsync(base, 0, lw_off, st));   // film sums and splats
-  // one instantiation: the bidirectional tracer is not specialised
+  // one instantiation: the bidirectional tracer is not specialised (the
+  // triangle-only instantiation of the same kernels, chosen per scene like
+  // the path tracer's, rendered the Cornell workload's identical image at
+  // 139.6 against 212.2 M samples/s)
   for(uint64_t first = 0; first < total; first += cap) {
     const uint32_t count = uint32_t(std::min<uint64_t>(cap, total - first));
     DG_CUDA(cudaMemsetAsync(ch.count, 0, kBdCases * sizeof(uint32_t), st));
