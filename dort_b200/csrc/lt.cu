@@ -10,9 +10,24 @@
 namespace dort_gpu {
 
 constexpr int kLtBlock = 128;
+// Resident blocks per SM the register allocation must allow: 8 (64
+// registers, with spills) ran the Cornell workload at 867 M samples/s
+// against 817 M with the block size alone (128 registers, 4 blocks) and 712 M
+// at 6; the light paths' visibility rays and splats wait on memory, which
+// more resident warps hide.  (An explicit minimum of 1 is not the same as
+// none: the compiler then took 180 registers.)
+#ifndef DORT_LT_MIN_BLOCKS
+#define DORT_LT_MIN_BLOCKS 8
+#endif
+// 0: the block size alone (the compiler picks the registers)
+#if DORT_LT_MIN_BLOCKS > 0
+#define DORT_LT_BOUNDS __launch_bounds__(kLtBlock, DORT_LT_MIN_BLOCKS)
+#else
+#define DORT_LT_BOUNDS __launch_bounds__(kLtBlock)
+#endif
 
 template<bool G>
-__global__ void __launch_bounds__(kLtBlock)
+__global__ void DORT_LT_BOUNDS
 lt_kernel(PtScene sc, PtParams pp, uint64_t paths, float* __restrict__ film,
           unsigned long long* __restrict__ counters) {
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;

@@ -43,8 +43,22 @@ DG_HD bool keep_sample(V3 L) {
          L.z >= 0.f;
 }
 
+// Resident blocks per SM the register allocation must allow: 5 (96
+// registers) against the block size alone (168 registers): the Cornell
+// workload 557 against 468 M samples/s, the 1080p frame 286.6 against 282.1
+// M (6 blocks: 573 and 273.4 M).
+#ifndef DORT_PT_MIN_BLOCKS
+#define DORT_PT_MIN_BLOCKS 5
+#endif
+// 0: the block size alone (the compiler picks the registers)
+#if DORT_PT_MIN_BLOCKS > 0
+#define DORT_PT_BOUNDS __launch_bounds__(kPtBlock, DORT_PT_MIN_BLOCKS)
+#else
+#define DORT_PT_BOUNDS __launch_bounds__(kPtBlock)
+#endif
+
 template<bool G>
-__global__ void __launch_bounds__(kPtBlock)
+__global__ void DORT_PT_BOUNDS
 pt_megakernel(PtScene sc, PtParams pp, uint32_t slices, uint32_t spp_per_slice,
               uint32_t per_slice, float4* __restrict__ partial,
               unsigned long long* __restrict__ ray_count) {
