@@ -184,6 +184,26 @@ def test_bdpt_device_equals_host_check_at_depth_13(cuda):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("min_depth,max_depth", [(2, 6), (4, 4), (1, 1)])
+def test_bdpt_device_equals_host_check_depth_window(min_depth, max_depth, cuda):
+    """Connections outside [min_depth + 2, max_depth + 2] vertices are
+    neither listed nor given a slot (a window of one length, and max_depth
+    1: no s, t >= 2 connection at all)."""
+    import dort_b200 as db
+    case = ref_scenes.case_by_name("box_glos_sphe_pin")
+    d = ref_scenes.build(case)
+    p = db.render_params(d["camera"], 20, 16, 16, min_depth=min_depth, max_depth=max_depth,
+                         seed=29, renderer="bdpt")
+    sc = db.scene_from_dict(d)
+    dev, _ = sc.render(p)
+    sc.close()
+    host = db.host_check_render(d, p)
+    assert host.mean() > 0
+    assert ptcheck.forked_pixels(dev, host, tol=1e-3) <= 3
+    assert abs(dev.mean() / host.mean() - 1) < 2e-3
+
+
+@pytest.mark.gpu
 def test_bdpt_frame_spanning_two_chunks(cuda):
     """32 x 32 x 1100 samples: more than one chunk of 2^20 samples, so the
     walk buffers, lists and slots are reused by the second chunk."""
