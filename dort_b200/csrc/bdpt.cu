@@ -79,6 +79,7 @@ struct BdptChunk {
   uint4* mask;                // slots holding a t >= 2 connection's value
   float* contrib;             // slot values: ((slot * 3 + channel) * cap + i)
   uint32_t* list[kBdCases];   // connections: i << 8 | s << 4 | t
+  uint32_t list_cap[kBdCases];  // entries each list holds (bd_case_cap x cap)
   uint32_t* count;            // list lengths
   uint32_t cap;               // samples per chunk
   uint32_t D;                 // max_depth + 2
@@ -193,16 +194,19 @@ bdpt_camera_walks(PtScene sc, PtParams pp, uint64_t first, uint32_t count, BdptC
         // list and position by case, without indexing an array by c
         uint32_t* dst;
         uint32_t at;
+        uint32_t lim;
         if(c == kBdCaseS0) {
-          dst = ch.list[0]; at = off[0]++;
+          dst = ch.list[0]; at = off[0]++; lim = ch.list_cap[0];
         } else if(c == kBdCaseS1) {
-          dst = ch.list[1]; at = off[1]++;
+          dst = ch.list[1]; at = off[1]++; lim = ch.list_cap[1];
         } else if(c == kBdCaseT1) {
-          dst = ch.list[2]; at = off[2]++;
+          dst = ch.list[2]; at = off[2]++; lim = ch.list_cap[2];
         } else {
-          dst = ch.list[3]; at = off[3]++;
+          dst = ch.list[3]; at = off[3]++; lim = ch.list_cap[3];
         }
-        dst[at] = code;
+        // the capacities bound every sample's count per case, so this never
+        // skips; it keeps a wrong count from writing past the list
+        if(at < lim) { dst[at] = code; }
       }
     }
   }
@@ -215,7 +219,7 @@ template<bool G, uint32_t CASE>
 __global__ void __launch_bounds__(kBdptBlock, DORT_BDPT_CONNECT_MIN_BLOCKS)
 bdpt_connect_kernel(PtScene sc, PtParams pp, BdptChunk ch, float* __restrict__ splat,
                     unsigned long long* __restrict__ counters) {
-  const uint32_t n = *(volatile uint32_t*)&ch.count[CASE];
+  const uint32_t n = min(*(volatile uint32_t*)&ch.count[CASE], ch.list_cap[CASE]);
   const uint32_t* __restrict__ list = ch.list[CASE];
   uint32_t rays = 0;
   for(uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
@@ -345,6 +349,7 @@ int launch_bdpt(dort_scene* s, const PtParams& pp, float* d_out, cudaStream_t st
   ch.contrib = reinterpret_cast<float*>(base + contrib_off);
   for(uint32_t c = 0; c < kBdCases; ++c) {
     ch.list[c] = reinterpret_cast<uint32_t*>(base + list_off[c]);
+    ch.list_cap[c] = std::max(1u, bd_case_cap(D, c)) * cap;
   }
   ch.count = reinterpret_cast<uint32_t*>(base + count_off);
   ch.cap = cap;

@@ -18,12 +18,18 @@ constexpr int kRaycastBlock = 128;
 // are limited so that it cannot wrap.
 constexpr size_t kRaycastMaxRays = 0xff000000u;
 
-// Launch bound without a minimum block count: the compiler then keeps the
-// kernel at 60-64 registers.  An explicit minimum of 1 raised it to 96
-// registers (2,044 against 2,472 Mrays/s on the ray-cast workload), and
-// minimums of 12 or 16 spill (1,309 / 692 Mrays/s).
+// Launch bound without a minimum block count (DORT_RAYCAST_MIN_BLOCKS
+// unset): the compiler then keeps the kernel at 60-64 registers, 2,476
+// Mrays/s on the ray-cast workload.  An explicit minimum of 1 raised it to 96
+// registers (2,044 Mrays/s); minimums of 9, 10, 12 and 16 measured 2,384,
+// 2,001, 1,309 and 692 Mrays/s.
+#ifdef DORT_RAYCAST_MIN_BLOCKS
+#define DORT_RAYCAST_BOUNDS __launch_bounds__(kRaycastBlock, DORT_RAYCAST_MIN_BLOCKS)
+#else
+#define DORT_RAYCAST_BOUNDS __launch_bounds__(kRaycastBlock)
+#endif
 template<bool ANY_HIT, int WT = kTriMt>
-__global__ void __launch_bounds__(kRaycastBlock)
+__global__ void DORT_RAYCAST_BOUNDS
 raycast_kernel(TraceScene sc, const float4* __restrict__ rays, uint32_t ray_count,
                uint32_t* __restrict__ out_prim, float* __restrict__ out_tb,
                uint32_t* __restrict__ work) {
