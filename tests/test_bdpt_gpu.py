@@ -215,6 +215,44 @@ def test_bdpt_frame_spanning_two_chunks(cuda):
     assert abs(dev.mean() / host.mean() - 1) < 1e-3
 
 
+@pytest.mark.gpu
+def test_bdpt_scene_without_lights_keeps_black_samples(cuda):
+    """No light: every sample is 0 and kept (sample_path returns at once),
+    and no connection is listed."""
+    import dort_b200 as db
+    from dort_b200 import scenes
+    sd = scenes.cornell_box()
+    sd["tri_emission"] = np.zeros_like(sd["tri_emission"])
+    sc = db.scene_from_dict(sd)
+    p = db.render_params(sd["camera"], 40, 30, 4, max_depth=8, renderer="bdpt")
+    img, st = sc.render(p)
+    sc.close()
+    assert st["samples"] == 40 * 30 * 4 and st["dropped"] == 0
+    assert not img.any()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("w,h,spp", [(1, 1, 3), (3, 1, 349526), (7, 5, 1)])
+def test_bdpt_small_and_ragged_sample_counts(w, h, spp, cuda):
+    """Partial warps and blocks: a single pixel with 3 samples, a frame whose
+    second chunk holds two samples (3 x 349,526 = 2^20 + 2), an odd 7 x 5
+    frame."""
+    import dort_b200 as db
+    from dort_b200 import scenes
+    sd = scenes.cornell_box()
+    p = db.render_params(sd["camera"], w, h, spp, max_depth=5, seed=13, renderer="bdpt")
+    sc = db.scene_from_dict(sd)
+    dev, st = sc.render(p)
+    sc.close()
+    assert st["samples"] + st["dropped"] == w * h * spp
+    host = db.host_check_render(sd, p)
+    assert np.isfinite(dev).all()
+    if spp > 1000:
+        assert abs(dev.mean() / host.mean() - 1) < 1e-3
+    else:
+        assert ptcheck.forked_pixels(dev, host, tol=1e-3) == 0
+
+
 def test_bdpt_fixture_is_consistent():
     """CPU: the fixture covers the reference's "bdpt" test scenes with the
     expected shapes."""
