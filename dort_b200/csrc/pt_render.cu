@@ -477,8 +477,8 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
     tn.deterministic = t->deterministic == 1 ? 1u : 0u;
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
-  if(tn.capacity < 32 || tn.capacity > (1u << 26)) {
-    err = "queue_capacity must be 32..2^26";
+  if(tn.capacity < 32 || tn.capacity > (1u << 27)) {
+    err = "queue_capacity must be 32..2^27";
     return false;
   }
   for(uint32_t b : {tn.trace_block, tn.shade_block}) {

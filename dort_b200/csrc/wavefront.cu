@@ -1167,6 +1167,12 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix, uint32_t ne
   if(wf->mem && wf->capacity == capacity && wf->npix_cap >= npix && wf->nee_mult == nee_mult) {
     return DORT_OK;
   }
+  // the direct-lighting queues' entries are counted in 32 bits
+  if(2ull * nee_mult * capacity > (1ull << 31)) {
+    return fail(DORT_ERR_INVALID, "queue_capacity x sampled lights too large: " +
+                std::to_string(capacity) + " path slots x " + std::to_string(nee_mult) +
+                " lights exceeds 2^30 direct-lighting entries per wave");
+  }
   wf_release(wf);
   auto al = [](size_t x) { return (x + 255) & ~size_t(255); };
   size_t Q = capacity;
