@@ -417,10 +417,10 @@ typedef struct dort_wavefront_tuning {
                                   the previous batch's traversals); blocks of
                                   at most 256 trace threads */
   uint32_t deterministic;      /* 0: auto (off), 1: on, 2: off -- the frame's
-                                  sums in a fixed order: every 4-sample work
-                                  unit's sum is stored apart (16 bytes per
-                                  pixel and unit) and the resolve adds them in
-                                  unit order, so that the same frame renders
+                                  sums in a fixed order: every sample's value
+                                  is stored apart (16 bytes per pixel and
+                                  sample) and the resolve adds them in
+                                  sample order, so that the same frame renders
                                   to the same bits (a path's shadow-ray
                                   additions are ordered too unless it has two
                                   in one wave: a background light under the
