@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "common.h"
+#include "wavefront.h"
 
 namespace dort_gpu {
 namespace {
@@ -77,8 +78,9 @@ int time_frame(dort_scene* sc, const dort_render_params* p, const dort_wavefront
 }
 
 uint64_t frame_units(const dort_render_params& p) {
-  // work units of 4 samples of one pixel (the wavefront's unit of work)
-  return uint64_t(p.width) * p.height * ((p.iterations + 3) / 4);
+  // the wavefront's work units: kWfUnitSamples samples of one pixel
+  return uint64_t(p.width) * p.height *
+         ((p.iterations + kWfUnitSamples - 1) / kWfUnitSamples);
 }
 
 bool fits(uint32_t cap, size_t free_bytes) {

@@ -493,10 +493,11 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
 static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTuning& tn,
                         std::string& err) {
   uint64_t tiles = uint64_t((pp.width + 7) / 8) * ((pp.height + 3) / 4);
-  uint64_t total = tiles * 32 * pp.spp;
-  // default: up to 2^24 path slots (about 5.5 GB of path state); more slots
-  // make fewer, fuller waves (1080p at 256 spp: 567 M samples/s at 2^22,
-  // 606 M at 2^24)
+  uint64_t total = tiles * 32 * ((pp.spp + kWfUnitSamples - 1) / kWfUnitSamples);
+  // default: up to 2^24 path slots (about 5.5 GB of path state) or the
+  // frame's work units; more slots make fewer, fuller waves (the 1080p frame
+  // at 256 spp: 567 M samples/s at 2^22, 606 M at 2^24 with 4-sample units;
+  // the autotuner goes up to 2^27)
   return read_tuning(t, uint32_t(std::min<uint64_t>(total, 1u << 24)), tn, err);
 }
 

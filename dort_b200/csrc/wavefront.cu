@@ -97,10 +97,7 @@ __device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor) {
 // stay full and their primary rays coherent.  1080p frame 725.8 / 698.2 /
 // 670.3 / 626.9 M samples/s with 1 / 2 / 4 / 8 samples per unit; Cornell
 // workload 1,097 / 973 / 869 M; adjoint 132 / 142 / 157 ms.
-#ifndef DORT_WF_CHUNK
-#define DORT_WF_CHUNK 1
-#endif
-constexpr uint32_t kChunk = DORT_WF_CHUNK;
+constexpr uint32_t kChunk = kWfUnitSamples;
 
 __device__ __forceinline__ void unit_to_pixel(const PtParams& pp, uint64_t uid, uint32_t& pixel,
                                               uint32_t& x, uint32_t& y, uint32_t& s0) {

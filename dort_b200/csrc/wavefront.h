@@ -9,6 +9,15 @@ struct dort_scene;
 
 namespace dort_gpu {
 
+// Samples of one pixel per work unit: a path slot takes a unit, traces its
+// samples one after another and adds their sum to the film once (the
+// wavefront, the autotuner's slot counts and the deterministic sums' memory
+// all count in units).
+#ifndef DORT_WF_CHUNK
+#define DORT_WF_CHUNK 1
+#endif
+constexpr uint32_t kWfUnitSamples = DORT_WF_CHUNK;
+
 struct WfTuning {
   uint32_t capacity;      // paths in flight
   uint32_t trace_block;   // threads per block of extend / shadow / neeb
