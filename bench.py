@@ -875,7 +875,9 @@ def measure_pt(args, ctx):
                        "stage_ms_per_frame": {k: round(stages[k], 3) for k in
                                               ("regen", "extend", "shade", "shadow", "neeb")},
                        "bvh_build": st["bvh_build"], "bvh_build_ms": round(st["bvh_ms"], 2),
-                       "l2": "frame state (path queues ~11 GB, image 25 MB) larger than L2"},
+                       # about 330 bytes of path state and queues per slot
+                       "l2": "frame state (path queues ~%.0f GB, image 25 MB) larger than L2"
+                             % (tuning["queue_capacity"] * 330 / 1e9)},
             "roofline": rl, "cpu_baseline": cpu,
             # per frame the caller passes its render parameters and reads the
             # image back; the scene (vertices, indices, materials, sky) goes to
