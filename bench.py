@@ -974,7 +974,8 @@ def measure_batch(args, ctx, steps, warmup, mega_warmup=True):
     # the batch tuning: 2^22 slots, or the autotuner's choice on a proxy
     # batch (every job at an eighth of its samples) with --tuning auto in a
     # batch run of its own
-    tuning = {"queue_capacity": 1 << 22, "sort_rays": args.sort_rays == "on"}
+    tuning = {"queue_capacity": args.queue_capacity or 1 << 22,
+              "sort_rays": args.sort_rays == "on"}
     tuned = None
     if args.tuning == "auto" and args.workload == "batch":
         from dort_b200 import autotune as at
@@ -1241,7 +1242,7 @@ def main():
                     help="wavefront tuning: the autotuner's choice on the frame, or the "
                          "fixed 2^25 slots / 128-thread blocks")
     ap.add_argument("--queue-capacity", type=int, default=0,
-                    help="pt1080p: path slots of the wavefront (implies a fixed tuning; "
+                    help="pt1080p, batch: path slots of the wavefront (implies a fixed tuning; "
                          "small values keep a profiled run's device memory small)")
     ap.add_argument("--stage-queues", default="off", choices=["on", "off"],
                     help="stage the shadow queue through bulk copies (TMA) into shared memory")

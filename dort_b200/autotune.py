@@ -3,7 +3,7 @@
 The search itself is native (dort_gpu_autotune_wavefront /
 dort_gpu_autotune_batch, csrc/autotune.cu): block sizes of the trace and
 shade stages ranked on a proxy frame of the caller's scene and camera, path
-slot capacities 2^22 .. 2^27 on the frame itself, each candidate timed with
+slot capacities 2^22 .. 2^28 on the frame itself, each candidate timed with
 CUDA events.  This module adds the one choice that needs the scene rebuilt,
 the BVH node width, by tuning each width's scene and keeping the fastest.
 

@@ -5,7 +5,7 @@
 //   stage 1, block sizes: every (trace, shade) pair of {64, 128, 256} on a
 //            proxy frame -- the frame's resolution, depth, camera and seed at
 //            a few samples per pixel -- at 2^22 path slots;
-//   stage 2, capacity:    2^22 .. 2^27 slots with the chosen
+//   stage 2, capacity:    2^22 .. 2^28 slots with the chosen
 //            blocks on the frame itself (all its samples: how many waves a
 //            frame takes, and so what a slot count costs, depends on the
 //            whole frame's work), skipping capacities beyond twice the
@@ -32,8 +32,8 @@ namespace {
 using Clock = std::chrono::steady_clock;
 
 constexpr uint32_t kBlocks[3] = {64, 128, 256};
-constexpr uint32_t kCapacities[6] = {1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26,
-                                      1u << 27};
+constexpr uint32_t kCapacities[7] = {1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26,
+                                      1u << 27, 1u << 28};
 constexpr double kBytesPerSlot = 340.0;
 
 double ms_since(Clock::time_point t0) {

@@ -477,8 +477,8 @@ static bool read_tuning(const dort_wavefront_tuning* t, uint32_t default_capacit
     tn.deterministic = t->deterministic == 1 ? 1u : 0u;
   }
   tn.capacity = (tn.capacity + 31u) & ~31u;
-  if(tn.capacity < 32 || tn.capacity > (1u << 27)) {
-    err = "queue_capacity must be 32..2^27";
+  if(tn.capacity < 32 || tn.capacity > (1u << 28)) {
+    err = "queue_capacity must be 32..2^28";
     return false;
   }
   for(uint32_t b : {tn.trace_block, tn.shade_block}) {
@@ -497,7 +497,7 @@ static bool make_tuning(const dort_wavefront_tuning* t, const PtParams& pp, WfTu
   // default: up to 2^24 path slots (about 5.5 GB of path state) or the
   // frame's work units; more slots make fewer, fuller waves (the 1080p frame
   // at 256 spp: 567 M samples/s at 2^22, 606 M at 2^24 with 4-sample units;
-  // the autotuner goes up to 2^27)
+  // the autotuner goes up to 2^28)
   return read_tuning(t, uint32_t(std::min<uint64_t>(total, 1u << 24)), tn, err);
 }
 

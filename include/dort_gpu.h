@@ -390,7 +390,7 @@ int dort_gpu_render_device_noalloc(dort_scene* scene, const dort_render_params* 
  * many entries per path slot). */
 typedef struct dort_wavefront_tuning {
   uint32_t struct_size;        /* sizeof(dort_wavefront_tuning) */
-  uint32_t queue_capacity;     /* paths in flight, at most 2^27 (0: auto,
+  uint32_t queue_capacity;     /* paths in flight, at most 2^28 (0: auto,
                                   up to 2^24 for a frame, 2^22 for a batch;
                                   each path slot holds about 330 bytes of
                                   device memory; more slots, fewer and
@@ -468,7 +468,7 @@ int dort_gpu_batch_destroy(dort_batch* batch);
  * tunings on the GPU and writes the fastest to out_tuning (struct_size set).
  * Block sizes (trace, shade) of {64, 128, 256} are ranked on a proxy frame
  * (the frame at up to 8 samples per pixel, 2^22 path slots); path-slot
- * capacities 2^22 .. 2^27 on the frame itself, skipping those beyond twice
+ * capacities 2^22 .. 2^28 on the frame itself, skipping those beyond twice
  * its work or beyond the free device memory (about 340 bytes per slot).
  * Each candidate runs twice, the faster run counts.  budget_ms bounds the
  * search (0: 30 s); when it runs out the best so far wins.  out_stats
