@@ -295,15 +295,16 @@ static size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 // kernel on every SM.
 template<uint32_t CASE>
 static int connect_blocks(int sms) {
-  static int per_sm = 0;
-  if(per_sm == 0) {
+  // computed once (a thread-safe static initialiser)
+  static const int per_sm = [] {
     int b = 0;
     if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, bdpt_connect_kernel<true, CASE>,
                                                      kBdptBlock, 0) != cudaSuccess || b < 1) {
+      cudaGetLastError();
       b = 4;
     }
-    per_sm = b;
-  }
+    return b;
+  }();
   return per_sm * sms;
 }
 
