@@ -533,7 +533,7 @@ REF_SAMPLE_W, REF_SAMPLE_H = 480, 270
 # (4,194,304 rays, waves 6-8 of the 16-spp frame), mean of three launches of
 # the ncu capture summarised in profiles/wf_extend_pt1080p.md: 777 MB, 185 B
 # per ray; reported as the roofline's traffic.
-EXTEND_TRAFFIC_BYTES = 777.0e6
+EXTEND_TRAFFIC_BYTES = 730.4e6
 EXTEND_TRAFFIC_RAYS = 4194304
 # The bound that applies to the extension stage beside the HBM roofline:
 # issue slots and latency.  Figures of one wf_extend launch under
