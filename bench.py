@@ -542,10 +542,11 @@ EXTEND_TRAFFIC_RAYS = 4194304
 # lts__throughput and gpu__dram_throughput as fractions of their peaks.
 EXTEND_LIMITER = {
     "bound": "issue slots and node-fetch latency (divergent traversal)",
-    "source": "ncu --set full of one wf_extend launch, profiles/wf_extend_pt1080p.md",
-    "issue_slots_busy": 0.453, "simt_efficiency": 9.34 / 32, "achieved_occupancy": 0.374,
-    "l2_throughput": 0.178, "dram_throughput": 0.082,
-    "top_stall": "long_scoreboard (L1/L2 node and stack loads), 9.24 cycles per issue",
+    "source": "ncu --set full of one full-queue wf_extend launch, "
+              "profiles/wf_extend_pt1080p.md",
+    "issue_slots_busy": 0.668, "simt_efficiency": 11.92 / 32, "achieved_occupancy": 0.534,
+    "occupancy_limit": 0.5625, "l2_throughput": 0.178, "dram_throughput": 0.072,
+    "top_stall": "long_scoreboard (L1/L2 node and stack loads), 6.02 cycles per issue",
 }
 
 _ref_worker_scene = None
