@@ -39,12 +39,13 @@ constexpr int kBdptBlock = 128;
 #ifndef DORT_BDPT_CHUNK_LOG2
 #define DORT_BDPT_CHUNK_LOG2 20
 #endif
-// samples per chunk (< 2^24: the list entries' sample field)
+// samples per chunk (< 2^24: the list entries' sample field); chunks of
+// 2^21 or 2^22 samples measured the same on the Cornell workload
 constexpr uint32_t kBdptChunk = 1u << DORT_BDPT_CHUNK_LOG2;
 // Resident blocks per SM the register allocation must allow (Cornell
 // workload, A/B against the compiler's 104-128 registers): connection
 // kernels at 6 blocks +13 %, at 8 (64 registers, some spill) another +4 %;
-// walk kernels at 5 (102 registers) +8 %, at 6 less.
+// walk kernels at 5 (96 registers) +8 %, at 6 less.
 #ifndef DORT_BDPT_CONNECT_MIN_BLOCKS
 #define DORT_BDPT_CONNECT_MIN_BLOCKS 8
 #endif
