@@ -23,6 +23,7 @@
 #include <string>
 #include <vector>
 
+#include "autotune_plan.h"
 #include "common.h"
 #include "wavefront.h"
 
@@ -34,7 +35,6 @@ using Clock = std::chrono::steady_clock;
 constexpr uint32_t kBlocks[3] = {64, 128, 256};
 constexpr uint32_t kCapacities[7] = {1u << 22, 1u << 23, 1u << 24, 1u << 25, 1u << 26,
                                       1u << 27, 1u << 28};
-constexpr double kBytesPerSlot = 340.0;
 
 double ms_since(Clock::time_point t0) {
   return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
@@ -83,8 +83,9 @@ uint64_t frame_units(const dort_render_params& p) {
          ((p.iterations + kWfUnitSamples - 1) / kWfUnitSamples);
 }
 
-bool fits(uint32_t cap, size_t free_bytes) {
-  return kBytesPerSlot * double(cap) <= 0.8 * double(free_bytes);
+// Lights a path vertex samples (the direct-lighting queues' multiplier).
+uint32_t nee_lights(const PtScene& sc, const dort_render_params& p) {
+  return p.sample_all_lights ? std::max(1u, sc.light_count) : 1u;
 }
 
 }  // namespace
@@ -136,6 +137,7 @@ extern "C" int dort_gpu_autotune_wavefront(dort_scene* scene, const dort_render_
   }
   // stage 2: capacities on the frame
   const uint64_t units = frame_units(*params);
+  const uint32_t nee = nee_lights(scene->pt, *params);
   uint32_t held = cap1;   // the slot count the scene's queues hold now
   double best2 = 1e300;
   dort_wavefront_tuning best_cap = best;
@@ -143,18 +145,26 @@ extern "C" int dort_gpu_autotune_wavefront(dort_scene* scene, const dort_render_
       uint32_t(std::min<uint64_t>(uint64_t(1) << 22, std::max<uint64_t>(32, units)));
   for(uint32_t cap : kCapacities) {
     if(rc != DORT_OK) { break; }
-    if(cap != kCapacities[0] && uint64_t(cap) > 2 * units) { continue; }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    if(cap != kCapacities[0] && !fits(cap, free_b + size_t(kBytesPerSlot * held))) { continue; }
+    if(!capacity_candidate(cap, cap == kCapacities[0], units, nee, free_b, held)) { continue; }
     if(best2 < 1e300 && ms_since(t0) + 2.0 * best2 > budget_ms) { cut = true; break; }
     dort_wavefront_tuning t = best;
     t.queue_capacity = uint32_t(std::min<uint64_t>(cap, std::max<uint64_t>(32, units)));
     double ms = 0.0;
-    rc = time_frame(scene, params, t, d_out, st, &ms);
-    held = t.queue_capacity;
+    const int r = time_frame(scene, params, t, d_out, st, &ms);
     ++timed;
-    if(rc == DORT_OK && ms < best2) { best2 = ms; best_cap = t; }
+    if(r == DORT_OK) {
+      held = t.queue_capacity;
+      if(ms < best2) { best2 = ms; best_cap = t; }
+    } else if(r == DORT_ERR_OOM && best2 < 1e300) {
+      // a larger capacity than the device holds after all: keep the best of
+      // the smaller ones (the scene's queues were released by the failure)
+      clear_error();
+      break;
+    } else {
+      rc = r;
+    }
   }
   cudaStreamDestroy(st);
   cudaFree(d_out);
@@ -179,10 +189,12 @@ extern "C" int dort_gpu_autotune_batch(const dort_batch_job* jobs, uint32_t job_
   // the proxy batch: every job at an eighth of its samples (at least 4)
   std::vector<dort_batch_job> proxy(jobs, jobs + job_count);
   uint64_t units = 0;
+  uint32_t nee = 1;
   for(auto& j : proxy) {
     j.params.iterations = std::max<uint32_t>(std::min<uint32_t>(4, j.params.iterations),
                                              j.params.iterations / 8);
     units += frame_units(j.params);
+    if(j.scene) { nee = std::max(nee, nee_lights(j.scene->pt, j.params)); }
   }
   cudaStream_t st = nullptr;
   DG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
@@ -197,10 +209,9 @@ extern "C" int dort_gpu_autotune_batch(const dort_batch_job* jobs, uint32_t job_
   const uint32_t caps[4] = {1u << 21, 1u << 22, 1u << 23, 1u << 24};
   for(uint32_t cap : caps) {
     if(rc != DORT_OK) { break; }
-    if(cap != caps[0] && uint64_t(cap) > 2 * units) { continue; }
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    if(!fits(cap, free_b)) { continue; }
+    if(cap != caps[0] && !capacity_candidate(cap, false, units, nee, free_b, 0)) { continue; }
     if(best_ms < 1e300 && ms_since(t0) + 2.0 * best_ms > budget_ms) { cut = true; break; }
     dort_wavefront_tuning t = make_tuning(cap, 128, 128);
     dort_batch* b = nullptr;

@@ -29,6 +29,7 @@
 #include <string>
 
 #include "adjoint.cuh"
+#include "autotune_plan.h"
 #include "common.h"
 #include "pt.cuh"
 #include "scene_build.h"
@@ -1174,7 +1175,7 @@ static int wf_alloc(Wavefront* wf, uint32_t capacity, uint32_t npix, uint32_t ne
     return DORT_OK;
   }
   // the direct-lighting queues' entries are counted in 32 bits
-  if(2ull * nee_mult * capacity > (1ull << 31)) {
+  if(!wavefront_entries_fit(capacity, nee_mult)) {
     return fail(DORT_ERR_INVALID, "queue_capacity x sampled lights too large: " +
                 std::to_string(capacity) + " path slots x " + std::to_string(nee_mult) +
                 " lights exceeds 2^30 direct-lighting entries per wave");
