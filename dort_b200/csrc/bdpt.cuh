@@ -26,39 +26,39 @@ constexpr uint32_t kBdptVerts = 16;   // vertices per walk: max_depth <= 13
 // samples/s on the Cornell workload.  DORT_BD_NOINLINE keeps them out of
 // line.
 #ifdef DORT_BD_NOINLINE
-#define DORT_BD_CALL __noinline__
+#define DORT_BD_FN __host__ __device__ __noinline__
 #else
-#define DORT_BD_CALL
+#define DORT_BD_FN DG_HD
 #endif
 template<bool ANY_HIT, bool G>
-DG_HD DORT_BD_CALL Hit bd_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
+DORT_BD_FN Hit bd_trace(const PtScene& sc, V3 o, float t_min, V3 d, float t_max) {
   return scene_trace<ANY_HIT, G>(sc, o, t_min, d, t_max);
 }
 template<bool G>
-DG_HD DORT_BD_CALL bool bd_visible(const PtScene& sc, V3 a, float ea, V3 b, float eb) {
+DORT_BD_FN bool bd_visible(const PtScene& sc, V3 a, float ea, V3 b, float eb) {
   return lt_visible<G>(sc, a, ea, b, eb);
 }
 template<bool G>
-DG_HD DORT_BD_CALL SurfaceHit bd_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
+DORT_BD_FN SurfaceHit bd_surface(const PtScene& sc, const Hit& h, V3 o, V3 d) {
   return surface_at<G>(sc, h, o, d);
 }
 template<bool G>
-DG_HD DORT_BD_CALL V3 bd_bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+DORT_BD_FN V3 bd_bsdf_eval(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
                                    uint32_t req) {
   return bsdf_eval<G>(m, fr, wi, wo, req);
 }
 template<bool G>
-DG_HD DORT_BD_CALL float bd_bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
+DORT_BD_FN float bd_bsdf_pdf(const DevMaterial& m, const Frame& fr, V3 wi, V3 wo,
                                      uint32_t req) {
   return bsdf_pdf<G>(m, fr, wi, wo, req);
 }
 template<bool G>
-DG_HD DORT_BD_CALL BsdfSample bd_bsdf_sample(const DevMaterial& m, const Frame& fr, V3 w,
+DORT_BD_FN BsdfSample bd_bsdf_sample(const DevMaterial& m, const Frame& fr, V3 w,
                                              uint32_t req, float u, float v, float c) {
   return bsdf_sample<G>(m, fr, w, req, u, v, c);
 }
 template<bool G>
-DG_HD DORT_BD_CALL LightSample bd_light_sample(const PtScene& sc, const DevLight& l, V3 p,
+DORT_BD_FN LightSample bd_light_sample(const PtScene& sc, const DevLight& l, V3 p,
                                                float eps, float u, float v) {
   return light_sample<G>(sc, l, p, eps, u, v);
 }
