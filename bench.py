@@ -2,8 +2,9 @@
 """Benchmark of the dort B200 hot path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl dort|reference]
-                    [--workload pt1080p|raycast|batch|adjoint] [--spp S]
+                    [--workload pt1080p|raycast|batch|adjoint|cornell] [--spp S]
                     [--converged-spp C] [--no-sub] [--no-cpu] [--no-e2e]
+                    [--renderer pt|lt|bdpt] [--engine megakernel|wavefront]
 
 Workload "pt1080p" (default; the wavefront configuration): 1920x1080, 256
 samples per pixel, max depth 16, a 1,997,122-triangle scene (geodesic
@@ -54,6 +55,13 @@ roofline  algorithmic bytes per launch = rays x (32 B ray + 16 B hit +
         triangles) measured on a sample of the same rays by the CPU leg.
 cpu_baseline  the reference's own BVH + triangle code (compiled from its
         sources into oracle/_ref) on all host cores over a bounded sample.
+
+Workloads "batch" (64 seeded scenes of 10k-500k random triangles in one
+wavefront launch, samples/s), "adjoint" (512x512, 64 spp, depth 6, 500k
+triangles: forward + backward ms) and "cornell" (the Cornell box at 256x256,
+64 spp, depth 8, with --renderer pt / lt / bdpt and, for pt, --engine
+megakernel / wavefront; samples/s) print their own lines; the first two are
+also the pt1080p line's sub-records.
 
 Multi-GPU (torchrun): every rank renders its own frame or casts its own 16M
 rays (weak scaling, no data exchange); value = all units / max-over-ranks
